@@ -1,0 +1,142 @@
+"""ctypes binding of the C ABI declared in include/g4b.h.
+
+The shared library is loaded from the package's ``lib/`` directory (built in
+tree by ``genesis4_cuda_port_b200.build``).  There is no fallback: if the
+library is missing or a call fails, an exception is raised.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+_LIBDIR = Path(__file__).resolve().parent / "lib"
+
+c_double_p = C.POINTER(C.c_double)
+c_int64_p = C.POINTER(C.c_int64)
+c_int_p = C.POINTER(C.c_int)
+c_uint64_p = C.POINTER(C.c_uint64)
+c_void_pp = C.POINTER(C.c_void_p)
+
+G4B_OK = 0
+G4B_FP64 = 0
+G4B_MIXED = 1
+
+
+class G4BError(RuntimeError):
+    """A g4b_* call returned a non-zero status."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(f"g4b error {code}: {message}")
+        self.code = code
+
+
+class Step(C.Structure):
+    """Mirror of ``g4b_step`` (include/g4b.h)."""
+
+    _fields_ = [
+        ("delz", C.c_double), ("aw", C.c_double), ("ax", C.c_double),
+        ("ay", C.c_double), ("kx", C.c_double), ("ky", C.c_double),
+        ("gradx", C.c_double), ("grady", C.c_double), ("ku", C.c_double),
+        ("gamma_ref", C.c_double), ("autophase", C.c_double),
+        ("qf", C.c_double), ("dqx", C.c_double), ("dqy", C.c_double),
+        ("cx", C.c_double), ("cy", C.c_double), ("chic_angle", C.c_double),
+        ("chic_lb", C.c_double), ("chic_ld", C.c_double),
+        ("chic_lt", C.c_double), ("in_undulator", C.c_int),
+        ("reserved", C.c_int),
+    ]
+
+    def __init__(self, **kw):
+        super().__init__()
+        for k, v in kw.items():
+            setattr(self, k, v)
+
+
+# name -> (restype, argtypes)
+_SIGS = {
+    "g4b_last_error": (C.c_char_p, []),
+    "g4b_version": (C.c_int, []),
+    "g4b_ctx_create": (C.c_int, [C.c_int, c_void_pp]),
+    "g4b_ctx_destroy": (C.c_int, [C.c_void_p]),
+    "g4b_ctx_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "g4b_ctx_get_stream": (C.c_void_p, [C.c_void_p]),
+    "g4b_ctx_synchronize": (C.c_int, [C.c_void_p]),
+    "g4b_ctx_launch_count": (C.c_int, [C.c_void_p, c_uint64_p]),
+    "g4b_ctx_sm_count": (C.c_int, [C.c_void_p, c_int_p]),
+    "g4b_field_create": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_double,
+                                   C.c_double, C.c_int, C.c_int, C.c_int,
+                                   c_void_pp]),
+    "g4b_field_destroy": (C.c_int, [C.c_void_p]),
+    "g4b_field_upload": (C.c_int, [C.c_void_p, c_double_p]),
+    "g4b_field_download": (C.c_int, [C.c_void_p, c_double_p]),
+    "g4b_field_set_first": (C.c_int, [C.c_void_p, C.c_int]),
+    "g4b_field_get_first": (C.c_int, [C.c_void_p, c_int_p]),
+    "g4b_field_device_bytes": (C.c_int, [C.c_void_p, c_uint64_p]),
+    "g4b_beam_create": (C.c_int, [C.c_void_p, C.c_int, c_int64_p, C.c_int,
+                                  C.c_double, c_void_pp]),
+    "g4b_beam_destroy": (C.c_int, [C.c_void_p]),
+    "g4b_beam_upload": (C.c_int, [C.c_void_p] + [c_double_p] * 6),
+    "g4b_beam_download": (C.c_int, [C.c_void_p] + [c_double_p] * 6),
+    "g4b_beam_set_current": (C.c_int, [C.c_void_p, c_double_p]),
+    "g4b_beam_set_eloss": (C.c_int, [C.c_void_p, c_double_p]),
+    "g4b_beam_device_bytes": (C.c_int, [C.c_void_p, c_uint64_p]),
+    "g4b_adi_create": (C.c_int, [C.c_void_p, c_void_pp]),
+    "g4b_adi_destroy": (C.c_int, [C.c_void_p]),
+    "g4b_adi_init": (C.c_int, [C.c_void_p, C.c_double, C.c_double,
+                               C.c_double, C.c_int]),
+    "g4b_adi_advance": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p,
+                                  C.POINTER(Step), C.c_double, C.c_int]),
+    "g4b_beam_track": (C.c_int, [C.c_void_p, C.POINTER(Step), C.c_double,
+                                 C.c_int]),
+    "g4b_beam_r56": (C.c_int, [C.c_void_p, C.POINTER(Step), C.c_double]),
+    "g4b_beam_advance": (C.c_int, [C.c_void_p, c_void_pp, c_double_p, C.c_int,
+                                   C.POINTER(Step)]),
+    "g4b_slippage": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_int,
+                               C.c_int, c_double_p, c_int_p]),
+    "g4b_diag_beam": (C.c_int, [C.c_void_p, C.c_int, C.c_int, c_double_p,
+                                c_double_p, c_double_p]),
+    "g4b_diag_field": (C.c_int, [C.c_void_p, c_double_p, c_double_p]),
+}
+
+_lib = None
+
+
+def lib_path() -> Path:
+    return _LIBDIR / "libg4b200.so"
+
+
+def load():
+    """Load libg4b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = lib_path()
+    if not path.exists():
+        raise RuntimeError(
+            f"{path} is missing: build it with `python -m genesis4_cuda_port_b200.build`"
+            " (there is no CPU fallback)")
+    lib = C.CDLL(str(path))
+    for name, (res, args) in _SIGS.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def declared_symbols():
+    """Every entry point the binding expects the library to export."""
+    return sorted(_SIGS)
+
+
+def check(rc: int) -> None:
+    if rc != G4B_OK:
+        msg = load().g4b_last_error()
+        raise G4BError(rc, msg.decode() if msg else "")
+
+
+def dptr(a):
+    """double* of a C-contiguous float64 numpy array (or None)."""
+    if a is None:
+        return None
+    assert a.dtype.name == "float64" and a.flags["C_CONTIGUOUS"], "need C-contiguous float64"
+    return a.ctypes.data_as(c_double_p)

@@ -1,0 +1,741 @@
+// g4b_adi.cu -- ADI field solver (FieldSolverADICUDA) for sm_100a.
+//
+// One field step = deposition + two fused half-step kernels:
+//
+//   pass X : for a band of W rows of one slice, 1-D bulk copies stage rows
+//            r0-1 .. r0+W of the field and rows r0 .. r0+W-1 of the source in
+//            shared memory; each warp forms R = u + i r d2y(u) + S for its row,
+//            solves (1 - i r d2x) u' = R, and immediately forms the second
+//            half-step's right-hand side R' = u' + i r d2x(u') + S (its
+//            Laplacian runs along the row just solved).  R' is written
+//            transposed ([slice][ix][iy]) through a TMA tensor store.
+//   pass Y : each warp loads one contiguous row of R' (a column of the plane),
+//            solves (1 - i r d2y) u'' = R' and writes u'' transposed back into
+//            the natural layout.
+//
+// The tridiagonal solve is the reference's Thomas algorithm
+// (src/Core/FieldSolverADICUDA.cpp:222-277) written as two first-order linear
+// recurrences, y_k = cbet_k R_k + q_k y_{k-1} and u_k = y_k + s_k u_{k+1}
+// with q_k = s_k = i r cbet_k, evaluated by a warp: every lane runs the
+// recurrence over its own M consecutive elements, the lane carries are
+// combined by a 5-step Kogge-Stone scan of affine maps, and each lane adds
+// its carry times a precomputed product of coefficients.  All coefficients
+// (cbet, prefix/suffix products, scan multipliers) depend only on ngrid and r
+// and are computed once on the host in FP64 (FieldSolverADICUDA::init,
+// :821-902).
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <new>
+
+#include "g4b_internal.cuh"
+
+namespace g4b {
+
+template <typename T> struct CT;
+template <> struct CT<double> { using type = double2; };
+template <> struct CT<float> { using type = float2; };
+
+template <typename C>
+__device__ __forceinline__ C cadd(C a, C b) { a.x += b.x; a.y += b.y; return a; }
+
+// a + b*c
+template <typename C>
+__device__ __forceinline__ C cfma(C b, C c, C a) {
+  C r;
+  r.x = fma(b.x, c.x, fma(-b.y, c.y, a.x));
+  r.y = fma(b.x, c.y, fma(b.y, c.x, a.y));
+  return r;
+}
+
+template <typename C>
+__device__ __forceinline__ C cmul(C b, C c) {
+  C r;
+  r.x = b.x * c.x - b.y * c.y;
+  r.y = b.x * c.y + b.y * c.x;
+  return r;
+}
+
+template <typename C, typename T>
+__device__ __forceinline__ C cmul_ir(T r, C c) {  // (i r) * c
+  C o;
+  o.x = -r * c.y;
+  o.y = r * c.x;
+  return o;
+}
+
+template <typename C>
+__device__ __forceinline__ C shfl_up_c(C v, int d) {
+  v.x = __shfl_up_sync(0xffffffffu, v.x, d);
+  v.y = __shfl_up_sync(0xffffffffu, v.y, d);
+  return v;
+}
+
+template <typename C>
+__device__ __forceinline__ C shfl_down_c(C v, int d) {
+  v.x = __shfl_down_sync(0xffffffffu, v.x, d);
+  v.y = __shfl_down_sync(0xffffffffu, v.y, d);
+  return v;
+}
+
+struct AdiPassArgs {
+  const void* in;      // pass X: field (natural); pass Y: R' (transposed)
+  const void* src;     // pass X only; nullptr = no source this step
+  const void* tab;     // lane-minor tables of this precision
+  int n, ld, nband;
+  int out_off;         // byte offset of the output staging tile
+  int bar_off;         // byte offset of the mbarrier
+  int box_rows, nbox;  // TMA store boxes per band
+  double r;
+  int* err;
+};
+
+template <typename T> struct BandW;
+template <> struct BandW<double> { static constexpr int value = 9; };
+template <> struct BandW<float> { static constexpr int value = 10; };
+
+template <typename T, int M, bool PX>
+__global__ void __launch_bounds__(BandW<T>::value * 32)
+    adi_pass_kernel(const AdiPassArgs a, const __grid_constant__ CUtensorMap tm_out) {
+  using C = typename CT<T>::type;
+  constexpr int W = BandW<T>::value;
+  extern __shared__ __align__(128) unsigned char smem[];
+  const int n = a.n, ld = a.ld;
+  const int band = blockIdx.x % a.nband;
+  const int s = blockIdx.x / a.nband;
+  const int r0 = band * W;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  constexpr int kTileRows = PX ? W + 2 : W;
+  const bool has_src = PX && a.src != nullptr;
+
+  C* tile = reinterpret_cast<C*>(smem);
+  C* stile = tile + kTileRows * ld;
+  C* out = reinterpret_cast<C*>(smem + a.out_off);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + a.bar_off);
+
+  if (tid == 0) {
+    ptx::mbar_init(bar, 1);
+    ptx::fence_mbar_init();
+  }
+  __syncthreads();
+
+  const size_t plane = (size_t)n * ld;
+  const int lo = PX ? max(r0 - 1, 0) : r0;
+  const int hi = PX ? min(r0 + W, n - 1) : min(r0 + W - 1, n - 1);
+  const int slot0 = PX ? lo - (r0 - 1) : 0;
+  if (tid == 0) {
+    const C* in = reinterpret_cast<const C*>(a.in) + (size_t)s * plane;
+    const uint32_t bytes_in = (uint32_t)((hi - lo + 1) * ld * sizeof(C));
+    const int shi = min(r0 + W - 1, n - 1);
+    const uint32_t bytes_s = has_src ? (uint32_t)((shi - r0 + 1) * ld * sizeof(C)) : 0u;
+    ptx::mbar_expect_tx(bar, bytes_in + bytes_s);
+    ptx::bulk_g2s(tile + slot0 * ld, in + (size_t)lo * ld, bytes_in, bar);
+    if (has_src) {
+      const C* sp = reinterpret_cast<const C*>(a.src) + (size_t)s * plane;
+      ptx::bulk_g2s(stile, sp + (size_t)r0 * ld, bytes_s, bar);
+    }
+  }
+  if (PX) {
+    // rows outside the plane are the zero Dirichlet halo (missing neighbour
+    // is zero, src/Core/FieldSolverADICUDA.cpp:197-207)
+    for (int t = 0; t < kTileRows; ++t) {
+      const int g = r0 - 1 + t;
+      if (g < 0 || g > n - 1)
+        for (int k = tid; k < ld; k += blockDim.x) tile[t * ld + k] = C{0, 0};
+    }
+  }
+  ptx::mbar_wait_bounded(bar, 0, a.err);
+  __syncthreads();
+
+  const T r = (T)a.r;
+  const C* tab = reinterpret_cast<const C*>(a.tab);
+  const C* tcb = tab;                // cbet        [M][32]
+  const C* tG = tab + M * 32;        // prefix prod [M][32]
+  const C* tH = tab + 2 * M * 32;    // suffix prod [M][32]
+  const C* tF = tab + 3 * M * 32;    // fwd scan    [5][32]
+  const C* tB = tF + 5 * 32;         // bwd scan    [5][32]
+  const int iy = r0 + warp;
+  const bool active = iy < n;
+  C v[M];
+
+  if (active) {
+#pragma unroll
+    for (int j = 0; j < M; ++j) {
+      const int k = lane * M + j;
+      C R = C{0, 0};
+      if (k < n) {
+        if (PX) {
+          const C u = tile[(warp + 1) * ld + k];
+          const C up = tile[(warp + 2) * ld + k];
+          const C dn = tile[warp * ld + k];
+          const T lr = up.x + dn.x - u.x * (T)2;
+          const T li = up.y + dn.y - u.y * (T)2;
+          R.x = u.x + (-r * li);
+          R.y = u.y + r * lr;
+          if (has_src) R = cadd(R, stile[warp * ld + k]);
+        } else {
+          R = tile[warp * ld + k];
+        }
+      }
+      v[j] = R;
+    }
+    // forward recurrence, local part
+    {
+      C cb = __ldg(&tcb[lane]);
+      v[0] = cmul(cb, v[0]);
+#pragma unroll
+      for (int j = 1; j < M; ++j) {
+        cb = __ldg(&tcb[j * 32 + lane]);
+        v[j] = cfma(cmul_ir(r, cb), v[j - 1], cmul(cb, v[j]));
+      }
+    }
+    // forward carry scan across lanes
+    C b = v[M - 1];
+#pragma unroll
+    for (int t = 0; t < 5; ++t) {
+      const int d = 1 << t;
+      const C o = shfl_up_c(b, d);
+      if (lane >= d) b = cfma(__ldg(&tF[t * 32 + lane]), o, b);
+    }
+    C yin = shfl_up_c(b, 1);
+    if (lane == 0) yin = C{0, 0};
+#pragma unroll
+    for (int j = 0; j < M; ++j) v[j] = cfma(__ldg(&tG[j * 32 + lane]), yin, v[j]);
+    // backward recurrence, local part
+#pragma unroll
+    for (int j = M - 2; j >= 0; --j) {
+      const C cb = __ldg(&tcb[j * 32 + lane]);
+      v[j] = cfma(cmul_ir(r, cb), v[j + 1], v[j]);
+    }
+    b = v[0];
+#pragma unroll
+    for (int t = 0; t < 5; ++t) {
+      const int d = 1 << t;
+      const C o = shfl_down_c(b, d);
+      if (lane + d < 32) b = cfma(__ldg(&tB[t * 32 + lane]), o, b);
+    }
+    C uin = shfl_down_c(b, 1);
+    if (lane == 31) uin = C{0, 0};
+#pragma unroll
+    for (int j = 0; j < M; ++j) v[j] = cfma(__ldg(&tH[j * 32 + lane]), uin, v[j]);
+  } else {
+#pragma unroll
+    for (int j = 0; j < M; ++j) v[j] = C{0, 0};
+    // keep the warp's shuffles matched with nothing: inactive warps do not
+    // take part in any warp-level exchange
+  }
+
+  if (PX && active) {
+    // R' = u' + i r d2x(u') + S  (src/Core/FieldSolverADICUDA.cpp:279-323)
+    C left = shfl_up_c(v[M - 1], 1);
+    if (lane == 0) left = C{0, 0};
+    C right = shfl_down_c(v[0], 1);
+    if (lane == 31) right = C{0, 0};
+    C w2[M];
+#pragma unroll
+    for (int j = 0; j < M; ++j) {
+      const int k = lane * M + j;
+      const C um = j > 0 ? v[j - 1] : left;
+      const C upp = j < M - 1 ? v[j + 1] : right;
+      const T lr = upp.x + um.x - v[j].x * (T)2;
+      const T li = upp.y + um.y - v[j].y * (T)2;
+      C R;
+      R.x = v[j].x + (-r * li);
+      R.y = v[j].y + r * lr;
+      if (has_src && k < n) R = cadd(R, stile[warp * ld + k]);
+      w2[j] = R;
+    }
+#pragma unroll
+    for (int j = 0; j < M; ++j) v[j] = w2[j];
+  }
+
+  if (active) {
+#pragma unroll
+    for (int j = 0; j < M; ++j) {
+      const int k = lane * M + j;
+      if (k < n) out[k * W + warp] = v[j];
+    }
+  }
+  ptx::fence_proxy_async();
+  __syncthreads();
+  if (tid == 0) {
+    for (int i = 0; i < a.nbox; ++i)
+      ptx::tma_store_3d(&tm_out, out + (size_t)i * a.box_rows * W, 2 * r0,
+                        i * a.box_rows, s);
+    ptx::bulk_commit();
+    ptx::bulk_wait_read0();
+  }
+}
+
+// ------------------------------------------------------------ deposition ---
+// Deterministic replacement of adi_zero_source_grid + adi_deposit_source_atomic
+// (src/Core/FieldSolverADICUDA.cpp:98-174).  One CTA per beam slice:
+//  1. a pass over the slice's particles finds the largest per-particle weight
+//     q = sqrt(faw2)/gamma and the bounding box of the touched cells;
+//  2. the box is accumulated in shared memory as int64 fixed point with the
+//     exponent 2^E chosen so that count * max q * 2^E < 2^62 (integer adds are
+//     associative, so the result does not depend on the order of the atomics);
+//  3. the CTA writes the whole target plane: scl * sum * 2^-E inside the box,
+//     zero elsewhere.  Boxes larger than shared memory are done in row bands.
+struct DepositArgs {
+  const double *x, *y, *gamma, *theta;
+  const int64_t* off;
+  const double* scl;
+  double2* src;
+  int nslice, n, ld, first, harm, acc_cells;
+  double gridmax, dgrid, ax, ay, kx, ky, gradx, grady;
+  int* err;
+};
+
+__device__ __forceinline__ bool dep_cell(const DepositArgs& a, double xp, double yp,
+                                         int& ix, int& iy, double& wx, double& wy) {
+  if (!(xp > -a.gridmax && xp < a.gridmax && yp > -a.gridmax && yp < a.gridmax))
+    return false;
+  const double wx_raw = (xp + a.gridmax) / a.dgrid;
+  const double wy_raw = (yp + a.gridmax) / a.dgrid;
+  ix = (int)floor(wx_raw);
+  iy = (int)floor(wy_raw);
+  if (ix < 0 || ix >= a.n - 1 || iy < 0 || iy >= a.n - 1) return false;
+  wx = 1.0 + (double)ix - wx_raw;
+  wy = 1.0 + (double)iy - wy_raw;
+  return true;
+}
+
+__device__ __forceinline__ double dep_weight(const DepositArgs& a, double xp,
+                                             double yp, double g) {
+  const double dx = xp - a.ax, dy = yp - a.ay;
+  const double faw2 = 1.0 + a.kx * dx * dx + a.ky * dy * dy +
+                      2.0 * (a.gradx * dx + a.grady * dy);
+  return sqrt(faw2) / g;
+}
+
+template <typename V>
+__device__ __forceinline__ V block_reduce(V v, V* sh, bool is_max) {
+  // fixed-order reduction: warp xor-tree, then warp 0 over the warp partials
+  for (int o = 16; o > 0; o >>= 1) {
+    V t = __shfl_xor_sync(0xffffffffu, v, o);
+    v = is_max ? (t > v ? t : v) : (t < v ? t : v);
+  }
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) sh[w] = v;
+  __syncthreads();
+  const int nw = blockDim.x >> 5;
+  V r = sh[0];
+  for (int i = 1; i < nw; ++i) r = is_max ? (sh[i] > r ? sh[i] : r) : (sh[i] < r ? sh[i] : r);
+  return r;
+}
+
+__global__ void __launch_bounds__(512) deposit_slice_kernel(const DepositArgs a) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ double shd[16];
+  __shared__ int shi[16];
+  unsigned long long* acc = reinterpret_cast<unsigned long long*>(smem);
+  const int bs = blockIdx.x;
+  const int tid = threadIdx.x;
+  const int target = (bs + a.first) % a.nslice;
+  const int n = a.n, ld = a.ld;
+  double2* S = a.src + (size_t)target * n * ld;
+  const int64_t p0 = a.off[bs], p1 = a.off[bs + 1];
+  const double scl = a.scl[bs];
+
+  double qmax = 0.0;
+  int ixmin = 1 << 30, iymin = 1 << 30, ixmax = -1, iymax = -1, cnt = 0;
+  if (scl != 0.0) {
+    for (int64_t p = p0 + tid; p < p1; p += blockDim.x) {
+      int ix, iy;
+      double wx, wy;
+      const double xp = a.x[p], yp = a.y[p];
+      if (!dep_cell(a, xp, yp, ix, iy, wx, wy)) continue;
+      const double q = fabs(dep_weight(a, xp, yp, a.gamma[p]));
+      qmax = q > qmax ? q : qmax;  // NaN propagates as "not greater"
+      if (!(q <= 1e300)) qmax = INFINITY;
+      ixmin = min(ixmin, ix);
+      ixmax = max(ixmax, ix);
+      iymin = min(iymin, iy);
+      iymax = max(iymax, iy);
+      ++cnt;
+    }
+  }
+  qmax = block_reduce<double>(qmax, shd, true);
+  ixmin = block_reduce<int>(ixmin, shi, false);
+  ixmax = block_reduce<int>(ixmax, shi, true);
+  iymin = block_reduce<int>(iymin, shi, false);
+  iymax = block_reduce<int>(iymax, shi, true);
+  // count: sum over threads (exact integer sum)
+  for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+  __syncthreads();
+  if ((tid & 31) == 0) shi[tid >> 5] = cnt;
+  __syncthreads();
+  int total = 0;
+  for (int i = 0; i < (int)(blockDim.x >> 5); ++i) total += shi[i];
+  __syncthreads();
+
+  const bool any = total > 0 && qmax > 0.0;
+  if (any && !(qmax < INFINITY)) {
+    if (tid == 0) atomicOr(a.err, kErrFixedRange);
+  }
+  const bool ok = any && qmax < INFINITY;
+  int bx0 = 0, by0 = 0, bw = 0, bh = 0;
+  double scale = 0.0, unscale = 0.0;
+  if (ok) {
+    bx0 = ixmin;
+    by0 = iymin;
+    bw = ixmax - ixmin + 2;  // corners ix..ix+1
+    bh = iymax - iymin + 2;
+    int e;
+    frexp(qmax * (double)total, &e);  // qmax*total < 2^e
+    scale = ldexp(1.0, 62 - e);
+    unscale = scl * ldexp(1.0, e - 62);
+  }
+  const int band_h = ok ? max(1, min(bh, a.acc_cells / bw)) : 0;
+  const double hphase = (double)a.harm;
+
+  // rows below the box
+  for (int row = 0; row < (ok ? by0 : n); ++row)
+    for (int k = tid; k < ld; k += blockDim.x) S[(size_t)row * ld + k] = make_double2(0.0, 0.0);
+
+  for (int yb = by0; ok && yb < by0 + bh; yb += band_h) {
+    const int hb = min(band_h, by0 + bh - yb);
+    for (int i = tid; i < 2 * hb * bw; i += blockDim.x) acc[i] = 0ull;
+    __syncthreads();
+    for (int64_t p = p0 + tid; p < p1; p += blockDim.x) {
+      int ix, iy;
+      double wx, wy;
+      const double xp = a.x[p], yp = a.y[p];
+      if (!dep_cell(a, xp, yp, ix, iy, wx, wy)) continue;
+      if (iy + 1 < yb || iy >= yb + hb) continue;
+      const double q = dep_weight(a, xp, yp, a.gamma[p]);
+      double sn, cs;
+      sincos(hphase * a.theta[p], &sn, &cs);
+      const double vre = sn * q * scale, vim = cs * q * scale;
+      const double w[4] = {wx * wy, (1.0 - wx) * wy, wx * (1.0 - wy),
+                           (1.0 - wx) * (1.0 - wy)};
+      const int cx[4] = {ix, ix + 1, ix, ix + 1};
+      const int cy[4] = {iy, iy, iy + 1, iy + 1};
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        const int ry = cy[c] - yb;
+        if (ry < 0 || ry >= hb) continue;
+        const int cell = ry * bw + (cx[c] - bx0);
+        atomicAdd(&acc[2 * cell], (unsigned long long)__double2ll_rn(vre * w[c]));
+        atomicAdd(&acc[2 * cell + 1], (unsigned long long)__double2ll_rn(vim * w[c]));
+      }
+    }
+    __syncthreads();
+    for (int i = tid; i < hb * ld; i += blockDim.x) {
+      const int ry = i / ld, k = i - ry * ld;
+      const int kx = k - bx0;
+      double2 val = make_double2(0.0, 0.0);
+      if (kx >= 0 && kx < bw && k < n) {
+        const int cell = ry * bw + kx;
+        val.x = (double)(long long)acc[2 * cell] * unscale;
+        val.y = (double)(long long)acc[2 * cell + 1] * unscale;
+      }
+      S[(size_t)(yb + ry) * ld + k] = val;
+    }
+    __syncthreads();
+  }
+  // rows above the box
+  for (int row = ok ? by0 + bh : n; row < n; ++row)
+    for (int k = tid; k < ld; k += blockDim.x) S[(size_t)row * ld + k] = make_double2(0.0, 0.0);
+}
+
+// adi_compute_slice_scl (src/Core/FieldSolverADICUDA.cpp:75-96)
+__global__ void slice_scl_kernel(int nslice, const int64_t* off, const double* current,
+                                 double fc, double xks, double dgrid, double delz,
+                                 double vacimp, double eev, double* scl) {
+  const int is = blockIdx.x * blockDim.x + threadIdx.x;
+  if (is >= nslice) return;
+  double s = 0.0;
+  const int64_t npar = off[is + 1] - off[is];
+  if (npar > 0) {
+    s = fc * vacimp * current[is] * xks * delz;
+    s /= 4.0 * eev * (double)npar * dgrid * dgrid;
+  }
+  scl[is] = s;
+}
+
+// ------------------------------------------------------------- host side ---
+
+static constexpr double kVacimp = 376.73031346177;  // upstream `vacimp`
+static constexpr double kEev = 510998.95;          // upstream `eev`
+
+template <typename T, int M, bool PX>
+static int launch_pass_t(g4b_field* f, const AdiPassArgs& args, const CUtensorMap& tm,
+                         size_t smem) {
+  constexpr int W = BandW<T>::value;
+  auto kern = adi_pass_kernel<T, M, PX>;
+  static bool configured = false;  // per instantiation
+  if (!configured) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         227 * 1024);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(adi_pass)");
+    configured = true;
+  }
+  const unsigned grid = (unsigned)(f->nslice * args.nband);
+  kern<<<grid, W * 32, smem, f->ctx->stream>>>(args, tm);
+  count_launch(f->ctx);
+  return check_launch(f->ctx, "adi_pass_kernel");
+}
+
+template <typename T, bool PX>
+static int launch_pass_m(int M, g4b_field* f, const AdiPassArgs& args,
+                         const CUtensorMap& tm, size_t smem) {
+  switch (M) {
+    case 1: return launch_pass_t<T, 1, PX>(f, args, tm, smem);
+    case 3: return launch_pass_t<T, 3, PX>(f, args, tm, smem);
+    case 5: return launch_pass_t<T, 5, PX>(f, args, tm, smem);
+    case 7: return launch_pass_t<T, 7, PX>(f, args, tm, smem);
+    case 9: return launch_pass_t<T, 9, PX>(f, args, tm, smem);
+    case 11: return launch_pass_t<T, 11, PX>(f, args, tm, smem);
+    case 13: return launch_pass_t<T, 13, PX>(f, args, tm, smem);
+    case 15: return launch_pass_t<T, 15, PX>(f, args, tm, smem);
+    case 17: return launch_pass_t<T, 17, PX>(f, args, tm, smem);
+    case 21: return launch_pass_t<T, 21, PX>(f, args, tm, smem);
+    case 25: return launch_pass_t<T, 25, PX>(f, args, tm, smem);
+    case 33: return launch_pass_t<T, 33, PX>(f, args, tm, smem);
+  }
+  return fail(G4B_ERR_RANGE, "adi: unsupported elements per lane");
+}
+
+int adi_run(g4b_adi* adi, g4b_field* f, const void* src_dense) {
+  const int n = f->ngrid, ld = f->ld, W = f->band_rows;
+  AdiPassArgs args{};
+  args.n = n;
+  args.ld = ld;
+  args.nband = (n + W - 1) / W;
+  args.r = adi->r;
+  args.err = f->ctx->d_error;
+  args.box_rows = f->store_box_rows;
+  args.nbox = f->store_nbox;
+  args.tab = f->precision == G4B_FP64 ? (const void*)adi->d_tab64 : (const void*)adi->d_tab32;
+  const size_t cb = f->cell_bytes;
+  const size_t out_bytes = (size_t)f->store_nbox * f->store_box_rows * W * cb;
+  auto smem_for = [&](bool px, bool src) {
+    size_t tile = (size_t)((px ? W + 2 : W) * ld) * cb;
+    if (px && src) tile += (size_t)W * ld * cb;
+    const size_t out_off = (tile + 127) / 128 * 128;
+    const size_t bar_off = (out_off + out_bytes + 15) / 16 * 16;
+    args.out_off = (int)out_off;
+    args.bar_off = (int)bar_off;
+    return bar_off + 16;
+  };
+  int rc;
+  // pass X: a -> b (transposed R')
+  args.in = f->a;
+  args.src = src_dense;
+  size_t smem = smem_for(true, src_dense != nullptr);
+  if (smem > 227 * 1024) return fail(G4B_ERR_RANGE, "adi: pass X tile exceeds shared memory");
+  rc = f->precision == G4B_FP64
+           ? launch_pass_m<double, true>(adi->M, f, args, f->tm_store_b, smem)
+           : launch_pass_m<float, true>(adi->M, f, args, f->tm_store_b, smem);
+  if (rc) return rc;
+  // pass Y: b -> a (natural)
+  args.in = f->b;
+  args.src = nullptr;
+  smem = smem_for(false, false);
+  rc = f->precision == G4B_FP64
+           ? launch_pass_m<double, false>(adi->M, f, args, f->tm_store_a, smem)
+           : launch_pass_m<float, false>(adi->M, f, args, f->tm_store_a, smem);
+  return rc;
+}
+
+}  // namespace g4b
+
+using namespace g4b;
+
+extern "C" {
+
+int g4b_adi_create(g4b_ctx* c, g4b_adi** out) {
+  if (!c || !out) return fail(G4B_ERR_ARG, "g4b_adi_create: null arg");
+  g4b_adi* a = new (std::nothrow) g4b_adi();
+  if (!a) return fail(G4B_ERR_NOMEM, "g4b_adi_create: host allocation");
+  a->ctx = c;
+  *out = a;
+  return G4B_OK;
+}
+
+int g4b_adi_destroy(g4b_adi* a) {
+  if (!a) return G4B_OK;
+  cudaSetDevice(a->ctx->device);
+  cudaStreamSynchronize(a->ctx->stream);
+  if (a->d_tab64) cudaFree(a->d_tab64);
+  if (a->d_tab32) cudaFree(a->d_tab32);
+  delete a;
+  return G4B_OK;
+}
+
+// FieldSolverADICUDA::init (src/Core/FieldSolverADICUDA.cpp:821-866): the
+// Thomas factors of the constant matrix, then the scan tables derived from
+// them, all in FP64.
+int g4b_adi_init(g4b_adi* a, double delz, double dgrid, double xks, int ngrid) {
+  if (!a) return fail(G4B_ERR_ARG, "g4b_adi_init: null adi");
+  if (ngrid < 2 || !(dgrid > 0) || !(xks > 0))
+    return fail(G4B_ERR_ARG, "g4b_adi_init: bad arguments");
+  if (a->ready && delz == a->delz && ngrid == a->ngrid && dgrid == a->dgrid &&
+      xks == a->xks)
+    return G4B_OK;
+  const int M = pick_M(ngrid);
+  if (!M) return fail(G4B_ERR_RANGE, "g4b_adi_init: ngrid above 1056 is not supported");
+  using cd = std::complex<double>;
+  const int n = ngrid;
+  const double r = 0.25 * delz / (xks * dgrid * dgrid);
+  std::vector<double> mupp(n), mmid(n), mlow(n);
+  mupp[0] = r;
+  mmid[0] = -2 * r;
+  mlow[0] = 0;
+  for (int i = 1; i < n - 1; ++i) {
+    mupp[i] = r;
+    mmid[i] = -2 * r;
+    mlow[i] = r;
+  }
+  mupp[n - 1] = 0;
+  mmid[n - 1] = -2 * r;
+  mlow[n - 1] = r;
+  std::vector<cd> c(n), cbet(n), cwet(n);
+  for (int i = 0; i < n; ++i) c[i] = cd(0.0, -mlow[i]);
+  cbet[0] = cd(1.0, 0.0) / cd(1.0, -mmid[0]);
+  cwet[0] = cd(0.0, 0.0);
+  for (int i = 1; i < n; ++i) {
+    cwet[i] = cd(0.0, -mupp[i - 1]) * cbet[i - 1];
+    cbet[i] = cd(1.0, 0.0) / (cd(1.0, -mmid[i]) - c[i] * cwet[i]);
+  }
+  // recurrence coefficients on the padded index range [0, 32M)
+  const int P = 32 * M;
+  std::vector<cd> cb(P, 0.0), q(P, 0.0), sv(P, 0.0), G(P), H(P);
+  for (int k = 0; k < n; ++k) cb[k] = cbet[k];
+  for (int k = 1; k < n; ++k) q[k] = -c[k] * cbet[k];         // y_k += q_k y_{k-1}
+  for (int k = 0; k + 1 < n; ++k) sv[k] = -cwet[k + 1];       // u_k += s_k u_{k+1}
+  std::vector<cd> A(32), B(32);
+  for (int L = 0; L < 32; ++L) {
+    const int k0 = L * M, k1 = k0 + M - 1;
+    cd g = 1.0;
+    for (int k = k0; k <= k1; ++k) {
+      g *= q[k];
+      G[k] = g;
+    }
+    cd h = 1.0;
+    for (int k = k1; k >= k0; --k) {
+      h *= sv[k];
+      H[k] = h;
+    }
+    A[L] = G[k1];
+    B[L] = H[k0];
+  }
+  const size_t tot = tab_total(M);
+  std::vector<double2> t64(tot);
+  auto put = [&](size_t i, cd v) { t64[i] = make_double2(v.real(), v.imag()); };
+  for (int j = 0; j < M; ++j)
+    for (int L = 0; L < 32; ++L) {
+      const int k = L * M + j;
+      put(tab_cbet(M) + j * 32 + L, cb[k]);
+      put(tab_G(M) + j * 32 + L, G[k]);
+      put(tab_H(M) + j * 32 + L, H[k]);
+    }
+  std::vector<cd> af = A, ab = B;
+  for (int t = 0; t < 5; ++t) {
+    const int d = 1 << t;
+    for (int L = 0; L < 32; ++L) {
+      put(tab_scanF(M) + t * 32 + L, af[L]);
+      put(tab_scanB(M) + t * 32 + L, ab[L]);
+    }
+    std::vector<cd> nf = af, nb = ab;
+    for (int L = 0; L < 32; ++L) {
+      if (L >= d) nf[L] = af[L] * af[L - d];
+      if (L + d < 32) nb[L] = ab[L] * ab[L + d];
+    }
+    af.swap(nf);
+    ab.swap(nb);
+  }
+  std::vector<float2> t32(tot);
+  for (size_t i = 0; i < tot; ++i) t32[i] = make_float2((float)t64[i].x, (float)t64[i].y);
+  g4b_ctx* ctx = a->ctx;
+  G4B_CUDA_TRY(cudaSetDevice(ctx->device));
+  if (a->d_tab64) {
+    cudaStreamSynchronize(ctx->stream);
+    cudaFree(a->d_tab64);
+    cudaFree(a->d_tab32);
+    a->d_tab64 = nullptr;
+    a->d_tab32 = nullptr;
+  }
+  G4B_CUDA_TRY(cudaMalloc(&a->d_tab64, tot * sizeof(double2)));
+  G4B_CUDA_TRY(cudaMalloc(&a->d_tab32, tot * sizeof(float2)));
+  G4B_CUDA_TRY(cudaMemcpyAsync(a->d_tab64, t64.data(), tot * sizeof(double2),
+                               cudaMemcpyHostToDevice, ctx->stream));
+  G4B_CUDA_TRY(cudaMemcpyAsync(a->d_tab32, t32.data(), tot * sizeof(float2),
+                               cudaMemcpyHostToDevice, ctx->stream));
+  G4B_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  a->ngrid = ngrid;
+  a->delz = delz;
+  a->dgrid = dgrid;
+  a->xks = xks;
+  a->r = r;
+  a->M = M;
+  a->ready = true;
+  return G4B_OK;
+}
+
+// FieldSolverADICUDA::advance (src/Core/FieldSolverADICUDA.cpp:638-818).
+int g4b_adi_advance(g4b_adi* adi, g4b_field* f, g4b_beam* b, const g4b_step* st,
+                    double fc, int enabled) {
+  if (!adi || !f || !b || !st) return fail(G4B_ERR_ARG, "g4b_adi_advance: null arg");
+  if (!adi->ready || adi->ngrid != f->ngrid)
+    return fail(G4B_ERR_STATE,
+                "g4b_adi_advance: called before g4b_adi_init for this ngrid");
+  if (b->nslice != f->nslice)
+    return fail(G4B_ERR_ARG, "g4b_adi_advance: beam and field slice counts differ");
+  if (f->precision != G4B_FP64 || b->precision != G4B_FP64)
+    return fail(G4B_ERR_ARG, "g4b_adi_advance: the drop-in path holds FP64 state");
+  g4b_ctx* c = f->ctx;
+  G4B_CUDA_TRY(cudaSetDevice(c->device));
+  const int harm = f->harm;
+  const bool do_source = st->in_undulator && enabled && (harm % 2) == 1;
+  const bool use_source = do_source && b->npart > 0;
+  const void* src = nullptr;
+  if (use_source) {
+    slice_scl_kernel<<<(b->nslice + 127) / 128, 128, 0, c->stream>>>(
+        b->nslice, b->d_off, b->d_current, fc, f->xks, f->dgrid, st->delz, kVacimp,
+        kEev, b->d_scl);
+    count_launch(c);
+    if (int rc = check_launch(c, "slice_scl_kernel")) return rc;
+    DepositArgs da{};
+    da.x = b->x;
+    da.y = b->y;
+    da.gamma = b->gamma;
+    da.theta = b->theta;
+    da.off = b->d_off;
+    da.scl = b->d_scl;
+    da.src = static_cast<double2*>(f->src);
+    da.nslice = f->nslice;
+    da.n = f->ngrid;
+    da.ld = f->ld;
+    da.first = f->first;
+    da.harm = harm;
+    da.gridmax = f->gridmax;
+    da.dgrid = f->dgrid;
+    da.ax = st->ax;
+    da.ay = st->ay;
+    da.kx = st->kx;
+    da.ky = st->ky;
+    da.gradx = st->gradx;
+    da.grady = st->grady;
+    da.err = c->d_error;
+    const size_t acc_bytes = 160 * 1024;
+    da.acc_cells = (int)(acc_bytes / 16);
+    static bool configured = false;
+    if (!configured) {
+      G4B_CUDA_TRY(cudaFuncSetAttribute(deposit_slice_kernel,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)acc_bytes));
+      configured = true;
+    }
+    deposit_slice_kernel<<<f->nslice, 512, acc_bytes, c->stream>>>(da);
+    count_launch(c);
+    if (int rc = check_launch(c, "deposit_slice_kernel")) return rc;
+    src = f->src;
+  }
+  return adi_run(adi, f, src);
+}
+
+}  // extern "C"

@@ -1,0 +1,479 @@
+// g4b_core.cu -- context, field and beam state, slippage, error plumbing.
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+
+#include "g4b_internal.cuh"
+
+namespace g4b {
+
+static thread_local std::string t_last_error;
+
+void set_error(const std::string& msg) { t_last_error = msg; }
+
+int fail(int code, const std::string& msg) {
+  set_error(msg);
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char* where) {
+  set_error(std::string(where) + ": " + cudaGetErrorString(e));
+  return e == cudaErrorMemoryAllocation ? G4B_ERR_NOMEM : G4B_ERR_CUDA;
+}
+
+int check_launch(g4b_ctx* ctx, const char* what) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, what);
+  (void)ctx;
+  return G4B_OK;
+}
+
+int read_device_error(g4b_ctx* ctx, const char* what) {
+  int h = 0;
+  G4B_CUDA_TRY(cudaMemcpyAsync(&h, ctx->d_error, sizeof(int),
+                               cudaMemcpyDeviceToHost, ctx->stream));
+  G4B_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  if (h != 0) {
+    G4B_CUDA_TRY(cudaMemsetAsync(ctx->d_error, 0, sizeof(int), ctx->stream));
+    char buf[160];
+    snprintf(buf, sizeof buf, "%s: device error flag 0x%x (%s%s%s)", what, h,
+             (h & kErrWaitTimeout) ? "wait timeout " : "",
+             (h & kErrFixedRange) ? "fixed-point range " : "",
+             (h & kErrBadSlice) ? "bad slice" : "");
+    return fail(G4B_ERR_DEVICE, buf);
+  }
+  return G4B_OK;
+}
+
+int pick_M(int n) {
+  static const int kM[] = {1, 3, 5, 7, 9, 11, 13, 15, 17, 21, 25, 33};
+  for (int m : kM)
+    if (32 * m >= n) return m;
+  return 0;
+}
+
+static int encode_store_map(g4b_ctx* ctx, CUtensorMap* map, void* base, int n,
+                            int ld, int nslice, size_t cell_bytes, int band,
+                            int box_rows) {
+  auto fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(ctx->encode_fn);
+  if (!fn) return fail(G4B_ERR_STATE, "cuTensorMapEncodeTiled unavailable");
+  const size_t real = cell_bytes / 2;
+  cuuint64_t dims[3] = {(cuuint64_t)2 * n, (cuuint64_t)n, (cuuint64_t)nslice};
+  cuuint64_t strides[2] = {(cuuint64_t)ld * cell_bytes,
+                           (cuuint64_t)n * ld * cell_bytes};
+  cuuint32_t box[3] = {(cuuint32_t)(2 * band), (cuuint32_t)box_rows, 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = fn(map,
+                  real == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64
+                            : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+                  3, base, dims, strides, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                  CU_TENSOR_MAP_L2_PROMOTION_NONE,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    char buf[128];
+    snprintf(buf, sizeof buf, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return fail(G4B_ERR_CUDA, buf);
+  }
+  return G4B_OK;
+}
+
+}  // namespace g4b
+
+using namespace g4b;
+
+extern "C" {
+
+const char* g4b_last_error(void) { return t_last_error.c_str(); }
+
+int g4b_version(void) { return 100; }
+
+int g4b_ctx_create(int device, g4b_ctx** out) {
+  if (!out) return fail(G4B_ERR_ARG, "g4b_ctx_create: null out");
+  *out = nullptr;
+  int ndev = 0;
+  G4B_CUDA_TRY(cudaGetDeviceCount(&ndev));
+  if (device < 0 || device >= ndev)
+    return fail(G4B_ERR_ARG, "g4b_ctx_create: device index out of range");
+  G4B_CUDA_TRY(cudaSetDevice(device));
+  cudaDeviceProp prop;
+  G4B_CUDA_TRY(cudaGetDeviceProperties(&prop, device));
+  if (prop.major < 10)
+    return fail(G4B_ERR_DEVICE, "g4b_ctx_create: this build targets sm_100a (B200)");
+  g4b_ctx* c = new (std::nothrow) g4b_ctx();
+  if (!c) return fail(G4B_ERR_NOMEM, "g4b_ctx_create: host allocation");
+  c->device = device;
+  c->sm_count = prop.multiProcessorCount;
+  cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    delete c;
+    return cuda_fail(e, "cudaStreamCreateWithFlags");
+  }
+  c->own_stream = true;
+  e = cudaMalloc(&c->d_error, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemset(c->d_error, 0, sizeof(int));
+  if (e != cudaSuccess) {
+    cudaStreamDestroy(c->stream);
+    delete c;
+    return cuda_fail(e, "cudaMalloc(error flag)");
+  }
+  cudaDriverEntryPointQueryResult q;
+  e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &c->encode_fn,
+                              cudaEnableDefault, &q);
+  if (e != cudaSuccess || q != cudaDriverEntryPointSuccess) c->encode_fn = nullptr;
+  *out = c;
+  return G4B_OK;
+}
+
+int g4b_ctx_destroy(g4b_ctx* c) {
+  if (!c) return G4B_OK;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->d_error) cudaFree(c->d_error);
+  if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return G4B_OK;
+}
+
+int g4b_ctx_set_stream(g4b_ctx* c, void* s) {
+  if (!c) return fail(G4B_ERR_ARG, "g4b_ctx_set_stream: null ctx");
+  if (s == nullptr) {
+    if (!c->own_stream) {
+      G4B_CUDA_TRY(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+      c->own_stream = true;
+    }
+    return G4B_OK;
+  }
+  if (c->own_stream && c->stream) {
+    cudaStreamSynchronize(c->stream);
+    cudaStreamDestroy(c->stream);
+  }
+  c->stream = static_cast<cudaStream_t>(s);
+  c->own_stream = false;
+  return G4B_OK;
+}
+
+void* g4b_ctx_get_stream(g4b_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+int g4b_ctx_synchronize(g4b_ctx* c) {
+  if (!c) return fail(G4B_ERR_ARG, "g4b_ctx_synchronize: null ctx");
+  G4B_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return read_device_error(c, "g4b_ctx_synchronize");
+}
+
+int g4b_ctx_launch_count(g4b_ctx* c, uint64_t* count) {
+  if (!c || !count) return fail(G4B_ERR_ARG, "g4b_ctx_launch_count: null arg");
+  *count = c->launches.load();
+  return G4B_OK;
+}
+
+int g4b_ctx_sm_count(g4b_ctx* c, int* count) {
+  if (!c || !count) return fail(G4B_ERR_ARG, "g4b_ctx_sm_count: null arg");
+  *count = c->sm_count;
+  return G4B_OK;
+}
+
+// ------------------------------------------------------------------ field ---
+
+int g4b_field_create(g4b_ctx* c, int nslice, int ngrid, double gridmax,
+                     double xlambda, int harm, int precision, int low_memory,
+                     g4b_field** out) {
+  if (!c || !out) return fail(G4B_ERR_ARG, "g4b_field_create: null arg");
+  *out = nullptr;
+  if (nslice <= 0 || ngrid < 2 || !(gridmax > 0) || !(xlambda > 0) || harm < 1)
+    return fail(G4B_ERR_ARG, "g4b_field_create: bad dimensions");
+  if (precision != G4B_FP64 && precision != G4B_MIXED)
+    return fail(G4B_ERR_ARG, "g4b_field_create: unknown precision");
+  if (pick_M(ngrid) == 0)
+    return fail(G4B_ERR_RANGE, "g4b_field_create: ngrid above 1056 is not supported");
+  G4B_CUDA_TRY(cudaSetDevice(c->device));
+  g4b_field* f = new (std::nothrow) g4b_field();
+  if (!f) return fail(G4B_ERR_NOMEM, "g4b_field_create: host allocation");
+  f->ctx = c;
+  f->nslice = nslice;
+  f->ngrid = ngrid;
+  f->harm = harm;
+  f->precision = precision;
+  f->low_memory = low_memory ? 1 : 0;
+  f->gridmax = gridmax;
+  f->dgrid = 2.0 * gridmax / (double)(ngrid - 1);  // Field::init, Field.cpp:61
+  f->xlambda = xlambda;
+  f->xks = 4.0 * std::asin(1.0) / xlambda;          // Field::init, Field.cpp:78
+  f->cell_bytes = precision == G4B_FP64 ? 16 : 8;
+  f->ld = precision == G4B_FP64 ? ngrid : ngrid + (ngrid & 1);
+  f->band_rows = precision == G4B_FP64 ? 9 : 10;
+  // TMA store boxes of <= 256 rows; a multiple of 8 rows keeps every box's
+  // shared-memory source 128-byte aligned (W * cell * 8 is a multiple of 128).
+  f->store_nbox = (ngrid + 255) / 256;
+  f->store_box_rows = ((ngrid + f->store_nbox - 1) / f->store_nbox + 7) / 8 * 8;
+  const size_t bytes = (size_t)nslice * ngrid * f->ld * f->cell_bytes + 256;
+  cudaError_t e = cudaMalloc(&f->a, bytes);
+  if (e == cudaSuccess) e = cudaMalloc(&f->b, bytes);
+  if (e == cudaSuccess) e = cudaMalloc(&f->src, bytes);
+  if (e == cudaSuccess) e = cudaMemsetAsync(f->a, 0, bytes, c->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(f->b, 0, bytes, c->stream);
+  if (e != cudaSuccess) {
+    g4b_field_destroy(f);
+    return cuda_fail(e, "g4b_field_create: device allocation");
+  }
+  f->bytes = 3 * bytes;
+  int rc = encode_store_map(c, &f->tm_store_b, f->b, ngrid, f->ld, nslice,
+                            f->cell_bytes, f->band_rows, f->store_box_rows);
+  if (rc == G4B_OK)
+    rc = encode_store_map(c, &f->tm_store_a, f->a, ngrid, f->ld, nslice,
+                          f->cell_bytes, f->band_rows, f->store_box_rows);
+  if (rc != G4B_OK) {
+    g4b_field_destroy(f);
+    return rc;
+  }
+  *out = f;
+  return G4B_OK;
+}
+
+int g4b_field_destroy(g4b_field* f) {
+  if (!f) return G4B_OK;
+  cudaSetDevice(f->ctx->device);
+  cudaStreamSynchronize(f->ctx->stream);
+  if (f->a) cudaFree(f->a);
+  if (f->b) cudaFree(f->b);
+  if (f->src) cudaFree(f->src);
+  delete f;
+  return G4B_OK;
+}
+
+// Host (re,im) doubles [slice][iy][ix] <-> device cells [slice][iy][ld].
+static int field_copy(g4b_field* f, double* host, bool upload) {
+  g4b_ctx* c = f->ctx;
+  G4B_CUDA_TRY(cudaSetDevice(c->device));
+  const size_t n = f->ngrid;
+  const size_t rows = (size_t)f->nslice * n;
+  if (f->precision == G4B_FP64) {
+    // pitch == row length: one contiguous copy
+    const size_t bytes = rows * n * 16;
+    if (upload)
+      G4B_CUDA_TRY(cudaMemcpyAsync(f->a, host, bytes, cudaMemcpyHostToDevice, c->stream));
+    else
+      G4B_CUDA_TRY(cudaMemcpyAsync(host, f->a, bytes, cudaMemcpyDeviceToHost, c->stream));
+    G4B_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return G4B_OK;
+  }
+  // mixed: convert through a host staging buffer of pitched float2 rows
+  std::vector<float> stage(rows * f->ld * 2, 0.0f);
+  if (upload) {
+    for (size_t r = 0; r < rows; ++r)
+      for (size_t i = 0; i < 2 * n; ++i) stage[r * 2 * f->ld + i] = (float)host[r * 2 * n + i];
+    G4B_CUDA_TRY(cudaMemcpyAsync(f->a, stage.data(), stage.size() * 4,
+                                 cudaMemcpyHostToDevice, c->stream));
+    G4B_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  } else {
+    G4B_CUDA_TRY(cudaMemcpyAsync(stage.data(), f->a, stage.size() * 4,
+                                 cudaMemcpyDeviceToHost, c->stream));
+    G4B_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    for (size_t r = 0; r < rows; ++r)
+      for (size_t i = 0; i < 2 * n; ++i) host[r * 2 * n + i] = stage[r * 2 * f->ld + i];
+  }
+  return G4B_OK;
+}
+
+int g4b_field_upload(g4b_field* f, const double* host) {
+  if (!f || !host) return fail(G4B_ERR_ARG, "g4b_field_upload: null arg");
+  return field_copy(f, const_cast<double*>(host), true);
+}
+
+int g4b_field_download(g4b_field* f, double* host) {
+  if (!f || !host) return fail(G4B_ERR_ARG, "g4b_field_download: null arg");
+  return field_copy(f, host, false);
+}
+
+int g4b_field_set_first(g4b_field* f, int first) {
+  if (!f || first < 0 || first >= f->nslice)
+    return fail(G4B_ERR_ARG, "g4b_field_set_first: bad argument");
+  f->first = first;
+  return G4B_OK;
+}
+
+int g4b_field_get_first(g4b_field* f, int* first) {
+  if (!f || !first) return fail(G4B_ERR_ARG, "g4b_field_get_first: null arg");
+  *first = f->first;
+  return G4B_OK;
+}
+
+int g4b_field_device_bytes(g4b_field* f, uint64_t* bytes) {
+  if (!f || !bytes) return fail(G4B_ERR_ARG, "g4b_field_device_bytes: null arg");
+  *bytes = f->bytes;
+  return G4B_OK;
+}
+
+// ------------------------------------------------------------------- beam ---
+
+static constexpr int kChunk = 256;  // particles per push CTA
+
+int g4b_beam_create(g4b_ctx* c, int nslice, const int64_t* off, int precision,
+                    double gamma_ref, g4b_beam** out) {
+  if (!c || !out || !off) return fail(G4B_ERR_ARG, "g4b_beam_create: null arg");
+  *out = nullptr;
+  if (nslice <= 0) return fail(G4B_ERR_ARG, "g4b_beam_create: nslice <= 0");
+  if (precision != G4B_FP64)
+    return fail(G4B_ERR_ARG, "g4b_beam_create: this entry point holds FP64 state");
+  if (off[0] != 0) return fail(G4B_ERR_ARG, "g4b_beam_create: slice_offsets[0] != 0");
+  for (int s = 0; s < nslice; ++s)
+    if (off[s + 1] < off[s])
+      return fail(G4B_ERR_ARG, "g4b_beam_create: slice_offsets not monotonic");
+  G4B_CUDA_TRY(cudaSetDevice(c->device));
+  g4b_beam* b = new (std::nothrow) g4b_beam();
+  if (!b) return fail(G4B_ERR_NOMEM, "g4b_beam_create: host allocation");
+  b->ctx = c;
+  b->nslice = nslice;
+  b->precision = precision;
+  b->gamma_ref = gamma_ref;
+  b->npart = off[nslice];
+  b->h_off.assign(off, off + nslice + 1);
+  std::vector<int4> chunks;
+  for (int s = 0; s < nslice; ++s) {
+    b->max_slice_np = std::max<int64_t>(b->max_slice_np, off[s + 1] - off[s]);
+    for (int64_t p = off[s]; p < off[s + 1]; p += kChunk) {
+      const int64_t e = std::min<int64_t>(p + kChunk, off[s + 1]);
+      chunks.push_back(make_int4(s, (int)(p & 0x7fffffff), (int)(e - p),
+                                 (int)(p >> 31)));
+    }
+  }
+  b->nchunk = (int)chunks.size();
+  const size_t np = (size_t)std::max<int64_t>(b->npart, 1);
+  cudaError_t e = cudaSuccess;
+  double** arrs[6] = {&b->x, &b->y, &b->px, &b->py, &b->gamma, &b->theta};
+  for (double** a : arrs)
+    if (e == cudaSuccess) e = cudaMalloc(a, np * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_off, (nslice + 1) * sizeof(int64_t));
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_current, nslice * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_eloss, nslice * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_scl, nslice * sizeof(double));
+  if (e == cudaSuccess)
+    e = cudaMalloc(&b->d_chunks, std::max(1, b->nchunk) * sizeof(int4));
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(b->d_off, off, (nslice + 1) * sizeof(int64_t),
+                        cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess && b->nchunk)
+    e = cudaMemcpyAsync(b->d_chunks, chunks.data(), chunks.size() * sizeof(int4),
+                        cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(b->d_current, 0, nslice * sizeof(double), c->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(b->d_eloss, 0, nslice * sizeof(double), c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) {
+    g4b_beam_destroy(b);
+    return cuda_fail(e, "g4b_beam_create: device allocation");
+  }
+  b->bytes = np * 6 * sizeof(double) + (nslice + 1) * 8 + 3 * nslice * 8 +
+             chunks.size() * sizeof(int4);
+  *out = b;
+  return G4B_OK;
+}
+
+int g4b_beam_destroy(g4b_beam* b) {
+  if (!b) return G4B_OK;
+  cudaSetDevice(b->ctx->device);
+  cudaStreamSynchronize(b->ctx->stream);
+  void* ptrs[] = {b->x, b->y, b->px, b->py, b->gamma, b->theta, b->d_off,
+                  b->d_current, b->d_eloss, b->d_scl, b->d_chunks};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  delete b;
+  return G4B_OK;
+}
+
+int g4b_beam_upload(g4b_beam* b, const double* x, const double* y,
+                    const double* px, const double* py, const double* gamma,
+                    const double* theta) {
+  if (!b || !x || !y || !px || !py || !gamma || !theta)
+    return fail(G4B_ERR_ARG, "g4b_beam_upload: null arg");
+  g4b_ctx* c = b->ctx;
+  G4B_CUDA_TRY(cudaSetDevice(c->device));
+  const size_t bytes = (size_t)b->npart * sizeof(double);
+  const double* src[6] = {x, y, px, py, gamma, theta};
+  double* dst[6] = {b->x, b->y, b->px, b->py, b->gamma, b->theta};
+  for (int i = 0; i < 6 && bytes; ++i)
+    G4B_CUDA_TRY(cudaMemcpyAsync(dst[i], src[i], bytes, cudaMemcpyHostToDevice, c->stream));
+  G4B_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return G4B_OK;
+}
+
+int g4b_beam_download(g4b_beam* b, double* x, double* y, double* px, double* py,
+                      double* gamma, double* theta) {
+  if (!b) return fail(G4B_ERR_ARG, "g4b_beam_download: null beam");
+  g4b_ctx* c = b->ctx;
+  G4B_CUDA_TRY(cudaSetDevice(c->device));
+  const size_t bytes = (size_t)b->npart * sizeof(double);
+  double* dst[6] = {x, y, px, py, gamma, theta};
+  const double* src[6] = {b->x, b->y, b->px, b->py, b->gamma, b->theta};
+  for (int i = 0; i < 6 && bytes; ++i)
+    if (dst[i])
+      G4B_CUDA_TRY(cudaMemcpyAsync(dst[i], src[i], bytes, cudaMemcpyDeviceToHost, c->stream));
+  G4B_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return G4B_OK;
+}
+
+int g4b_beam_set_current(g4b_beam* b, const double* current) {
+  if (!b || !current) return fail(G4B_ERR_ARG, "g4b_beam_set_current: null arg");
+  G4B_CUDA_TRY(cudaSetDevice(b->ctx->device));
+  G4B_CUDA_TRY(cudaMemcpyAsync(b->d_current, current, b->nslice * sizeof(double),
+                               cudaMemcpyHostToDevice, b->ctx->stream));
+  G4B_CUDA_TRY(cudaStreamSynchronize(b->ctx->stream));
+  return G4B_OK;
+}
+
+int g4b_beam_set_eloss(g4b_beam* b, const double* eloss) {
+  if (!b) return fail(G4B_ERR_ARG, "g4b_beam_set_eloss: null beam");
+  G4B_CUDA_TRY(cudaSetDevice(b->ctx->device));
+  if (!eloss) {
+    G4B_CUDA_TRY(cudaMemsetAsync(b->d_eloss, 0, b->nslice * sizeof(double), b->ctx->stream));
+  } else {
+    G4B_CUDA_TRY(cudaMemcpyAsync(b->d_eloss, eloss, b->nslice * sizeof(double),
+                                 cudaMemcpyHostToDevice, b->ctx->stream));
+  }
+  G4B_CUDA_TRY(cudaStreamSynchronize(b->ctx->stream));
+  return G4B_OK;
+}
+
+int g4b_beam_device_bytes(g4b_beam* b, uint64_t* bytes) {
+  if (!b || !bytes) return fail(G4B_ERR_ARG, "g4b_beam_device_bytes: null arg");
+  *bytes = b->bytes;
+  return G4B_OK;
+}
+
+// --------------------------------------------------------------- slippage ---
+// ControlCUDA::applySlippage, single rank (src/Core/ControlCUDA.cpp:148-252):
+// the field never moves; `first` rotates and the plane entering the window is
+// zeroed, so the result is bit-exact by construction.
+int g4b_slippage(g4b_field* f, double shift, double sample, int time_run,
+                 int periodic, double* accuslip, int* nshift) {
+  if (!f || !accuslip) return fail(G4B_ERR_ARG, "g4b_slippage: null arg");
+  if (nshift) *nshift = 0;
+  if (!time_run) return G4B_OK;
+  g4b_ctx* c = f->ctx;
+  G4B_CUDA_TRY(cudaSetDevice(c->device));
+  *accuslip += shift;
+  const int ns = f->nslice;
+  const size_t plane_bytes = (size_t)f->ngrid * f->ld * f->cell_bytes;
+  int count = 0;
+  int direction = 1;
+  while (std::fabs(*accuslip) > sample * 0.8) {
+    direction = *accuslip < 0 ? -1 : 1;
+    *accuslip -= sample * direction;
+    int last = (f->first + ns - 1) % ns;
+    if (direction < 0) last = (last + 1) % ns;
+    if (!periodic) {
+      G4B_CUDA_TRY(cudaMemsetAsync(static_cast<char*>(f->a) + plane_bytes * last, 0,
+                                   plane_bytes, c->stream));
+    }
+    f->first = last;
+    if (direction < 0) f->first = (last + 1) % ns;
+    ++count;
+  }
+  if (nshift) *nshift = count;
+  return G4B_OK;
+}
+
+}  // extern "C"

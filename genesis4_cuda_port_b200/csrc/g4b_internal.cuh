@@ -1,0 +1,214 @@
+// g4b_internal.cuh -- private state and device helpers of the sm_100a core.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <atomic>
+#include <string>
+#include <vector>
+
+#include "../../include/g4b.h"
+
+namespace g4b {
+
+// ---------------------------------------------------------------- errors ----
+void set_error(const std::string& msg);
+int fail(int code, const std::string& msg);
+int cuda_fail(cudaError_t e, const char* where);
+
+#define G4B_CUDA_TRY(expr)                                  \
+  do {                                                      \
+    cudaError_t _e = (expr);                                \
+    if (_e != cudaSuccess) return ::g4b::cuda_fail(_e, #expr); \
+  } while (0)
+
+// Device-side error flag bits (written by kernels, read by the host).
+enum : int {
+  kErrWaitTimeout = 1,     // an mbarrier wait exceeded its iteration bound
+  kErrFixedRange = 2,      // a deposit value fell outside its fixed-point range
+  kErrBadSlice = 4,        // a particle index/slice outside the state
+};
+
+// Spin bound of every mbarrier wait: far above any legitimate wait.
+constexpr uint32_t kWaitSpinLimit = 1u << 26;
+
+// ----------------------------------------------------------------- state ----
+struct TensorMapEncoder;
+
+}  // namespace g4b
+
+struct g4b_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int sm_count = 0;
+  std::atomic<uint64_t> launches{0};
+  int* d_error = nullptr;  // device error flag (bit set, see kErr*)
+  void* encode_fn = nullptr;  // cuTensorMapEncodeTiled
+};
+
+struct g4b_field {
+  g4b_ctx* ctx = nullptr;
+  int nslice = 0, ngrid = 0, ld = 0;  // ld: row pitch in cells
+  int harm = 1, precision = G4B_FP64, low_memory = 0, first = 0;
+  double gridmax = 0, dgrid = 0, xlambda = 0, xks = 0;
+  size_t cell_bytes = 16;   // sizeof(complex) on the device
+  void* a = nullptr;        // state, natural layout [slice][iy][ld]
+  void* b = nullptr;        // pass-Y right-hand side, transposed [slice][ix][ld]
+  void* src = nullptr;      // source grid, natural layout
+  // TMA tensor maps for the transposed stores of the two ADI passes.
+  CUtensorMap tm_store_b;   // pass X writes b
+  CUtensorMap tm_store_a;   // pass Y writes a
+  int store_box_rows = 0;   // rows per TMA store box
+  int store_nbox = 0;       // boxes per band
+  int band_rows = 0;        // W: rows (warps) per CTA
+  uint64_t bytes = 0;
+};
+
+struct g4b_beam {
+  g4b_ctx* ctx = nullptr;
+  int nslice = 0, precision = G4B_FP64;
+  int64_t npart = 0;
+  double gamma_ref = 0;
+  std::vector<int64_t> h_off;
+  int64_t* d_off = nullptr;
+  // FP64 state
+  double *x = nullptr, *y = nullptr, *px = nullptr, *py = nullptr;
+  double *gamma = nullptr, *theta = nullptr;
+  double* d_current = nullptr;
+  double* d_eloss = nullptr;
+  double* d_scl = nullptr;           // per-slice source scale
+  // CTA work chunks: (slice, begin, end) over the particle index space.
+  int nchunk = 0;
+  int4* d_chunks = nullptr;          // x = slice, y = begin lo, z = end lo, w = hi bits
+  int64_t max_slice_np = 0;
+  uint64_t bytes = 0;
+};
+
+struct g4b_adi {
+  g4b_ctx* ctx = nullptr;
+  int ngrid = 0;
+  double delz = 0, dgrid = 0, xks = 0, r = 0;
+  int M = 0;                 // elements per lane (odd)
+  // Tables in lane-minor order, complex (double2) and their FP32 copies.
+  double2* d_tab64 = nullptr;   // [3][M][32]: cbet, G, H ; then [2][5][32] scans
+  float2* d_tab32 = nullptr;
+  bool ready = false;
+};
+
+namespace g4b {
+
+// Launch bookkeeping: every kernel launch goes through this.
+inline void count_launch(g4b_ctx* ctx, int n = 1) { ctx->launches += n; }
+
+int check_launch(g4b_ctx* ctx, const char* what);
+int read_device_error(g4b_ctx* ctx, const char* what);
+
+// Shared ADI entry used by the drop-in and the fused path.
+int adi_run(g4b_adi* adi, g4b_field* f, const void* src_dense);
+
+// Lane-minor table offsets (in complex elements).
+inline size_t tab_cbet(int M) { (void)M; return 0; }
+inline size_t tab_G(int M) { return (size_t)M * 32; }
+inline size_t tab_H(int M) { return (size_t)2 * M * 32; }
+inline size_t tab_scanF(int M) { return (size_t)3 * M * 32; }
+inline size_t tab_scanB(int M) { return (size_t)3 * M * 32 + 5 * 32; }
+inline size_t tab_total(int M) { return (size_t)3 * M * 32 + 10 * 32; }
+
+int pick_M(int n);
+
+}  // namespace g4b
+
+// ------------------------------------------------------------ PTX helpers ---
+#if defined(__CUDACC__)
+namespace g4b {
+namespace ptx {
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(count)
+               : "memory");
+}
+
+__device__ __forceinline__ void fence_mbar_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void fence_proxy_async() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile(
+      "mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(
+          smem_u32(bar)),
+      "r"(bytes)
+      : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait: returns false (and sets the device error flag) if the phase
+// did not complete within kWaitSpinLimit polls.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity,
+                                                  int* err_flag) {
+  for (uint32_t i = 0; i < kWaitSpinLimit; ++i) {
+    if (mbar_try_wait(bar, parity)) return true;
+  }
+  atomicOr(err_flag, kErrWaitTimeout);
+  return false;
+}
+
+// 1-D bulk copy global -> shared, completing on an mbarrier.  Both addresses
+// 16-byte aligned, size a multiple of 16.
+__device__ __forceinline__ void bulk_g2s(void* dst_smem, const void* src_gmem,
+                                         uint32_t bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cta.global.mbarrier::complete_tx::bytes "
+      "[%0], [%1], %2, [%3];" ::"r"(smem_u32(dst_smem)),
+      "l"(src_gmem), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// Tensor store shared -> global (3-D box), bulk-group completion.
+__device__ __forceinline__ void tma_store_3d(const CUtensorMap* map,
+                                             const void* src_smem, int x, int y,
+                                             int z) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.global.shared::cta.bulk_group "
+      "[%0, {%2, %3, %4}], [%1];" ::"l"(map),
+      "r"(smem_u32(src_smem)), "r"(x), "r"(y), "r"(z)
+      : "memory");
+}
+
+__device__ __forceinline__ void bulk_commit() {
+  asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+
+__device__ __forceinline__ void bulk_wait_read0() {
+  asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+
+__device__ __forceinline__ void bulk_wait0() {
+  asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+}
+
+}  // namespace ptx
+}  // namespace g4b
+#endif

@@ -1,0 +1,235 @@
+"""Python handles over the C ABI (include/g4b.h).
+
+These mirror the reference's device-state objects and solver classes:
+``Context`` (genesis4_cuda runtime helpers), ``FieldState``
+(Genesis4FieldSoA), ``BeamState`` (Genesis4BeamSoA), ``FieldSolverADICUDA``,
+``BeamSolverCUDA``/``TrackBeamCUDA`` entry points, ``ControlCUDA.applySlippage``
+and the device part of ``DiagnosticCUDA``.  Every call goes through
+libg4b200.so; errors raise ``G4BError``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import G4B_FP64, G4B_MIXED, Step, check, dptr  # noqa: F401
+
+
+class Context:
+    """A device and the CUDA stream all work of this context is issued on."""
+
+    def __init__(self, device: int = 0):
+        self.lib = _lib.load()
+        h = C.c_void_p()
+        check(self.lib.g4b_ctx_create(device, C.byref(h)))
+        self.h = h
+        self.device = device
+
+    @property
+    def stream(self) -> int:
+        return self.lib.g4b_ctx_get_stream(self.h) or 0
+
+    def set_stream(self, stream_ptr: int | None) -> None:
+        check(self.lib.g4b_ctx_set_stream(self.h, C.c_void_p(stream_ptr or 0)))
+
+    def synchronize(self) -> None:
+        check(self.lib.g4b_ctx_synchronize(self.h))
+
+    def launch_count(self) -> int:
+        v = C.c_uint64()
+        check(self.lib.g4b_ctx_launch_count(self.h, C.byref(v)))
+        return int(v.value)
+
+    def sm_count(self) -> int:
+        v = C.c_int()
+        check(self.lib.g4b_ctx_sm_count(self.h, C.byref(v)))
+        return int(v.value)
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.g4b_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class FieldState:
+    """Radiation field of ``nslice`` planes, ngrid x ngrid complex cells."""
+
+    def __init__(self, ctx: Context, nslice: int, ngrid: int, gridmax: float,
+                 xlambda: float, harm: int = 1, precision: int = G4B_FP64,
+                 low_memory: bool = False):
+        self.ctx, self.lib = ctx, ctx.lib
+        self.nslice, self.ngrid, self.gridmax = nslice, ngrid, gridmax
+        self.xlambda, self.harm, self.precision = xlambda, harm, precision
+        self.dgrid = 2.0 * gridmax / (ngrid - 1)
+        self.xks = 2.0 * np.pi / xlambda
+        self.accuslip = 0.0
+        h = C.c_void_p()
+        check(self.lib.g4b_field_create(ctx.h, nslice, ngrid, gridmax, xlambda,
+                                        harm, precision, int(low_memory),
+                                        C.byref(h)))
+        self.h = h
+
+    def upload(self, cells: np.ndarray) -> None:
+        a = np.ascontiguousarray(cells, dtype=np.complex128).reshape(-1)
+        assert a.size == self.nslice * self.ngrid ** 2
+        check(self.lib.g4b_field_upload(self.h, dptr(a.view(np.float64))))
+
+    def download(self) -> np.ndarray:
+        out = np.empty((self.nslice, self.ngrid, self.ngrid), np.complex128)
+        check(self.lib.g4b_field_download(self.h, dptr(out.reshape(-1).view(np.float64))))
+        return out
+
+    @property
+    def first(self) -> int:
+        v = C.c_int()
+        check(self.lib.g4b_field_get_first(self.h, C.byref(v)))
+        return int(v.value)
+
+    @first.setter
+    def first(self, value: int) -> None:
+        check(self.lib.g4b_field_set_first(self.h, int(value)))
+
+    def device_bytes(self) -> int:
+        v = C.c_uint64()
+        check(self.lib.g4b_field_device_bytes(self.h, C.byref(v)))
+        return int(v.value)
+
+    def apply_slippage(self, shift: float, sample: float, time_run: bool = True,
+                       periodic: bool = False) -> int:
+        """ControlCUDA::applySlippage; returns the number of slice shifts."""
+        acc = C.c_double(self.accuslip)
+        ns = C.c_int()
+        check(self.lib.g4b_slippage(self.h, shift, sample, int(time_run),
+                                    int(periodic), C.byref(acc), C.byref(ns)))
+        self.accuslip = acc.value
+        return int(ns.value)
+
+    def diagnostics(self):
+        """Raw per-slice sums (7) and centre cell, indexed by beam slice."""
+        stats = np.empty((self.nslice, 7))
+        center = np.empty((self.nslice, 2))
+        check(self.lib.g4b_diag_field(self.h, dptr(stats.reshape(-1)),
+                                      dptr(center.reshape(-1))))
+        return stats, center
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.g4b_field_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class BeamState:
+    """Slice-contiguous FP64 particles x, y, px, py, gamma, theta."""
+
+    NAMES = ("x", "y", "px", "py", "gamma", "theta")
+
+    def __init__(self, ctx: Context, slice_offsets, gamma_ref: float,
+                 precision: int = G4B_FP64):
+        self.ctx, self.lib = ctx, ctx.lib
+        off = np.ascontiguousarray(slice_offsets, dtype=np.int64)
+        self.offsets = off
+        self.nslice = len(off) - 1
+        self.npart = int(off[-1])
+        self.gamma_ref = gamma_ref
+        h = C.c_void_p()
+        check(self.lib.g4b_beam_create(ctx.h, self.nslice,
+                                       off.ctypes.data_as(_lib.c_int64_p),
+                                       precision, gamma_ref, C.byref(h)))
+        self.h = h
+
+    def upload(self, parts: dict) -> None:
+        arrs = [np.ascontiguousarray(parts[k], dtype=np.float64) for k in self.NAMES]
+        for a in arrs:
+            assert a.size == self.npart
+        check(self.lib.g4b_beam_upload(self.h, *[dptr(a) for a in arrs]))
+
+    def download(self) -> dict:
+        out = {k: np.empty(self.npart) for k in self.NAMES}
+        check(self.lib.g4b_beam_download(self.h, *[dptr(out[k]) for k in self.NAMES]))
+        return out
+
+    def set_current(self, current) -> None:
+        a = np.ascontiguousarray(current, dtype=np.float64)
+        assert a.size == self.nslice
+        check(self.lib.g4b_beam_set_current(self.h, dptr(a)))
+
+    def set_eloss(self, eloss=None) -> None:
+        a = None if eloss is None else np.ascontiguousarray(eloss, dtype=np.float64)
+        check(self.lib.g4b_beam_set_eloss(self.h, dptr(a)))
+
+    # TrackBeamCUDA::track / applyR56 and BeamSolverCUDA::advance
+    def track(self, step: Step, delz: float, last: bool) -> None:
+        check(self.lib.g4b_beam_track(self.h, C.byref(step), delz, int(last)))
+
+    def apply_r56(self, step: Step, lambda0: float) -> None:
+        check(self.lib.g4b_beam_r56(self.h, C.byref(step), lambda0))
+
+    def advance(self, fields, fc, step: Step) -> None:
+        n = len(fields)
+        hs = (C.c_void_p * n)(*[f.h.value for f in fields])
+        fcs = np.ascontiguousarray(fc, dtype=np.float64)
+        check(self.lib.g4b_beam_advance(self.h, C.cast(hs, _lib.c_void_pp),
+                                        dptr(fcs), n, C.byref(step)))
+
+    def diagnostics(self, nharm: int = 1, need_aux: bool = True):
+        stats = np.empty((self.nslice, 23))
+        bre = np.empty((self.nslice, nharm))
+        bim = np.empty((self.nslice, nharm))
+        check(self.lib.g4b_diag_beam(self.h, nharm, int(need_aux),
+                                     dptr(stats.reshape(-1)), dptr(bre.reshape(-1)),
+                                     dptr(bim.reshape(-1))))
+        return stats, bre, bim
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.g4b_beam_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class FieldSolverADICUDA:
+    """The reference's FieldSolverADICUDA: init (factorise) and advance."""
+
+    def __init__(self, ctx: Context):
+        self.ctx, self.lib = ctx, ctx.lib
+        h = C.c_void_p()
+        check(self.lib.g4b_adi_create(ctx.h, C.byref(h)))
+        self.h = h
+
+    def init(self, delz: float, dgrid: float, xks: float, ngrid: int) -> None:
+        check(self.lib.g4b_adi_init(self.h, delz, dgrid, xks, ngrid))
+
+    def advance(self, field: FieldState, beam: BeamState, step: Step, fc: float,
+                enabled: bool = True) -> None:
+        check(self.lib.g4b_adi_advance(self.h, field.h, beam.h, C.byref(step), fc,
+                                       int(enabled)))
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.g4b_adi_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,191 @@
+/*
+ * g4b.h -- C ABI of the B200 (sm_100a) GENESIS 1.3 v4 time-stepping core.
+ *
+ * Every entry point returns an int status (G4B_OK == 0).  Nothing is thrown
+ * across the ABI; g4b_last_error() returns the message of the last failing
+ * call made on the calling thread.  All handles are opaque.  All work of a
+ * context is issued on one CUDA stream (the context's own, or one the caller
+ * sets with g4b_ctx_set_stream); entry points that return data to host memory
+ * synchronise that stream, all others are asynchronous.
+ *
+ * Layouts crossing the ABI are the reference's host layouts:
+ *   field  : complex<double> cells, [slice][iy][ix], interleaved (re, im)
+ *            (Field::field, include/Field.h:66 of the reference);
+ *   beam   : six double arrays x, y, px, py, gamma, theta, slice-contiguous,
+ *            with int64 slice offsets (Genesis4BeamSoA,
+ *            include/Genesis4BeamSoA.h:7-21 of the reference).
+ * Device layouts are private (see the design notes shipped with the library).
+ *
+ * Each declaration names the reference member function it replaces
+ * (paths relative to the mulingLHY/Genesis4_CUDA_port tree).
+ */
+#ifndef G4B_H_
+#define G4B_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+enum {
+  G4B_OK = 0,
+  G4B_ERR_ARG = 1,      /* bad argument (null handle, size mismatch, ...)   */
+  G4B_ERR_CUDA = 2,     /* a CUDA runtime call failed                       */
+  G4B_ERR_STATE = 3,    /* call made in the wrong state (e.g. no ADI init)  */
+  G4B_ERR_NOMEM = 4,    /* device allocation failed                         */
+  G4B_ERR_RANGE = 5,    /* size outside what the kernels support            */
+  G4B_ERR_DEVICE = 6    /* a kernel raised its device-side error flag       */
+};
+
+/* ---- precision of the device state -------------------------------------- */
+enum {
+  G4B_FP64 = 0,   /* plain FP64: the drop-in form                          */
+  G4B_MIXED = 1   /* FP32 field/source/particles, FP64 phase theta          */
+};
+
+typedef struct g4b_ctx g4b_ctx;
+typedef struct g4b_field g4b_field;
+typedef struct g4b_beam g4b_beam;
+typedef struct g4b_adi g4b_adi;
+
+/* Per-step lattice values the kernels consume.  This is the subset of the
+ * upstream Undulator API that the reference's CUDA path reads each step:
+ * getUndulatorParameters / getQuadrupoleParameters / getCorrectorParameters /
+ * getChicaneParameters (src/Core/TrackBeamCUDA.cpp:163-167), ax..grady[istep]
+ * (src/Core/FieldSolverADICUDA.cpp:722-729, src/Core/BeamSolverCUDA.cpp:619-631),
+ * getaw/getku/autophase/getGammaRef (src/Core/BeamSolverCUDA.cpp:514-522),
+ * inUndulator (src/Core/FieldSolverADICUDA.cpp:697). */
+typedef struct g4b_step {
+  double delz;         /* step length [m]                                   */
+  double aw;           /* rms undulator parameter                           */
+  double ax, ay;       /* undulator axis offsets [m]                        */
+  double kx, ky;       /* natural focusing, already scaled by ku^2 [1/m^2]  */
+  double gradx, grady; /* transverse gradient [1/m]                         */
+  double ku;           /* undulator wavenumber, 0 outside undulators        */
+  double gamma_ref;    /* reference energy gamma0                           */
+  double autophase;    /* phase shift added to theta before the push        */
+  double qf;           /* quadrupole k1 [1/m^2]                             */
+  double dqx, dqy;     /* quadrupole offsets [m]                            */
+  double cx, cy;       /* corrector kicks [rad]                             */
+  double chic_angle, chic_lb, chic_ld, chic_lt; /* chicane geometry         */
+  int in_undulator;    /* und->inUndulator()                                */
+  int reserved;
+} g4b_step;
+
+/* ---- errors / version ---------------------------------------------------- */
+const char* g4b_last_error(void);
+int g4b_version(void);
+
+/* ---- context: device, stream, launch counter -----------------------------
+ * Replaces genesis4_cuda::initialize / stream / synchronize
+ * (include/Genesis4CudaRuntime.h:25-50): the reference runs everything on the
+ * legacy default stream; a context owns (or borrows) one explicit stream. */
+int g4b_ctx_create(int device, g4b_ctx** out);
+int g4b_ctx_destroy(g4b_ctx* ctx);
+int g4b_ctx_set_stream(g4b_ctx* ctx, void* cuda_stream); /* NULL = own stream */
+void* g4b_ctx_get_stream(g4b_ctx* ctx);
+int g4b_ctx_synchronize(g4b_ctx* ctx);
+/* Number of kernels this library launched on ctx so far. */
+int g4b_ctx_launch_count(g4b_ctx* ctx, uint64_t* count);
+/* SM count of the context's device. */
+int g4b_ctx_sm_count(g4b_ctx* ctx, int* count);
+
+/* ---- field state -----------------------------------------------------------
+ * Replaces Genesis4FieldSoA + Field::init_fieldSoA/pack_field_to_soa/
+ * unpack_soa_to_field (include/Genesis4FieldSoA.h:7-17,
+ * src/Core/Field.cpp:582-674).  gridmax, xlambda and harm follow Field::init
+ * (src/Core/Field.cpp:50-83): dgrid = 2*gridmax/(ngrid-1), xks = 2*pi/xlambda.
+ * low_memory selects the reference's `low_memory_adisolver` mode (no separate
+ * source grid; README.md:36-44). */
+int g4b_field_create(g4b_ctx* ctx, int nslice, int ngrid, double gridmax,
+                     double xlambda, int harm, int precision, int low_memory,
+                     g4b_field** out);
+int g4b_field_destroy(g4b_field* f);
+int g4b_field_upload(g4b_field* f, const double* host_cells);   /* 2*nslice*ngrid^2 */
+int g4b_field_download(g4b_field* f, double* host_cells);
+/* Field::first: index of the storage slice holding beam slice 0
+ * (include/Field.h:68). */
+int g4b_field_set_first(g4b_field* f, int first);
+int g4b_field_get_first(g4b_field* f, int* first);
+/* Bytes of device memory the field holds (state + solver scratch). */
+int g4b_field_device_bytes(g4b_field* f, uint64_t* bytes);
+
+/* ---- beam state ------------------------------------------------------------
+ * Replaces Genesis4BeamSoA + Beam::init_beamSoA/pack_beam_to_soa/
+ * unpack_soa_to_beam (include/Genesis4BeamSoA.h:7-21,
+ * src/Core/Beam.cpp:342-525).  slice_offsets has nslice+1 entries. */
+int g4b_beam_create(g4b_ctx* ctx, int nslice, const int64_t* slice_offsets,
+                    int precision, double gamma_ref, g4b_beam** out);
+int g4b_beam_destroy(g4b_beam* b);
+int g4b_beam_upload(g4b_beam* b, const double* x, const double* y,
+                    const double* px, const double* py, const double* gamma,
+                    const double* theta);
+int g4b_beam_download(g4b_beam* b, double* x, double* y, double* px, double* py,
+                      double* gamma, double* theta);
+/* Beam::current per slice [A] (include/Beam.h:69); uploaded once, kept on
+ * the device (the reference re-uploads it every field step,
+ * src/Core/FieldSolverADICUDA.cpp:700-702). */
+int g4b_beam_set_current(g4b_beam* b, const double* current);
+/* Per-slice longitudinal field loss -longESC/511000 that the push subtracts
+ * (src/Core/BeamSolverCUDA.cpp:549-560).  NULL clears it to zero. */
+int g4b_beam_set_eloss(g4b_beam* b, const double* slice_eloss);
+int g4b_beam_device_bytes(g4b_beam* b, uint64_t* bytes);
+
+/* ---- ADI field solver --------------------------------------------------------
+ * FieldSolverADICUDA (include/FieldSolverADICUDA.h:20-25). */
+int g4b_adi_create(g4b_ctx* ctx, g4b_adi** out);
+int g4b_adi_destroy(g4b_adi* adi);
+/* FieldSolverADICUDA::init (src/Core/FieldSolverADICUDA.cpp:821-902):
+ * factorises the constant tridiagonal (1+2ir, -ir) with r = delz/(4 xks dgrid^2)
+ * in FP64; recomputes only when delz or ngrid change. */
+int g4b_adi_init(g4b_adi* adi, double delz, double dgrid, double xks, int ngrid);
+/* FieldSolverADICUDA::advance (src/Core/FieldSolverADICUDA.cpp:638-818):
+ * source deposition (if in_undulator, the field is enabled and harm is odd)
+ * and the two ADI half-steps.  fc is und->fc(harm). */
+int g4b_adi_advance(g4b_adi* adi, g4b_field* f, g4b_beam* b,
+                    const g4b_step* st, double fc, int enabled);
+
+/* ---- beam solver ------------------------------------------------------------
+ * TrackBeamCUDA::track (src/Core/TrackBeamCUDA.cpp:156-204), including the
+ * chicane matrix on the first half step and the corrector kick on the last. */
+int g4b_beam_track(g4b_beam* b, const g4b_step* st, double delz, int last_step);
+/* TrackBeamCUDA::applyR56 (src/Core/TrackBeamCUDA.cpp:257-278). */
+int g4b_beam_r56(g4b_beam* b, const g4b_step* st, double lambda0);
+/* BeamSolverCUDA::advance (src/Core/BeamSolverCUDA.cpp:449-683): RK4 of
+ * (gamma, theta) with the bilinear field sample frozen per step, summed over
+ * nfield <= 8 fields.  fc[i] = und->fc(harm_i); xks_fund = field xks / harm.
+ * xku is und->getku(), replaced by xks_fund/(2 gamma_ref^2) when zero. */
+int g4b_beam_advance(g4b_beam* b, g4b_field* const* fields, const double* fc,
+                     int nfield, const g4b_step* st);
+
+/* ---- slippage -----------------------------------------------------------------
+ * ControlCUDA::applySlippage, single rank (src/Core/ControlCUDA.cpp:148-252):
+ * accuslip += shift; while |accuslip| > 0.8*sample shift `first` by one slice
+ * and zero the plane entering the window (unless periodic).  Returns the
+ * number of whole-slice shifts in *nshift (may be NULL). */
+int g4b_slippage(g4b_field* f, double shift, double sample, int time_run,
+                 int periodic, double* accuslip, int* nshift);
+
+/* ---- diagnostics -----------------------------------------------------------------
+ * Device part of DiagnosticCUDA::calcBeam (src/Core/DiagnosticCUDA.cpp:188-303,
+ * :414-447): per slice the 23 raw sums/extrema in the reference's order
+ * (g1,g2,x1,x2,y1,y2,px1,px2,py1,py2,xpx,ypy,count,xmin,xmax,pxmin,pxmax,
+ * ymin,ymax,pymin,pymax,gmin,gmax) into stats[nslice*23], and the bunching
+ * sums sum(cos h theta), sum(sin h theta), h = 1..nharm, into
+ * bre/bim[nslice*nharm].  Host arrays; the call synchronises. */
+int g4b_diag_beam(g4b_beam* b, int nharm, int need_aux, double* stats,
+                  double* bre, double* bim);
+/* Device part of DiagnosticCUDA::calcField (src/Core/DiagnosticCUDA.cpp:305-363,
+ * :633-659): per beam slice is = (nslice + storage_slice - first) % nslice the
+ * 7 sums (power, x1, x2, y1, y2, ff_re, ff_im) into stats[nslice*7] and the
+ * centre cell (ngrid^2-1)/2 into center[nslice*2] (re, im). */
+int g4b_diag_field(g4b_field* f, double* stats, double* center);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* G4B_H_ */

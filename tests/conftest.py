@@ -1,0 +1,12 @@
+"""Test configuration: repo root on sys.path and the `gpu` marker."""
+import sys
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent.parent
+if str(ROOT) not in sys.path:
+    sys.path.insert(0, str(ROOT))
+
+
+def pytest_configure(config):
+    config.addinivalue_line(
+        "markers", "gpu: needs a B200 (runs the CUDA kernels through the C ABI)")
