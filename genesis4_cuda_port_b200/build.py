@@ -101,8 +101,7 @@ def build_host() -> Path:
             list(ex.map(_run, jobs))
     if objs and (jobs or _newer(HOST_LIB, objs + [DEVICE_LIB])):
         _run([CXX, "-shared", "-o", str(HOST_LIB), *map(str, objs),
-              "-L", str(LIB), "-lg4b200", "-Wl,-rpath,$ORIGIN",
-              "-L", "/usr/local/cuda/lib64", "-lcudart"])
+              "-L", str(LIB), "-lg4b200", "-Wl,-rpath,$ORIGIN"])
     return HOST_LIB
 
 

@@ -474,8 +474,10 @@ static int launch_pass_t(g4b_field* f, const AdiPassArgs& args, const CUtensorMa
     configured = true;
   }
   const unsigned grid = (unsigned)(f->nslice * args.nband);
-  kern<<<grid, W * 32, smem, f->ctx->stream>>>(args, tm);
-  count_launch(f->ctx);
+  {
+    LaunchScope ls(f->ctx, PX ? "adi_pass_x" : "adi_pass_y");
+    kern<<<grid, W * 32, smem, f->ctx->stream>>>(args, tm);
+  }
   return check_launch(f->ctx, "adi_pass_kernel");
 }
 
@@ -694,10 +696,12 @@ int g4b_adi_advance(g4b_adi* adi, g4b_field* f, g4b_beam* b, const g4b_step* st,
   const bool use_source = do_source && b->npart > 0;
   const void* src = nullptr;
   if (use_source) {
-    slice_scl_kernel<<<(b->nslice + 127) / 128, 128, 0, c->stream>>>(
-        b->nslice, b->d_off, b->d_current, fc, f->xks, f->dgrid, st->delz, kVacimp,
-        kEev, b->d_scl);
-    count_launch(c);
+    {
+      LaunchScope ls(c, "slice_scl");
+      slice_scl_kernel<<<(b->nslice + 127) / 128, 128, 0, c->stream>>>(
+          b->nslice, b->d_off, b->d_current, fc, f->xks, f->dgrid, st->delz, kVacimp,
+          kEev, b->d_scl);
+    }
     if (int rc = check_launch(c, "slice_scl_kernel")) return rc;
     DepositArgs da{};
     da.x = b->x;
@@ -730,8 +734,10 @@ int g4b_adi_advance(g4b_adi* adi, g4b_field* f, g4b_beam* b, const g4b_step* st,
                                         (int)acc_bytes));
       configured = true;
     }
-    deposit_slice_kernel<<<f->nslice, 512, acc_bytes, c->stream>>>(da);
-    count_launch(c);
+    {
+      LaunchScope ls(c, "deposit");
+      deposit_slice_kernel<<<f->nslice, 512, acc_bytes, c->stream>>>(da);
+    }
     if (int rc = check_launch(c, "deposit_slice_kernel")) return rc;
     src = f->src;
   }

@@ -335,8 +335,10 @@ int g4b_beam_track(g4b_beam* b, const g4b_step* st, double delz, int last_step) 
     a.m32 = m.v[3][2];
     a.m33 = m.v[3][3];
   }
-  track_kernel<<<grid_for(c, b->npart, 256), 256, 0, c->stream>>>(a);
-  count_launch(c);
+  {
+    LaunchScope ls(c, "track");
+    track_kernel<<<grid_for(c, b->npart, 256), 256, 0, c->stream>>>(a);
+  }
   return check_launch(c, "track_kernel");
 }
 
@@ -351,9 +353,11 @@ int g4b_beam_r56(g4b_beam* b, const g4b_step* st, double lambda0) {
                 2 * ld * std::tan(angle) / std::cos(angle)) *
                angle;
   r56 = r56 * 4 * std::asin(1.0) / lambda0 / st->gamma_ref;
-  r56_kernel<<<grid_for(c, b->npart, 256), 256, 0, c->stream>>>(b->npart, b->gamma, b->theta,
-                                                                r56, st->gamma_ref);
-  count_launch(c);
+  {
+    LaunchScope ls(c, "r56");
+    r56_kernel<<<grid_for(c, b->npart, 256), 256, 0, c->stream>>>(b->npart, b->gamma,
+                                                                  b->theta, r56, st->gamma_ref);
+  }
   return check_launch(c, "r56_kernel");
 }
 
@@ -407,11 +411,13 @@ int g4b_beam_advance(g4b_beam* b, g4b_field* const* fields, const double* fc, in
   a.ky = st->ky;
   a.gradx = st->gradx;
   a.grady = st->grady;
-  if (nfield == 1)
-    push_kernel<1><<<b->nchunk, 256, 0, c->stream>>>(a);
-  else
-    push_kernel<0><<<b->nchunk, 256, 0, c->stream>>>(a);
-  count_launch(c);
+  {
+    LaunchScope ls(c, "push");
+    if (nfield == 1)
+      push_kernel<1><<<b->nchunk, 256, 0, c->stream>>>(a);
+    else
+      push_kernel<0><<<b->nchunk, 256, 0, c->stream>>>(a);
+  }
   return check_launch(c, "push_kernel");
 }
 

@@ -49,6 +49,60 @@ int read_device_error(g4b_ctx* ctx, const char* what) {
   return G4B_OK;
 }
 
+static cudaEvent_t pool_get(Profiler& p) {
+  if (!p.pool.empty()) {
+    cudaEvent_t e = p.pool.back();
+    p.pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+static void prof_resolve(g4b_ctx* c) {
+  Profiler& p = c->prof;
+  if (p.pending.empty()) return;
+  cudaStreamSynchronize(c->stream);
+  for (auto& q : p.pending) {
+    float t = 0.f;
+    if (cudaEventElapsedTime(&t, q.a, q.b) == cudaSuccess) {
+      p.count[q.name] += 1;
+      p.ms[q.name] += t;
+    }
+    p.pool.push_back(q.a);
+    p.pool.push_back(q.b);
+  }
+  p.pending.clear();
+}
+
+void prof_begin(g4b_ctx* c, const char* name) {
+  Profiler& p = c->prof;
+  if (!p.on) return;
+  int id = -1;
+  for (size_t i = 0; i < p.names.size(); ++i)
+    if (p.names[i] == name) id = (int)i;
+  if (id < 0) {
+    id = (int)p.names.size();
+    p.names.push_back(name);
+    p.count.push_back(0);
+    p.ms.push_back(0.0);
+  }
+  p.open_a = pool_get(p);
+  p.open_name = id;
+  cudaEventRecord(p.open_a, c->stream);
+}
+
+void prof_end(g4b_ctx* c) {
+  Profiler& p = c->prof;
+  if (!p.on || p.open_name < 0) return;
+  cudaEvent_t b = pool_get(p);
+  cudaEventRecord(b, c->stream);
+  p.pending.push_back({p.open_name, p.open_a, b});
+  p.open_name = -1;
+  if (p.pending.size() > 8192) prof_resolve(c);
+}
+
 int pick_M(int n) {
   static const int kM[] = {1, 3, 5, 7, 9, 11, 13, 15, 17, 21, 25, 33};
   for (int m : kM)
@@ -134,6 +188,11 @@ int g4b_ctx_destroy(g4b_ctx* c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   if (c->d_error) cudaFree(c->d_error);
+  for (auto& q : c->prof.pending) {
+    cudaEventDestroy(q.a);
+    cudaEventDestroy(q.b);
+  }
+  for (auto e : c->prof.pool) cudaEventDestroy(e);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return G4B_OK;
@@ -168,6 +227,39 @@ int g4b_ctx_synchronize(g4b_ctx* c) {
 int g4b_ctx_launch_count(g4b_ctx* c, uint64_t* count) {
   if (!c || !count) return fail(G4B_ERR_ARG, "g4b_ctx_launch_count: null arg");
   *count = c->launches.load();
+  return G4B_OK;
+}
+
+int g4b_ctx_profile(g4b_ctx* c, int enable) {
+  if (!c) return fail(G4B_ERR_ARG, "g4b_ctx_profile: null ctx");
+  G4B_CUDA_TRY(cudaSetDevice(c->device));
+  prof_resolve(c);
+  Profiler& p = c->prof;
+  if (enable) {
+    p.names.clear();
+    p.count.clear();
+    p.ms.clear();
+  }
+  p.on = enable != 0;
+  return G4B_OK;
+}
+
+int g4b_ctx_profile_read(g4b_ctx* c, int max_kernels, char* names, uint64_t* counts,
+                         double* total_ms, int* nkernels) {
+  if (!c || !nkernels) return fail(G4B_ERR_ARG, "g4b_ctx_profile_read: null arg");
+  G4B_CUDA_TRY(cudaSetDevice(c->device));
+  prof_resolve(c);
+  Profiler& p = c->prof;
+  const int n = (int)p.names.size();
+  *nkernels = n;
+  for (int i = 0; i < n && i < max_kernels; ++i) {
+    if (names) {
+      std::strncpy(names + 64 * i, p.names[i].c_str(), 63);
+      names[64 * i + 63] = 0;
+    }
+    if (counts) counts[i] = p.count[i];
+    if (total_ms) total_ms[i] = p.ms[i];
+  }
   return G4B_OK;
 }
 

@@ -242,10 +242,12 @@ int g4b_diag_beam(g4b_beam* b, int nharm, int need_aux, double* stats, double* b
   double* d_stats = scratch.d;
   double* d_bre = d_stats + ns * 23;
   double* d_bim = d_bre + ns * nharm;
-  beam_diag_kernel<<<b->nslice, kDiagThreads, 0, c->stream>>>(
-      b->nslice, nharm, need_aux, b->d_off, b->x, b->y, b->px, b->py, b->gamma, b->theta,
-      d_stats, d_bre, d_bim);
-  count_launch(c);
+  {
+    LaunchScope ls(c, "diag_beam");
+    beam_diag_kernel<<<b->nslice, kDiagThreads, 0, c->stream>>>(
+        b->nslice, nharm, need_aux, b->d_off, b->x, b->y, b->px, b->py, b->gamma, b->theta,
+        d_stats, d_bre, d_bim);
+  }
   if (int rc = check_launch(c, "beam_diag_kernel")) return rc;
   G4B_CUDA_TRY(cudaMemcpyAsync(stats, d_stats, ns * 23 * sizeof(double),
                                cudaMemcpyDeviceToHost, c->stream));
@@ -266,15 +268,17 @@ int g4b_diag_field(g4b_field* f, double* stats, double* center) {
   if (int rc = ensure(scratch, ns * 9)) return rc;
   double* d_stats = scratch.d;
   double* d_center = d_stats + ns * 7;
-  if (f->precision == G4B_FP64)
-    field_diag_kernel<double2><<<f->nslice, kDiagThreads, 0, c->stream>>>(
-        f->nslice, f->ngrid, f->ld, f->first, static_cast<const double2*>(f->a), d_stats,
-        d_center);
-  else
-    field_diag_kernel<float2><<<f->nslice, kDiagThreads, 0, c->stream>>>(
-        f->nslice, f->ngrid, f->ld, f->first, static_cast<const float2*>(f->a), d_stats,
-        d_center);
-  count_launch(c);
+  {
+    LaunchScope ls(c, "diag_field");
+    if (f->precision == G4B_FP64)
+      field_diag_kernel<double2><<<f->nslice, kDiagThreads, 0, c->stream>>>(
+          f->nslice, f->ngrid, f->ld, f->first, static_cast<const double2*>(f->a), d_stats,
+          d_center);
+    else
+      field_diag_kernel<float2><<<f->nslice, kDiagThreads, 0, c->stream>>>(
+          f->nslice, f->ngrid, f->ld, f->first, static_cast<const float2*>(f->a), d_stats,
+          d_center);
+  }
   if (int rc = check_launch(c, "field_diag_kernel")) return rc;
   G4B_CUDA_TRY(cudaMemcpyAsync(stats, d_stats, ns * 7 * sizeof(double),
                                cudaMemcpyDeviceToHost, c->stream));

@@ -39,6 +39,24 @@ struct TensorMapEncoder;
 
 }  // namespace g4b
 
+namespace g4b {
+// Per-kernel CUDA-event timing on the context's stream (off by default).
+struct Profiler {
+  bool on = false;
+  struct Pending {
+    int name;
+    cudaEvent_t a, b;
+  };
+  std::vector<std::string> names;
+  std::vector<uint64_t> count;
+  std::vector<double> ms;
+  std::vector<Pending> pending;
+  std::vector<cudaEvent_t> pool;
+  cudaEvent_t open_a = nullptr;
+  int open_name = -1;
+};
+}  // namespace g4b
+
 struct g4b_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -47,6 +65,7 @@ struct g4b_ctx {
   std::atomic<uint64_t> launches{0};
   int* d_error = nullptr;  // device error flag (bit set, see kErr*)
   void* encode_fn = nullptr;  // cuTensorMapEncodeTiled
+  g4b::Profiler prof;
 };
 
 struct g4b_field {
@@ -102,6 +121,19 @@ namespace g4b {
 
 // Launch bookkeeping: every kernel launch goes through this.
 inline void count_launch(g4b_ctx* ctx, int n = 1) { ctx->launches += n; }
+
+// Brackets one kernel launch with profiler events when profiling is on:
+//   { LaunchScope ls(ctx, "name"); kernel<<<...>>>(...); }
+void prof_begin(g4b_ctx* ctx, const char* name);
+void prof_end(g4b_ctx* ctx);
+struct LaunchScope {
+  g4b_ctx* c;
+  LaunchScope(g4b_ctx* ctx, const char* name) : c(ctx) { prof_begin(ctx, name); }
+  ~LaunchScope() {
+    prof_end(c);
+    count_launch(c);
+  }
+};
 
 int check_launch(g4b_ctx* ctx, const char* what);
 int read_device_error(g4b_ctx* ctx, const char* what);

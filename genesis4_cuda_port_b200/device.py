@@ -42,6 +42,25 @@ class Context:
         check(self.lib.g4b_ctx_launch_count(self.h, C.byref(v)))
         return int(v.value)
 
+    def profile(self, enable: bool) -> None:
+        """Per-kernel CUDA-event timing on this context's stream."""
+        check(self.lib.g4b_ctx_profile(self.h, int(enable)))
+
+    def profile_read(self) -> dict:
+        """{kernel name: (launches, total ms)} since profiling was enabled."""
+        n = C.c_int()
+        check(self.lib.g4b_ctx_profile_read(self.h, 0, None, None, None, C.byref(n)))
+        k = n.value
+        names = C.create_string_buffer(64 * max(k, 1))
+        counts = (C.c_uint64 * max(k, 1))()
+        ms = (C.c_double * max(k, 1))()
+        check(self.lib.g4b_ctx_profile_read(self.h, k, names, counts, ms, C.byref(n)))
+        out = {}
+        for i in range(k):
+            nm = names.raw[64 * i:64 * (i + 1)].split(b"\0")[0].decode()
+            out[nm] = (int(counts[i]), float(ms[i]))
+        return out
+
     def sm_count(self) -> int:
         v = C.c_int()
         check(self.lib.g4b_ctx_sm_count(self.h, C.byref(v)))

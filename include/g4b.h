@@ -92,6 +92,13 @@ int g4b_ctx_synchronize(g4b_ctx* ctx);
 int g4b_ctx_launch_count(g4b_ctx* ctx, uint64_t* count);
 /* SM count of the context's device. */
 int g4b_ctx_sm_count(g4b_ctx* ctx, int* count);
+/* Per-kernel CUDA-event timing on the context's stream (the reference only
+ * has wall-clock phase timers, src/Core/Gencore.cpp:163-270).  Enabling
+ * clears the totals; reading synchronises the stream.  names receives
+ * 64-byte NUL-terminated kernel names. */
+int g4b_ctx_profile(g4b_ctx* ctx, int enable);
+int g4b_ctx_profile_read(g4b_ctx* ctx, int max_kernels, char* names,
+                         uint64_t* counts, double* total_ms, int* nkernels);
 
 /* ---- field state -----------------------------------------------------------
  * Replaces Genesis4FieldSoA + Field::init_fieldSoA/pack_field_to_soa/

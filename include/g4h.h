@@ -1,0 +1,83 @@
+/*
+ * g4h.h -- C ABI of the C++ host layer (libg4host.so) that sits above g4b.h:
+ * input decks, lattice expansion into per-step undulator tables, beam and
+ * field loading, and the Gencore step driver with the reference's
+ * Field / Beam / FieldSolver / BeamSolver objects.
+ *
+ * Upstream GENESIS 1.3 v4 provides these parts to the reference (they are not
+ * in the reference tree itself); this layer re-derives the subset the hot
+ * path needs from published FEL physics.  Status codes follow g4b.h.
+ */
+#ifndef G4H_H_
+#define G4H_H_
+
+#include <stdint.h>
+
+#include "g4b.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+const char* g4h_last_error(void);
+
+/* ---- beam loading (upstream Loading / QuietStart / ShotNoise) -----------
+ * Quiet start: each slice holds npart particles in npart/nbins beamlets of
+ * nbins particles spaced 2*pi/nbins in phase; the beamlets' (x, y, px, py,
+ * gamma, theta0) come from a Hammersley/Halton set (bases 2, 3, 5, 7, 11, 13)
+ * mapped to a Gaussian through the inverse normal CDF.  Shot noise perturbs
+ * the beamlet phases so that <|b_h|^2> = 1/N_e per harmonic (Fawley,
+ * PRST-AB 5, 070701, 2002). */
+typedef struct g4h_beam_spec {
+  int nslice;
+  int npart;          /* particles per slice                              */
+  int nbins;          /* particles per beamlet                            */
+  int shotnoise;      /* 0/1                                              */
+  uint64_t seed;
+  double gamma0;      /* mean gamma                                       */
+  double delgam;      /* rms gamma spread (absolute)                      */
+  double ex, ey;      /* normalised emittances [m rad]                    */
+  double betax, betay, alphax, alphay;
+  double xcenter, ycenter, pxcenter, pycenter;
+  double reflength;   /* lambda0 [m]                                       */
+  double slicelength; /* reflength * sample [m]                           */
+} g4h_beam_spec;
+
+/* Writes npart*nslice particles (slice-contiguous) and the nslice+1 offsets;
+ * current[nslice] gives each slice's current [A] (shot-noise amplitude). */
+int g4h_load_beam(const g4h_beam_spec* spec, const double* current,
+                  double* x, double* y, double* px, double* py,
+                  double* gamma, double* theta, int64_t* slice_offsets);
+
+/* Gaussian mode of power P [W] and waist w0 [m] on an ngrid^2 grid of half
+ * width gridmax, at wavelength xlambda; writes interleaved complex cells of
+ * one plane (the reference's field normalisation, P = sum |u|^2
+ * (dgrid eev/ks)^2 / vacimp). */
+int g4h_gaussian_field(int ngrid, double gridmax, double xlambda, double power,
+                       double w0, double* cells);
+
+/* ---- lattice -> per-step undulator tables (upstream Lattice/Undulator) ---- */
+typedef struct g4h_lattice g4h_lattice;
+
+/* Parses a .lat file subset (UNDULATOR, DRIFT, QUADRUPOLE, CORRECTOR,
+ * CHICANE, PHASESHIFTER, MARKER, LINE with n*element repetition) and expands
+ * `beamline` into steps of at most delz (undulators: delz per step). */
+int g4h_lattice_parse(const char* text, const char* beamline, double delz,
+                      double gamma0, double lambda0, g4h_lattice** out);
+int g4h_lattice_destroy(g4h_lattice* lat);
+int g4h_lattice_nstep(g4h_lattice* lat, int* nstep);
+/* Step i: the kernel parameters, plus the upstream Undulator values the
+ * driver needs: slippage (in units of lambda0), fc (coupling aw*JJ_h for
+ * harmonic h, filled for h = 1..nharm), z at step end and the marker bits. */
+int g4h_lattice_step(g4h_lattice* lat, int i, g4b_step* st, double* slippage,
+                     double* z, int* marker);
+int g4h_lattice_fc(g4h_lattice* lat, int i, int harm, double* fc);
+
+/* Planar / helical coupling factor aw * JJ_h (upstream Undulator::fc). */
+double g4h_coupling(double aw, int harm, int helical);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* G4H_H_ */
