@@ -51,6 +51,16 @@ class Step(C.Structure):
             setattr(self, k, v)
 
 
+class RunDesc(C.Structure):
+    """Mirror of ``g4b_run_desc`` (include/g4b.h)."""
+
+    _fields_ = [("nslice", C.c_int), ("nfield", C.c_int), ("harm", C.c_int * 8),
+                ("ngrid", C.c_int * 8), ("gridmax", C.c_double * 8),
+                ("lambda0", C.c_double), ("gamma_ref", C.c_double),
+                ("sample", C.c_double), ("time_run", C.c_int), ("periodic", C.c_int),
+                ("nbunch", C.c_int), ("precision", C.c_int)]
+
+
 # name -> (restype, argtypes)
 _SIGS = {
     "g4b_last_error": (C.c_char_p, []),
@@ -98,6 +108,20 @@ _SIGS = {
     "g4b_diag_beam": (C.c_int, [C.c_void_p, C.c_int, C.c_int, c_double_p,
                                 c_double_p, c_double_p]),
     "g4b_diag_field": (C.c_int, [C.c_void_p, c_double_p, c_double_p]),
+    "g4b_run_create": (C.c_int, [C.c_void_p, C.POINTER(RunDesc), c_int64_p, c_void_pp]),
+    "g4b_run_destroy": (C.c_int, [C.c_void_p]),
+    "g4b_run_upload_beam": (C.c_int, [C.c_void_p] + [c_double_p] * 6),
+    "g4b_run_download_beam": (C.c_int, [C.c_void_p] + [c_double_p] * 6),
+    "g4b_run_upload_field": (C.c_int, [C.c_void_p, C.c_int, c_double_p, C.c_int]),
+    "g4b_run_download_field": (C.c_int, [C.c_void_p, C.c_int, c_double_p, c_int_p]),
+    "g4b_run_set_current": (C.c_int, [C.c_void_p, c_double_p]),
+    "g4b_run_set_eloss": (C.c_int, [C.c_void_p, c_double_p]),
+    "g4b_run_set_lattice": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(Step), c_double_p,
+                                      c_double_p, C.c_int]),
+    "g4b_run_advance": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int]),
+    "g4b_run_prepare": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "g4b_run_history": (C.c_int, [C.c_void_p, C.c_int, c_double_p, c_double_p]),
+    "g4b_run_device_bytes": (C.c_int, [C.c_void_p, c_uint64_p]),
 }
 
 _lib = None

@@ -80,7 +80,9 @@ __device__ __forceinline__ C shfl_down_c(C v, int d) {
 
 struct AdiPassArgs {
   const void* in;      // pass X: field (natural); pass Y: R' (transposed)
-  const void* src;     // pass X only; nullptr = no source this step
+  const void* src;     // pass X only: compact per-slice source tiles; nullptr = none
+  const int4* desc;    // per-slice source tile (x0, y0, width, height); width 0 = none
+  size_t src_cap;      // cells reserved per slice in `src`
   const void* tab;     // lane-minor tables of this precision
   int n, ld, nband;
   int out_off;         // byte offset of the output staging tile
@@ -88,6 +90,13 @@ struct AdiPassArgs {
   int box_rows, nbox;  // TMA store boxes per band
   double r;
   int* err;
+  // pass Y extras (fused form): planes [zero_start, zero_start+zero_count)
+  // (mod nslice) are written as zeros (the slippage of this step), and, when
+  // diag is non-null, each CTA writes 9 partial sums of the plane it solved
+  // (power, x1, x2, y1, y2, sum re, sum im, centre re, centre im) to
+  // diag[(slice * nband + band) * 9].
+  int nslice, zero_start, zero_count;
+  double* diag;
 };
 
 template <typename T> struct BandW;
@@ -123,16 +132,24 @@ __global__ void __launch_bounds__(BandW<T>::value * 32)
   const int lo = PX ? max(r0 - 1, 0) : r0;
   const int hi = PX ? min(r0 + W, n - 1) : min(r0 + W - 1, n - 1);
   const int slot0 = PX ? lo - (r0 - 1) : 0;
+  // the source is non-zero only on the slice's tile: rows [sy0, sy0+sbh),
+  // columns [sx0, sx0+sbw); stile holds the tile rows of this band
+  const int4 sd = has_src ? __ldg(&a.desc[s]) : make_int4(0, 0, 0, 0);
+  const int sx0 = sd.x, sbw = sd.z;
+  const int srow_lo = max(r0, sd.y);
+  const int srow_hi = min(min(r0 + W, n), sd.y + sd.w);
+  const bool band_src = has_src && sbw > 0 && srow_lo < srow_hi;
   if (tid == 0) {
     const C* in = reinterpret_cast<const C*>(a.in) + (size_t)s * plane;
     const uint32_t bytes_in = (uint32_t)((hi - lo + 1) * ld * sizeof(C));
-    const int shi = min(r0 + W - 1, n - 1);
-    const uint32_t bytes_s = has_src ? (uint32_t)((shi - r0 + 1) * ld * sizeof(C)) : 0u;
+    const uint32_t bytes_s =
+        band_src ? (uint32_t)((srow_hi - srow_lo) * sbw * sizeof(C)) : 0u;
     ptx::mbar_expect_tx(bar, bytes_in + bytes_s);
     ptx::bulk_g2s(tile + slot0 * ld, in + (size_t)lo * ld, bytes_in, bar);
-    if (has_src) {
-      const C* sp = reinterpret_cast<const C*>(a.src) + (size_t)s * plane;
-      ptx::bulk_g2s(stile, sp + (size_t)r0 * ld, bytes_s, bar);
+    if (band_src) {
+      const C* sp = reinterpret_cast<const C*>(a.src) + (size_t)s * a.src_cap +
+                    (size_t)(srow_lo - sd.y) * sbw;
+      ptx::bulk_g2s(stile + (srow_lo - r0) * sbw, sp, bytes_s, bar);
     }
   }
   if (PX) {
@@ -156,6 +173,8 @@ __global__ void __launch_bounds__(BandW<T>::value * 32)
   const C* tB = tF + 5 * 32;         // bwd scan    [5][32]
   const int iy = r0 + warp;
   const bool active = iy < n;
+  const bool row_src = band_src && iy >= srow_lo && iy < srow_hi;
+  const C* srow = stile + warp * sbw - sx0;  // srow[k] for k in [sx0, sx0+sbw)
   C v[M];
 
   if (active) {
@@ -172,7 +191,7 @@ __global__ void __launch_bounds__(BandW<T>::value * 32)
           const T li = up.y + dn.y - u.y * (T)2;
           R.x = u.x + (-r * li);
           R.y = u.y + r * lr;
-          if (has_src) R = cadd(R, stile[warp * ld + k]);
+          if (row_src && k >= sx0 && k < sx0 + sbw) R = cadd(R, srow[k]);
         } else {
           R = tile[warp * ld + k];
         }
@@ -242,13 +261,67 @@ __global__ void __launch_bounds__(BandW<T>::value * 32)
       C R;
       R.x = v[j].x + (-r * li);
       R.y = v[j].y + r * lr;
-      if (has_src && k < n) R = cadd(R, stile[warp * ld + k]);
+      if (row_src && k >= sx0 && k < sx0 + sbw) R = cadd(R, srow[k]);
       w2[j] = R;
     }
 #pragma unroll
     for (int j = 0; j < M; ++j) v[j] = w2[j];
   }
 
+  if (!PX && a.zero_count > 0) {
+    const int zs = (s - a.zero_start + a.nslice) % a.nslice;
+    if (zs < a.zero_count) {
+#pragma unroll
+      for (int j = 0; j < M; ++j) v[j] = C{0, 0};
+    }
+  }
+  if (!PX && a.diag != nullptr) {
+    // field diagnostics of this band (g4_field_slice_reduce_kernel,
+    // src/Core/DiagnosticCUDA.cpp:305-363): this warp holds column
+    // ix = r0 + warp, rows iy = lane*M + j of the solved plane
+    __shared__ double dpart[BandW<T>::value][9];
+    const double shift = -0.5 * (double)(n - 1);
+    const double dx = (double)iy + shift;  // iy is the column index in pass Y
+    double sp = 0, sx1 = 0, sx2 = 0, sy1 = 0, sy2 = 0, sre = 0, sim = 0;
+    double cre = 0, cim = 0;
+    const int ic = (n * n - 1) / 2;
+    const int icy = ic / n, icx = ic - icy * n;
+    if (active) {
+#pragma unroll
+      for (int j = 0; j < M; ++j) {
+        const int k = lane * M + j;
+        if (k < n) {
+          const double re = (double)v[j].x, im = (double)v[j].y;
+          const double wei = re * re + im * im;
+          const double dy = (double)k + shift;
+          sp += wei;
+          sy1 += dy * wei;
+          sy2 += dy * dy * wei;
+          sre += re;
+          sim += im;
+          if (iy == icx && k == icy) {
+            cre = re;
+            cim = im;
+          }
+        }
+      }
+      sx1 = dx * sp;
+      sx2 = dx * dx * sp;
+    }
+    double vals[9] = {sp, sx1, sx2, sy1, sy2, sre, sim, cre, cim};
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+      double t = vals[q];
+      for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+      if (lane == 0) dpart[warp][q] = t;
+    }
+    __syncthreads();
+    if (tid < 9) {
+      double t = dpart[0][tid];
+      for (int w = 1; w < W; ++w) t += dpart[w][tid];
+      a.diag[((size_t)s * a.nband + band) * 9 + tid] = t;
+    }
+  }
   if (active) {
 #pragma unroll
     for (int j = 0; j < M; ++j) {
@@ -275,13 +348,17 @@ __global__ void __launch_bounds__(BandW<T>::value * 32)
 //  2. the box is accumulated in shared memory as int64 fixed point with the
 //     exponent 2^E chosen so that count * max q * 2^E < 2^62 (integer adds are
 //     associative, so the result does not depend on the order of the atomics);
-//  3. the CTA writes the whole target plane: scl * sum * 2^-E inside the box,
-//     zero elsewhere.  Boxes larger than shared memory are done in row bands.
+//  3. the CTA writes only the box, scl * sum * 2^-E, as a compact tile of the
+//     target slice, and the tile's (x0, y0, width, height) descriptor; the
+//     source is zero outside the box.  Boxes larger than the shared-memory
+//     accumulator are done in row bands.
 struct DepositArgs {
   const double *x, *y, *gamma, *theta;
   const int64_t* off;
   const double* scl;
-  double2* src;
+  double2* src;        // compact tiles, src_cap cells per slice
+  int4* desc;          // per target slice
+  size_t src_cap;
   int nslice, n, ld, first, harm, acc_cells;
   double gridmax, dgrid, ax, ay, kx, ky, gradx, grady;
   int* err;
@@ -334,8 +411,7 @@ __global__ void __launch_bounds__(512) deposit_slice_kernel(const DepositArgs a)
   const int bs = blockIdx.x;
   const int tid = threadIdx.x;
   const int target = (bs + a.first) % a.nslice;
-  const int n = a.n, ld = a.ld;
-  double2* S = a.src + (size_t)target * n * ld;
+  double2* S = a.src + (size_t)target * a.src_cap;
   const int64_t p0 = a.off[bs], p1 = a.off[bs + 1];
   const double scl = a.scl[bs];
 
@@ -348,8 +424,8 @@ __global__ void __launch_bounds__(512) deposit_slice_kernel(const DepositArgs a)
       const double xp = a.x[p], yp = a.y[p];
       if (!dep_cell(a, xp, yp, ix, iy, wx, wy)) continue;
       const double q = fabs(dep_weight(a, xp, yp, a.gamma[p]));
-      qmax = q > qmax ? q : qmax;  // NaN propagates as "not greater"
-      if (!(q <= 1e300)) qmax = INFINITY;
+      qmax = q > qmax ? q : qmax;
+      if (!(q <= 1e300)) qmax = INFINITY;  // NaN or inf
       ixmin = min(ixmin, ix);
       ixmax = max(ixmax, ix);
       iymin = min(iymin, iy);
@@ -362,7 +438,6 @@ __global__ void __launch_bounds__(512) deposit_slice_kernel(const DepositArgs a)
   ixmax = block_reduce<int>(ixmax, shi, true);
   iymin = block_reduce<int>(iymin, shi, false);
   iymax = block_reduce<int>(iymax, shi, true);
-  // count: sum over threads (exact integer sum)
   for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
   __syncthreads();
   if ((tid & 31) == 0) shi[tid >> 5] = cnt;
@@ -372,9 +447,7 @@ __global__ void __launch_bounds__(512) deposit_slice_kernel(const DepositArgs a)
   __syncthreads();
 
   const bool any = total > 0 && qmax > 0.0;
-  if (any && !(qmax < INFINITY)) {
-    if (tid == 0) atomicOr(a.err, kErrFixedRange);
-  }
+  if (any && !(qmax < INFINITY) && tid == 0) atomicOr(a.err, kErrFixedRange);
   const bool ok = any && qmax < INFINITY;
   int bx0 = 0, by0 = 0, bw = 0, bh = 0;
   double scale = 0.0, unscale = 0.0;
@@ -388,14 +461,12 @@ __global__ void __launch_bounds__(512) deposit_slice_kernel(const DepositArgs a)
     scale = ldexp(1.0, 62 - e);
     unscale = scl * ldexp(1.0, e - 62);
   }
-  const int band_h = ok ? max(1, min(bh, a.acc_cells / bw)) : 0;
+  if (tid == 0) a.desc[target] = make_int4(bx0, by0, ok ? bw : 0, bh);
+  if (!ok) return;
+  const int band_h = max(1, min(bh, a.acc_cells / bw));
   const double hphase = (double)a.harm;
 
-  // rows below the box
-  for (int row = 0; row < (ok ? by0 : n); ++row)
-    for (int k = tid; k < ld; k += blockDim.x) S[(size_t)row * ld + k] = make_double2(0.0, 0.0);
-
-  for (int yb = by0; ok && yb < by0 + bh; yb += band_h) {
+  for (int yb = by0; yb < by0 + bh; yb += band_h) {
     const int hb = min(band_h, by0 + bh - yb);
     for (int i = tid; i < 2 * hb * bw; i += blockDim.x) acc[i] = 0ull;
     __syncthreads();
@@ -423,22 +494,15 @@ __global__ void __launch_bounds__(512) deposit_slice_kernel(const DepositArgs a)
       }
     }
     __syncthreads();
-    for (int i = tid; i < hb * ld; i += blockDim.x) {
-      const int ry = i / ld, k = i - ry * ld;
-      const int kx = k - bx0;
-      double2 val = make_double2(0.0, 0.0);
-      if (kx >= 0 && kx < bw && k < n) {
-        const int cell = ry * bw + kx;
-        val.x = (double)(long long)acc[2 * cell] * unscale;
-        val.y = (double)(long long)acc[2 * cell + 1] * unscale;
-      }
-      S[(size_t)(yb + ry) * ld + k] = val;
+    double2* out = S + (size_t)(yb - by0) * bw;
+    for (int i = tid; i < hb * bw; i += blockDim.x) {
+      double2 val;
+      val.x = (double)(long long)acc[2 * i] * unscale;
+      val.y = (double)(long long)acc[2 * i + 1] * unscale;
+      out[i] = val;
     }
     __syncthreads();
   }
-  // rows above the box
-  for (int row = ok ? by0 + bh : n; row < n; ++row)
-    for (int k = tid; k < ld; k += blockDim.x) S[(size_t)row * ld + k] = make_double2(0.0, 0.0);
 }
 
 // adi_compute_slice_scl (src/Core/FieldSolverADICUDA.cpp:75-96)
@@ -462,23 +526,58 @@ static constexpr double kVacimp = 376.73031346177;  // upstream `vacimp`
 static constexpr double kEev = 510998.95;          // upstream `eev`
 
 template <typename T, int M, bool PX>
+static int configure_pass_t(int device) {
+  static uint64_t configured = 0;  // per instantiation, one bit per device
+  if (device < 64 && (configured >> device) & 1) return G4B_OK;
+  cudaError_t e = cudaFuncSetAttribute(adi_pass_kernel<T, M, PX>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(adi_pass)");
+  if (device < 64) configured |= 1ull << device;
+  return G4B_OK;
+}
+
+template <typename T, int M, bool PX>
 static int launch_pass_t(g4b_field* f, const AdiPassArgs& args, const CUtensorMap& tm,
                          size_t smem) {
   constexpr int W = BandW<T>::value;
   auto kern = adi_pass_kernel<T, M, PX>;
-  static bool configured = false;  // per instantiation
-  if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         227 * 1024);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(adi_pass)");
-    configured = true;
-  }
+  if (int rc = configure_pass_t<T, M, PX>(f->ctx->device)) return rc;
   const unsigned grid = (unsigned)(f->nslice * args.nband);
   {
     LaunchScope ls(f->ctx, PX ? "adi_pass_x" : "adi_pass_y");
     kern<<<grid, W * 32, smem, f->ctx->stream>>>(args, tm);
   }
   return check_launch(f->ctx, "adi_pass_kernel");
+}
+
+template <typename T, bool PX>
+static int configure_pass_m(int M, int device) {
+  switch (M) {
+    case 1: return configure_pass_t<T, 1, PX>(device);
+    case 3: return configure_pass_t<T, 3, PX>(device);
+    case 5: return configure_pass_t<T, 5, PX>(device);
+    case 7: return configure_pass_t<T, 7, PX>(device);
+    case 9: return configure_pass_t<T, 9, PX>(device);
+    case 11: return configure_pass_t<T, 11, PX>(device);
+    case 13: return configure_pass_t<T, 13, PX>(device);
+    case 15: return configure_pass_t<T, 15, PX>(device);
+    case 17: return configure_pass_t<T, 17, PX>(device);
+    case 21: return configure_pass_t<T, 21, PX>(device);
+    case 25: return configure_pass_t<T, 25, PX>(device);
+    case 33: return configure_pass_t<T, 33, PX>(device);
+  }
+  return fail(G4B_ERR_RANGE, "adi: unsupported elements per lane");
+}
+
+int adi_configure(g4b_field* f) {
+  const int M = pick_M(f->ngrid);
+  const int d = f->ctx->device;
+  if (f->precision == G4B_FP64) {
+    if (int rc = configure_pass_m<double, true>(M, d)) return rc;
+    return configure_pass_m<double, false>(M, d);
+  }
+  if (int rc = configure_pass_m<float, true>(M, d)) return rc;
+  return configure_pass_m<float, false>(M, d);
 }
 
 template <typename T, bool PX>
@@ -501,7 +600,8 @@ static int launch_pass_m(int M, g4b_field* f, const AdiPassArgs& args,
   return fail(G4B_ERR_RANGE, "adi: unsupported elements per lane");
 }
 
-int adi_run(g4b_adi* adi, g4b_field* f, const void* src_dense) {
+int adi_run(g4b_adi* adi, g4b_field* f, const void* src, const int4* desc,
+            const AdiYExtras* ex) {
   const int n = f->ngrid, ld = f->ld, W = f->band_rows;
   AdiPassArgs args{};
   args.n = n;
@@ -526,8 +626,10 @@ int adi_run(g4b_adi* adi, g4b_field* f, const void* src_dense) {
   int rc;
   // pass X: a -> b (transposed R')
   args.in = f->a;
-  args.src = src_dense;
-  size_t smem = smem_for(true, src_dense != nullptr);
+  args.src = src;
+  args.desc = desc;
+  args.src_cap = (size_t)f->ngrid * f->ld;
+  size_t smem = smem_for(true, src != nullptr);
   if (smem > 227 * 1024) return fail(G4B_ERR_RANGE, "adi: pass X tile exceeds shared memory");
   rc = f->precision == G4B_FP64
            ? launch_pass_m<double, true>(adi->M, f, args, f->tm_store_b, smem)
@@ -536,6 +638,12 @@ int adi_run(g4b_adi* adi, g4b_field* f, const void* src_dense) {
   // pass Y: b -> a (natural)
   args.in = f->b;
   args.src = nullptr;
+  args.nslice = f->nslice;
+  if (ex) {
+    args.zero_start = ex->zero_start;
+    args.zero_count = ex->zero_count;
+    args.diag = ex->diag;
+  }
   smem = smem_for(false, false);
   rc = f->precision == G4B_FP64
            ? launch_pass_m<double, false>(adi->M, f, args, f->tm_store_a, smem)
@@ -711,6 +819,8 @@ int g4b_adi_advance(g4b_adi* adi, g4b_field* f, g4b_beam* b, const g4b_step* st,
     da.off = b->d_off;
     da.scl = b->d_scl;
     da.src = static_cast<double2*>(f->src);
+    da.desc = f->desc;
+    da.src_cap = (size_t)f->ngrid * f->ld;
     da.nslice = f->nslice;
     da.n = f->ngrid;
     da.ld = f->ld;
@@ -725,7 +835,7 @@ int g4b_adi_advance(g4b_adi* adi, g4b_field* f, g4b_beam* b, const g4b_step* st,
     da.gradx = st->gradx;
     da.grady = st->grady;
     da.err = c->d_error;
-    const size_t acc_bytes = 160 * 1024;
+    const size_t acc_bytes = 96 * 1024;
     da.acc_cells = (int)(acc_bytes / 16);
     static bool configured = false;
     if (!configured) {
@@ -741,7 +851,7 @@ int g4b_adi_advance(g4b_adi* adi, g4b_field* f, g4b_beam* b, const g4b_step* st,
     if (int rc = check_launch(c, "deposit_slice_kernel")) return rc;
     src = f->src;
   }
-  return adi_run(adi, f, src);
+  return adi_run(adi, f, src, f->desc, nullptr);
 }
 
 }  // extern "C"

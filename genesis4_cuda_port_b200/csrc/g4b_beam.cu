@@ -292,6 +292,14 @@ static unsigned grid_for(g4b_ctx* c, int64_t n, int block) {
 
 using namespace g4b;
 
+// Row-major 4x4 chicane matrix (build_chicane_matrix,
+// src/Core/TrackBeamCUDA.cpp:93-148), shared with the fused form.
+void g4b_chicane_matrix(double angle, double lb, double ld, double lt, double* out) {
+  const Mat4 m = chicane_matrix(angle, lb, ld, lt);
+  for (int i = 0; i < 4; ++i)
+    for (int j = 0; j < 4; ++j) out[4 * i + j] = m.v[i][j];
+}
+
 extern "C" {
 
 // TrackBeamCUDA::track (src/Core/TrackBeamCUDA.cpp:156-204)

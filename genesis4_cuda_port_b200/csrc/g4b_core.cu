@@ -306,6 +306,8 @@ int g4b_field_create(g4b_ctx* c, int nslice, int ngrid, double gridmax,
   cudaError_t e = cudaMalloc(&f->a, bytes);
   if (e == cudaSuccess) e = cudaMalloc(&f->b, bytes);
   if (e == cudaSuccess) e = cudaMalloc(&f->src, bytes);
+  if (e == cudaSuccess) e = cudaMalloc(&f->desc, nslice * sizeof(int4));
+  if (e == cudaSuccess) e = cudaMemsetAsync(f->desc, 0, nslice * sizeof(int4), c->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(f->a, 0, bytes, c->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(f->b, 0, bytes, c->stream);
   if (e != cudaSuccess) {
@@ -333,6 +335,7 @@ int g4b_field_destroy(g4b_field* f) {
   if (f->a) cudaFree(f->a);
   if (f->b) cudaFree(f->b);
   if (f->src) cudaFree(f->src);
+  if (f->desc) cudaFree(f->desc);
   delete f;
   return G4B_OK;
 }

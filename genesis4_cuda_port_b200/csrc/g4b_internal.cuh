@@ -76,7 +76,8 @@ struct g4b_field {
   size_t cell_bytes = 16;   // sizeof(complex) on the device
   void* a = nullptr;        // state, natural layout [slice][iy][ld]
   void* b = nullptr;        // pass-Y right-hand side, transposed [slice][ix][ld]
-  void* src = nullptr;      // source grid, natural layout
+  void* src = nullptr;      // source: compact per-slice tiles (n*ld cells reserved each)
+  int4* desc = nullptr;     // per-slice source tile (x0, y0, width, height)
   // TMA tensor maps for the transposed stores of the two ADI passes.
   CUtensorMap tm_store_b;   // pass X writes b
   CUtensorMap tm_store_a;   // pass Y writes a
@@ -138,8 +139,18 @@ struct LaunchScope {
 int check_launch(g4b_ctx* ctx, const char* what);
 int read_device_error(g4b_ctx* ctx, const char* what);
 
-// Shared ADI entry used by the drop-in and the fused path.
-int adi_run(g4b_adi* adi, g4b_field* f, const void* src_dense);
+// Shared ADI entry used by the drop-in and the fused path.  The extras of the
+// fused form (may be null): zero the planes the step's slippage zeroes, and
+// write per-band field-diagnostic partial sums (9 per band).
+struct AdiYExtras {
+  int zero_start, zero_count;
+  double* diag;
+};
+int adi_run(g4b_adi* adi, g4b_field* f, const void* src, const int4* desc,
+            const AdiYExtras* ex);
+// Sets the launch attributes of the ADI kernels for this field's grid (done
+// before any stream capture).
+int adi_configure(g4b_field* f);
 
 // Lane-minor table offsets (in complex elements).
 inline size_t tab_cbet(int M) { (void)M; return 0; }

@@ -1,0 +1,1186 @@
+// g4b_run.cu -- the fused mixed-precision form: a whole FEL run resident on
+// the device, advanced by a fixed sequence of kernels per step that a CUDA
+// graph replays.
+//
+// Device state (per particle 28 bytes): x,y and px,py as float2 pairs, the
+// energy as an FP32 offset dg = gamma - gamma_ref (keeps the ~0.01 per-step
+// energy changes above FP32 resolution), the ponderomotive phase theta in
+// FP64.  Fields are complex64.  Per step:
+//   K1 beam_step : transverse half step (+chicane), RK4 push with the frozen
+//                  bilinear field sample, R56, transverse half step
+//                  (+corrector), and each slice's bounding box of touched
+//                  cells (integer atomics, order independent);
+//   K2 deposit_diag : per slice, the beam diagnostics (FP64 sums) and the
+//                  deterministic int64 fixed-point deposition of every field's
+//                  source into a compact tile;
+//   K3/K4 ADI passes per field (pass Y also zeroes the planes this step's
+//                  slippage zeroes and writes field-diagnostic partials);
+//   K5 diag_finalize : per-slice field diagnostics into the history buffer.
+// The theta derivative ks(1-1/b) + ku is evaluated cancellation-free in FP64
+// as ku - ks*eps/(b(1+b)), eps = btper0/gamma^2 (the two ~ku terms cancel to
+// the detuning).  Slippage is the host's integer index model: `first` and the
+// zeroed planes of every step are known before the step is enqueued.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <new>
+#include <tuple>
+#include <vector>
+
+#include "g4b_internal.cuh"
+
+namespace g4b {
+
+constexpr int kRunFields = 8;
+constexpr int kMaxBunch = 8;
+constexpr int kBeamRec = 23;  // reference stats order (DiagnosticCUDA.cpp:102-125)
+
+struct MixField {
+  const float2* cells;
+  int first, n, ld, nslice, harm, do_source;
+  float gridmax, dgrid;
+  float rtmp;      // fc / xks_h
+  int4* bbox;      // [nslice]: ixmin, iymin, ixmax, iymax
+};
+
+struct PlaneMapF {
+  int mode;
+  float strength, offset;
+};
+
+struct BeamStepArgs {
+  float2 *xy, *pxy;
+  float* dg;
+  double* th;
+  const int4* chunks;
+  const double* eloss;
+  MixField f[kRunFields];
+  int nfield;
+  float gref_f, aw, aw2, ax, ay, kx, ky, gradx, grady, half;
+  double gref, xks, xku, delz, autophase;
+  PlaneMapF xm, ym;
+  int pre;            // 1 chicane before the first half step
+  float m00, m01, m10, m11, m22, m23, m32, m33;
+  int post;           // 1 corrector before the second half step
+  float cx, cy;
+  int has_r56;
+  double r56, r56_off;
+  int* err;
+};
+
+__device__ __forceinline__ void plane_f(const PlaneMapF m, float delz, float& c, float& p,
+                                        float gz) {
+  if (m.mode == 0) {
+    c += p * delz / gz;
+    return;
+  }
+  if (m.mode == 1) {
+    const float foc = sqrtf(m.strength / gz);
+    float sn, cs;
+    sincosf(foc * delz, &sn, &cs);
+    const float a2 = sn / foc, a3 = -a2 * foc * foc;
+    const float xt = c - m.offset;
+    c = cs * xt + a2 * p / gz + m.offset;
+    p = a3 * xt * gz + cs * p;
+    return;
+  }
+  const float foc = sqrtf(-m.strength / gz);
+  const float om = foc * delz;
+  const float a1 = coshf(om), a2 = sinhf(om) / foc, a3 = a2 * foc * foc;
+  const float xt = c - m.offset;
+  c = a1 * xt + a2 * p / gz + m.offset;
+  p = a3 * xt * gz + a1 * p;
+}
+
+// Reduce an FP64 angle to [-pi, pi) before FP32 trigonometry.
+__device__ __forceinline__ float reduce_angle(double a) {
+  const double twopi = 6.283185307179586476925287;
+  return (float)(a - twopi * rint(a * (1.0 / twopi)));
+}
+
+// cell of the deposit / gather in FP32 (the same arithmetic in K1 and K2)
+__device__ __forceinline__ bool cell_f(const MixField& f, float x, float y, int& ix, int& iy,
+                                       float& wx, float& wy) {
+  const float gm = f.gridmax;
+  if (!(x > -gm && x < gm && y > -gm && y < gm)) return false;
+  const float wxr = (x + gm) / f.dgrid, wyr = (y + gm) / f.dgrid;
+  ix = (int)floorf(wxr);
+  iy = (int)floorf(wyr);
+  if (ix < 0 || ix >= f.n - 1 || iy < 0 || iy >= f.n - 1) return false;
+  wx = 1.0f + (float)ix - wxr;
+  wy = 1.0f + (float)iy - wyr;
+  return true;
+}
+
+__global__ void __launch_bounds__(256) beam_step_kernel(const BeamStepArgs a) {
+  __shared__ int sbb[kRunFields][4][8];
+  const int4 ch = a.chunks[blockIdx.x];
+  const int slice = ch.x;
+  const int tid = threadIdx.x;
+  const bool live = tid < ch.z;
+  const int64_t ip = (((int64_t)ch.w) << 31) + (int64_t)(unsigned)ch.y + tid;
+  int bb[kRunFields][4];
+#pragma unroll
+  for (int f = 0; f < kRunFields; ++f) {
+    bb[f][0] = bb[f][1] = 1 << 30;
+    bb[f][2] = bb[f][3] = -1;
+  }
+  if (live) {
+    float2 xy = a.xy[ip], pp = a.pxy[ip];
+    float x = xy.x, y = xy.y, px = pp.x, py = pp.y;
+    float d = a.dg[ip];
+    double t = a.th[ip];
+    // TrackBeamCUDA::track, first half (src/Core/TrackBeamCUDA.cpp:156-204)
+    {
+      const float g = a.gref_f + d;
+      if (a.pre) {
+        const float gz = sqrtf(g * g - 1.0f - px * px - py * py);
+        float tmp = x;
+        x = a.m00 * tmp + a.m01 * px / gz;
+        px = a.m10 * tmp * gz + a.m11 * px;
+        tmp = y;
+        y = a.m22 * tmp + a.m23 * py / gz;
+        py = a.m32 * tmp * gz + a.m33 * py;
+      }
+      const float gz = sqrtf(g * g - 1.0f - a.aw2 - px * px - py * py);
+      plane_f(a.xm, a.half, x, px, gz);
+      plane_f(a.ym, a.half, y, py, gz);
+    }
+    // BeamSolverCUDA::advance push (src/Core/BeamSolverCUDA.cpp:226-409)
+    t += a.autophase;
+    const float dxu = x - a.ax, dyu = y - a.ay;
+    const float awloc = 1.0f + 0.5f * (a.kx * dxu * dxu + a.ky * dyu * dyu) + a.gradx * dxu +
+                        a.grady * dyu;
+    const float btpar = 1.0f + px * px + py * py + a.aw2 * awloc * awloc;
+    const float ez = (float)a.eloss[slice];
+    float rr[kRunFields], ri[kRunFields], c0[kRunFields], s0[kRunFields];
+    const double t0 = t;
+#pragma unroll
+    for (int f = 0; f < kRunFields; ++f) {
+      rr[f] = ri[f] = 0.f;
+      c0[f] = 1.f;
+      s0[f] = 0.f;
+      if (f >= a.nfield) continue;
+      const MixField& F = a.f[f];
+      int ix, iy;
+      float wx, wy;
+      if (cell_f(F, x, y, ix, iy, wx, wy)) {
+        const int islice = (slice + F.first) % F.nslice;
+        const float2* c = F.cells + (size_t)islice * F.n * F.ld + (size_t)iy * F.ld + ix;
+        const float2 c00 = __ldg(c), c10 = __ldg(c + 1), c01 = __ldg(c + F.ld),
+                     c11 = __ldg(c + F.ld + 1);
+        const float w00 = wx * wy, w10 = (1.f - wx) * wy, w01 = wx * (1.f - wy),
+                    w11 = (1.f - wx) * (1.f - wy);
+        const float cre = c00.x * w00 + c10.x * w10 + c01.x * w01 + c11.x * w11;
+        const float cim = c00.y * w00 + c10.y * w10 + c01.y * w01 + c11.y * w11;
+        const float sc = F.rtmp * awloc;
+        rr[f] = sc * cre;
+        ri[f] = -sc * cim;
+      }
+      sincosf(reduce_angle((double)F.harm * t0), &s0[f], &c0[f]);
+    }
+    const float ztemp1 = (float)(-2.0 / a.xks);
+    auto ode = [&](float ds, double ts, float& kg, double& kp) {
+      const double gs = a.gref + (double)ds;
+      const double inv_g2 = 1.0 / (gs * gs);
+      const float dth = (float)(ts - t0);
+      float ctr = 0.f, cti = 0.f;
+#pragma unroll
+      for (int f = 0; f < kRunFields; ++f) {
+        if (f >= a.nfield) break;
+        float sd, cd;
+        sincosf((float)a.f[f].harm * dth, &sd, &cd);
+        const float c = c0[f] * cd - s0[f] * sd;
+        const float s = s0[f] * cd + c0[f] * sd;
+        ctr += rr[f] * c + ri[f] * s;
+        cti += ri[f] * c - rr[f] * s;
+      }
+      const float btper0 = btpar + ztemp1 * ctr;
+      const double eps = (double)btper0 * inv_g2;
+      double fe;
+      float b0;
+      if (eps < 1e-5) {
+        fe = 0.5 + eps * (0.375 + eps * 0.3125);
+        b0 = (float)(1.0 - 0.5 * eps);
+      } else {
+        const double b = sqrt(1.0 - eps);
+        fe = 1.0 / (b * (1.0 + b));
+        b0 = (float)b;
+      }
+      kp += a.xku - a.xks * eps * fe;
+      kg += cti / b0 / (float)gs - ez;
+    };
+    // Genesis RK4 accumulator form (src/Core/BeamSolverCUDA.cpp:258-299)
+    float k2g = 0.f, k3g;
+    double k2p = 0.0, k3p;
+    ode(d, t, k2g, k2p);
+    float stf = (float)(0.5 * a.delz);
+    double stp = 0.5 * a.delz;
+    d += stf * k2g;
+    t += stp * k2p;
+    k3g = k2g;
+    k3p = k2p;
+    k2g = 0.f;
+    k2p = 0.0;
+    ode(d, t, k2g, k2p);
+    d += stf * (k2g - k3g);
+    t += stp * (k2p - k3p);
+    k3g /= 6.0f;
+    k3p /= 6.0;
+    k2g *= -0.5f;
+    k2p *= -0.5;
+    ode(d, t, k2g, k2p);
+    stf = (float)a.delz;
+    stp = a.delz;
+    d += stf * k2g;
+    t += stp * k2p;
+    k3g -= k2g;
+    k3p -= k2p;
+    k2g *= 2.0f;
+    k2p *= 2.0;
+    ode(d, t, k2g, k2p);
+    d += stf * (k3g + k2g / 6.0f);
+    t += stp * (k3p + k2p / 6.0);
+    // applyR56 (src/Core/TrackBeamCUDA.cpp:257-278): theta += R56 (gamma - gamma0)
+    if (a.has_r56) t += a.r56 * ((double)d + a.r56_off);
+    // second half (+corrector on the last half step)
+    {
+      if (a.post) {
+        px += a.cx;
+        py += a.cy;
+      }
+      const float g = a.gref_f + d;
+      const float gz = sqrtf(g * g - 1.0f - a.aw2 - px * px - py * py);
+      plane_f(a.xm, a.half, x, px, gz);
+      plane_f(a.ym, a.half, y, py, gz);
+    }
+    a.xy[ip] = make_float2(x, y);
+    a.pxy[ip] = make_float2(px, py);
+    a.dg[ip] = d;
+    a.th[ip] = t;
+#pragma unroll
+    for (int f = 0; f < kRunFields; ++f) {
+      if (f >= a.nfield) break;
+      int ix, iy;
+      float wx, wy;
+      if (a.f[f].do_source && cell_f(a.f[f], x, y, ix, iy, wx, wy)) {
+        bb[f][0] = min(bb[f][0], ix);
+        bb[f][1] = min(bb[f][1], iy);
+        bb[f][2] = max(bb[f][2], ix);
+        bb[f][3] = max(bb[f][3], iy);
+      }
+    }
+  }
+  // per-CTA bounding boxes -> per-slice (integer min/max: order independent)
+  const int w = tid >> 5, l = tid & 31;
+#pragma unroll
+  for (int f = 0; f < kRunFields; ++f) {
+    if (f >= a.nfield) break;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      int v = bb[f][q];
+      for (int o = 16; o > 0; o >>= 1) {
+        const int u = __shfl_xor_sync(0xffffffffu, v, o);
+        v = q < 2 ? min(v, u) : max(v, u);
+      }
+      if (l == 0) sbb[f][q][w] = v;
+    }
+  }
+  __syncthreads();
+  if (tid < 4 * a.nfield) {
+    const int f = tid >> 2, q = tid & 3;
+    int v = sbb[f][q][0];
+    for (int i = 1; i < 8; ++i) v = q < 2 ? min(v, sbb[f][q][i]) : max(v, sbb[f][q][i]);
+    if (a.f[f].do_source) {
+      int* b = reinterpret_cast<int*>(&a.f[f].bbox[slice]) + q;
+      if (q < 2) {
+        if (v < (1 << 30)) atomicMin(b, v);
+      } else if (v >= 0) {
+        atomicMax(b, v);
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------ deposit + beam diag --
+struct DepField {
+  float2* src;        // compact tiles, cap cells per slice
+  int4* desc;
+  int4* bbox;
+  size_t cap;
+  int first, n, ld, nslice, harm, do_source;
+  float gridmax, dgrid;
+  double fc, xks, dgrid_d;
+};
+
+struct DepDiagArgs {
+  const float2 *xy, *pxy;
+  const float* dg;
+  const double* th;
+  const int64_t* off;
+  const double* current;
+  DepField f[kRunFields];
+  int nfield, nbunch, need_aux, acc_cells;
+  float ax, ay, kx, ky, gradx, grady;
+  double gref, delz, fixed_scale, qbound;
+  double* beam_hist;  // [nslice][23 + 2*nbunch] for this step
+  int* err;
+};
+
+__global__ void __launch_bounds__(512) deposit_diag_kernel(const DepDiagArgs a) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ double dpart[16][kBeamRec + 2 * kMaxBunch];
+  __shared__ int4 sbox[kRunFields];
+  unsigned long long* acc = reinterpret_cast<unsigned long long*>(smem);
+  const int bs = blockIdx.x, tid = threadIdx.x, w = tid >> 5, l = tid & 31;
+  const int64_t p0 = a.off[bs], p1 = a.off[bs + 1];
+  const int rec = kBeamRec + 2 * a.nbunch;
+  if (tid < a.nfield) {
+    sbox[tid] = a.f[tid].bbox[bs];
+    // reset for the next step's beam_step
+    a.f[tid].bbox[bs] = make_int4(1 << 30, 1 << 30, -1, -1);
+  }
+  __syncthreads();
+
+  // ---- beam diagnostics: one pass, FP64 sums of the FP32 state ----
+  double v[kBeamRec];
+#pragma unroll
+  for (int k = 0; k < 13; ++k) v[k] = 0.0;
+  v[13] = 1.0e5; v[14] = -1.0e5; v[15] = 1.0e5; v[16] = -1.0e5;
+  v[17] = 1.0e5; v[18] = -1.0e5; v[19] = 1.0e5; v[20] = -1.0e5;
+  v[21] = 1.0e7; v[22] = 1.0;
+  double sdg = 0.0, sdg2 = 0.0;
+  double bre[kMaxBunch], bim[kMaxBunch];
+#pragma unroll
+  for (int h = 0; h < kMaxBunch; ++h) bre[h] = bim[h] = 0.0;
+  for (int64_t p = p0 + tid; p < p1; p += blockDim.x) {
+    const float2 xy = a.xy[p], pp = a.pxy[p];
+    const double x = xy.x, y = xy.y, px = pp.x, py = pp.y;
+    const double dgv = a.dg[p];
+    const double g = a.gref + dgv;
+    sdg += dgv;
+    sdg2 += dgv * dgv;
+    v[2] += x; v[3] += x * x; v[4] += y; v[5] += y * y;
+    v[6] += px; v[7] += px * px; v[8] += py; v[9] += py * py;
+    v[10] += x * px; v[11] += y * py; v[12] += 1.0;
+    if (a.need_aux) {
+      v[13] = fmin(v[13], x); v[14] = fmax(v[14], x);
+      v[15] = fmin(v[15], px); v[16] = fmax(v[16], px);
+      v[17] = fmin(v[17], y); v[18] = fmax(v[18], y);
+      v[19] = fmin(v[19], py); v[20] = fmax(v[20], py);
+      v[21] = fmin(v[21], g); v[22] = fmax(v[22], g);
+    }
+    float s1, c1;
+    sincosf(reduce_angle(a.th[p]), &s1, &c1);
+    float ch = c1, sh = s1;
+#pragma unroll
+    for (int h = 0; h < kMaxBunch; ++h) {
+      if (h >= a.nbunch) break;
+      bre[h] += ch;
+      bim[h] += sh;
+      const float nc = ch * c1 - sh * s1, ns = sh * c1 + ch * s1;
+      ch = nc;
+      sh = ns;
+    }
+  }
+  {
+    const double N = v[12];
+    v[0] = N * a.gref + sdg;
+    v[1] = N * a.gref * a.gref + 2.0 * a.gref * sdg + sdg2;
+  }
+#pragma unroll
+  for (int k = 0; k < kBeamRec; ++k) {
+    double t = v[k];
+    const int op = k < 13 ? 0 : ((k - 13) % 2 == 0 ? 1 : 2);
+    for (int o = 16; o > 0; o >>= 1) {
+      const double u = __shfl_xor_sync(0xffffffffu, t, o);
+      t = op == 0 ? t + u : (op == 1 ? fmin(t, u) : fmax(t, u));
+    }
+    if (l == 0) dpart[w][k] = t;
+  }
+#pragma unroll
+  for (int h = 0; h < kMaxBunch; ++h) {
+    if (h >= a.nbunch) break;
+    double tr = bre[h], ti = bim[h];
+    for (int o = 16; o > 0; o >>= 1) {
+      tr += __shfl_xor_sync(0xffffffffu, tr, o);
+      ti += __shfl_xor_sync(0xffffffffu, ti, o);
+    }
+    if (l == 0) {
+      dpart[w][kBeamRec + 2 * h] = tr;
+      dpart[w][kBeamRec + 2 * h + 1] = ti;
+    }
+  }
+  __syncthreads();
+  if (tid < rec) {
+    const int op = tid < 13 ? 0 : (tid < kBeamRec ? ((tid - 13) % 2 == 0 ? 1 : 2) : 0);
+    double t = dpart[0][tid];
+    const int nw = blockDim.x >> 5;
+    for (int i = 1; i < nw; ++i) {
+      const double u = dpart[i][tid];
+      t = op == 0 ? t + u : (op == 1 ? fmin(t, u) : fmax(t, u));
+    }
+    if (tid >= 13 && tid < kBeamRec && !a.need_aux) t = 0.0;
+    a.beam_hist[(size_t)bs * rec + tid] = t;
+  }
+
+  // ---- deposition of every field with a source this step ----
+  const double npd = (double)(p1 - p0);
+  for (int fi = 0; fi < a.nfield; ++fi) {
+    const DepField& F = a.f[fi];
+    if (!F.do_source) continue;
+    const int target = (bs + F.first) % F.nslice;
+    const int4 bb = sbox[fi];
+    // adi_compute_slice_scl (src/Core/FieldSolverADICUDA.cpp:75-96)
+    double scl = 0.0;
+    if (npd > 0) {
+      scl = F.fc * 376.73031346177 * a.current[bs] * F.xks * a.delz;
+      scl /= 4.0 * 510998.95 * npd * F.dgrid_d * F.dgrid_d;
+    }
+    if (bb.z < 0 || scl == 0.0) {
+      if (tid == 0) F.desc[target] = make_int4(0, 0, 0, 0);
+      continue;
+    }
+    int bx0 = bb.x, bw = bb.z - bb.x + 2;
+    const int by0 = bb.y, bh = bb.w - bb.y + 2;
+    if (bw & 1) {  // even tile width keeps the rows 16-byte aligned
+      ++bw;
+      if (bx0 + bw > F.ld) --bx0;
+    }
+    if (tid == 0) F.desc[target] = make_int4(bx0, by0, bw, bh);
+    const int band_h = max(1, min(bh, a.acc_cells / bw));
+    const double unscale = scl / a.fixed_scale;
+    const float fh = (float)F.harm;
+    for (int yb = by0; yb < by0 + bh; yb += band_h) {
+      const int hb = min(band_h, by0 + bh - yb);
+      __syncthreads();
+      for (int i = tid; i < 2 * hb * bw; i += blockDim.x) acc[i] = 0ull;
+      __syncthreads();
+      for (int64_t p = p0 + tid; p < p1; p += blockDim.x) {
+        const float2 xy = a.xy[p];
+        int ix, iy;
+        float wx, wy;
+        MixField mf;
+        mf.gridmax = F.gridmax;
+        mf.dgrid = F.dgrid;
+        mf.n = F.n;
+        if (!cell_f(mf, xy.x, xy.y, ix, iy, wx, wy)) continue;
+        if (iy + 1 < yb || iy >= yb + hb) continue;
+        const float dxu = xy.x - a.ax, dyu = xy.y - a.ay;
+        const float faw2 = 1.0f + a.kx * dxu * dxu + a.ky * dyu * dyu +
+                           2.0f * (a.gradx * dxu + a.grady * dyu);
+        double q = (double)sqrtf(faw2) / (a.gref + (double)a.dg[p]);
+        if (!(fabs(q) <= a.qbound)) {
+          atomicOr(a.err, kErrFixedRange);
+          q = 0.0;
+        }
+        float sn, cs;
+        sincosf(reduce_angle((double)fh * a.th[p]), &sn, &cs);
+        const double vre = (double)sn * q * a.fixed_scale;
+        const double vim = (double)cs * q * a.fixed_scale;
+        const float ws[4] = {wx * wy, (1.f - wx) * wy, wx * (1.f - wy), (1.f - wx) * (1.f - wy)};
+        const int cx[4] = {ix, ix + 1, ix, ix + 1};
+        const int cy[4] = {iy, iy, iy + 1, iy + 1};
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          const int ry = cy[c] - yb, rx = cx[c] - bx0;
+          if (ry < 0 || ry >= hb) continue;
+          if (rx < 0 || rx >= bw) {
+            atomicOr(a.err, kErrBadSlice);
+            continue;
+          }
+          const int cell = ry * bw + rx;
+          atomicAdd(&acc[2 * cell], (unsigned long long)__double2ll_rn(vre * ws[c]));
+          atomicAdd(&acc[2 * cell + 1], (unsigned long long)__double2ll_rn(vim * ws[c]));
+        }
+      }
+      __syncthreads();
+      float2* out = F.src + (size_t)target * F.cap + (size_t)(yb - by0) * bw;
+      for (int i = tid; i < hb * bw; i += blockDim.x)
+        out[i] = make_float2((float)((double)(long long)acc[2 * i] * unscale),
+                             (float)((double)(long long)acc[2 * i + 1] * unscale));
+    }
+  }
+}
+
+// ---------------------------------------------------------- diag finalize --
+// Field diagnostics per beam slice is = (nslice + storage - first) % nslice
+// (src/Core/DiagnosticCUDA.cpp:320) from the pass-Y band partials.
+struct FinalizeArgs {
+  const double* part[kRunFields];  // [nslice][nband][9]
+  int nband[kRunFields];
+  int first_after[kRunFields];
+  int nfield, nslice;
+  double* field_hist;  // [nfield][nslice][9] for this step
+};
+
+__global__ void diag_finalize_kernel(const FinalizeArgs a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.nfield * a.nslice) return;
+  const int f = i / a.nslice, s = i - f * a.nslice;
+  const double* p = a.part[f] + (size_t)s * a.nband[f] * 9;
+  double v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int b = 0; b < a.nband[f]; ++b)
+    for (int q = 0; q < 9; ++q) v[q] += p[b * 9 + q];
+  const int is = (a.nslice + s - a.first_after[f]) % a.nslice;
+  double* o = a.field_hist + ((size_t)f * a.nslice + is) * 9;
+  for (int q = 0; q < 9; ++q) o[q] = v[q];
+}
+
+static PlaneMapF plane_map_f(double strength, double offset) {
+  PlaneMapF m{0, (float)strength, 0.f};
+  if (strength == 0.0) return m;
+  m.offset = (float)(offset / strength);
+  m.mode = strength > 0.0 ? 1 : 2;
+  return m;
+}
+
+}  // namespace g4b
+
+using namespace g4b;
+
+struct StepPlan {
+  g4b_step st;
+  double fc[kRunFields];
+  int first_before[kRunFields], first_after[kRunFields];
+  int zero_start[kRunFields], zero_count[kRunFields];
+  int adi_index[kRunFields];
+};
+
+struct RunFieldState {
+  g4b_field* f = nullptr;
+  std::vector<g4b_adi*> adis;   // one factorisation per distinct delz
+  std::vector<double> adi_delz;
+  int harm = 1;
+  int4* d_bbox = nullptr;
+  double* d_part = nullptr;
+  int nband = 0;
+  double accuslip = 0.0;        // host slippage model
+  int first = 0;
+};
+
+struct g4b_run {
+  g4b_ctx* ctx = nullptr;
+  g4b_run_desc desc{};
+  int nslice = 0, nfield = 0;
+  int64_t npart = 0, max_np = 0;
+  int64_t* d_off = nullptr;
+  int4* d_chunks = nullptr;
+  int nchunk = 0;
+  float2 *xy = nullptr, *pxy = nullptr;
+  float* dg = nullptr;
+  double* th = nullptr;
+  double *d_current = nullptr, *d_eloss = nullptr;
+  std::vector<double> h_current;
+  RunFieldState fs[kRunFields];
+  // lattice
+  std::vector<g4b_step> steps;
+  std::vector<double> fc;   // [nstep][nfield]
+  std::vector<double> slip;
+  // history of diagnostics: per step beam [nslice][rec] then fields
+  double* d_hist = nullptr;
+  int hist_steps = 0;
+  size_t rec_beam = 0, step_doubles = 0;
+  double fixed_scale = 0, qbound = 0;
+  // cached graph
+  cudaGraphExec_t gexec = nullptr;
+  int g_first = -1, g_n = 0;
+  std::vector<int> g_state;
+  uint64_t bytes = 0;
+};
+
+// Chicane transfer matrix shared with the drop-in tracking (row-major 4x4).
+void g4b_chicane_matrix(double angle, double lb, double ld, double lt, double* m);
+
+namespace {
+
+constexpr int kRunChunk = 256;
+constexpr size_t kAccBytes = 128 * 1024;
+
+int plan_step(g4b_run* r, int i, StepPlan& p) {
+  p.st = r->steps[i];
+  for (int f = 0; f < r->nfield; ++f) {
+    RunFieldState& F = r->fs[f];
+    p.fc[f] = r->fc[(size_t)i * r->nfield + f];
+    p.first_before[f] = F.first;
+    // slippage model of ControlCUDA::applySlippage (src/Core/ControlCUDA.cpp:148-252)
+    int zs = 0, zc = 0;
+    if (r->desc.time_run) {
+      F.accuslip += r->slip[i];
+      const int ns = r->nslice;
+      int direction = 1;
+      while (std::fabs(F.accuslip) > r->desc.sample * 0.8) {
+        direction = F.accuslip < 0 ? -1 : 1;
+        F.accuslip -= r->desc.sample * direction;
+        int last = (F.first + ns - 1) % ns;
+        if (direction < 0) last = (last + 1) % ns;
+        if (!r->desc.periodic) {
+          if (zc == 0) {
+            zs = last;
+            zc = 1;
+          } else if (direction > 0 && (last + 1) % ns == zs) {
+            zs = last;
+            ++zc;
+          } else if (direction < 0 && (zs + zc) % ns == last) {
+            ++zc;
+          } else {
+            return fail(G4B_ERR_RANGE, "g4b_run: slippage changes direction within one step");
+          }
+        }
+        F.first = last;
+        if (direction < 0) F.first = (last + 1) % ns;
+      }
+    }
+    p.zero_start[f] = zs;
+    p.zero_count[f] = std::min(zc, r->nslice);
+    p.first_after[f] = F.first;
+    int k = -1;
+    for (size_t j = 0; j < F.adi_delz.size(); ++j)
+      if (F.adi_delz[j] == p.st.delz) k = (int)j;
+    if (k < 0) return fail(G4B_ERR_STATE, "g4b_run: step length without a factorisation");
+    p.adi_index[f] = k;
+  }
+  return G4B_OK;
+}
+
+int enqueue_step(g4b_run* r, int i, const StepPlan& p) {
+  g4b_ctx* c = r->ctx;
+  const g4b_step& st = p.st;
+  const double gref = r->desc.gamma_ref;
+  // particles store dg = gamma - (float)gamma_ref; every kernel rebuilds gamma
+  // from that same FP32-rounded reference
+  const double gbase = (double)(float)gref;
+  // K1
+  if (r->npart > 0) {
+    BeamStepArgs a{};
+    a.xy = r->xy;
+    a.pxy = r->pxy;
+    a.dg = r->dg;
+    a.th = r->th;
+    a.chunks = r->d_chunks;
+    a.eloss = r->d_eloss;
+    a.nfield = r->nfield;
+    double xks_local = 1.0;
+    for (int f = 0; f < r->nfield; ++f) {
+      const RunFieldState& F = r->fs[f];
+      MixField& m = a.f[f];
+      m.cells = static_cast<const float2*>(F.f->a);
+      m.first = p.first_before[f];
+      m.n = F.f->ngrid;
+      m.ld = F.f->ld;
+      m.nslice = r->nslice;
+      m.harm = F.harm;
+      m.do_source = st.in_undulator && (F.harm % 2) == 1;
+      m.gridmax = (float)F.f->gridmax;
+      m.dgrid = (float)F.f->dgrid;
+      m.rtmp = (float)(p.fc[f] / F.f->xks);
+      m.bbox = F.d_bbox;
+      xks_local = F.f->xks / (double)F.harm;
+    }
+    a.gref = gbase;
+    a.gref_f = (float)gref;
+    a.xks = xks_local;
+    a.xku = st.ku != 0.0 ? st.ku : xks_local * 0.5 / gref / gref;
+    a.delz = st.delz;
+    a.half = (float)(0.5 * st.delz);
+    a.autophase = st.autophase;
+    a.aw = (float)st.aw;
+    a.aw2 = (float)(st.aw * st.aw);
+    a.ax = (float)st.ax;
+    a.ay = (float)st.ay;
+    a.kx = (float)st.kx;
+    a.ky = (float)st.ky;
+    a.gradx = (float)st.gradx;
+    a.grady = (float)st.grady;
+    const double betpar0 = std::sqrt(1 - (1 + st.aw * st.aw) / gref / gref);
+    const double quad = st.qf * gref;
+    const double qnatx = st.kx * st.aw * st.aw / gref / betpar0;
+    const double qnaty = st.ky * st.aw * st.aw / gref / betpar0;
+    a.xm = plane_map_f(quad + qnatx, quad * st.dqx + qnatx * st.ax);
+    a.ym = plane_map_f(-quad + qnaty, -quad * st.dqy + qnaty * st.ay);
+    if (st.chic_angle != 0) {
+      // chicane matrix from the drop-in path's builder (TrackBeamCUDA.cpp:93-148)
+      double m[16];
+      g4b_chicane_matrix(st.chic_angle, st.chic_lb, st.chic_ld, st.chic_lt, m);
+      a.pre = 1;
+      a.m00 = (float)m[0];
+      a.m01 = (float)m[1];
+      a.m10 = (float)m[4];
+      a.m11 = (float)m[5];
+      a.m22 = (float)m[10];
+      a.m23 = (float)m[11];
+      a.m32 = (float)m[14];
+      a.m33 = (float)m[15];
+      const double ang = st.chic_angle, lb = st.chic_lb, ld = st.chic_ld;
+      double r56 = (4 * lb / std::sin(ang) * (1 - ang / std::tan(ang)) +
+                    2 * ld * std::tan(ang) / std::cos(ang)) * ang;
+      a.r56 = r56 * 4 * std::asin(1.0) / r->desc.lambda0 / gref;
+      a.r56_off = gbase - gref;  // gamma - gamma0 = dg + (gbase - gamma0)
+      a.has_r56 = 1;
+    }
+    if (st.cx != 0 || st.cy != 0) {
+      a.post = 1;
+      a.cx = (float)(st.cx * gref);
+      a.cy = (float)(st.cy * gref);
+    }
+    a.err = c->d_error;
+    LaunchScope ls(c, "run_beam_step");
+    beam_step_kernel<<<r->nchunk, kRunChunk, 0, c->stream>>>(a);
+  }
+  if (int rc = check_launch(c, "beam_step_kernel")) return rc;
+  // K2
+  double* step_hist = r->d_hist + (size_t)(i % r->hist_steps) * r->step_doubles;
+  {
+    DepDiagArgs a{};
+    a.xy = r->xy;
+    a.pxy = r->pxy;
+    a.dg = r->dg;
+    a.th = r->th;
+    a.off = r->d_off;
+    a.current = r->d_current;
+    a.nfield = r->nfield;
+    a.nbunch = r->desc.nbunch;
+    a.need_aux = 1;
+    a.acc_cells = (int)(kAccBytes / 16);
+    a.ax = (float)st.ax;
+    a.ay = (float)st.ay;
+    a.kx = (float)st.kx;
+    a.ky = (float)st.ky;
+    a.gradx = (float)st.gradx;
+    a.grady = (float)st.grady;
+    a.gref = gbase;
+    a.delz = st.delz;
+    a.fixed_scale = r->fixed_scale;
+    a.qbound = r->qbound;
+    a.beam_hist = step_hist;
+    a.err = c->d_error;
+    for (int f = 0; f < r->nfield; ++f) {
+      const RunFieldState& F = r->fs[f];
+      DepField& d = a.f[f];
+      d.src = static_cast<float2*>(F.f->src);
+      d.desc = F.f->desc;
+      d.bbox = F.d_bbox;
+      d.cap = (size_t)F.f->ngrid * F.f->ld;
+      d.first = p.first_before[f];
+      d.n = F.f->ngrid;
+      d.ld = F.f->ld;
+      d.nslice = r->nslice;
+      d.harm = F.harm;
+      d.do_source = st.in_undulator && (F.harm % 2) == 1 && p.fc[f] != 0.0;
+      d.gridmax = (float)F.f->gridmax;
+      d.dgrid = (float)F.f->dgrid;
+      d.dgrid_d = F.f->dgrid;
+      d.fc = p.fc[f];
+      d.xks = F.f->xks;
+    }
+    LaunchScope ls(c, "run_deposit_diag");
+    deposit_diag_kernel<<<r->nslice, 512, kAccBytes, c->stream>>>(a);
+  }
+  if (int rc = check_launch(c, "deposit_diag_kernel")) return rc;
+  // K3/K4 per field
+  for (int f = 0; f < r->nfield; ++f) {
+    RunFieldState& F = r->fs[f];
+    F.f->first = p.first_before[f];
+    const bool src = st.in_undulator && (F.harm % 2) == 1 && p.fc[f] != 0.0 && r->npart > 0;
+    AdiYExtras ex{p.zero_start[f], p.zero_count[f], F.d_part};
+    if (int rc = adi_run(F.adis[p.adi_index[f]], F.f, src ? F.f->src : nullptr, F.f->desc, &ex))
+      return rc;
+    F.f->first = p.first_after[f];
+  }
+  // K5
+  {
+    FinalizeArgs a{};
+    a.nfield = r->nfield;
+    a.nslice = r->nslice;
+    a.field_hist = step_hist + r->rec_beam * r->nslice;
+    for (int f = 0; f < r->nfield; ++f) {
+      a.part[f] = r->fs[f].d_part;
+      a.nband[f] = r->fs[f].nband;
+      a.first_after[f] = p.first_after[f];
+    }
+    const int n = r->nfield * r->nslice;
+    LaunchScope ls(c, "run_diag_finalize");
+    diag_finalize_kernel<<<(n + 127) / 128, 128, 0, c->stream>>>(a);
+  }
+  return check_launch(c, "diag_finalize_kernel");
+}
+
+std::vector<int> state_key(g4b_run* r) {
+  std::vector<int> k;
+  for (int f = 0; f < r->nfield; ++f) {
+    k.push_back(r->fs[f].first);
+    double a = r->fs[f].accuslip;
+    int v[2];
+    std::memcpy(v, &a, 8);
+    k.push_back(v[0]);
+    k.push_back(v[1]);
+  }
+  return k;
+}
+
+}  // namespace
+
+extern "C" {
+
+int g4b_run_create(g4b_ctx* c, const g4b_run_desc* d, const int64_t* off, g4b_run** out) {
+  if (!c || !d || !off || !out) return fail(G4B_ERR_ARG, "g4b_run_create: null arg");
+  *out = nullptr;
+  if (d->nslice <= 0 || d->nfield < 1 || d->nfield > kRunFields || d->nbunch < 1 ||
+      d->nbunch > kMaxBunch || !(d->gamma_ref > 1) || !(d->lambda0 > 0) || !(d->sample > 0))
+    return fail(G4B_ERR_ARG, "g4b_run_create: bad descriptor");
+  if (d->precision != G4B_MIXED)
+    return fail(G4B_ERR_ARG, "g4b_run_create: the fused run holds mixed-precision state");
+  if (off[0] != 0) return fail(G4B_ERR_ARG, "g4b_run_create: slice_offsets[0] != 0");
+  G4B_CUDA_TRY(cudaSetDevice(c->device));
+  auto r = new (std::nothrow) g4b_run();
+  if (!r) return fail(G4B_ERR_NOMEM, "g4b_run_create: host allocation");
+  r->ctx = c;
+  r->desc = *d;
+  r->nslice = d->nslice;
+  r->nfield = d->nfield;
+  r->npart = off[d->nslice];
+  std::vector<int4> chunks;
+  for (int s = 0; s < d->nslice; ++s) {
+    if (off[s + 1] < off[s]) {
+      delete r;
+      return fail(G4B_ERR_ARG, "g4b_run_create: slice offsets not monotonic");
+    }
+    r->max_np = std::max<int64_t>(r->max_np, off[s + 1] - off[s]);
+    for (int64_t p = off[s]; p < off[s + 1]; p += kRunChunk) {
+      const int64_t e = std::min<int64_t>(p + kRunChunk, off[s + 1]);
+      chunks.push_back(make_int4(s, (int)(p & 0x7fffffff), (int)(e - p), (int)(p >> 31)));
+    }
+  }
+  r->nchunk = (int)chunks.size();
+  const size_t np = (size_t)std::max<int64_t>(r->npart, 1);
+  cudaError_t e = cudaSuccess;
+  auto A = [&](void** p, size_t b) {
+    if (e == cudaSuccess) e = cudaMalloc(p, b);
+    if (e == cudaSuccess) r->bytes += b;
+  };
+  A((void**)&r->xy, np * 8);
+  A((void**)&r->pxy, np * 8);
+  A((void**)&r->dg, np * 4);
+  A((void**)&r->th, np * 8);
+  A((void**)&r->d_off, (d->nslice + 1) * 8);
+  A((void**)&r->d_chunks, std::max(1, r->nchunk) * sizeof(int4));
+  A((void**)&r->d_current, d->nslice * 8);
+  A((void**)&r->d_eloss, d->nslice * 8);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(r->d_off, off, (d->nslice + 1) * 8, cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess && r->nchunk)
+    e = cudaMemcpyAsync(r->d_chunks, chunks.data(), chunks.size() * sizeof(int4),
+                        cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(r->d_current, 0, d->nslice * 8, c->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(r->d_eloss, 0, d->nslice * 8, c->stream);
+  if (e != cudaSuccess) {
+    g4b_run_destroy(r);
+    return cuda_fail(e, "g4b_run_create: device allocation");
+  }
+  for (int f = 0; f < d->nfield; ++f) {
+    RunFieldState& F = r->fs[f];
+    F.harm = d->harm[f];
+    int rc = g4b_field_create(c, d->nslice, d->ngrid[f], d->gridmax[f],
+                              d->lambda0 / (double)d->harm[f], d->harm[f], G4B_MIXED, 0, &F.f);
+    if (rc) {
+      g4b_run_destroy(r);
+      return rc;
+    }
+    r->bytes += F.f->bytes;
+    F.nband = (F.f->ngrid + F.f->band_rows - 1) / F.f->band_rows;
+    A((void**)&F.d_bbox, d->nslice * sizeof(int4));
+    A((void**)&F.d_part, (size_t)d->nslice * F.nband * 9 * 8);
+    if (e != cudaSuccess) {
+      g4b_run_destroy(r);
+      return cuda_fail(e, "g4b_run_create: device allocation");
+    }
+    std::vector<int4> init(d->nslice, make_int4(1 << 30, 1 << 30, -1, -1));
+    e = cudaMemcpyAsync(F.d_bbox, init.data(), init.size() * sizeof(int4),
+                        cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) {
+      g4b_run_destroy(r);
+      return cuda_fail(e, "g4b_run_create: bbox init");
+    }
+  }
+  r->rec_beam = kBeamRec + 2 * d->nbunch;
+  r->step_doubles = (size_t)d->nslice * (r->rec_beam + 9 * d->nfield);
+  // fixed point of the deposition: |q| = sqrt(faw2)/gamma <= 4/gamma_ref,
+  // slice sums <= max_np * qbound < 2^62
+  r->qbound = 4.0 / d->gamma_ref;
+  int ex;
+  std::frexp((double)std::max<int64_t>(r->max_np, 1) * r->qbound, &ex);
+  r->fixed_scale = std::ldexp(1.0, 62 - ex);
+  cudaFuncSetAttribute(deposit_diag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)kAccBytes);
+  *out = r;
+  return G4B_OK;
+}
+
+int g4b_run_destroy(g4b_run* r) {
+  if (!r) return G4B_OK;
+  cudaSetDevice(r->ctx->device);
+  cudaStreamSynchronize(r->ctx->stream);
+  if (r->gexec) cudaGraphExecDestroy(r->gexec);
+  void* ptrs[] = {r->xy, r->pxy, r->dg, r->th, r->d_off, r->d_chunks, r->d_current,
+                  r->d_eloss, r->d_hist};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  for (int f = 0; f < kRunFields; ++f) {
+    RunFieldState& F = r->fs[f];
+    for (g4b_adi* a : F.adis) g4b_adi_destroy(a);
+    if (F.f) g4b_field_destroy(F.f);
+    if (F.d_bbox) cudaFree(F.d_bbox);
+    if (F.d_part) cudaFree(F.d_part);
+  }
+  delete r;
+  return G4B_OK;
+}
+
+int g4b_run_upload_beam(g4b_run* r, const double* x, const double* y, const double* px,
+                        const double* py, const double* gamma, const double* theta) {
+  if (!r || !x || !y || !px || !py || !gamma || !theta)
+    return fail(G4B_ERR_ARG, "g4b_run_upload_beam: null arg");
+  G4B_CUDA_TRY(cudaSetDevice(r->ctx->device));
+  const size_t n = (size_t)r->npart;
+  std::vector<float2> xy(n), pp(n);
+  std::vector<float> dg(n);
+  const float gf = (float)r->desc.gamma_ref;
+  for (size_t i = 0; i < n; ++i) {
+    xy[i] = make_float2((float)x[i], (float)y[i]);
+    pp[i] = make_float2((float)px[i], (float)py[i]);
+    dg[i] = (float)(gamma[i] - (double)gf);
+  }
+  cudaStream_t s = r->ctx->stream;
+  if (n) {
+    G4B_CUDA_TRY(cudaMemcpyAsync(r->xy, xy.data(), n * 8, cudaMemcpyHostToDevice, s));
+    G4B_CUDA_TRY(cudaMemcpyAsync(r->pxy, pp.data(), n * 8, cudaMemcpyHostToDevice, s));
+    G4B_CUDA_TRY(cudaMemcpyAsync(r->dg, dg.data(), n * 4, cudaMemcpyHostToDevice, s));
+    G4B_CUDA_TRY(cudaMemcpyAsync(r->th, theta, n * 8, cudaMemcpyHostToDevice, s));
+  }
+  G4B_CUDA_TRY(cudaStreamSynchronize(s));
+  return G4B_OK;
+}
+
+int g4b_run_download_beam(g4b_run* r, double* x, double* y, double* px, double* py,
+                          double* gamma, double* theta) {
+  if (!r) return fail(G4B_ERR_ARG, "g4b_run_download_beam: null run");
+  G4B_CUDA_TRY(cudaSetDevice(r->ctx->device));
+  const size_t n = (size_t)r->npart;
+  std::vector<float2> xy(n), pp(n);
+  std::vector<float> dg(n);
+  cudaStream_t s = r->ctx->stream;
+  if (n) {
+    G4B_CUDA_TRY(cudaMemcpyAsync(xy.data(), r->xy, n * 8, cudaMemcpyDeviceToHost, s));
+    G4B_CUDA_TRY(cudaMemcpyAsync(pp.data(), r->pxy, n * 8, cudaMemcpyDeviceToHost, s));
+    G4B_CUDA_TRY(cudaMemcpyAsync(dg.data(), r->dg, n * 4, cudaMemcpyDeviceToHost, s));
+    if (theta) G4B_CUDA_TRY(cudaMemcpyAsync(theta, r->th, n * 8, cudaMemcpyDeviceToHost, s));
+  }
+  G4B_CUDA_TRY(cudaStreamSynchronize(s));
+  const double gf = (double)(float)r->desc.gamma_ref;
+  for (size_t i = 0; i < n; ++i) {
+    if (x) x[i] = xy[i].x;
+    if (y) y[i] = xy[i].y;
+    if (px) px[i] = pp[i].x;
+    if (py) py[i] = pp[i].y;
+    if (gamma) gamma[i] = gf + (double)dg[i];
+  }
+  return read_device_error(r->ctx, "g4b_run_download_beam");
+}
+
+int g4b_run_upload_field(g4b_run* r, int fi, const double* cells, int first) {
+  if (!r || fi < 0 || fi >= r->nfield || !cells)
+    return fail(G4B_ERR_ARG, "g4b_run_upload_field: bad argument");
+  RunFieldState& F = r->fs[fi];
+  if (int rc = g4b_field_upload(F.f, cells)) return rc;
+  if (int rc = g4b_field_set_first(F.f, first)) return rc;
+  F.first = first;
+  F.accuslip = 0.0;
+  return G4B_OK;
+}
+
+int g4b_run_download_field(g4b_run* r, int fi, double* cells, int* first) {
+  if (!r || fi < 0 || fi >= r->nfield || !cells)
+    return fail(G4B_ERR_ARG, "g4b_run_download_field: bad argument");
+  RunFieldState& F = r->fs[fi];
+  if (int rc = g4b_field_download(F.f, cells)) return rc;
+  if (first) *first = F.first;
+  return read_device_error(r->ctx, "g4b_run_download_field");
+}
+
+int g4b_run_set_current(g4b_run* r, const double* current) {
+  if (!r || !current) return fail(G4B_ERR_ARG, "g4b_run_set_current: null arg");
+  G4B_CUDA_TRY(cudaSetDevice(r->ctx->device));
+  G4B_CUDA_TRY(cudaMemcpyAsync(r->d_current, current, r->nslice * 8, cudaMemcpyHostToDevice,
+                               r->ctx->stream));
+  G4B_CUDA_TRY(cudaStreamSynchronize(r->ctx->stream));
+  return G4B_OK;
+}
+
+int g4b_run_set_eloss(g4b_run* r, const double* eloss) {
+  if (!r) return fail(G4B_ERR_ARG, "g4b_run_set_eloss: null run");
+  G4B_CUDA_TRY(cudaSetDevice(r->ctx->device));
+  if (eloss)
+    G4B_CUDA_TRY(cudaMemcpyAsync(r->d_eloss, eloss, r->nslice * 8, cudaMemcpyHostToDevice,
+                                 r->ctx->stream));
+  else
+    G4B_CUDA_TRY(cudaMemsetAsync(r->d_eloss, 0, r->nslice * 8, r->ctx->stream));
+  G4B_CUDA_TRY(cudaStreamSynchronize(r->ctx->stream));
+  return G4B_OK;
+}
+
+int g4b_run_set_lattice(g4b_run* r, int nstep, const g4b_step* steps, const double* fc,
+                        const double* slip, int hist_steps) {
+  if (!r || nstep <= 0 || !steps || !fc || !slip)
+    return fail(G4B_ERR_ARG, "g4b_run_set_lattice: bad argument");
+  G4B_CUDA_TRY(cudaSetDevice(r->ctx->device));
+  r->steps.assign(steps, steps + nstep);
+  r->fc.assign(fc, fc + (size_t)nstep * r->nfield);
+  r->slip.assign(slip, slip + nstep);
+  // one FP64 factorisation per distinct step length and field grid
+  for (int f = 0; f < r->nfield; ++f) {
+    RunFieldState& F = r->fs[f];
+    for (int i = 0; i < nstep; ++i) {
+      const double dz = steps[i].delz;
+      if (std::find(F.adi_delz.begin(), F.adi_delz.end(), dz) != F.adi_delz.end()) continue;
+      g4b_adi* a = nullptr;
+      if (int rc = g4b_adi_create(r->ctx, &a)) return rc;
+      if (int rc = g4b_adi_init(a, dz, F.f->dgrid, F.f->xks, F.f->ngrid)) {
+        g4b_adi_destroy(a);
+        return rc;
+      }
+      F.adis.push_back(a);
+      F.adi_delz.push_back(dz);
+    }
+    if (int rc = adi_configure(F.f)) return rc;
+  }
+  const int hs = hist_steps > 0 ? hist_steps : nstep;
+  if (r->d_hist) cudaFree(r->d_hist);
+  r->d_hist = nullptr;
+  G4B_CUDA_TRY(cudaMalloc(&r->d_hist, (size_t)hs * r->step_doubles * 8));
+  G4B_CUDA_TRY(cudaMemsetAsync(r->d_hist, 0, (size_t)hs * r->step_doubles * 8, r->ctx->stream));
+  r->hist_steps = hs;
+  if (r->gexec) {
+    cudaGraphExecDestroy(r->gexec);
+    r->gexec = nullptr;
+  }
+  return G4B_OK;
+}
+
+static int run_capture(g4b_run* r, int first_step, int nsteps, cudaGraphExec_t* out) {
+  g4b_ctx* c = r->ctx;
+  cudaGraph_t g = nullptr;
+  G4B_CUDA_TRY(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+  int rc = G4B_OK;
+  for (int k = 0; k < nsteps && rc == G4B_OK; ++k) {
+    const int i = (first_step + k) % (int)r->steps.size();
+    StepPlan p;
+    rc = plan_step(r, i, p);
+    if (rc == G4B_OK) rc = enqueue_step(r, first_step + k, p);
+  }
+  cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+  if (rc) {
+    if (g) cudaGraphDestroy(g);
+    return rc;
+  }
+  if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+  e = cudaGraphInstantiate(out, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
+  return G4B_OK;
+}
+
+// Enqueue lattice steps [first_step, first_step + nsteps) (indices wrap).
+// use_graph: 0 = direct launches; 1 = replay a CUDA graph of the whole
+// range (captured on first use and reused while the range and the slippage
+// state match).
+static int run_capture(g4b_run* r, int first_step, int nsteps, cudaGraphExec_t* out);
+
+static int run_prepare(g4b_run* r, int first_step, int nsteps) {
+  std::vector<int> key = state_key(r);
+  const bool hit = r->gexec && r->g_first == first_step && r->g_n == nsteps && r->g_state == key;
+  if (hit) return G4B_OK;
+  if (r->gexec) cudaGraphExecDestroy(r->gexec);
+  r->gexec = nullptr;
+  // capture advances the host slippage model; restore it afterwards
+  int first[kRunFields];
+  double acc[kRunFields];
+  for (int f = 0; f < r->nfield; ++f) {
+    first[f] = r->fs[f].first;
+    acc[f] = r->fs[f].accuslip;
+  }
+  int rc = run_capture(r, first_step, nsteps, &r->gexec);
+  for (int f = 0; f < r->nfield; ++f) {
+    r->fs[f].first = first[f];
+    r->fs[f].accuslip = acc[f];
+    r->fs[f].f->first = first[f];
+  }
+  if (rc) return rc;
+  r->g_first = first_step;
+  r->g_n = nsteps;
+  r->g_state = key;
+  return G4B_OK;
+}
+
+// Capture (without launching) the CUDA graph of steps [first_step,
+// first_step + nsteps) from the current state, for a later g4b_run_advance
+// with use_graph on the same range.
+int g4b_run_prepare(g4b_run* r, int first_step, int nsteps) {
+  if (!r || nsteps <= 0 || first_step < 0) return fail(G4B_ERR_ARG, "g4b_run_prepare: bad arg");
+  if (r->steps.empty()) return fail(G4B_ERR_STATE, "g4b_run_prepare: no lattice");
+  G4B_CUDA_TRY(cudaSetDevice(r->ctx->device));
+  return run_prepare(r, first_step, nsteps);
+}
+
+int g4b_run_advance(g4b_run* r, int first_step, int nsteps, int use_graph) {
+  if (!r || nsteps < 0 || first_step < 0) return fail(G4B_ERR_ARG, "g4b_run_advance: bad arg");
+  if (r->steps.empty()) return fail(G4B_ERR_STATE, "g4b_run_advance: no lattice");
+  G4B_CUDA_TRY(cudaSetDevice(r->ctx->device));
+  if (!use_graph) {
+    for (int k = 0; k < nsteps; ++k) {
+      const int i = (first_step + k) % (int)r->steps.size();
+      StepPlan p;
+      if (int rc = plan_step(r, i, p)) return rc;
+      if (int rc = enqueue_step(r, first_step + k, p)) return rc;
+    }
+    return G4B_OK;
+  }
+  if (int rc = run_prepare(r, first_step, nsteps)) return rc;
+  r->ctx->launches += (uint64_t)nsteps * (3 + 2 * r->nfield);
+  G4B_CUDA_TRY(cudaGraphLaunch(r->gexec, r->ctx->stream));
+  // advance the host model exactly as the captured steps did
+  for (int k = 0; k < nsteps; ++k) {
+    StepPlan p;
+    if (int rc = plan_step(r, (first_step + k) % (int)r->steps.size(), p)) return rc;
+    for (int f = 0; f < r->nfield; ++f) r->fs[f].f->first = p.first_after[f];
+  }
+  return G4B_OK;
+}
+
+// Diagnostics of lattice step `step` (the history keeps the last hist_steps
+// steps): beam[nslice*(23+2*nbunch)] in the reference's stats order, field
+// [nfield*nslice*9] = power, x1, x2, y1, y2, farfield re/im, centre re/im,
+// indexed by beam slice.  Synchronises.
+int g4b_run_history(g4b_run* r, int step, double* beam, double* field) {
+  if (!r || step < 0) return fail(G4B_ERR_ARG, "g4b_run_history: bad arg");
+  if (!r->d_hist) return fail(G4B_ERR_STATE, "g4b_run_history: no lattice");
+  G4B_CUDA_TRY(cudaSetDevice(r->ctx->device));
+  const double* h = r->d_hist + (size_t)(step % r->hist_steps) * r->step_doubles;
+  const size_t nb = (size_t)r->nslice * r->rec_beam;
+  if (beam)
+    G4B_CUDA_TRY(cudaMemcpyAsync(beam, h, nb * 8, cudaMemcpyDeviceToHost, r->ctx->stream));
+  if (field)
+    G4B_CUDA_TRY(cudaMemcpyAsync(field, h + nb, (size_t)r->nfield * r->nslice * 9 * 8,
+                                 cudaMemcpyDeviceToHost, r->ctx->stream));
+  G4B_CUDA_TRY(cudaStreamSynchronize(r->ctx->stream));
+  return read_device_error(r->ctx, "g4b_run_history");
+}
+
+int g4b_run_device_bytes(g4b_run* r, uint64_t* bytes) {
+  if (!r || !bytes) return fail(G4B_ERR_ARG, "g4b_run_device_bytes: null arg");
+  *bytes = r->bytes + (uint64_t)r->hist_steps * r->step_doubles * 8;
+  return G4B_OK;
+}
+
+}  // extern "C"

@@ -14,7 +14,7 @@ import ctypes as C
 import numpy as np
 
 from . import _lib
-from ._lib import G4B_FP64, G4B_MIXED, Step, check, dptr  # noqa: F401
+from ._lib import G4B_FP64, G4B_MIXED, RunDesc, Step, check, dptr  # noqa: F401
 
 
 class Context:
@@ -245,6 +245,103 @@ class FieldSolverADICUDA:
     def close(self) -> None:
         if getattr(self, "h", None):
             self.lib.g4b_adi_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Run:
+    """The fused mixed-precision form: a whole FEL run resident on the device
+    (beam + up to 8 fields sharing the slicing), advanced per lattice step by
+    fused kernels replayed as a CUDA graph (g4b_run_* in include/g4b.h)."""
+
+    def __init__(self, ctx: Context, slice_offsets, *, fields, lambda0: float,
+                 gamma_ref: float, sample: float = 1.0, time_run: bool = True,
+                 periodic: bool = False, nbunch: int = 1):
+        """fields: list of (harm, ngrid, gridmax)."""
+        self.ctx, self.lib = ctx, ctx.lib
+        off = np.ascontiguousarray(slice_offsets, dtype=np.int64)
+        self.offsets = off
+        self.nslice = len(off) - 1
+        self.npart = int(off[-1])
+        self.fields = list(fields)
+        self.nbunch = nbunch
+        d = RunDesc()
+        d.nslice = self.nslice
+        d.nfield = len(self.fields)
+        for i, (h, n, gm) in enumerate(self.fields):
+            d.harm[i], d.ngrid[i], d.gridmax[i] = h, n, gm
+        d.lambda0, d.gamma_ref, d.sample = lambda0, gamma_ref, sample
+        d.time_run, d.periodic, d.nbunch, d.precision = int(time_run), int(periodic), nbunch, G4B_MIXED
+        h = C.c_void_p()
+        check(self.lib.g4b_run_create(ctx.h, C.byref(d), off.ctypes.data_as(_lib.c_int64_p),
+                                      C.byref(h)))
+        self.h = h
+
+    def upload_beam(self, parts: dict) -> None:
+        arrs = [np.ascontiguousarray(parts[k], dtype=np.float64) for k in BeamState.NAMES]
+        check(self.lib.g4b_run_upload_beam(self.h, *[dptr(a) for a in arrs]))
+
+    def download_beam(self) -> dict:
+        out = {k: np.empty(self.npart) for k in BeamState.NAMES}
+        check(self.lib.g4b_run_download_beam(self.h, *[dptr(out[k]) for k in BeamState.NAMES]))
+        return out
+
+    def upload_field(self, i: int, cells, first: int = 0) -> None:
+        a = np.ascontiguousarray(cells, dtype=np.complex128).reshape(-1)
+        check(self.lib.g4b_run_upload_field(self.h, i, dptr(a.view(np.float64)), first))
+
+    def download_field(self, i: int):
+        n = self.fields[i][1]
+        out = np.empty((self.nslice, n, n), np.complex128)
+        first = C.c_int()
+        check(self.lib.g4b_run_download_field(self.h, i, dptr(out.reshape(-1).view(np.float64)),
+                                              C.byref(first)))
+        return out, int(first.value)
+
+    def set_current(self, current) -> None:
+        a = np.ascontiguousarray(np.broadcast_to(current, (self.nslice,)), dtype=np.float64)
+        check(self.lib.g4b_run_set_current(self.h, dptr(a)))
+
+    def set_eloss(self, eloss=None) -> None:
+        a = None if eloss is None else np.ascontiguousarray(eloss, dtype=np.float64)
+        check(self.lib.g4b_run_set_eloss(self.h, dptr(a)))
+
+    def set_lattice(self, steps, fc, slip, hist_steps: int = 0) -> None:
+        n = len(steps)
+        arr = (Step * n)(*steps)
+        fcs = np.ascontiguousarray(fc, dtype=np.float64).reshape(n, len(self.fields))
+        sl = np.ascontiguousarray(slip, dtype=np.float64)
+        check(self.lib.g4b_run_set_lattice(self.h, n, arr, dptr(fcs.reshape(-1)), dptr(sl),
+                                           hist_steps))
+
+    def advance(self, first_step: int, nsteps: int, graph: bool = True) -> None:
+        check(self.lib.g4b_run_advance(self.h, first_step, nsteps, int(graph)))
+
+    def prepare(self, first_step: int, nsteps: int) -> None:
+        """Capture the CUDA graph of a step range without launching it."""
+        check(self.lib.g4b_run_prepare(self.h, first_step, nsteps))
+
+    def history(self, step: int):
+        """(beam stats [nslice, 23+2*nbunch], field stats [nfield, nslice, 9])."""
+        beam = np.empty((self.nslice, 23 + 2 * self.nbunch))
+        field = np.empty((len(self.fields), self.nslice, 9))
+        check(self.lib.g4b_run_history(self.h, step, dptr(beam.reshape(-1)),
+                                       dptr(field.reshape(-1))))
+        return beam, field
+
+    def device_bytes(self) -> int:
+        v = C.c_uint64()
+        check(self.lib.g4b_run_device_bytes(self.h, C.byref(v)))
+        return int(v.value)
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.g4b_run_destroy(self.h)
             self.h = None
 
     def __del__(self):

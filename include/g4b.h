@@ -191,6 +191,63 @@ int g4b_diag_beam(g4b_beam* b, int nharm, int need_aux, double* stats,
  * centre cell (ngrid^2-1)/2 into center[nslice*2] (re, im). */
 int g4b_diag_field(g4b_field* f, double* stats, double* center);
 
+/* ---- fused mixed-precision run -------------------------------------------
+ * A whole FEL run resident on the device: FP32 particles and complex64
+ * fields with the phase theta in FP64, advanced per lattice step by a fused
+ * beam step (TrackBeamCUDA::track + BeamSolverCUDA::advance + applyR56 +
+ * TrackBeamCUDA::track), a fused deposition + beam diagnostics, the two ADI
+ * passes per field (FieldSolverADICUDA::advance, with the slippage of
+ * ControlCUDA::applySlippage and the field part of DiagnosticCUDA folded into
+ * the second pass), replayed as one CUDA graph.  Beam and fields share the
+ * slicing; fields may differ in harmonic and grid.  No counterpart class in
+ * the reference: it composes the reference's per-step calls in
+ * src/Core/Gencore.cpp:172-254. */
+typedef struct g4b_run g4b_run;
+
+typedef struct g4b_run_desc {
+  int nslice;
+  int nfield;           /* 1..8                                             */
+  int harm[8];          /* field harmonics                                  */
+  int ngrid[8];
+  double gridmax[8];
+  double lambda0;       /* reference (fundamental) wavelength [m]           */
+  double gamma_ref;
+  double sample;        /* slicelength / reflength                          */
+  int time_run;         /* slippage on                                      */
+  int periodic;
+  int nbunch;           /* bunching harmonics in the diagnostics (1..8)     */
+  int precision;        /* G4B_MIXED                                        */
+} g4b_run_desc;
+
+int g4b_run_create(g4b_ctx* ctx, const g4b_run_desc* desc,
+                   const int64_t* slice_offsets, g4b_run** out);
+int g4b_run_destroy(g4b_run* run);
+int g4b_run_upload_beam(g4b_run* run, const double* x, const double* y,
+                        const double* px, const double* py, const double* gamma,
+                        const double* theta);
+int g4b_run_download_beam(g4b_run* run, double* x, double* y, double* px,
+                          double* py, double* gamma, double* theta);
+int g4b_run_upload_field(g4b_run* run, int ifield, const double* cells, int first);
+int g4b_run_download_field(g4b_run* run, int ifield, double* cells, int* first);
+int g4b_run_set_current(g4b_run* run, const double* current);
+int g4b_run_set_eloss(g4b_run* run, const double* slice_eloss);
+/* Per-step tables: steps[nstep], fc[nstep*nfield] (und->fc(harm) per field),
+ * slip[nstep] (und->slippage(), units of lambda0); keeps the diagnostics of
+ * the last hist_steps steps (0 = nstep). */
+int g4b_run_set_lattice(g4b_run* run, int nstep, const g4b_step* steps,
+                        const double* fc, const double* slip, int hist_steps);
+/* Enqueue lattice steps [first_step, first_step+nsteps) (asynchronous); with
+ * use_graph the range is captured once as a CUDA graph and replayed. */
+int g4b_run_advance(g4b_run* run, int first_step, int nsteps, int use_graph);
+/* Capture the graph of that range from the current state without launching
+ * it (so a timed g4b_run_advance only replays). */
+int g4b_run_prepare(g4b_run* run, int first_step, int nsteps);
+/* Diagnostics of one step: beam[nslice*(23+2*nbunch)] (raw sums in the
+ * order of g4b_diag_beam, bunching interleaved re,im), field[nfield*nslice*9]
+ * (the 7 sums of g4b_diag_field, then the centre cell re, im). */
+int g4b_run_history(g4b_run* run, int step, double* beam, double* field);
+int g4b_run_device_bytes(g4b_run* run, uint64_t* bytes);
+
 #ifdef __cplusplus
 }
 #endif
