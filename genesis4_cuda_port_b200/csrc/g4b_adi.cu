@@ -529,8 +529,12 @@ template <typename T, int M, bool PX>
 static int configure_pass_t(int device) {
   static uint64_t configured = 0;  // per instantiation, one bit per device
   if (device < 64 && (configured >> device) & 1) return G4B_OK;
-  cudaError_t e = cudaFuncSetAttribute(adi_pass_kernel<T, M, PX>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+  // static + dynamic shared memory must fit the 227 KB a CTA may use
+  cudaFuncAttributes fa;
+  cudaError_t e = cudaFuncGetAttributes(&fa, adi_pass_kernel<T, M, PX>);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaFuncGetAttributes(adi_pass)");
+  e = cudaFuncSetAttribute(adi_pass_kernel<T, M, PX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           227 * 1024 - (int)fa.sharedSizeBytes);
   if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(adi_pass)");
   if (device < 64) configured |= 1ull << device;
   return G4B_OK;
@@ -630,7 +634,7 @@ int adi_run(g4b_adi* adi, g4b_field* f, const void* src, const int4* desc,
   args.desc = desc;
   args.src_cap = (size_t)f->ngrid * f->ld;
   size_t smem = smem_for(true, src != nullptr);
-  if (smem > 227 * 1024) return fail(G4B_ERR_RANGE, "adi: pass X tile exceeds shared memory");
+  if (smem + 2048 > 227 * 1024) return fail(G4B_ERR_RANGE, "adi: pass X tile exceeds shared memory");
   rc = f->precision == G4B_FP64
            ? launch_pass_m<double, true>(adi->M, f, args, f->tm_store_b, smem)
            : launch_pass_m<float, true>(adi->M, f, args, f->tm_store_b, smem);
@@ -662,16 +666,17 @@ int g4b_adi_create(g4b_ctx* c, g4b_adi** out) {
   g4b_adi* a = new (std::nothrow) g4b_adi();
   if (!a) return fail(G4B_ERR_NOMEM, "g4b_adi_create: host allocation");
   a->ctx = c;
+  ctx_retain(c);
   *out = a;
   return G4B_OK;
 }
 
 int g4b_adi_destroy(g4b_adi* a) {
   if (!a) return G4B_OK;
-  cudaSetDevice(a->ctx->device);
-  cudaStreamSynchronize(a->ctx->stream);
+  ctx_quiesce(a->ctx);
   if (a->d_tab64) cudaFree(a->d_tab64);
   if (a->d_tab32) cudaFree(a->d_tab32);
+  ctx_release(a->ctx);
   delete a;
   return G4B_OK;
 }

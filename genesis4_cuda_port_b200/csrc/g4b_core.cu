@@ -103,6 +103,15 @@ void prof_end(g4b_ctx* c) {
   if (p.pending.size() > 8192) prof_resolve(c);
 }
 
+void ctx_release(g4b_ctx* c) {
+  if (--c->refs == 0) delete c;
+}
+
+void ctx_quiesce(g4b_ctx* c) {
+  cudaSetDevice(c->device);
+  if (!c->destroyed && c->stream) cudaStreamSynchronize(c->stream);
+}
+
 int pick_M(int n) {
   static const int kM[] = {1, 3, 5, 7, 9, 11, 13, 15, 17, 21, 25, 33};
   for (int m : kM)
@@ -184,17 +193,22 @@ int g4b_ctx_create(int device, g4b_ctx** out) {
 }
 
 int g4b_ctx_destroy(g4b_ctx* c) {
-  if (!c) return G4B_OK;
+  if (!c || c->destroyed) return G4B_OK;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   if (c->d_error) cudaFree(c->d_error);
+  c->d_error = nullptr;
   for (auto& q : c->prof.pending) {
     cudaEventDestroy(q.a);
     cudaEventDestroy(q.b);
   }
+  c->prof.pending.clear();
   for (auto e : c->prof.pool) cudaEventDestroy(e);
+  c->prof.pool.clear();
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
-  delete c;
+  c->stream = nullptr;
+  c->destroyed = true;
+  ctx_release(c);
   return G4B_OK;
 }
 
@@ -286,6 +300,7 @@ int g4b_field_create(g4b_ctx* c, int nslice, int ngrid, double gridmax,
   g4b_field* f = new (std::nothrow) g4b_field();
   if (!f) return fail(G4B_ERR_NOMEM, "g4b_field_create: host allocation");
   f->ctx = c;
+  ctx_retain(c);
   f->nslice = nslice;
   f->ngrid = ngrid;
   f->harm = harm;
@@ -330,12 +345,12 @@ int g4b_field_create(g4b_ctx* c, int nslice, int ngrid, double gridmax,
 
 int g4b_field_destroy(g4b_field* f) {
   if (!f) return G4B_OK;
-  cudaSetDevice(f->ctx->device);
-  cudaStreamSynchronize(f->ctx->stream);
+  ctx_quiesce(f->ctx);
   if (f->a) cudaFree(f->a);
   if (f->b) cudaFree(f->b);
   if (f->src) cudaFree(f->src);
   if (f->desc) cudaFree(f->desc);
+  ctx_release(f->ctx);
   delete f;
   return G4B_OK;
 }
@@ -422,6 +437,7 @@ int g4b_beam_create(g4b_ctx* c, int nslice, const int64_t* off, int precision,
   g4b_beam* b = new (std::nothrow) g4b_beam();
   if (!b) return fail(G4B_ERR_NOMEM, "g4b_beam_create: host allocation");
   b->ctx = c;
+  ctx_retain(c);
   b->nslice = nslice;
   b->precision = precision;
   b->gamma_ref = gamma_ref;
@@ -469,12 +485,12 @@ int g4b_beam_create(g4b_ctx* c, int nslice, const int64_t* off, int precision,
 
 int g4b_beam_destroy(g4b_beam* b) {
   if (!b) return G4B_OK;
-  cudaSetDevice(b->ctx->device);
-  cudaStreamSynchronize(b->ctx->stream);
+  ctx_quiesce(b->ctx);
   void* ptrs[] = {b->x, b->y, b->px, b->py, b->gamma, b->theta, b->d_off,
                   b->d_current, b->d_eloss, b->d_scl, b->d_chunks};
   for (void* p : ptrs)
     if (p) cudaFree(p);
+  ctx_release(b->ctx);
   delete b;
   return G4B_OK;
 }

@@ -66,6 +66,11 @@ struct g4b_ctx {
   int* d_error = nullptr;  // device error flag (bit set, see kErr*)
   void* encode_fn = nullptr;  // cuTensorMapEncodeTiled
   g4b::Profiler prof;
+  // lifetime: the handle plus every object created on it hold a reference;
+  // g4b_ctx_destroy releases the handle's, so objects may be destroyed after
+  // their context (the struct lives until the last reference goes)
+  std::atomic<int> refs{1};
+  bool destroyed = false;
 };
 
 struct g4b_field {
@@ -119,6 +124,12 @@ struct g4b_adi {
 };
 
 namespace g4b {
+
+// Context lifetime helpers (see g4b_ctx::refs).
+inline void ctx_retain(g4b_ctx* c) { c->refs++; }
+void ctx_release(g4b_ctx* c);
+// Make the context's device current and drain its stream, if it is still open.
+void ctx_quiesce(g4b_ctx* c);
 
 // Launch bookkeeping: every kernel launch goes through this.
 inline void count_launch(g4b_ctx* ctx, int n = 1) { ctx->launches += n; }

@@ -836,6 +836,7 @@ int g4b_run_create(g4b_ctx* c, const g4b_run_desc* d, const int64_t* off, g4b_ru
   auto r = new (std::nothrow) g4b_run();
   if (!r) return fail(G4B_ERR_NOMEM, "g4b_run_create: host allocation");
   r->ctx = c;
+  ctx_retain(c);
   r->desc = *d;
   r->nslice = d->nslice;
   r->nfield = d->nfield;
@@ -920,8 +921,7 @@ int g4b_run_create(g4b_ctx* c, const g4b_run_desc* d, const int64_t* off, g4b_ru
 
 int g4b_run_destroy(g4b_run* r) {
   if (!r) return G4B_OK;
-  cudaSetDevice(r->ctx->device);
-  cudaStreamSynchronize(r->ctx->stream);
+  ctx_quiesce(r->ctx);
   if (r->gexec) cudaGraphExecDestroy(r->gexec);
   void* ptrs[] = {r->xy, r->pxy, r->dg, r->th, r->d_off, r->d_chunks, r->d_current,
                   r->d_eloss, r->d_hist};
@@ -934,6 +934,7 @@ int g4b_run_destroy(g4b_run* r) {
     if (F.d_bbox) cudaFree(F.d_bbox);
     if (F.d_part) cudaFree(F.d_part);
   }
+  ctx_release(r->ctx);
   delete r;
   return G4B_OK;
 }
