@@ -45,7 +45,14 @@ class Workload:
 
     @property
     def lambda0(self) -> float:
-        return self.lambdau * (1 + self.aw ** 2) / (2 * self.gamma0 ** 2)
+        """Resonant wavelength of the beam's mean particle: the on-axis
+        lambda_u (1 + aw^2) / (2 gamma^2) corrected for the matched beam's mean
+        transverse momentum <px^2 + py^2> = 2 gamma eps_n / beta and the planar
+        undulator's natural-focusing field rise aw^2 ku^2 <y^2>."""
+        ku = 2 * math.pi / self.lambdau
+        p2 = 2 * self.gamma0 * self.emit_n / self.beta
+        foc = self.aw ** 2 * ku * ku * self.emit_n * self.beta / self.gamma0
+        return self.lambdau * (1 + self.aw ** 2 + p2 + foc) / (2 * self.gamma0 ** 2)
 
     @property
     def delz(self) -> float:
