@@ -180,9 +180,15 @@ __global__ void __launch_bounds__(256) beam_step_kernel(const BeamStepArgs a) {
       }
       sincosf(reduce_angle((double)F.harm * t0), &s0[f], &c0[f]);
     }
-    const float ztemp1 = (float)(-2.0 / a.xks);
+    // btper0 = btpar - (2/ks) Re(c): the field term is ~1e-10 of btpar ~ 2,
+    // far below FP32 resolution, so the sum and eps are formed in FP64 (an
+    // FP32 sum would round up or down with the particle's phase and inject a
+    // spurious phase-correlated detuning)
+    const double ztemp1 = -2.0 / a.xks;
+    const double btpar_d = (double)btpar;
+    const double d0 = (double)d;
     auto ode = [&](float ds, double ts, float& kg, double& kp) {
-      const double gs = a.gref + (double)ds;
+      const double gs = a.gref + d0 + (double)ds;
       const double inv_g2 = 1.0 / (gs * gs);
       const float dth = (float)(ts - t0);
       float ctr = 0.f, cti = 0.f;
@@ -196,8 +202,8 @@ __global__ void __launch_bounds__(256) beam_step_kernel(const BeamStepArgs a) {
         ctr += rr[f] * c + ri[f] * s;
         cti += ri[f] * c - rr[f] * s;
       }
-      const float btper0 = btpar + ztemp1 * ctr;
-      const double eps = (double)btper0 * inv_g2;
+      const double btper0 = btpar_d + ztemp1 * (double)ctr;
+      const double eps = btper0 * inv_g2;
       double fe;
       float b0;
       if (eps < 1e-5) {
@@ -211,37 +217,41 @@ __global__ void __launch_bounds__(256) beam_step_kernel(const BeamStepArgs a) {
       kp += a.xku - a.xks * eps * fe;
       kg += cti / b0 / (float)gs - ez;
     };
-    // Genesis RK4 accumulator form (src/Core/BeamSolverCUDA.cpp:258-299)
+    // Genesis RK4 accumulator form (src/Core/BeamSolverCUDA.cpp:258-299) on
+    // the step's energy increment dd (small, so FP32 keeps its relative
+    // precision); the stored offset is rounded once at the end
+    float dd = 0.f;
     float k2g = 0.f, k3g;
     double k2p = 0.0, k3p;
-    ode(d, t, k2g, k2p);
+    ode(dd, t, k2g, k2p);
     float stf = (float)(0.5 * a.delz);
     double stp = 0.5 * a.delz;
-    d += stf * k2g;
+    dd += stf * k2g;
     t += stp * k2p;
     k3g = k2g;
     k3p = k2p;
     k2g = 0.f;
     k2p = 0.0;
-    ode(d, t, k2g, k2p);
-    d += stf * (k2g - k3g);
+    ode(dd, t, k2g, k2p);
+    dd += stf * (k2g - k3g);
     t += stp * (k2p - k3p);
     k3g /= 6.0f;
     k3p /= 6.0;
     k2g *= -0.5f;
     k2p *= -0.5;
-    ode(d, t, k2g, k2p);
+    ode(dd, t, k2g, k2p);
     stf = (float)a.delz;
     stp = a.delz;
-    d += stf * k2g;
+    dd += stf * k2g;
     t += stp * k2p;
     k3g -= k2g;
     k3p -= k2p;
     k2g *= 2.0f;
     k2p *= 2.0;
-    ode(d, t, k2g, k2p);
-    d += stf * (k3g + k2g / 6.0f);
+    ode(dd, t, k2g, k2p);
+    dd += stf * (k3g + k2g / 6.0f);
     t += stp * (k3p + k2p / 6.0);
+    d = (float)(d0 + (double)dd);
     // applyR56 (src/Core/TrackBeamCUDA.cpp:257-278): theta += R56 (gamma - gamma0)
     if (a.has_r56) t += a.r56 * ((double)d + a.r56_off);
     // second half (+corrector on the last half step)
