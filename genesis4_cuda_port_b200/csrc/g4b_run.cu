@@ -28,6 +28,8 @@
 #include <tuple>
 #include <vector>
 
+#include <cooperative_groups.h>
+
 #include "g4b_internal.cuh"
 
 namespace g4b {
@@ -39,7 +41,7 @@ constexpr int kBeamRec = 23;  // reference stats order (DiagnosticCUDA.cpp:102-1
 struct MixField {
   const float2* cells;
   int first, n, ld, nslice, harm, do_source;
-  float gridmax, dgrid;
+  float gridmax, dgrid, inv_dgrid;
   float rtmp;      // fc / xks_h
   int4* bbox;      // [nslice]: ixmin, iymin, ixmax, iymax
 };
@@ -69,28 +71,51 @@ struct BeamStepArgs {
   int* err;
 };
 
-__device__ __forceinline__ void plane_f(const PlaneMapF m, float delz, float& c, float& p,
-                                        float gz) {
+// Thick-lens map of one plane over `half` (advance_focusing_plane,
+// src/Core/TrackBeamCUDA.cpp:27-59) for strength s with k = s/gz and
+// w2 = k half^2: a1 = cos w, a2 = sin(w)/sqrt(k), a3 = -k a2 (cosh/sinh for
+// k < 0, drift for k = 0).  For |w2| < 1e-2 (every undulator and quadrupole
+// step of practical lattices) the functions are their Taylor series in w2
+// (truncation < w2^4/40320 < 3e-13); larger phases use the closed forms.
+__device__ __forceinline__ void plane_f(const PlaneMapF m, float half, float& c, float& p,
+                                        float gz, float inv_gz) {
   if (m.mode == 0) {
-    c += p * delz / gz;
+    c += p * half * inv_gz;
     return;
   }
-  if (m.mode == 1) {
-    const float foc = sqrtf(m.strength / gz);
+  const float k = m.strength * inv_gz;
+  const float w2 = k * half * half;
+  float a1, a2;
+  if (fabsf(w2) < 1e-2f) {
+    a1 = 1.0f + w2 * (-0.5f + w2 * (1.0f / 24.0f + w2 * (-1.0f / 720.0f)));
+    a2 = half * (1.0f + w2 * (-1.0f / 6.0f + w2 * (1.0f / 120.0f + w2 * (-1.0f / 5040.0f))));
+  } else if (k > 0.f) {
+    const float foc = sqrtf(k);
     float sn, cs;
-    sincosf(foc * delz, &sn, &cs);
-    const float a2 = sn / foc, a3 = -a2 * foc * foc;
-    const float xt = c - m.offset;
-    c = cs * xt + a2 * p / gz + m.offset;
-    p = a3 * xt * gz + cs * p;
-    return;
+    sincosf(foc * half, &sn, &cs);
+    a1 = cs;
+    a2 = sn / foc;
+  } else {
+    const float foc = sqrtf(-k);
+    a1 = coshf(foc * half);
+    a2 = sinhf(foc * half) / foc;
   }
-  const float foc = sqrtf(-m.strength / gz);
-  const float om = foc * delz;
-  const float a1 = coshf(om), a2 = sinhf(om) / foc, a3 = a2 * foc * foc;
+  const float a3 = -a2 * k;
   const float xt = c - m.offset;
-  c = a1 * xt + a2 * p / gz + m.offset;
+  c = a1 * xt + a2 * p * inv_gz + m.offset;
   p = a3 * xt * gz + a1 * p;
+}
+
+// sin and cos of a small angle (|a| < 0.1: Taylor to a^9, error < 3e-17);
+// larger angles use sincosf.
+__device__ __forceinline__ void sincos_small(float a, float& s, float& c) {
+  if (fabsf(a) < 0.1f) {
+    const float a2 = a * a;
+    s = a * (1.0f + a2 * (-1.0f / 6.0f + a2 * (1.0f / 120.0f + a2 * (-1.0f / 5040.0f))));
+    c = 1.0f + a2 * (-0.5f + a2 * (1.0f / 24.0f + a2 * (-1.0f / 720.0f)));
+  } else {
+    sincosf(a, &s, &c);
+  }
 }
 
 // Reduce an FP64 angle to [-pi, pi) before FP32 trigonometry.
@@ -104,7 +129,7 @@ __device__ __forceinline__ bool cell_f(const MixField& f, float x, float y, int&
                                        float& wx, float& wy) {
   const float gm = f.gridmax;
   if (!(x > -gm && x < gm && y > -gm && y < gm)) return false;
-  const float wxr = (x + gm) / f.dgrid, wyr = (y + gm) / f.dgrid;
+  const float wxr = (x + gm) * f.inv_dgrid, wyr = (y + gm) * f.inv_dgrid;
   ix = (int)floorf(wxr);
   iy = (int)floorf(wyr);
   if (ix < 0 || ix >= f.n - 1 || iy < 0 || iy >= f.n - 1) return false;
@@ -113,16 +138,20 @@ __device__ __forceinline__ bool cell_f(const MixField& f, float x, float y, int&
   return true;
 }
 
+// NF: number of fields when known at compile time (1, 2), 0 = up to 8.
+template <int NF>
 __global__ void __launch_bounds__(256) beam_step_kernel(const BeamStepArgs a) {
+  constexpr int kF = NF > 0 ? NF : kRunFields;
+  const int nfield = NF > 0 ? NF : a.nfield;
   __shared__ int sbb[kRunFields][4][8];
   const int4 ch = a.chunks[blockIdx.x];
   const int slice = ch.x;
   const int tid = threadIdx.x;
   const bool live = tid < ch.z;
   const int64_t ip = (((int64_t)ch.w) << 31) + (int64_t)(unsigned)ch.y + tid;
-  int bb[kRunFields][4];
+  int bb[kF][4];
 #pragma unroll
-  for (int f = 0; f < kRunFields; ++f) {
+  for (int f = 0; f < kF; ++f) {
     bb[f][0] = bb[f][1] = 1 << 30;
     bb[f][2] = bb[f][3] = -1;
   }
@@ -143,9 +172,10 @@ __global__ void __launch_bounds__(256) beam_step_kernel(const BeamStepArgs a) {
         y = a.m22 * tmp + a.m23 * py / gz;
         py = a.m32 * tmp * gz + a.m33 * py;
       }
-      const float gz = sqrtf(g * g - 1.0f - a.aw2 - px * px - py * py);
-      plane_f(a.xm, a.half, x, px, gz);
-      plane_f(a.ym, a.half, y, py, gz);
+      const float gz2 = g * g - 1.0f - a.aw2 - px * px - py * py;
+      const float inv_gz = rsqrtf(gz2), gz = gz2 * inv_gz;
+      plane_f(a.xm, a.half, x, px, gz, inv_gz);
+      plane_f(a.ym, a.half, y, py, gz, inv_gz);
     }
     // BeamSolverCUDA::advance push (src/Core/BeamSolverCUDA.cpp:226-409)
     t += a.autophase;
@@ -154,14 +184,14 @@ __global__ void __launch_bounds__(256) beam_step_kernel(const BeamStepArgs a) {
                         a.grady * dyu;
     const float btpar = 1.0f + px * px + py * py + a.aw2 * awloc * awloc;
     const float ez = (float)a.eloss[slice];
-    float rr[kRunFields], ri[kRunFields], c0[kRunFields], s0[kRunFields];
+    float rr[kF], ri[kF], c0[kF], s0[kF];
     const double t0 = t;
 #pragma unroll
-    for (int f = 0; f < kRunFields; ++f) {
+    for (int f = 0; f < kF; ++f) {
       rr[f] = ri[f] = 0.f;
       c0[f] = 1.f;
       s0[f] = 0.f;
-      if (f >= a.nfield) continue;
+      if (f >= nfield) continue;
       const MixField& F = a.f[f];
       int ix, iy;
       float wx, wy;
@@ -187,16 +217,19 @@ __global__ void __launch_bounds__(256) beam_step_kernel(const BeamStepArgs a) {
     const double ztemp1 = -2.0 / a.xks;
     const double btpar_d = (double)btpar;
     const double d0 = (double)d;
+    const double g0 = a.gref + d0;
+    const double inv_g0 = 1.0 / g0;  // the stage energies differ from g0 by ~1e-9
     auto ode = [&](float ds, double ts, float& kg, double& kp) {
-      const double gs = a.gref + d0 + (double)ds;
-      const double inv_g2 = 1.0 / (gs * gs);
+      const double del = (double)ds * inv_g0;                // (gs - g0) / g0
+      const double inv_gs = inv_g0 * (1.0 + del * (-1.0 + del));
+      const double inv_g2 = inv_gs * inv_gs;
       const float dth = (float)(ts - t0);
       float ctr = 0.f, cti = 0.f;
 #pragma unroll
-      for (int f = 0; f < kRunFields; ++f) {
-        if (f >= a.nfield) break;
+      for (int f = 0; f < kF; ++f) {
+        if (f >= nfield) break;
         float sd, cd;
-        sincosf((float)a.f[f].harm * dth, &sd, &cd);
+        sincos_small((float)a.f[f].harm * dth, sd, cd);
         const float c = c0[f] * cd - s0[f] * sd;
         const float s = s0[f] * cd + c0[f] * sd;
         ctr += rr[f] * c + ri[f] * s;
@@ -204,18 +237,17 @@ __global__ void __launch_bounds__(256) beam_step_kernel(const BeamStepArgs a) {
       }
       const double btper0 = btpar_d + ztemp1 * (double)ctr;
       const double eps = btper0 * inv_g2;
-      double fe;
-      float b0;
+      double fe, inv_b0;
       if (eps < 1e-5) {
         fe = 0.5 + eps * (0.375 + eps * 0.3125);
-        b0 = (float)(1.0 - 0.5 * eps);
+        inv_b0 = 1.0 + eps * (0.5 + eps * 0.375);
       } else {
         const double b = sqrt(1.0 - eps);
         fe = 1.0 / (b * (1.0 + b));
-        b0 = (float)b;
+        inv_b0 = 1.0 / b;
       }
       kp += a.xku - a.xks * eps * fe;
-      kg += cti / b0 / (float)gs - ez;
+      kg += cti * (float)(inv_b0 * inv_gs) - ez;
     };
     // Genesis RK4 accumulator form (src/Core/BeamSolverCUDA.cpp:258-299) on
     // the step's energy increment dd (small, so FP32 keeps its relative
@@ -261,17 +293,18 @@ __global__ void __launch_bounds__(256) beam_step_kernel(const BeamStepArgs a) {
         py += a.cy;
       }
       const float g = a.gref_f + d;
-      const float gz = sqrtf(g * g - 1.0f - a.aw2 - px * px - py * py);
-      plane_f(a.xm, a.half, x, px, gz);
-      plane_f(a.ym, a.half, y, py, gz);
+      const float gz2 = g * g - 1.0f - a.aw2 - px * px - py * py;
+      const float inv_gz = rsqrtf(gz2), gz = gz2 * inv_gz;
+      plane_f(a.xm, a.half, x, px, gz, inv_gz);
+      plane_f(a.ym, a.half, y, py, gz, inv_gz);
     }
     a.xy[ip] = make_float2(x, y);
     a.pxy[ip] = make_float2(px, py);
     a.dg[ip] = d;
     a.th[ip] = t;
 #pragma unroll
-    for (int f = 0; f < kRunFields; ++f) {
-      if (f >= a.nfield) break;
+    for (int f = 0; f < kF; ++f) {
+      if (f >= nfield) break;
       int ix, iy;
       float wx, wy;
       if (a.f[f].do_source && cell_f(a.f[f], x, y, ix, iy, wx, wy)) {
@@ -285,8 +318,8 @@ __global__ void __launch_bounds__(256) beam_step_kernel(const BeamStepArgs a) {
   // per-CTA bounding boxes -> per-slice (integer min/max: order independent)
   const int w = tid >> 5, l = tid & 31;
 #pragma unroll
-  for (int f = 0; f < kRunFields; ++f) {
-    if (f >= a.nfield) break;
+  for (int f = 0; f < kF; ++f) {
+    if (f >= nfield) break;
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
       int v = bb[f][q];
@@ -298,7 +331,7 @@ __global__ void __launch_bounds__(256) beam_step_kernel(const BeamStepArgs a) {
     }
   }
   __syncthreads();
-  if (tid < 4 * a.nfield) {
+  if (tid < 4 * nfield) {
     const int f = tid >> 2, q = tid & 3;
     int v = sbb[f][q][0];
     for (int i = 1; i < 8; ++i) v = q < 2 ? min(v, sbb[f][q][i]) : max(v, sbb[f][q][i]);
@@ -320,7 +353,7 @@ struct DepField {
   int4* bbox;
   size_t cap;
   int first, n, ld, nslice, harm, do_source;
-  float gridmax, dgrid;
+  float gridmax, dgrid, inv_dgrid;
   double fc, xks, dgrid_d;
 };
 
@@ -338,105 +371,121 @@ struct DepDiagArgs {
   int* err;
 };
 
-__global__ void __launch_bounds__(512) deposit_diag_kernel(const DepDiagArgs a) {
+// One 4-CTA cluster per slice.  Each CTA reads a quarter of the slice's
+// particles once: it accumulates the beam-diagnostic sums of its quarter and
+// deposits its particles into the fixed-point accumulator, which is spread
+// over the cluster's shared memory (CTA k owns a quarter of the tile rows;
+// DSMEM 64-bit integer atomics, so the result is order independent).  The
+// CTA sums are combined by rank 0 in rank order.
+constexpr int kDepCluster = 4;
+constexpr int kDepThreads = 256;
+constexpr size_t kDepAccBytes = 64 * 1024;  // per CTA: 4096 cells
+
+__global__ void __cluster_dims__(kDepCluster, 1, 1) __launch_bounds__(kDepThreads, 2)
+    deposit_diag_kernel(const DepDiagArgs a) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cluster = cg::this_cluster();
   extern __shared__ __align__(128) unsigned char smem[];
-  __shared__ double dpart[16][kBeamRec + 2 * kMaxBunch];
+  __shared__ double dpart[kDepThreads / 32][kBeamRec + 2 * kMaxBunch];
+  __shared__ double cta_sum[kBeamRec + 2 * kMaxBunch];
   __shared__ int4 sbox[kRunFields];
   unsigned long long* acc = reinterpret_cast<unsigned long long*>(smem);
-  const int bs = blockIdx.x, tid = threadIdx.x, w = tid >> 5, l = tid & 31;
+  const int rank = (int)cluster.block_rank();
+  const int bs = blockIdx.x / kDepCluster;
+  const int tid = threadIdx.x, w = tid >> 5, l = tid & 31;
   const int64_t p0 = a.off[bs], p1 = a.off[bs + 1];
+  const int64_t np = p1 - p0;
+  const int64_t q0 = p0 + np * rank / kDepCluster, q1 = p0 + np * (rank + 1) / kDepCluster;
   const int rec = kBeamRec + 2 * a.nbunch;
-  if (tid < a.nfield) {
-    sbox[tid] = a.f[tid].bbox[bs];
-    // reset for the next step's beam_step
-    a.f[tid].bbox[bs] = make_int4(1 << 30, 1 << 30, -1, -1);
-  }
-  __syncthreads();
+  if (tid < a.nfield) sbox[tid] = a.f[tid].bbox[bs];
+  cluster.sync();  // every rank holds the boxes
+  if (rank == 0 && tid < a.nfield) a.f[tid].bbox[bs] = make_int4(1 << 30, 1 << 30, -1, -1);
 
-  // ---- beam diagnostics: one pass, FP64 sums of the FP32 state ----
-  double v[kBeamRec];
+  // ---- beam diagnostics of this CTA's particles (FP64 sums) ----
+  {
+    double v[kBeamRec];
 #pragma unroll
-  for (int k = 0; k < 13; ++k) v[k] = 0.0;
-  v[13] = 1.0e5; v[14] = -1.0e5; v[15] = 1.0e5; v[16] = -1.0e5;
-  v[17] = 1.0e5; v[18] = -1.0e5; v[19] = 1.0e5; v[20] = -1.0e5;
-  v[21] = 1.0e7; v[22] = 1.0;
-  double sdg = 0.0, sdg2 = 0.0;
-  double bre[kMaxBunch], bim[kMaxBunch];
+    for (int k = 0; k < 13; ++k) v[k] = 0.0;
+    v[13] = 1.0e5; v[14] = -1.0e5; v[15] = 1.0e5; v[16] = -1.0e5;
+    v[17] = 1.0e5; v[18] = -1.0e5; v[19] = 1.0e5; v[20] = -1.0e5;
+    v[21] = 1.0e7; v[22] = 1.0;
+    double sdg = 0.0, sdg2 = 0.0;
+    double bre[kMaxBunch], bim[kMaxBunch];
 #pragma unroll
-  for (int h = 0; h < kMaxBunch; ++h) bre[h] = bim[h] = 0.0;
-  for (int64_t p = p0 + tid; p < p1; p += blockDim.x) {
-    const float2 xy = a.xy[p], pp = a.pxy[p];
-    const double x = xy.x, y = xy.y, px = pp.x, py = pp.y;
-    const double dgv = a.dg[p];
-    const double g = a.gref + dgv;
-    sdg += dgv;
-    sdg2 += dgv * dgv;
-    v[2] += x; v[3] += x * x; v[4] += y; v[5] += y * y;
-    v[6] += px; v[7] += px * px; v[8] += py; v[9] += py * py;
-    v[10] += x * px; v[11] += y * py; v[12] += 1.0;
-    if (a.need_aux) {
-      v[13] = fmin(v[13], x); v[14] = fmax(v[14], x);
-      v[15] = fmin(v[15], px); v[16] = fmax(v[16], px);
-      v[17] = fmin(v[17], y); v[18] = fmax(v[18], y);
-      v[19] = fmin(v[19], py); v[20] = fmax(v[20], py);
-      v[21] = fmin(v[21], g); v[22] = fmax(v[22], g);
+    for (int h = 0; h < kMaxBunch; ++h) bre[h] = bim[h] = 0.0;
+    for (int64_t p = q0 + tid; p < q1; p += kDepThreads) {
+      const float2 xy = a.xy[p], pp = a.pxy[p];
+      const double x = xy.x, y = xy.y, px = pp.x, py = pp.y;
+      const double dgv = a.dg[p];
+      const double g = a.gref + dgv;
+      sdg += dgv;
+      sdg2 += dgv * dgv;
+      v[2] += x; v[3] += x * x; v[4] += y; v[5] += y * y;
+      v[6] += px; v[7] += px * px; v[8] += py; v[9] += py * py;
+      v[10] += x * px; v[11] += y * py; v[12] += 1.0;
+      if (a.need_aux) {
+        v[13] = fmin(v[13], x); v[14] = fmax(v[14], x);
+        v[15] = fmin(v[15], px); v[16] = fmax(v[16], px);
+        v[17] = fmin(v[17], y); v[18] = fmax(v[18], y);
+        v[19] = fmin(v[19], py); v[20] = fmax(v[20], py);
+        v[21] = fmin(v[21], g); v[22] = fmax(v[22], g);
+      }
+      float s1, c1;
+      sincosf(reduce_angle(a.th[p]), &s1, &c1);
+      float ch = c1, sh = s1;
+#pragma unroll
+      for (int h = 0; h < kMaxBunch; ++h) {
+        if (h >= a.nbunch) break;
+        bre[h] += ch;
+        bim[h] += sh;
+        const float nc = ch * c1 - sh * s1, ns = sh * c1 + ch * s1;
+        ch = nc;
+        sh = ns;
+      }
     }
-    float s1, c1;
-    sincosf(reduce_angle(a.th[p]), &s1, &c1);
-    float ch = c1, sh = s1;
+    {
+      const double N = v[12];
+      v[0] = N * a.gref + sdg;
+      v[1] = N * a.gref * a.gref + 2.0 * a.gref * sdg + sdg2;
+    }
+#pragma unroll
+    for (int k = 0; k < kBeamRec; ++k) {
+      double t = v[k];
+      const int op = k < 13 ? 0 : ((k - 13) % 2 == 0 ? 1 : 2);
+      for (int o = 16; o > 0; o >>= 1) {
+        const double u = __shfl_xor_sync(0xffffffffu, t, o);
+        t = op == 0 ? t + u : (op == 1 ? fmin(t, u) : fmax(t, u));
+      }
+      if (l == 0) dpart[w][k] = t;
+    }
 #pragma unroll
     for (int h = 0; h < kMaxBunch; ++h) {
       if (h >= a.nbunch) break;
-      bre[h] += ch;
-      bim[h] += sh;
-      const float nc = ch * c1 - sh * s1, ns = sh * c1 + ch * s1;
-      ch = nc;
-      sh = ns;
+      double tr = bre[h], ti = bim[h];
+      for (int o = 16; o > 0; o >>= 1) {
+        tr += __shfl_xor_sync(0xffffffffu, tr, o);
+        ti += __shfl_xor_sync(0xffffffffu, ti, o);
+      }
+      if (l == 0) {
+        dpart[w][kBeamRec + 2 * h] = tr;
+        dpart[w][kBeamRec + 2 * h + 1] = ti;
+      }
     }
-  }
-  {
-    const double N = v[12];
-    v[0] = N * a.gref + sdg;
-    v[1] = N * a.gref * a.gref + 2.0 * a.gref * sdg + sdg2;
-  }
-#pragma unroll
-  for (int k = 0; k < kBeamRec; ++k) {
-    double t = v[k];
-    const int op = k < 13 ? 0 : ((k - 13) % 2 == 0 ? 1 : 2);
-    for (int o = 16; o > 0; o >>= 1) {
-      const double u = __shfl_xor_sync(0xffffffffu, t, o);
-      t = op == 0 ? t + u : (op == 1 ? fmin(t, u) : fmax(t, u));
+    __syncthreads();
+    if (tid < rec) {
+      const int op = tid < 13 ? 0 : (tid < kBeamRec ? ((tid - 13) % 2 == 0 ? 1 : 2) : 0);
+      double t = dpart[0][tid];
+      for (int i = 1; i < kDepThreads / 32; ++i) {
+        const double u = dpart[i][tid];
+        t = op == 0 ? t + u : (op == 1 ? fmin(t, u) : fmax(t, u));
+      }
+      cta_sum[tid] = t;
     }
-    if (l == 0) dpart[w][k] = t;
-  }
-#pragma unroll
-  for (int h = 0; h < kMaxBunch; ++h) {
-    if (h >= a.nbunch) break;
-    double tr = bre[h], ti = bim[h];
-    for (int o = 16; o > 0; o >>= 1) {
-      tr += __shfl_xor_sync(0xffffffffu, tr, o);
-      ti += __shfl_xor_sync(0xffffffffu, ti, o);
-    }
-    if (l == 0) {
-      dpart[w][kBeamRec + 2 * h] = tr;
-      dpart[w][kBeamRec + 2 * h + 1] = ti;
-    }
-  }
-  __syncthreads();
-  if (tid < rec) {
-    const int op = tid < 13 ? 0 : (tid < kBeamRec ? ((tid - 13) % 2 == 0 ? 1 : 2) : 0);
-    double t = dpart[0][tid];
-    const int nw = blockDim.x >> 5;
-    for (int i = 1; i < nw; ++i) {
-      const double u = dpart[i][tid];
-      t = op == 0 ? t + u : (op == 1 ? fmin(t, u) : fmax(t, u));
-    }
-    if (tid >= 13 && tid < kBeamRec && !a.need_aux) t = 0.0;
-    a.beam_hist[(size_t)bs * rec + tid] = t;
   }
 
   // ---- deposition of every field with a source this step ----
-  const double npd = (double)(p1 - p0);
+  const double npd = (double)np;
+  const int acc_cells = (int)(kDepAccBytes / 16);
   for (int fi = 0; fi < a.nfield; ++fi) {
     const DepField& F = a.f[fi];
     if (!F.do_source) continue;
@@ -449,7 +498,7 @@ __global__ void __launch_bounds__(512) deposit_diag_kernel(const DepDiagArgs a) 
       scl /= 4.0 * 510998.95 * npd * F.dgrid_d * F.dgrid_d;
     }
     if (bb.z < 0 || scl == 0.0) {
-      if (tid == 0) F.desc[target] = make_int4(0, 0, 0, 0);
+      if (rank == 0 && tid == 0) F.desc[target] = make_int4(0, 0, 0, 0);
       continue;
     }
     int bx0 = bb.x, bw = bb.z - bb.x + 2;
@@ -458,25 +507,26 @@ __global__ void __launch_bounds__(512) deposit_diag_kernel(const DepDiagArgs a) 
       ++bw;
       if (bx0 + bw > F.ld) --bx0;
     }
-    if (tid == 0) F.desc[target] = make_int4(bx0, by0, bw, bh);
-    const int band_h = max(1, min(bh, a.acc_cells / bw));
+    if (rank == 0 && tid == 0) F.desc[target] = make_int4(bx0, by0, bw, bh);
+    const int hk = (bh + kDepCluster - 1) / kDepCluster;  // rows owned per rank
+    const int band = max(1, min(hk, acc_cells / bw));     // owned rows per pass
     const double unscale = scl / a.fixed_scale;
     const float fh = (float)F.harm;
-    for (int yb = by0; yb < by0 + bh; yb += band_h) {
-      const int hb = min(band_h, by0 + bh - yb);
-      __syncthreads();
-      for (int i = tid; i < 2 * hb * bw; i += blockDim.x) acc[i] = 0ull;
-      __syncthreads();
-      for (int64_t p = p0 + tid; p < p1; p += blockDim.x) {
+    MixField mf;
+    mf.gridmax = F.gridmax;
+    mf.dgrid = F.dgrid;
+    mf.inv_dgrid = F.inv_dgrid;
+    mf.n = F.n;
+    for (int yb = 0; yb < hk; yb += band) {
+      const int hb = min(band, hk - yb);
+      __syncthreads();  // the previous band's tile write has finished reading acc
+      for (int i = tid; i < 2 * hb * bw; i += kDepThreads) acc[i] = 0ull;
+      cluster.sync();
+      for (int64_t p = q0 + tid; p < q1; p += kDepThreads) {
         const float2 xy = a.xy[p];
         int ix, iy;
         float wx, wy;
-        MixField mf;
-        mf.gridmax = F.gridmax;
-        mf.dgrid = F.dgrid;
-        mf.n = F.n;
         if (!cell_f(mf, xy.x, xy.y, ix, iy, wx, wy)) continue;
-        if (iy + 1 < yb || iy >= yb + hb) continue;
         const float dxu = xy.x - a.ax, dyu = xy.y - a.ay;
         const float faw2 = 1.0f + a.kx * dxu * dxu + a.ky * dyu * dyu +
                            2.0f * (a.gradx * dxu + a.grady * dyu);
@@ -494,24 +544,44 @@ __global__ void __launch_bounds__(512) deposit_diag_kernel(const DepDiagArgs a) 
         const int cy[4] = {iy, iy, iy + 1, iy + 1};
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
-          const int ry = cy[c] - yb, rx = cx[c] - bx0;
-          if (ry < 0 || ry >= hb) continue;
-          if (rx < 0 || rx >= bw) {
+          const int rel = cy[c] - by0;
+          const int owner = rel / hk;
+          const int row = rel - owner * hk - yb;
+          const int rx = cx[c] - bx0;
+          if (row < 0 || row >= hb) continue;
+          if (rel < 0 || owner >= kDepCluster || rx < 0 || rx >= bw) {
             atomicOr(a.err, kErrBadSlice);
             continue;
           }
-          const int cell = ry * bw + rx;
-          atomicAdd(&acc[2 * cell], (unsigned long long)__double2ll_rn(vre * ws[c]));
-          atomicAdd(&acc[2 * cell + 1], (unsigned long long)__double2ll_rn(vim * ws[c]));
+          unsigned long long* dst = cluster.map_shared_rank(acc, owner) + 2 * (row * bw + rx);
+          atomicAdd(dst, (unsigned long long)__double2ll_rn(vre * ws[c]));
+          atomicAdd(dst + 1, (unsigned long long)__double2ll_rn(vim * ws[c]));
         }
       }
-      __syncthreads();
-      float2* out = F.src + (size_t)target * F.cap + (size_t)(yb - by0) * bw;
-      for (int i = tid; i < hb * bw; i += blockDim.x)
+      cluster.sync();
+      // this rank's rows of the band: tile rows rank*hk + yb .. + hb
+      const int r0 = rank * hk + yb;
+      const int nr = max(0, min(hb, bh - r0));
+      float2* out = F.src + (size_t)target * F.cap + (size_t)r0 * bw;
+      for (int i = tid; i < nr * bw; i += kDepThreads)
         out[i] = make_float2((float)((double)(long long)acc[2 * i] * unscale),
                              (float)((double)(long long)acc[2 * i + 1] * unscale));
     }
   }
+
+  // ---- combine the CTA diagnostic sums in rank order ----
+  cluster.sync();
+  if (rank == 0 && tid < rec) {
+    const int op = tid < 13 ? 0 : (tid < kBeamRec ? ((tid - 13) % 2 == 0 ? 1 : 2) : 0);
+    double t = cta_sum[tid];
+    for (int r = 1; r < kDepCluster; ++r) {
+      const double u = cluster.map_shared_rank(cta_sum, r)[tid];
+      t = op == 0 ? t + u : (op == 1 ? fmin(t, u) : fmax(t, u));
+    }
+    if (tid >= 13 && tid < kBeamRec && !a.need_aux) t = 0.0;
+    a.beam_hist[(size_t)bs * rec + tid] = t;
+  }
+  cluster.sync();  // keep every CTA's shared memory alive until rank 0 has read it
 }
 
 // ---------------------------------------------------------- diag finalize --
@@ -606,7 +676,6 @@ void g4b_chicane_matrix(double angle, double lb, double ld, double lt, double* m
 namespace {
 
 constexpr int kRunChunk = 256;
-constexpr size_t kAccBytes = 128 * 1024;
 
 int plan_step(g4b_run* r, int i, StepPlan& p) {
   p.st = r->steps[i];
@@ -684,6 +753,7 @@ int enqueue_step(g4b_run* r, int i, const StepPlan& p) {
       m.do_source = st.in_undulator && (F.harm % 2) == 1;
       m.gridmax = (float)F.f->gridmax;
       m.dgrid = (float)F.f->dgrid;
+      m.inv_dgrid = (float)(1.0 / F.f->dgrid);
       m.rtmp = (float)(p.fc[f] / F.f->xks);
       m.bbox = F.d_bbox;
       xks_local = F.f->xks / (double)F.harm;
@@ -736,7 +806,12 @@ int enqueue_step(g4b_run* r, int i, const StepPlan& p) {
     }
     a.err = c->d_error;
     LaunchScope ls(c, "run_beam_step");
-    beam_step_kernel<<<r->nchunk, kRunChunk, 0, c->stream>>>(a);
+    if (r->nfield == 1)
+      beam_step_kernel<1><<<r->nchunk, kRunChunk, 0, c->stream>>>(a);
+    else if (r->nfield == 2)
+      beam_step_kernel<2><<<r->nchunk, kRunChunk, 0, c->stream>>>(a);
+    else
+      beam_step_kernel<0><<<r->nchunk, kRunChunk, 0, c->stream>>>(a);
   }
   if (int rc = check_launch(c, "beam_step_kernel")) return rc;
   // K2
@@ -752,7 +827,7 @@ int enqueue_step(g4b_run* r, int i, const StepPlan& p) {
     a.nfield = r->nfield;
     a.nbunch = r->desc.nbunch;
     a.need_aux = 1;
-    a.acc_cells = (int)(kAccBytes / 16);
+    a.acc_cells = (int)(kDepAccBytes / 16);
     a.ax = (float)st.ax;
     a.ay = (float)st.ay;
     a.kx = (float)st.kx;
@@ -780,12 +855,13 @@ int enqueue_step(g4b_run* r, int i, const StepPlan& p) {
       d.do_source = st.in_undulator && (F.harm % 2) == 1 && p.fc[f] != 0.0;
       d.gridmax = (float)F.f->gridmax;
       d.dgrid = (float)F.f->dgrid;
+      d.inv_dgrid = (float)(1.0 / F.f->dgrid);
       d.dgrid_d = F.f->dgrid;
       d.fc = p.fc[f];
       d.xks = F.f->xks;
     }
     LaunchScope ls(c, "run_deposit_diag");
-    deposit_diag_kernel<<<r->nslice, 512, kAccBytes, c->stream>>>(a);
+    deposit_diag_kernel<<<r->nslice * kDepCluster, kDepThreads, kDepAccBytes, c->stream>>>(a);
   }
   if (int rc = check_launch(c, "deposit_diag_kernel")) return rc;
   // K3/K4 per field
@@ -924,7 +1000,7 @@ int g4b_run_create(g4b_ctx* c, const g4b_run_desc* d, const int64_t* off, g4b_ru
   std::frexp((double)std::max<int64_t>(r->max_np, 1) * r->qbound, &ex);
   r->fixed_scale = std::ldexp(1.0, 62 - ex);
   cudaFuncSetAttribute(deposit_diag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)kAccBytes);
+                       (int)kDepAccBytes);
   *out = r;
   return G4B_OK;
 }
