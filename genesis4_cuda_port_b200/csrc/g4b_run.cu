@@ -28,8 +28,6 @@
 #include <tuple>
 #include <vector>
 
-#include <cooperative_groups.h>
-
 #include "g4b_internal.cuh"
 
 namespace g4b {
@@ -367,41 +365,39 @@ struct DepDiagArgs {
   int nfield, nbunch, need_aux, acc_cells;
   float ax, ay, kx, ky, gradx, grady;
   double gref, delz, fixed_scale, qbound;
-  double* beam_hist;  // [nslice][23 + 2*nbunch] for this step
+  double* beam_part;  // [nslice * kDepBands][23 + 2*nbunch] partial sums
   int* err;
 };
 
-// One 4-CTA cluster per slice.  Each CTA reads a quarter of the slice's
-// particles once: it accumulates the beam-diagnostic sums of its quarter and
-// deposits its particles into the fixed-point accumulator, which is spread
-// over the cluster's shared memory (CTA k owns a quarter of the tile rows;
-// DSMEM 64-bit integer atomics, so the result is order independent).  The
-// CTA sums are combined by rank 0 in rank order.
-constexpr int kDepCluster = 4;
+// Deposition + beam diagnostics, kDepBands CTAs per slice.  CTA k of a slice
+// owns rows [k*hk, (k+1)*hk) of the slice's source tile (hk = ceil(h/kDepBands))
+// and a fixed-point accumulator for them in its own shared memory; it scans
+// the positions of all the slice's particles (L2-resident after the first of
+// the slice's CTAs) and deposits only the corners that fall in its rows, with
+// shared-memory 64-bit integer atomics (order independent).  CTA k also sums
+// the beam diagnostics of the k-th quarter of the particles; the finalize
+// kernel adds the quarters in order.
+constexpr int kDepBands = 4;
 constexpr int kDepThreads = 256;
 constexpr size_t kDepAccBytes = 64 * 1024;  // per CTA: 4096 cells
 
-__global__ void __cluster_dims__(kDepCluster, 1, 1) __launch_bounds__(kDepThreads, 2)
-    deposit_diag_kernel(const DepDiagArgs a) {
-  namespace cg = cooperative_groups;
-  cg::cluster_group cluster = cg::this_cluster();
+// NB: bunching harmonics accumulated (1, or up to kMaxBunch)
+template <int NB>
+__global__ void __launch_bounds__(kDepThreads, NB == 1 ? 3 : 2) deposit_diag_kernel(const DepDiagArgs a) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ double dpart[kDepThreads / 32][kBeamRec + 2 * kMaxBunch];
-  __shared__ double cta_sum[kBeamRec + 2 * kMaxBunch];
   __shared__ int4 sbox[kRunFields];
   unsigned long long* acc = reinterpret_cast<unsigned long long*>(smem);
-  const int rank = (int)cluster.block_rank();
-  const int bs = blockIdx.x / kDepCluster;
+  const int bs = blockIdx.x / kDepBands, kb = blockIdx.x - bs * kDepBands;
   const int tid = threadIdx.x, w = tid >> 5, l = tid & 31;
   const int64_t p0 = a.off[bs], p1 = a.off[bs + 1];
   const int64_t np = p1 - p0;
-  const int64_t q0 = p0 + np * rank / kDepCluster, q1 = p0 + np * (rank + 1) / kDepCluster;
+  const int64_t q0 = p0 + np * kb / kDepBands, q1 = p0 + np * (kb + 1) / kDepBands;
   const int rec = kBeamRec + 2 * a.nbunch;
   if (tid < a.nfield) sbox[tid] = a.f[tid].bbox[bs];
-  cluster.sync();  // every rank holds the boxes
-  if (rank == 0 && tid < a.nfield) a.f[tid].bbox[bs] = make_int4(1 << 30, 1 << 30, -1, -1);
+  __syncthreads();
 
-  // ---- beam diagnostics of this CTA's particles (FP64 sums) ----
+  // ---- beam diagnostics of this CTA's quarter (FP64 sums) ----
   {
     double v[kBeamRec];
 #pragma unroll
@@ -410,9 +406,9 @@ __global__ void __cluster_dims__(kDepCluster, 1, 1) __launch_bounds__(kDepThread
     v[17] = 1.0e5; v[18] = -1.0e5; v[19] = 1.0e5; v[20] = -1.0e5;
     v[21] = 1.0e7; v[22] = 1.0;
     double sdg = 0.0, sdg2 = 0.0;
-    double bre[kMaxBunch], bim[kMaxBunch];
+    double bre[NB], bim[NB];
 #pragma unroll
-    for (int h = 0; h < kMaxBunch; ++h) bre[h] = bim[h] = 0.0;
+    for (int h = 0; h < NB; ++h) bre[h] = bim[h] = 0.0;
     for (int64_t p = q0 + tid; p < q1; p += kDepThreads) {
       const float2 xy = a.xy[p], pp = a.pxy[p];
       const double x = xy.x, y = xy.y, px = pp.x, py = pp.y;
@@ -434,7 +430,7 @@ __global__ void __cluster_dims__(kDepCluster, 1, 1) __launch_bounds__(kDepThread
       sincosf(reduce_angle(a.th[p]), &s1, &c1);
       float ch = c1, sh = s1;
 #pragma unroll
-      for (int h = 0; h < kMaxBunch; ++h) {
+      for (int h = 0; h < NB; ++h) {
         if (h >= a.nbunch) break;
         bre[h] += ch;
         bim[h] += sh;
@@ -459,7 +455,7 @@ __global__ void __cluster_dims__(kDepCluster, 1, 1) __launch_bounds__(kDepThread
       if (l == 0) dpart[w][k] = t;
     }
 #pragma unroll
-    for (int h = 0; h < kMaxBunch; ++h) {
+    for (int h = 0; h < NB; ++h) {
       if (h >= a.nbunch) break;
       double tr = bre[h], ti = bim[h];
       for (int o = 16; o > 0; o >>= 1) {
@@ -479,7 +475,8 @@ __global__ void __cluster_dims__(kDepCluster, 1, 1) __launch_bounds__(kDepThread
         const double u = dpart[i][tid];
         t = op == 0 ? t + u : (op == 1 ? fmin(t, u) : fmax(t, u));
       }
-      cta_sum[tid] = t;
+      if (tid >= 13 && tid < kBeamRec && !a.need_aux) t = 0.0;
+      a.beam_part[(size_t)blockIdx.x * rec + tid] = t;
     }
   }
 
@@ -498,7 +495,7 @@ __global__ void __cluster_dims__(kDepCluster, 1, 1) __launch_bounds__(kDepThread
       scl /= 4.0 * 510998.95 * npd * F.dgrid_d * F.dgrid_d;
     }
     if (bb.z < 0 || scl == 0.0) {
-      if (rank == 0 && tid == 0) F.desc[target] = make_int4(0, 0, 0, 0);
+      if (kb == 0 && tid == 0) F.desc[target] = make_int4(0, 0, 0, 0);
       continue;
     }
     int bx0 = bb.x, bw = bb.z - bb.x + 2;
@@ -507,9 +504,10 @@ __global__ void __cluster_dims__(kDepCluster, 1, 1) __launch_bounds__(kDepThread
       ++bw;
       if (bx0 + bw > F.ld) --bx0;
     }
-    if (rank == 0 && tid == 0) F.desc[target] = make_int4(bx0, by0, bw, bh);
-    const int hk = (bh + kDepCluster - 1) / kDepCluster;  // rows owned per rank
-    const int band = max(1, min(hk, acc_cells / bw));     // owned rows per pass
+    if (kb == 0 && tid == 0) F.desc[target] = make_int4(bx0, by0, bw, bh);
+    const int hk = (bh + kDepBands - 1) / kDepBands;   // tile rows owned by this CTA
+    const int row0 = kb * hk, nrow = max(0, min(hk, bh - row0));
+    const int band = max(1, min(max(nrow, 1), acc_cells / bw));
     const double unscale = scl / a.fixed_scale;
     const float fh = (float)F.harm;
     MixField mf;
@@ -517,16 +515,18 @@ __global__ void __cluster_dims__(kDepCluster, 1, 1) __launch_bounds__(kDepThread
     mf.dgrid = F.dgrid;
     mf.inv_dgrid = F.inv_dgrid;
     mf.n = F.n;
-    for (int yb = 0; yb < hk; yb += band) {
-      const int hb = min(band, hk - yb);
-      __syncthreads();  // the previous band's tile write has finished reading acc
+    for (int yb = 0; yb < nrow; yb += band) {
+      const int hb = min(band, nrow - yb);
+      const int ylo = by0 + row0 + yb;  // first grid row of this pass
+      __syncthreads();
       for (int i = tid; i < 2 * hb * bw; i += kDepThreads) acc[i] = 0ull;
-      cluster.sync();
-      for (int64_t p = q0 + tid; p < q1; p += kDepThreads) {
+      __syncthreads();
+      for (int64_t p = p0 + tid; p < p1; p += kDepThreads) {
         const float2 xy = a.xy[p];
         int ix, iy;
         float wx, wy;
         if (!cell_f(mf, xy.x, xy.y, ix, iy, wx, wy)) continue;
+        if (iy + 1 < ylo || iy >= ylo + hb) continue;
         const float dxu = xy.x - a.ax, dyu = xy.y - a.ay;
         const float faw2 = 1.0f + a.kx * dxu * dxu + a.ky * dyu * dyu +
                            2.0f * (a.gradx * dxu + a.grady * dyu);
@@ -544,44 +544,30 @@ __global__ void __cluster_dims__(kDepCluster, 1, 1) __launch_bounds__(kDepThread
         const int cy[4] = {iy, iy, iy + 1, iy + 1};
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
-          const int rel = cy[c] - by0;
-          const int owner = rel / hk;
-          const int row = rel - owner * hk - yb;
-          const int rx = cx[c] - bx0;
-          if (row < 0 || row >= hb) continue;
-          if (rel < 0 || owner >= kDepCluster || rx < 0 || rx >= bw) {
+          const int ry = cy[c] - ylo, rx = cx[c] - bx0;
+          if (ry < 0 || ry >= hb) continue;
+          if (rx < 0 || rx >= bw) {
             atomicOr(a.err, kErrBadSlice);
             continue;
           }
-          unsigned long long* dst = cluster.map_shared_rank(acc, owner) + 2 * (row * bw + rx);
-          atomicAdd(dst, (unsigned long long)__double2ll_rn(vre * ws[c]));
-          atomicAdd(dst + 1, (unsigned long long)__double2ll_rn(vim * ws[c]));
+          const int cell = ry * bw + rx;
+          atomicAdd(&acc[2 * cell], (unsigned long long)__double2ll_rn(vre * ws[c]));
+          atomicAdd(&acc[2 * cell + 1], (unsigned long long)__double2ll_rn(vim * ws[c]));
         }
       }
-      cluster.sync();
-      // this rank's rows of the band: tile rows rank*hk + yb .. + hb
-      const int r0 = rank * hk + yb;
-      const int nr = max(0, min(hb, bh - r0));
-      float2* out = F.src + (size_t)target * F.cap + (size_t)r0 * bw;
-      for (int i = tid; i < nr * bw; i += kDepThreads)
+      __syncthreads();
+      float2* out = F.src + (size_t)target * F.cap + (size_t)(row0 + yb) * bw;
+      for (int i = tid; i < hb * bw; i += kDepThreads)
         out[i] = make_float2((float)((double)(long long)acc[2 * i] * unscale),
                              (float)((double)(long long)acc[2 * i + 1] * unscale));
     }
   }
+}
 
-  // ---- combine the CTA diagnostic sums in rank order ----
-  cluster.sync();
-  if (rank == 0 && tid < rec) {
-    const int op = tid < 13 ? 0 : (tid < kBeamRec ? ((tid - 13) % 2 == 0 ? 1 : 2) : 0);
-    double t = cta_sum[tid];
-    for (int r = 1; r < kDepCluster; ++r) {
-      const double u = cluster.map_shared_rank(cta_sum, r)[tid];
-      t = op == 0 ? t + u : (op == 1 ? fmin(t, u) : fmax(t, u));
-    }
-    if (tid >= 13 && tid < kBeamRec && !a.need_aux) t = 0.0;
-    a.beam_hist[(size_t)bs * rec + tid] = t;
-  }
-  cluster.sync();  // keep every CTA's shared memory alive until rank 0 has read it
+// Resets the per-slice boxes after the deposition has read them.
+__global__ void bbox_reset_kernel(int4* bbox, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) bbox[i] = make_int4(1 << 30, 1 << 30, -1, -1);
 }
 
 // ---------------------------------------------------------- diag finalize --
@@ -589,23 +575,50 @@ __global__ void __cluster_dims__(kDepCluster, 1, 1) __launch_bounds__(kDepThread
 // (src/Core/DiagnosticCUDA.cpp:320) from the pass-Y band partials.
 struct FinalizeArgs {
   const double* part[kRunFields];  // [nslice][nband][9]
+  int4* bbox[kRunFields];
   int nband[kRunFields];
   int first_after[kRunFields];
-  int nfield, nslice;
-  double* field_hist;  // [nfield][nslice][9] for this step
+  int nfield, nslice, rec;
+  const double* beam_part;  // [nslice * kDepBands][rec]
+  double* beam_hist;        // [nslice][rec] for this step
+  double* field_hist;       // [nfield][nslice][9] for this step
 };
 
+// Per-slice reductions in fixed order: field diagnostics per beam slice
+// is = (nslice + storage - first) % nslice (src/Core/DiagnosticCUDA.cpp:320)
+// from the pass-Y band partials, the beam diagnostics from the deposition
+// CTAs' quarters; also resets the deposition boxes for the next step.
 __global__ void diag_finalize_kernel(const FinalizeArgs a) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= a.nfield * a.nslice) return;
-  const int f = i / a.nslice, s = i - f * a.nslice;
-  const double* p = a.part[f] + (size_t)s * a.nband[f] * 9;
-  double v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-  for (int b = 0; b < a.nband[f]; ++b)
-    for (int q = 0; q < 9; ++q) v[q] += p[b * 9 + q];
-  const int is = (a.nslice + s - a.first_after[f]) % a.nslice;
-  double* o = a.field_hist + ((size_t)f * a.nslice + is) * 9;
-  for (int q = 0; q < 9; ++q) o[q] = v[q];
+  const int nf = a.nfield * a.nslice;
+  const int nb = a.nslice * a.rec;
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nf + nb + nf; i += stride) {
+    if (i < nf) {
+      const int f = i / a.nslice, s = i - f * a.nslice;
+      const double* p = a.part[f] + (size_t)s * a.nband[f] * 9;
+      double v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+      for (int b = 0; b < a.nband[f]; ++b)
+        for (int q = 0; q < 9; ++q) v[q] += p[b * 9 + q];
+      const int is = (a.nslice + s - a.first_after[f]) % a.nslice;
+      double* o = a.field_hist + ((size_t)f * a.nslice + is) * 9;
+      for (int q = 0; q < 9; ++q) o[q] = v[q];
+    } else if (i < nf + nb) {
+      const int j = i - nf;
+      const int s = j / a.rec, k = j - s * a.rec;
+      const int op = k < 13 ? 0 : (k < kBeamRec ? ((k - 13) % 2 == 0 ? 1 : 2) : 0);
+      const double* p = a.beam_part + (size_t)s * kDepBands * a.rec + k;
+      double t = p[0];
+      for (int b = 1; b < kDepBands; ++b) {
+        const double u = p[(size_t)b * a.rec];
+        t = op == 0 ? t + u : (op == 1 ? fmin(t, u) : fmax(t, u));
+      }
+      a.beam_hist[(size_t)s * a.rec + k] = t;
+    } else {
+      const int j = i - nf - nb;
+      const int f = j / a.nslice, s = j - f * a.nslice;
+      a.bbox[f][s] = make_int4(1 << 30, 1 << 30, -1, -1);
+    }
+  }
 }
 
 static PlaneMapF plane_map_f(double strength, double offset) {
@@ -660,6 +673,7 @@ struct g4b_run {
   std::vector<double> slip;
   // history of diagnostics: per step beam [nslice][rec] then fields
   double* d_hist = nullptr;
+  double* d_beam_part = nullptr;   // deposition CTAs' beam-diagnostic partials
   int hist_steps = 0;
   size_t rec_beam = 0, step_doubles = 0;
   double fixed_scale = 0, qbound = 0;
@@ -838,7 +852,7 @@ int enqueue_step(g4b_run* r, int i, const StepPlan& p) {
     a.delz = st.delz;
     a.fixed_scale = r->fixed_scale;
     a.qbound = r->qbound;
-    a.beam_hist = step_hist;
+    a.beam_part = r->d_beam_part;
     a.err = c->d_error;
     for (int f = 0; f < r->nfield; ++f) {
       const RunFieldState& F = r->fs[f];
@@ -861,7 +875,11 @@ int enqueue_step(g4b_run* r, int i, const StepPlan& p) {
       d.xks = F.f->xks;
     }
     LaunchScope ls(c, "run_deposit_diag");
-    deposit_diag_kernel<<<r->nslice * kDepCluster, kDepThreads, kDepAccBytes, c->stream>>>(a);
+    if (r->desc.nbunch == 1)
+      deposit_diag_kernel<1><<<r->nslice * kDepBands, kDepThreads, kDepAccBytes, c->stream>>>(a);
+    else
+      deposit_diag_kernel<kMaxBunch>
+          <<<r->nslice * kDepBands, kDepThreads, kDepAccBytes, c->stream>>>(a);
   }
   if (int rc = check_launch(c, "deposit_diag_kernel")) return rc;
   // K3/K4 per field
@@ -880,14 +898,18 @@ int enqueue_step(g4b_run* r, int i, const StepPlan& p) {
     a.nfield = r->nfield;
     a.nslice = r->nslice;
     a.field_hist = step_hist + r->rec_beam * r->nslice;
+    a.beam_hist = step_hist;
+    a.beam_part = r->d_beam_part;
+    a.rec = (int)r->rec_beam;
     for (int f = 0; f < r->nfield; ++f) {
       a.part[f] = r->fs[f].d_part;
+      a.bbox[f] = r->fs[f].d_bbox;
       a.nband[f] = r->fs[f].nband;
       a.first_after[f] = p.first_after[f];
     }
-    const int n = r->nfield * r->nslice;
+    const int n = 2 * r->nfield * r->nslice + r->nslice * (int)r->rec_beam;
     LaunchScope ls(c, "run_diag_finalize");
-    diag_finalize_kernel<<<(n + 127) / 128, 128, 0, c->stream>>>(a);
+    diag_finalize_kernel<<<(n + 255) / 256, 256, 0, c->stream>>>(a);
   }
   return check_launch(c, "diag_finalize_kernel");
 }
@@ -992,6 +1014,11 @@ int g4b_run_create(g4b_ctx* c, const g4b_run_desc* d, const int64_t* off, g4b_ru
     }
   }
   r->rec_beam = kBeamRec + 2 * d->nbunch;
+  A((void**)&r->d_beam_part, (size_t)d->nslice * kDepBands * r->rec_beam * 8);
+  if (e != cudaSuccess) {
+    g4b_run_destroy(r);
+    return cuda_fail(e, "g4b_run_create: device allocation");
+  }
   r->step_doubles = (size_t)d->nslice * (r->rec_beam + 9 * d->nfield);
   // fixed point of the deposition: |q| = sqrt(faw2)/gamma <= 4/gamma_ref,
   // slice sums <= max_np * qbound < 2^62
@@ -999,8 +1026,10 @@ int g4b_run_create(g4b_ctx* c, const g4b_run_desc* d, const int64_t* off, g4b_ru
   int ex;
   std::frexp((double)std::max<int64_t>(r->max_np, 1) * r->qbound, &ex);
   r->fixed_scale = std::ldexp(1.0, 62 - ex);
-  cudaFuncSetAttribute(deposit_diag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaFuncSetAttribute(deposit_diag_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)kDepAccBytes);
+  cudaFuncSetAttribute(deposit_diag_kernel<kMaxBunch>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDepAccBytes);
   *out = r;
   return G4B_OK;
 }
@@ -1010,7 +1039,7 @@ int g4b_run_destroy(g4b_run* r) {
   ctx_quiesce(r->ctx);
   if (r->gexec) cudaGraphExecDestroy(r->gexec);
   void* ptrs[] = {r->xy, r->pxy, r->dg, r->th, r->d_off, r->d_chunks, r->d_current,
-                  r->d_eloss, r->d_hist};
+                  r->d_eloss, r->d_hist, r->d_beam_part};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (int f = 0; f < kRunFields; ++f) {
