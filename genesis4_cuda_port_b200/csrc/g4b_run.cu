@@ -481,8 +481,16 @@ __global__ void __launch_bounds__(kDepThreads, NB == 1 ? 3 : 2) deposit_diag_ker
   }
 
   // ---- deposition of every field with a source this step ----
+  // Accumulator: per cell re_hi, re_lo, im_hi, im_lo (32-bit words); a
+  // fixed-point contribution c (|c| < 2^46) is added as hi = c >> 16 (signed)
+  // and lo = c & 0xffff with native 32-bit atomics: the sums stay exact
+  // (sum lo < 2^32 for <= 65536 contributions per cell) and the cell value is
+  // hi * 2^16 + lo.
+  __shared__ int qcount;
+  __shared__ int queue[kDepThreads * 4];
   const double npd = (double)np;
   const int acc_cells = (int)(kDepAccBytes / 16);
+  unsigned int* acc32 = reinterpret_cast<unsigned int*>(smem);
   for (int fi = 0; fi < a.nfield; ++fi) {
     const DepField& F = a.f[fi];
     if (!F.do_source) continue;
@@ -519,47 +527,80 @@ __global__ void __launch_bounds__(kDepThreads, NB == 1 ? 3 : 2) deposit_diag_ker
       const int hb = min(band, nrow - yb);
       const int ylo = by0 + row0 + yb;  // first grid row of this pass
       __syncthreads();
-      for (int i = tid; i < 2 * hb * bw; i += kDepThreads) acc[i] = 0ull;
+      for (int i = tid; i < 4 * hb * bw; i += kDepThreads) acc32[i] = 0u;
+      if (tid == 0) qcount = 0;
       __syncthreads();
-      for (int64_t p = p0 + tid; p < p1; p += kDepThreads) {
-        const float2 xy = a.xy[p];
-        int ix, iy;
-        float wx, wy;
-        if (!cell_f(mf, xy.x, xy.y, ix, iy, wx, wy)) continue;
-        if (iy + 1 < ylo || iy >= ylo + hb) continue;
-        const float dxu = xy.x - a.ax, dyu = xy.y - a.ay;
-        const float faw2 = 1.0f + a.kx * dxu * dxu + a.ky * dyu * dyu +
-                           2.0f * (a.gradx * dxu + a.grady * dyu);
-        double q = (double)sqrtf(faw2) / (a.gref + (double)a.dg[p]);
-        if (!(fabs(q) <= a.qbound)) {
-          atomicOr(a.err, kErrFixedRange);
-          q = 0.0;
-        }
-        float sn, cs;
-        sincosf(reduce_angle((double)fh * a.th[p]), &sn, &cs);
-        const double vre = (double)sn * q * a.fixed_scale;
-        const double vim = (double)cs * q * a.fixed_scale;
-        const float ws[4] = {wx * wy, (1.f - wx) * wy, wx * (1.f - wy), (1.f - wx) * (1.f - wy)};
-        const int cx[4] = {ix, ix + 1, ix, ix + 1};
-        const int cy[4] = {iy, iy, iy + 1, iy + 1};
+      for (int64_t base = p0; base < p1; base += 4 * kDepThreads) {
+        // 1. queue the particles with a corner in this pass's rows
 #pragma unroll
-        for (int c = 0; c < 4; ++c) {
-          const int ry = cy[c] - ylo, rx = cx[c] - bx0;
-          if (ry < 0 || ry >= hb) continue;
-          if (rx < 0 || rx >= bw) {
-            atomicOr(a.err, kErrBadSlice);
-            continue;
+        for (int k = 0; k < 4; ++k) {
+          const int64_t p = base + k * kDepThreads + tid;
+          bool take = false;
+          if (p < p1) {
+            const float2 xy = a.xy[p];
+            int ix, iy;
+            float wx, wy;
+            take = cell_f(mf, xy.x, xy.y, ix, iy, wx, wy) && iy + 1 >= ylo && iy < ylo + hb;
           }
-          const int cell = ry * bw + rx;
-          atomicAdd(&acc[2 * cell], (unsigned long long)__double2ll_rn(vre * ws[c]));
-          atomicAdd(&acc[2 * cell + 1], (unsigned long long)__double2ll_rn(vim * ws[c]));
+          const unsigned m = __ballot_sync(0xffffffffu, take);
+          int wbase = 0;
+          if (l == 0 && m) wbase = atomicAdd(&qcount, __popc(m));
+          wbase = __shfl_sync(0xffffffffu, wbase, 0);
+          if (take) queue[wbase + __popc(m & ((1u << l) - 1))] = (int)(p - p0);
         }
+        __syncthreads();
+        const int nq = qcount;
+        // 2. deposit the queued particles (dense)
+        for (int e = tid; e < nq; e += kDepThreads) {
+          const int64_t p = p0 + queue[e];
+          const float2 xy = a.xy[p];
+          int ix, iy;
+          float wx, wy;
+          cell_f(mf, xy.x, xy.y, ix, iy, wx, wy);
+          const float dxu = xy.x - a.ax, dyu = xy.y - a.ay;
+          const float faw2 = 1.0f + a.kx * dxu * dxu + a.ky * dyu * dyu +
+                             2.0f * (a.gradx * dxu + a.grady * dyu);
+          double q = (double)sqrtf(faw2) / (a.gref + (double)a.dg[p]);
+          if (!(fabs(q) <= a.qbound)) {
+            atomicOr(a.err, kErrFixedRange);
+            q = 0.0;
+          }
+          float sn, cs;
+          sincosf(reduce_angle((double)fh * a.th[p]), &sn, &cs);
+          const double vre = (double)sn * q * a.fixed_scale;
+          const double vim = (double)cs * q * a.fixed_scale;
+          const float ws[4] = {wx * wy, (1.f - wx) * wy, wx * (1.f - wy),
+                               (1.f - wx) * (1.f - wy)};
+          const int cx[4] = {ix, ix + 1, ix, ix + 1};
+          const int cy[4] = {iy, iy, iy + 1, iy + 1};
+#pragma unroll
+          for (int c = 0; c < 4; ++c) {
+            const int ry = cy[c] - ylo, rx = cx[c] - bx0;
+            if (ry < 0 || ry >= hb) continue;
+            if (rx < 0 || rx >= bw) {
+              atomicOr(a.err, kErrBadSlice);
+              continue;
+            }
+            const long long cr = __double2ll_rn(vre * ws[c]);
+            const long long ci = __double2ll_rn(vim * ws[c]);
+            unsigned int* w4 = acc32 + 4 * (ry * bw + rx);
+            atomicAdd(reinterpret_cast<int*>(w4), (int)(cr >> 16));
+            atomicAdd(w4 + 1, (unsigned int)(cr & 0xffff));
+            atomicAdd(reinterpret_cast<int*>(w4 + 2), (int)(ci >> 16));
+            atomicAdd(w4 + 3, (unsigned int)(ci & 0xffff));
+          }
+        }
+        __syncthreads();
+        if (tid == 0) qcount = 0;
+        __syncthreads();
       }
-      __syncthreads();
       float2* out = F.src + (size_t)target * F.cap + (size_t)(row0 + yb) * bw;
-      for (int i = tid; i < hb * bw; i += kDepThreads)
-        out[i] = make_float2((float)((double)(long long)acc[2 * i] * unscale),
-                             (float)((double)(long long)acc[2 * i + 1] * unscale));
+      for (int i = tid; i < hb * bw; i += kDepThreads) {
+        const unsigned int* w4 = acc32 + 4 * i;
+        const long long vr = (long long)(int)w4[0] * 65536 + (long long)w4[1];
+        const long long vi = (long long)(int)w4[2] * 65536 + (long long)w4[3];
+        out[i] = make_float2((float)((double)vr * unscale), (float)((double)vi * unscale));
+      }
     }
   }
 }
@@ -1021,11 +1062,15 @@ int g4b_run_create(g4b_ctx* c, const g4b_run_desc* d, const int64_t* off, g4b_ru
   }
   r->step_doubles = (size_t)d->nslice * (r->rec_beam + 9 * d->nfield);
   // fixed point of the deposition: |q| = sqrt(faw2)/gamma <= 4/gamma_ref,
-  // slice sums <= max_np * qbound < 2^62
+  // slice sums <= max_np * qbound < 2^46 (split 32-bit accumulation)
   r->qbound = 4.0 / d->gamma_ref;
+  if (r->max_np > 65536) {
+    g4b_run_destroy(r);
+    return fail(G4B_ERR_RANGE, "g4b_run_create: more than 65536 particles in a slice");
+  }
   int ex;
   std::frexp((double)std::max<int64_t>(r->max_np, 1) * r->qbound, &ex);
-  r->fixed_scale = std::ldexp(1.0, 62 - ex);
+  r->fixed_scale = std::ldexp(1.0, 46 - ex);  // slice sums < 2^46
   cudaFuncSetAttribute(deposit_diag_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)kDepAccBytes);
   cudaFuncSetAttribute(deposit_diag_kernel<kMaxBunch>,
