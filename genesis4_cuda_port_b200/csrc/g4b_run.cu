@@ -550,63 +550,51 @@ __global__ void __launch_bounds__(kDepThreads, NB == 1 ? 3 : 2) deposit_diag_ker
         }
         __syncthreads();
         const int nq = qcount;
-        // 2. deposit the queued particles (dense).  Lanes holding particles of
-        // the same cell (quiet-start beamlets are adjacent) sum their
-        // contributions with warp reductions; one leader per cell does the
-        // shared-memory atomics.
-        for (int e0 = w * 32; e0 < nq; e0 += kDepThreads) {
-          const int e = e0 + l;
-          const bool valid = e < nq;
-          int ix = 0, iy = 0;
-          float wx = 0.f, wy = 0.f;
-          double vre = 0.0, vim = 0.0;
-          if (valid) {
-            const int64_t p = p0 + queue[e];
-            const float2 xy = a.xy[p];
-            cell_f(mf, xy.x, xy.y, ix, iy, wx, wy);
-            const float dxu = xy.x - a.ax, dyu = xy.y - a.ay;
-            const float faw2 = 1.0f + a.kx * dxu * dxu + a.ky * dyu * dyu +
-                               2.0f * (a.gradx * dxu + a.grady * dyu);
-            double q = (double)sqrtf(faw2) / (a.gref + (double)a.dg[p]);
-            if (!(fabs(q) <= a.qbound)) {
-              atomicOr(a.err, kErrFixedRange);
-              q = 0.0;
-            }
-            float sn, cs;
-            sincosf(reduce_angle((double)fh * a.th[p]), &sn, &cs);
-            vre = (double)sn * q * a.fixed_scale;
-            vim = (double)cs * q * a.fixed_scale;
+        // 2. deposit the queued particles (dense).  Quiet-start beamlets put
+        // up to 4 particles of one cell at adjacent queue entries; each warp
+        // takes 128 entries with lane l handling e0 + 4l + k in pass k, so
+        // the members of a beamlet never meet in one atomic instruction.
+        for (int e0 = (tid >> 5) * 128; e0 < nq; e0 += kDepThreads * 4)
+#pragma unroll 1
+        for (int k = 0; k < 4; ++k) {
+          const int e = e0 + 4 * (tid & 31) + k;
+          if (e >= nq) continue;
+          const int64_t p = p0 + queue[e];
+          const float2 xy = a.xy[p];
+          int ix, iy;
+          float wx, wy;
+          cell_f(mf, xy.x, xy.y, ix, iy, wx, wy);
+          const float dxu = xy.x - a.ax, dyu = xy.y - a.ay;
+          const float faw2 = 1.0f + a.kx * dxu * dxu + a.ky * dyu * dyu +
+                             2.0f * (a.gradx * dxu + a.grady * dyu);
+          double q = (double)sqrtf(faw2) / (a.gref + (double)a.dg[p]);
+          if (!(fabs(q) <= a.qbound)) {
+            atomicOr(a.err, kErrFixedRange);
+            q = 0.0;
           }
-          const int key = valid ? iy * F.n + ix : -1 - l;
-          const unsigned grp = __match_any_sync(0xffffffffu, key);
-          const bool leader = (int)(__ffs(grp) - 1) == l;
-          const float ws[4] = {wx * wy, (1.f - wx) * wy, wx * (1.f - wy), (1.f - wx) * (1.f - wy)};
+          float sn, cs;
+          sincosf(reduce_angle((double)fh * a.th[p]), &sn, &cs);
+          const double vre = (double)sn * q * a.fixed_scale;
+          const double vim = (double)cs * q * a.fixed_scale;
+          const float ws[4] = {wx * wy, (1.f - wx) * wy, wx * (1.f - wy),
+                               (1.f - wx) * (1.f - wy)};
           const int cx[4] = {ix, ix + 1, ix, ix + 1};
           const int cy[4] = {iy, iy, iy + 1, iy + 1};
 #pragma unroll
           for (int c = 0; c < 4; ++c) {
             const int ry = cy[c] - ylo, rx = cx[c] - bx0;
-            const bool in = valid && ry >= 0 && ry < hb;  // same for the whole group
-            long long cr = 0, ci = 0;
-            if (in) {
-              cr = __double2ll_rn(vre * ws[c]);
-              ci = __double2ll_rn(vim * ws[c]);
+            if (ry < 0 || ry >= hb) continue;
+            if (rx < 0 || rx >= bw) {
+              atomicOr(a.err, kErrBadSlice);
+              continue;
             }
-            const int rh = __reduce_add_sync(grp, (int)(cr >> 16));
-            const unsigned rl = __reduce_add_sync(grp, (unsigned)(cr & 0xffff));
-            const int ih = __reduce_add_sync(grp, (int)(ci >> 16));
-            const unsigned il = __reduce_add_sync(grp, (unsigned)(ci & 0xffff));
-            if (leader && in) {
-              if (rx < 0 || rx >= bw) {
-                atomicOr(a.err, kErrBadSlice);
-                continue;
-              }
-              unsigned int* w4 = acc32 + 4 * (ry * bw + rx);
-              atomicAdd(reinterpret_cast<int*>(w4), rh);
-              atomicAdd(w4 + 1, rl);
-              atomicAdd(reinterpret_cast<int*>(w4 + 2), ih);
-              atomicAdd(w4 + 3, il);
-            }
+            const long long cr = __double2ll_rn(vre * ws[c]);
+            const long long ci = __double2ll_rn(vim * ws[c]);
+            unsigned int* w4 = acc32 + 4 * (ry * bw + rx);
+            atomicAdd(reinterpret_cast<int*>(w4), (int)(cr >> 16));
+            atomicAdd(w4 + 1, (unsigned int)(cr & 0xffff));
+            atomicAdd(reinterpret_cast<int*>(w4 + 2), (int)(ci >> 16));
+            atomicAdd(w4 + 3, (unsigned int)(ci & 0xffff));
           }
         }
         __syncthreads();
