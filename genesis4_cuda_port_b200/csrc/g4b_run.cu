@@ -379,7 +379,8 @@ struct DepDiagArgs {
 // kernel adds the quarters in order.
 constexpr int kDepBands = 4;
 constexpr int kDepThreads = 256;
-constexpr size_t kDepAccBytes = 64 * 1024;  // per CTA: 4096 cells
+constexpr size_t kDepAccBytes = 54 * 1024;  // per CTA: 3456 cells
+constexpr int kDepQueue = 8192;             // particles scanned per batch
 
 // NB: bunching harmonics accumulated (1, or up to kMaxBunch)
 template <int NB>
@@ -487,7 +488,7 @@ __global__ void __launch_bounds__(kDepThreads, NB == 1 ? 3 : 2) deposit_diag_ker
   // (sum lo < 2^32 for <= 65536 contributions per cell) and the cell value is
   // hi * 2^16 + lo.
   __shared__ int qcount;
-  __shared__ int queue[kDepThreads * 4];
+  __shared__ unsigned short queue[kDepQueue];  // offsets within the batch
   const double npd = (double)np;
   const int acc_cells = (int)(kDepAccBytes / 16);
   unsigned int* acc32 = reinterpret_cast<unsigned int*>(smem);
@@ -530,14 +531,14 @@ __global__ void __launch_bounds__(kDepThreads, NB == 1 ? 3 : 2) deposit_diag_ker
       for (int i = tid; i < 4 * hb * bw; i += kDepThreads) acc32[i] = 0u;
       if (tid == 0) qcount = 0;
       __syncthreads();
-      for (int64_t base = p0; base < p1; base += 4 * kDepThreads) {
+      for (int64_t base = p0; base < p1; base += kDepQueue) {
+        const int cnt = (int)min<int64_t>(kDepQueue, p1 - base);
         // 1. queue the particles with a corner in this pass's rows
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-          const int64_t p = base + k * kDepThreads + tid;
+        for (int i0 = 0; i0 < cnt; i0 += kDepThreads) {
+          const int i = i0 + tid;
           bool take = false;
-          if (p < p1) {
-            const float2 xy = a.xy[p];
+          if (i < cnt) {
+            const float2 xy = a.xy[base + i];
             int ix, iy;
             float wx, wy;
             take = cell_f(mf, xy.x, xy.y, ix, iy, wx, wy) && iy + 1 >= ylo && iy < ylo + hb;
@@ -546,20 +547,14 @@ __global__ void __launch_bounds__(kDepThreads, NB == 1 ? 3 : 2) deposit_diag_ker
           int wbase = 0;
           if (l == 0 && m) wbase = atomicAdd(&qcount, __popc(m));
           wbase = __shfl_sync(0xffffffffu, wbase, 0);
-          if (take) queue[wbase + __popc(m & ((1u << l) - 1))] = (int)(p - p0);
+          if (take) queue[wbase + __popc(m & ((1u << l) - 1))] = (unsigned short)i;
         }
         __syncthreads();
         const int nq = qcount;
-        // 2. deposit the queued particles (dense).  Quiet-start beamlets put
-        // up to 4 particles of one cell at adjacent queue entries; each warp
-        // takes 128 entries with lane l handling e0 + 4l + k in pass k, so
-        // the members of a beamlet never meet in one atomic instruction.
-        for (int e0 = (tid >> 5) * 128; e0 < nq; e0 += kDepThreads * 4)
-#pragma unroll 1
-        for (int k = 0; k < 4; ++k) {
-          const int e = e0 + 4 * (tid & 31) + k;
-          if (e >= nq) continue;
-          const int64_t p = p0 + queue[e];
+        // 2. deposit the queued particles (dense, independent iterations)
+#pragma unroll 2
+        for (int e = tid; e < nq; e += kDepThreads) {
+          const int64_t p = base + queue[e];
           const float2 xy = a.xy[p];
           int ix, iy;
           float wx, wy;
