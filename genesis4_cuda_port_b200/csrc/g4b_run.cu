@@ -379,8 +379,7 @@ struct DepDiagArgs {
 // kernel adds the quarters in order.
 constexpr int kDepBands = 4;
 constexpr int kDepThreads = 256;
-constexpr size_t kDepAccBytes = 54 * 1024;  // per CTA: 3456 cells
-constexpr int kDepQueue = 8192;             // particles scanned per batch
+constexpr size_t kDepAccBytes = 64 * 1024;  // per CTA: 4096 cells
 
 // NB: bunching harmonics accumulated (1, or up to kMaxBunch)
 template <int NB>
@@ -488,7 +487,7 @@ __global__ void __launch_bounds__(kDepThreads, NB == 1 ? 3 : 2) deposit_diag_ker
   // (sum lo < 2^32 for <= 65536 contributions per cell) and the cell value is
   // hi * 2^16 + lo.
   __shared__ int qcount;
-  __shared__ unsigned short queue[kDepQueue];  // offsets within the batch
+  __shared__ int queue[kDepThreads * 4];
   const double npd = (double)np;
   const int acc_cells = (int)(kDepAccBytes / 16);
   unsigned int* acc32 = reinterpret_cast<unsigned int*>(smem);
@@ -531,14 +530,14 @@ __global__ void __launch_bounds__(kDepThreads, NB == 1 ? 3 : 2) deposit_diag_ker
       for (int i = tid; i < 4 * hb * bw; i += kDepThreads) acc32[i] = 0u;
       if (tid == 0) qcount = 0;
       __syncthreads();
-      for (int64_t base = p0; base < p1; base += kDepQueue) {
-        const int cnt = (int)min<int64_t>(kDepQueue, p1 - base);
+      for (int64_t base = p0; base < p1; base += 4 * kDepThreads) {
         // 1. queue the particles with a corner in this pass's rows
-        for (int i0 = 0; i0 < cnt; i0 += kDepThreads) {
-          const int i = i0 + tid;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          const int64_t p = base + k * kDepThreads + tid;
           bool take = false;
-          if (i < cnt) {
-            const float2 xy = a.xy[base + i];
+          if (p < p1) {
+            const float2 xy = a.xy[p];
             int ix, iy;
             float wx, wy;
             take = cell_f(mf, xy.x, xy.y, ix, iy, wx, wy) && iy + 1 >= ylo && iy < ylo + hb;
@@ -547,14 +546,13 @@ __global__ void __launch_bounds__(kDepThreads, NB == 1 ? 3 : 2) deposit_diag_ker
           int wbase = 0;
           if (l == 0 && m) wbase = atomicAdd(&qcount, __popc(m));
           wbase = __shfl_sync(0xffffffffu, wbase, 0);
-          if (take) queue[wbase + __popc(m & ((1u << l) - 1))] = (unsigned short)i;
+          if (take) queue[wbase + __popc(m & ((1u << l) - 1))] = (int)(p - p0);
         }
         __syncthreads();
         const int nq = qcount;
-        // 2. deposit the queued particles (dense, independent iterations)
-#pragma unroll 2
+        // 2. deposit the queued particles (dense)
         for (int e = tid; e < nq; e += kDepThreads) {
-          const int64_t p = base + queue[e];
+          const int64_t p = p0 + queue[e];
           const float2 xy = a.xy[p];
           int ix, iy;
           float wx, wy;
