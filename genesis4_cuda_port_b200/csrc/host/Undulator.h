@@ -42,7 +42,12 @@ class Undulator {
   double autophase() const { return steps[istep_].st.autophase; }
   double slippage() const { return steps[istep_].slip; }
   double getz() const { return istep_ < 0 ? 0.0 : steps[istep_].z; }
-  int getMarker() const { return istep_ < 0 ? 0 : steps[istep_].marker; }
+  // markers acting at the start of the current step: those placed after the
+  // previous step (after the loop: those after the last step)
+  int getMarker() const {
+    const int k = istep_ < (int)steps.size() ? istep_ : (int)steps.size();
+    return k <= 0 ? 0 : steps[k - 1].marker;
+  }
   bool outstep() const { return ((istep_ + 1) % output_step) == 0 || istep_ + 1 == nstep(); }
   int outlength() const { return 1 + (nstep() + output_step - 1) / output_step; }
   double fc(int harm) const;

@@ -31,6 +31,20 @@ class BeamSpec(C.Structure):
             setattr(self, k, v)
 
 
+class DeckSummary(C.Structure):
+    """Mirror of ``g4h_deck_summary``."""
+
+    _fields_ = [("nslice", C.c_int), ("npart", C.c_int), ("nstep", C.c_int),
+                ("nfield", C.c_int), ("harm", C.c_int * 8), ("ngrid", C.c_int * 8),
+                ("gridmax", C.c_double * 8), ("lambda0", C.c_double),
+                ("gamma0", C.c_double), ("sample", C.c_double), ("time_run", C.c_int),
+                ("periodic", C.c_int), ("precision", C.c_int), ("low_memory", C.c_int),
+                ("output_step", C.c_int), ("nout", C.c_int), ("bunchharm", C.c_int),
+                ("nrun", C.c_int), ("betax", C.c_double), ("alphax", C.c_double),
+                ("betay", C.c_double), ("alphay", C.c_double), ("current", C.c_double),
+                ("zend", C.c_double)]
+
+
 _h = None
 
 
@@ -57,6 +71,17 @@ def load():
     h.g4h_lattice_fc.argtypes = [C.c_void_p, C.c_int, C.c_int, _lib.c_double_p]
     h.g4h_coupling.restype = C.c_double
     h.g4h_coupling.argtypes = [C.c_double, C.c_int, C.c_int]
+    h.g4h_deck_parse.argtypes = [C.c_char_p, C.c_char_p, C.c_char_p, _lib.c_void_pp]
+    h.g4h_deck_destroy.argtypes = [C.c_void_p]
+    h.g4h_deck_info.argtypes = [C.c_void_p, C.POINTER(DeckSummary)]
+    h.g4h_deck_run.argtypes = [C.c_void_p, _lib.c_void_pp]
+    h.g4h_result_destroy.argtypes = [C.c_void_p]
+    h.g4h_result_info.argtypes = [C.c_void_p, _lib.c_int_p, _lib.c_int_p, _lib.c_int_p,
+                                  _lib.c_int_p, _lib.c_double_p]
+    h.g4h_result_keys.argtypes = [C.c_void_p, C.c_int, C.c_char_p, C.c_int, _lib.c_int_p]
+    h.g4h_result_get.argtypes = [C.c_void_p, C.c_int, C.c_char_p, _lib.c_double_p,
+                                 C.c_int64, _lib.c_int64_p]
+    h.g4h_result_field.argtypes = [C.c_void_p, C.c_int, _lib.c_double_p, _lib.c_int_p]
     _h = h
     return h
 
@@ -123,6 +148,95 @@ class Lattice:
         try:
             if getattr(self, "h", None):
                 load().g4h_lattice_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+
+class Deck:
+    """An input deck (.in namelists + .lat beamline), parsed and expanded on
+    the host; ``run()`` executes its &track on the GPU (Gencore::run with the
+    CUDA classes, or the fused mixed-precision run for ``precision = mixed``)."""
+
+    def __init__(self, text: str, lattice: str | None = None, base_dir: str | None = None):
+        h = C.c_void_p()
+        _check(load().g4h_deck_parse(text.encode(), lattice.encode() if lattice is not None
+                                     else None, (base_dir or "").encode(), C.byref(h)))
+        self.h = h
+        s = DeckSummary()
+        _check(load().g4h_deck_info(h, C.byref(s)))
+        self.summary = s
+
+    @classmethod
+    def from_file(cls, path: str):
+        p = Path(path)
+        return cls(p.read_text(), None, str(p.parent))
+
+    def info(self) -> dict:
+        s = self.summary
+        d = {k: getattr(s, k) for k, _ in DeckSummary._fields_ }
+        for k in ("harm", "ngrid", "gridmax"):
+            d[k] = list(d[k])[: s.nfield]
+        return d
+
+    def run(self) -> "Result":
+        r = C.c_void_p()
+        _check(load().g4h_deck_run(self.h, C.byref(r)))
+        return Result(r)
+
+    def __del__(self):
+        try:
+            if getattr(self, "h", None):
+                load().g4h_deck_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+
+class Result:
+    """Diagnostics of one deck run: ``beam[key]`` and ``field[i][key]`` are
+    arrays shaped (nz, nslice) for per-slice records and (nz,) for Global/
+    records, as DiagnosticCUDA::calcBeam / calcField fill them."""
+
+    def __init__(self, h):
+        self.h = h
+        nz, ns, nf, nst, sec = C.c_int(), C.c_int(), C.c_int(), C.c_int(), C.c_double()
+        _check(load().g4h_result_info(h, C.byref(nz), C.byref(ns), C.byref(nf), C.byref(nst),
+                                      C.byref(sec)))
+        self.nz, self.nslice, self.nfield = nz.value, ns.value, nf.value
+        self.nsteps, self.seconds = nst.value, sec.value
+        self.z = self._get(-1, "z")
+        self.beam = self._group(0)
+        self.field = [self._group(i + 1) for i in range(self.nfield)]
+
+    def _get(self, group, key):
+        n = C.c_int64()
+        _check(load().g4h_result_get(self.h, group, key.encode(), None, 0, C.byref(n)))
+        out = np.empty(n.value)
+        _check(load().g4h_result_get(self.h, group, key.encode(), dptr(out), n.value, None))
+        if group < 0 or key.startswith("Global/") or key in ("dgrid", "gridspacing", "ngrid"):
+            return out
+        return out.reshape(self.nz, self.nslice)
+
+    def _group(self, g):
+        need = C.c_int()
+        _check(load().g4h_result_keys(self.h, g, None, 0, C.byref(need)))
+        buf = C.create_string_buffer(need.value)
+        _check(load().g4h_result_keys(self.h, g, buf, need.value, None))
+        return {k: self._get(g, k) for k in buf.value.decode().split("\n") if k}
+
+    def final_field(self, i: int = 0):
+        ngrid = int(self.field[i]["ngrid"][0])
+        out = np.empty((self.nslice, ngrid, ngrid), np.complex128)
+        first = C.c_int()
+        _check(load().g4h_result_field(self.h, i, dptr(out.reshape(-1).view(np.float64)),
+                                       C.byref(first)))
+        return out, first.value
+
+    def __del__(self):
+        try:
+            if getattr(self, "h", None):
+                load().g4h_result_destroy(self.h)
                 self.h = None
         except Exception:
             pass

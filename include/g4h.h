@@ -76,6 +76,48 @@ int g4h_lattice_fc(g4h_lattice* lat, int i, int harm, double* fc);
 /* Planar / helical coupling factor aw * JJ_h (upstream Undulator::fc). */
 double g4h_coupling(double aw, int harm, int helical);
 
+/* ---- input decks and the Track driver ------------------------------------
+ * g4h_deck_parse reads a .in deck (&setup, &lattice, &time, &field..., &beam,
+ * &track; the reference's &track keys, src/Main/Track.cpp:8-104, plus
+ * `precision = fp64 | mixed`) and expands its lattice (lattice_text, or the
+ * file &setup names, relative to base_dir).  Parsing needs no GPU.
+ * g4h_deck_run then loads the beam and fields and runs Gencore::run
+ * (src/Core/Gencore.cpp:19-315) with the CUDA classes, or the fused
+ * mixed-precision run; the diagnostics are kept in a g4h_result. */
+typedef struct g4h_deck g4h_deck;
+typedef struct g4h_result g4h_result;
+
+typedef struct g4h_deck_summary {
+  int nslice, npart, nstep, nfield;
+  int harm[8], ngrid[8];
+  double gridmax[8];
+  double lambda0, gamma0, sample;
+  int time_run, periodic, precision, low_memory;
+  int output_step, nout, bunchharm;
+  int nrun;  /* steps taken: up to the first stop marker (zstop) */
+  double betax, alphax, betay, alphay;  /* after &lattice zmatch */
+  double current, zend;
+} g4h_deck_summary;
+
+int g4h_deck_parse(const char* deck_text, const char* lattice_text, const char* base_dir,
+                   g4h_deck** out);
+int g4h_deck_destroy(g4h_deck* deck);
+int g4h_deck_info(g4h_deck* deck, g4h_deck_summary* summary);
+int g4h_deck_run(g4h_deck* deck, g4h_result** out);
+int g4h_result_destroy(g4h_result* res);
+/* nz output records, slices, fields, steps taken, seconds in the loop */
+int g4h_result_info(g4h_result* res, int* nz, int* nslice, int* nfield, int* nsteps,
+                    double* seconds);
+/* Record names of group 0 (beam) or 1..nfield (field i-1), '\n'-separated
+ * (the keys of DiagnosticCUDA::calcBeam / calcField). */
+int g4h_result_keys(g4h_result* res, int group, char* buf, int buflen, int* needed);
+/* One record (group -1, key "z": the output positions); nz*nslice values
+ * for per-slice records, nz for Global/ records. */
+int g4h_result_get(g4h_result* res, int group, const char* key, double* out,
+                   int64_t capacity, int64_t* length);
+/* Final cells of field i (2*nslice*ngrid^2 doubles) and its `first`. */
+int g4h_result_field(g4h_result* res, int ifield, double* cells, int* first);
+
 #ifdef __cplusplus
 }
 #endif
