@@ -155,3 +155,69 @@ def test_quiet_start_bunching_vanishes():
     assert abs(bre[0, 0]) / theta.size < 1e-14 and abs(bim[0, 0]) / theta.size < 1e-14
     assert abs(bre[0, 2]) / theta.size < 1e-13
     assert stats[0, 12] == theta.size
+
+
+def test_uniform_field_push_is_classic_rk4():
+    """In a uniform field the gather returns the same value everywhere, so
+    the step is one classic RK4 step of (gamma, theta) with a frozen
+    coupling: compare with a numpy RK4 of the ODE of
+    src/Core/BeamSolverCUDA.cpp:146-223 (Genesis's accumulator form is the
+    same scheme)."""
+    off, parts = synth.beam(2, 200, seed=8)
+    step = synth.und_step(autophase=0.1)
+    n, gridmax = 17, 200e-6
+    u0 = 4e13 * np.exp(0.7j)
+    cells = np.full((2, n, n), u0, np.complex128)
+    fc = synth.coupling()
+    ks = 2 * np.pi / synth.LAMBDA0
+    fields = [dict(cells=cells, gridmax=gridmax, xlambda=synth.LAMBDA0, fc=fc)]
+    before = synth.copy_parts(parts)
+    orc.push(off, step, fields, parts)
+    x, y, px, py = before["x"], before["y"], before["px"], before["py"]
+    awloc = 1 + 0.5 * (step.kx * x * x + step.ky * y * y)
+    btpar = 1 + px * px + py * py + step.aw ** 2 * awloc ** 2
+    rpart = (fc / ks) * awloc * np.conj(u0)
+
+    def f(g, th):
+        c = rpart * np.exp(-1j * th)
+        b0 = np.sqrt(1 - (btpar - 2 / ks * c.real) / (g * g))
+        return c.imag / b0 / g, ks * (1 - 1 / b0) + step.ku
+
+    g, th = before["gamma"].copy(), before["theta"] + step.autophase
+    h = step.delz
+    k1 = f(g, th)
+    k2 = f(g + h / 2 * k1[0], th + h / 2 * k1[1])
+    k3 = f(g + h / 2 * k2[0], th + h / 2 * k2[1])
+    k4 = f(g + h * k3[0], th + h * k3[1])
+    g1 = g + h / 6 * (k1[0] + 2 * k2[0] + 2 * k3[0] + k4[0])
+    th1 = th + h / 6 * (k1[1] + 2 * k2[1] + 2 * k3[1] + k4[1])
+    inside = (np.abs(x) < gridmax * (1 - 2 / (n - 1))) & (np.abs(y) < gridmax * (1 - 2 / (n - 1)))
+    assert inside.mean() > 0.9
+    assert np.max(np.abs(g1 - before["gamma"])[inside]) > 1e-5  # the field does work
+    np.testing.assert_allclose(parts["gamma"][inside], g1[inside], rtol=1e-13)
+    np.testing.assert_allclose(parts["theta"][inside], th1[inside], rtol=0, atol=1e-9)
+
+
+def test_diagnostic_sums_match_numpy():
+    off, parts = synth.beam(3, 400, seed=9, ragged=True)
+    stats, bre, bim = orc.diag_beam(off, parts, nharm=2)
+    for s in range(3):
+        sl = slice(off[s], off[s + 1])
+        x, px, g, th = parts["x"][sl], parts["px"][sl], parts["gamma"][sl], parts["theta"][sl]
+        ref = [g.sum(), (g * g).sum(), x.sum(), (x * x).sum()]
+        np.testing.assert_allclose(stats[s, :4], ref, rtol=1e-12, atol=1e-300)
+        np.testing.assert_allclose(stats[s, 10], (x * px).sum(), rtol=1e-12, atol=1e-300)
+        assert stats[s, 12] == off[s + 1] - off[s]
+        np.testing.assert_allclose(bre[s, 1], np.cos(2 * th).sum(), rtol=1e-10, atol=1e-10)
+        np.testing.assert_allclose(bim[s, 0], np.sin(th).sum(), rtol=1e-10, atol=1e-10)
+    cells = synth.field(2, 21, 100e-6, seed=10)
+    fs, cen = orc.diag_field(cells, 1)
+    for s0 in range(2):
+        s = (2 + s0 - 1) % 2
+        w = np.abs(cells[s0]) ** 2
+        d = np.arange(21) - 10.0
+        np.testing.assert_allclose(fs[s, 0], w.sum(), rtol=1e-12)
+        np.testing.assert_allclose(fs[s, 1], (w * d[None, :]).sum(), rtol=1e-10, atol=1e-6 * w.sum())
+        np.testing.assert_allclose(fs[s, 4], (w * d[:, None] ** 2).sum(), rtol=1e-12)
+        np.testing.assert_allclose(fs[s, 5] + 1j * fs[s, 6], cells[s0].sum(), rtol=1e-12)
+        np.testing.assert_allclose(cen[s], [cells[s0, 10, 10].real, cells[s0, 10, 10].imag])
