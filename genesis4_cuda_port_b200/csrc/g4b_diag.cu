@@ -4,6 +4,9 @@
 // every moment in registers; reductions run in a fixed order (warp xor tree,
 // then warps in index order), so results are reproducible run to run.
 #include <algorithm>
+#include <atomic>
+#include <mutex>
+#include <string>
 #include <vector>
 
 #include "g4b_internal.cuh"
@@ -226,6 +229,44 @@ int ensure(DiagScratch& s, size_t n) {
 }
 }  // namespace
 
+namespace {
+
+// ---- field diagnostics with fixed scratch ----------------------------------
+// Some callers must not allocate device memory when they ask for the field
+// statistics: a host that hands the device's memory to its own pool and
+// forbids growth during a run, or a loop whose latency budget has no room for
+// cudaMalloc's implicit device-wide synchronisation.  For them the scratch of
+// field_diag_kernel lives in one fixed file-scope device array instead of the
+// grow-on-demand buffer above.  Its size bounds the slices per call.
+constexpr int kStaticDiagMaxSlices = 4096;               // 4096 x 9 doubles = 288 KiB
+static __device__ __align__(256) double g_field_diag_scratch[kStaticDiagMaxSlices * 9];
+
+constexpr int kStaticDiagMaxDevices = 64;
+std::atomic<double*> g_field_diag_scratch_ptr[kStaticDiagMaxDevices];
+std::mutex g_field_diag_scratch_mutex;
+
+// Address of the array on `device` (which must be current).  The first call
+// on a device asks the runtime for the symbol address (which may load the
+// module); later calls read the cached pointer.
+int static_diag_scratch(int device, double** out) {
+  if (device < 0 || device >= kStaticDiagMaxDevices)
+    return fail(G4B_ERR_RANGE, "g4b_diag_field_static: device index above 63");
+  double* p = g_field_diag_scratch_ptr[device].load(std::memory_order_acquire);
+  if (!p) {
+    std::lock_guard<std::mutex> lock(g_field_diag_scratch_mutex);
+    p = g_field_diag_scratch_ptr[device].load(std::memory_order_relaxed);
+    if (!p) {
+      const cudaError_t e = cudaGetSymbolAddress((void**)&p, g_field_diag_scratch);
+      if (e != cudaSuccess) return cuda_fail(e, "g4b_diag_field_static: cudaGetSymbolAddress");
+      g_field_diag_scratch_ptr[device].store(p, std::memory_order_release);
+    }
+  }
+  *out = p;
+  return G4B_OK;
+}
+
+}  // namespace
+
 extern "C" {
 
 int g4b_diag_beam(g4b_beam* b, int nharm, int need_aux, double* stats, double* bre,
@@ -279,6 +320,40 @@ int g4b_diag_field(g4b_field* f, double* stats, double* center) {
           f->nslice, f->ngrid, f->ld, f->first, static_cast<const float2*>(f->a), d_stats,
           d_center);
   }
+  if (int rc = check_launch(c, "field_diag_kernel")) return rc;
+  G4B_CUDA_TRY(cudaMemcpyAsync(stats, d_stats, ns * 7 * sizeof(double),
+                               cudaMemcpyDeviceToHost, c->stream));
+  G4B_CUDA_TRY(cudaMemcpyAsync(center, d_center, ns * 2 * sizeof(double),
+                               cudaMemcpyDeviceToHost, c->stream));
+  G4B_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return G4B_OK;
+}
+
+// Same statistics as g4b_diag_field, with the device scratch in a fixed
+// file-scope array: nothing is allocated on the device or through the CUDA
+// runtime's allocators.  Every scratch entry the call reads back is written
+// by its own kernel first, so no part of the array has to start at zero.
+int g4b_diag_field_static(g4b_field* f, double* stats, double* center) {
+  if (!f || !stats || !center) return fail(G4B_ERR_ARG, "g4b_diag_field_static: null arg");
+  if (f->nslice > kStaticDiagMaxSlices)
+    return fail(G4B_ERR_RANGE, "g4b_diag_field_static: " + std::to_string(f->nslice) +
+                                   " slices exceed the fixed scratch of " +
+                                   std::to_string(kStaticDiagMaxSlices));
+  g4b_ctx* c = f->ctx;
+  G4B_CUDA_TRY(cudaSetDevice(c->device));
+  double* d_stats = nullptr;
+  if (int rc = static_diag_scratch(c->device, &d_stats)) return rc;
+  const size_t ns = f->nslice;
+  double* d_center = d_stats + ns * 7;
+  if (f->precision == G4B_FP64)
+    field_diag_kernel<double2><<<f->nslice, kDiagThreads, 0, c->stream>>>(
+        f->nslice, f->ngrid, f->ld, f->first, static_cast<const double2*>(f->a), d_stats,
+        d_center);
+  else
+    field_diag_kernel<float2><<<f->nslice, kDiagThreads, 0, c->stream>>>(
+        f->nslice, f->ngrid, f->ld, f->first, static_cast<const float2*>(f->a), d_stats,
+        d_center);
+  count_launch(c);
   if (int rc = check_launch(c, "field_diag_kernel")) return rc;
   G4B_CUDA_TRY(cudaMemcpyAsync(stats, d_stats, ns * 7 * sizeof(double),
                                cudaMemcpyDeviceToHost, c->stream));

@@ -190,6 +190,17 @@ int g4b_diag_beam(g4b_beam* b, int nharm, int need_aux, double* stats,
  * 7 sums (power, x1, x2, y1, y2, ff_re, ff_im) into stats[nslice*7] and the
  * centre cell (ngrid^2-1)/2 into center[nslice*2] (re, im). */
 int g4b_diag_field(g4b_field* f, double* stats, double* center);
+/* g4b_diag_field with no allocation at call time: no counterpart in the
+ * reference (its DiagnosticCUDA grows device buffers on demand,
+ * src/Core/DiagnosticCUDA.cpp:633-648).  The device scratch is one fixed
+ * array in the library, so nslice is limited to 4096 (G4B_ERR_RANGE
+ * beyond).  The first call on a device looks up that array's address (which
+ * may load the module): make it before any stream capture on that device.
+ * No part of the scratch needs to start at zero.  All calls on one device
+ * share the array: calls that overlap in time on the same device (two host
+ * threads, or two contexts on one device) race and must be serialised by the
+ * caller.  Synchronises the context's stream, like g4b_diag_field. */
+int g4b_diag_field_static(g4b_field* f, double* stats, double* center);
 
 /* ---- fused mixed-precision run -------------------------------------------
  * A whole FEL run resident on the device: FP32 particles and complex64
