@@ -11,7 +11,7 @@
 //                  (+corrector), and each slice's bounding box of touched
 //                  cells (integer atomics, order independent);
 //   K2 deposit_diag : per slice, the beam diagnostics (FP64 sums) and the
-//                  deterministic int64 fixed-point deposition of every field's
+//                  deterministic exact-integer deposition of every field's
 //                  source into a compact tile;
 //   K3/K4 ADI passes per field (pass Y also zeroes the planes this step's
 //                  slippage zeroes and writes field-diagnostic partials);
@@ -362,42 +362,53 @@ struct DepDiagArgs {
   const int64_t* off;
   const double* current;
   DepField f[kRunFields];
-  int nfield, nbunch, need_aux, acc_cells;
-  float ax, ay, kx, ky, gradx, grady;
-  double gref, delz, fixed_scale, qbound;
-  double* beam_part;  // [nslice * kDepBands][23 + 2*nbunch] partial sums
+  int nfield, nbunch, need_aux;
+  float ax, ay, kx, ky, gradx, grady, gref_f;
+  double gref, delz;
+  double* beam_part;  // [nslice * kDepParts][23 + 2*nbunch] partial sums
   int* err;
 };
 
-// Deposition + beam diagnostics, kDepBands CTAs per slice.  CTA k of a slice
-// owns rows [k*hk, (k+1)*hk) of the slice's source tile (hk = ceil(h/kDepBands))
-// and a fixed-point accumulator for them in its own shared memory; it scans
-// the positions of all the slice's particles (L2-resident after the first of
-// the slice's CTAs) and deposits only the corners that fall in its rows, with
-// shared-memory 64-bit integer atomics (order independent).  CTA k also sums
-// the beam diagnostics of the k-th quarter of the particles; the finalize
-// kernel adds the quarters in order.
-constexpr int kDepBands = 4;
+// Deposition + beam diagnostics, one CTA per slice.
+//
+// The beam diagnostics are FP64 sums over the slice's particles (one pass).
+// The deposition (adi_deposit_source_atomic, FieldSolverADICUDA.cpp:98-174)
+// is a deterministic per-cell reduction in exact integer arithmetic:
+//   1. a first pass counts the particles per base cell (ix, iy) of the tile
+//      and finds the slice's largest charge |q|;
+//   2. the largest number M of contributions any output cell receives (the
+//      sum of the counts of its four base cells) fixes the slice's scale
+//      S = 2^30 / (M qmax), so every contribution rounds to an int32 with
+//      |c| <= 2^30 / M and no cell sum can overflow;
+//   3. a second pass adds each particle's four bilinear contributions
+//      c = rint(S q w (sin h theta, cos h theta)) with 32-bit shared-memory
+//      integer atomics (re and im in separate planes, so the 32 lanes of a
+//      warp spread over the banks).
+// Integer addition is associative, so the source does not depend on the
+// order in which threads add, and each contribution keeps FP32 resolution
+// (2^-24 relative).  The tile is the slice's bounding box of touched cells
+// (from K1); tiles larger than kDepMaxCells are processed in row bands.
+constexpr int kDepParts = 1;          // beam-diagnostic partial records per slice
 constexpr int kDepThreads = 256;
-constexpr size_t kDepAccBytes = 64 * 1024;  // per CTA: 4096 cells
+constexpr int kDepMaxCells = 12288;   // output cells per band
+constexpr size_t kDepSmem = (size_t)kDepMaxCells * 8;
 
 // NB: bunching harmonics accumulated (1, or up to kMaxBunch)
 template <int NB>
-__global__ void __launch_bounds__(kDepThreads, NB == 1 ? 3 : 2) deposit_diag_kernel(const DepDiagArgs a) {
+__global__ void __launch_bounds__(kDepThreads, 2) deposit_diag_kernel(const DepDiagArgs a) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ double dpart[kDepThreads / 32][kBeamRec + 2 * kMaxBunch];
   __shared__ int4 sbox[kRunFields];
-  unsigned long long* acc = reinterpret_cast<unsigned long long*>(smem);
-  const int bs = blockIdx.x / kDepBands, kb = blockIdx.x - bs * kDepBands;
+  __shared__ int wsum[kDepThreads / 32];
+  __shared__ float wmax[kDepThreads / 32];
+  const int bs = blockIdx.x;
   const int tid = threadIdx.x, w = tid >> 5, l = tid & 31;
   const int64_t p0 = a.off[bs], p1 = a.off[bs + 1];
   const int64_t np = p1 - p0;
-  const int64_t q0 = p0 + np * kb / kDepBands, q1 = p0 + np * (kb + 1) / kDepBands;
   const int rec = kBeamRec + 2 * a.nbunch;
   if (tid < a.nfield) sbox[tid] = a.f[tid].bbox[bs];
-  __syncthreads();
 
-  // ---- beam diagnostics of this CTA's quarter (FP64 sums) ----
+  // ---- beam diagnostics of the slice (FP64 sums) ----
   {
     double v[kBeamRec];
 #pragma unroll
@@ -409,7 +420,7 @@ __global__ void __launch_bounds__(kDepThreads, NB == 1 ? 3 : 2) deposit_diag_ker
     double bre[NB], bim[NB];
 #pragma unroll
     for (int h = 0; h < NB; ++h) bre[h] = bim[h] = 0.0;
-    for (int64_t p = q0 + tid; p < q1; p += kDepThreads) {
+    for (int64_t p = p0 + tid; p < p1; p += kDepThreads) {
       const float2 xy = a.xy[p], pp = a.pxy[p];
       const double x = xy.x, y = xy.y, px = pp.x, py = pp.y;
       const double dgv = a.dg[p];
@@ -476,21 +487,15 @@ __global__ void __launch_bounds__(kDepThreads, NB == 1 ? 3 : 2) deposit_diag_ker
         t = op == 0 ? t + u : (op == 1 ? fmin(t, u) : fmax(t, u));
       }
       if (tid >= 13 && tid < kBeamRec && !a.need_aux) t = 0.0;
-      a.beam_part[(size_t)blockIdx.x * rec + tid] = t;
+      a.beam_part[(size_t)bs * rec + tid] = t;
     }
   }
 
   // ---- deposition of every field with a source this step ----
-  // Accumulator: per cell re_hi, re_lo, im_hi, im_lo (32-bit words); a
-  // fixed-point contribution c (|c| < 2^46) is added as hi = c >> 16 (signed)
-  // and lo = c & 0xffff with native 32-bit atomics: the sums stay exact
-  // (sum lo < 2^32 for <= 65536 contributions per cell) and the cell value is
-  // hi * 2^16 + lo.
-  __shared__ int qcount;
-  __shared__ int queue[kDepThreads * 4];
+  int* are = reinterpret_cast<int*>(smem);        // [hb * bw] real parts
+  int* aim = are + kDepMaxCells;                  // [hb * bw] imaginary parts
+  int* hist = are;  // step 1: counts per base cell, (hb + 1) * bw <= 2 kDepMaxCells
   const double npd = (double)np;
-  const int acc_cells = (int)(kDepAccBytes / 16);
-  unsigned int* acc32 = reinterpret_cast<unsigned int*>(smem);
   for (int fi = 0; fi < a.nfield; ++fi) {
     const DepField& F = a.f[fi];
     if (!F.do_source) continue;
@@ -503,7 +508,7 @@ __global__ void __launch_bounds__(kDepThreads, NB == 1 ? 3 : 2) deposit_diag_ker
       scl /= 4.0 * 510998.95 * npd * F.dgrid_d * F.dgrid_d;
     }
     if (bb.z < 0 || scl == 0.0) {
-      if (kb == 0 && tid == 0) F.desc[target] = make_int4(0, 0, 0, 0);
+      if (tid == 0) F.desc[target] = make_int4(0, 0, 0, 0);
       continue;
     }
     int bx0 = bb.x, bw = bb.z - bb.x + 2;
@@ -512,95 +517,112 @@ __global__ void __launch_bounds__(kDepThreads, NB == 1 ? 3 : 2) deposit_diag_ker
       ++bw;
       if (bx0 + bw > F.ld) --bx0;
     }
-    if (kb == 0 && tid == 0) F.desc[target] = make_int4(bx0, by0, bw, bh);
-    const int hk = (bh + kDepBands - 1) / kDepBands;   // tile rows owned by this CTA
-    const int row0 = kb * hk, nrow = max(0, min(hk, bh - row0));
-    const int band = max(1, min(max(nrow, 1), acc_cells / bw));
-    const double unscale = scl / a.fixed_scale;
+    if (tid == 0) F.desc[target] = make_int4(bx0, by0, bw, bh);
+    const int hband = max(1, kDepMaxCells / bw);
     const float fh = (float)F.harm;
     MixField mf;
     mf.gridmax = F.gridmax;
     mf.dgrid = F.dgrid;
     mf.inv_dgrid = F.inv_dgrid;
     mf.n = F.n;
-    for (int yb = 0; yb < nrow; yb += band) {
-      const int hb = min(band, nrow - yb);
-      const int ylo = by0 + row0 + yb;  // first grid row of this pass
+    for (int yb = 0; yb < bh; yb += hband) {
+      const int hb = min(hband, bh - yb);
+      const int ylo = by0 + yb;  // first grid row of this band
+      const int nout = hb * bw, nbase = (hb + 1) * bw;
       __syncthreads();
-      for (int i = tid; i < 4 * hb * bw; i += kDepThreads) acc32[i] = 0u;
-      if (tid == 0) qcount = 0;
+      for (int i = tid; i < nbase; i += kDepThreads) hist[i] = 0;
       __syncthreads();
-      for (int64_t base = p0; base < p1; base += 4 * kDepThreads) {
-        // 1. queue the particles with a corner in this pass's rows
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-          const int64_t p = base + k * kDepThreads + tid;
-          bool take = false;
-          if (p < p1) {
-            const float2 xy = a.xy[p];
-            int ix, iy;
-            float wx, wy;
-            take = cell_f(mf, xy.x, xy.y, ix, iy, wx, wy) && iy + 1 >= ylo && iy < ylo + hb;
-          }
-          const unsigned m = __ballot_sync(0xffffffffu, take);
-          int wbase = 0;
-          if (l == 0 && m) wbase = atomicAdd(&qcount, __popc(m));
-          wbase = __shfl_sync(0xffffffffu, wbase, 0);
-          if (take) queue[wbase + __popc(m & ((1u << l) - 1))] = (int)(p - p0);
+      // 1. counts per base cell (ext row iy - ylo + 1) and the largest |q|
+      float qmax = 0.f;
+      for (int64_t p = p0 + tid; p < p1; p += kDepThreads) {
+        const float2 xy = a.xy[p];
+        int ix, iy;
+        float wx, wy;
+        if (!cell_f(mf, xy.x, xy.y, ix, iy, wx, wy) || iy + 1 < ylo || iy >= ylo + hb) continue;
+        const int ex = ix - bx0, ey = iy - ylo + 1;
+        if (ex < 0 || ex > bw - 2) {
+          atomicOr(a.err, kErrBadSlice);
+          continue;
         }
-        __syncthreads();
-        const int nq = qcount;
-        // 2. deposit the queued particles (dense)
-        for (int e = tid; e < nq; e += kDepThreads) {
-          const int64_t p = p0 + queue[e];
-          const float2 xy = a.xy[p];
-          int ix, iy;
-          float wx, wy;
-          cell_f(mf, xy.x, xy.y, ix, iy, wx, wy);
-          const float dxu = xy.x - a.ax, dyu = xy.y - a.ay;
-          const float faw2 = 1.0f + a.kx * dxu * dxu + a.ky * dyu * dyu +
-                             2.0f * (a.gradx * dxu + a.grady * dyu);
-          double q = (double)sqrtf(faw2) / (a.gref + (double)a.dg[p]);
-          if (!(fabs(q) <= a.qbound)) {
-            atomicOr(a.err, kErrFixedRange);
-            q = 0.0;
-          }
-          float sn, cs;
-          sincosf(reduce_angle((double)fh * a.th[p]), &sn, &cs);
-          const double vre = (double)sn * q * a.fixed_scale;
-          const double vim = (double)cs * q * a.fixed_scale;
-          const float ws[4] = {wx * wy, (1.f - wx) * wy, wx * (1.f - wy),
-                               (1.f - wx) * (1.f - wy)};
-          const int cx[4] = {ix, ix + 1, ix, ix + 1};
-          const int cy[4] = {iy, iy, iy + 1, iy + 1};
-#pragma unroll
-          for (int c = 0; c < 4; ++c) {
-            const int ry = cy[c] - ylo, rx = cx[c] - bx0;
-            if (ry < 0 || ry >= hb) continue;
-            if (rx < 0 || rx >= bw) {
-              atomicOr(a.err, kErrBadSlice);
-              continue;
-            }
-            const long long cr = __double2ll_rn(vre * ws[c]);
-            const long long ci = __double2ll_rn(vim * ws[c]);
-            unsigned int* w4 = acc32 + 4 * (ry * bw + rx);
-            atomicAdd(reinterpret_cast<int*>(w4), (int)(cr >> 16));
-            atomicAdd(w4 + 1, (unsigned int)(cr & 0xffff));
-            atomicAdd(reinterpret_cast<int*>(w4 + 2), (int)(ci >> 16));
-            atomicAdd(w4 + 3, (unsigned int)(ci & 0xffff));
-          }
+        atomicAdd(&hist[ey * bw + ex], 1);
+        const float dxu = xy.x - a.ax, dyu = xy.y - a.ay;
+        const float faw2 = 1.0f + a.kx * dxu * dxu + a.ky * dyu * dyu +
+                           2.0f * (a.gradx * dxu + a.grady * dyu);
+        qmax = fmaxf(qmax, sqrtf(faw2) / (a.gref_f + a.dg[p]));
+      }
+      __syncthreads();
+      // 2. M = max over output cells of the contributions it receives
+      int mloc = 0;
+      for (int o = tid; o < nout; o += kDepThreads) {
+        const int r = o / bw, x = o - r * bw;
+        int m = hist[(r + 1) * bw + x] + hist[r * bw + x];
+        if (x > 0) m += hist[(r + 1) * bw + x - 1] + hist[r * bw + x - 1];
+        mloc = max(mloc, m);
+      }
+      for (int o = 16; o > 0; o >>= 1) {
+        mloc = max(mloc, __shfl_xor_sync(0xffffffffu, mloc, o));
+        qmax = fmaxf(qmax, __shfl_xor_sync(0xffffffffu, qmax, o));
+      }
+      if (l == 0) {
+        wsum[w] = mloc;
+        wmax[w] = qmax;
+      }
+      __syncthreads();
+      int M = wsum[0];
+      float qm = wmax[0];
+      for (int i = 1; i < kDepThreads / 32; ++i) {
+        M = max(M, wsum[i]);
+        qm = fmaxf(qm, wmax[i]);
+      }
+      float2* out = F.src + (size_t)target * F.cap + (size_t)yb * bw;
+      if (M == 0 || !(qm > 0.f) || !(qm < 3.0e38f)) {
+        if (M > 0) atomicOr(a.err, kErrFixedRange);  // non-finite charge
+        for (int i = tid; i < nout; i += kDepThreads) out[i] = make_float2(0.f, 0.f);
+        continue;
+      }
+      const double S = 1073741824.0 / ((double)M * (double)qm);  // 2^30 / (M qmax)
+      const float Sf = (float)S;
+      for (int i = tid; i < nout; i += kDepThreads) {
+        are[i] = 0;
+        aim[i] = 0;
+      }
+      __syncthreads();
+      // 3. exact integer accumulation of the bilinear contributions
+      for (int64_t p = p0 + tid; p < p1; p += kDepThreads) {
+        const float2 xy = a.xy[p];
+        int ix, iy;
+        float wx, wy;
+        if (!cell_f(mf, xy.x, xy.y, ix, iy, wx, wy) || iy + 1 < ylo || iy >= ylo + hb) continue;
+        const int ex = ix - bx0, ey = iy - ylo;  // output row of the lower corners
+        if (ex < 0 || ex > bw - 2) continue;
+        const float dxu = xy.x - a.ax, dyu = xy.y - a.ay;
+        const float faw2 = 1.0f + a.kx * dxu * dxu + a.ky * dyu * dyu +
+                           2.0f * (a.gradx * dxu + a.grady * dyu);
+        const float q = fminf(sqrtf(faw2) / (a.gref_f + a.dg[p]), qm) * Sf;
+        float sn, cs;
+        sincosf(reduce_angle((double)fh * a.th[p]), &sn, &cs);
+        const float vre = sn * q, vim = cs * q;
+        const float w00 = wx * wy, w10 = (1.f - wx) * wy, w01 = wx * (1.f - wy),
+                    w11 = (1.f - wx) * (1.f - wy);
+        if (ey >= 0) {
+          const int o = ey * bw + ex;
+          atomicAdd(&are[o], __float2int_rn(vre * w00));
+          atomicAdd(&aim[o], __float2int_rn(vim * w00));
+          atomicAdd(&are[o + 1], __float2int_rn(vre * w10));
+          atomicAdd(&aim[o + 1], __float2int_rn(vim * w10));
         }
-        __syncthreads();
-        if (tid == 0) qcount = 0;
-        __syncthreads();
+        if (ey + 1 < hb) {
+          const int o = (ey + 1) * bw + ex;
+          atomicAdd(&are[o], __float2int_rn(vre * w01));
+          atomicAdd(&aim[o], __float2int_rn(vim * w01));
+          atomicAdd(&are[o + 1], __float2int_rn(vre * w11));
+          atomicAdd(&aim[o + 1], __float2int_rn(vim * w11));
+        }
       }
-      float2* out = F.src + (size_t)target * F.cap + (size_t)(row0 + yb) * bw;
-      for (int i = tid; i < hb * bw; i += kDepThreads) {
-        const unsigned int* w4 = acc32 + 4 * i;
-        const long long vr = (long long)(int)w4[0] * 65536 + (long long)w4[1];
-        const long long vi = (long long)(int)w4[2] * 65536 + (long long)w4[3];
-        out[i] = make_float2((float)((double)vr * unscale), (float)((double)vi * unscale));
-      }
+      __syncthreads();
+      const double unscale = scl / S;
+      for (int i = tid; i < nout; i += kDepThreads)
+        out[i] = make_float2((float)((double)are[i] * unscale), (float)((double)aim[i] * unscale));
     }
   }
 }
@@ -620,7 +642,7 @@ struct FinalizeArgs {
   int nband[kRunFields];
   int first_after[kRunFields];
   int nfield, nslice, rec;
-  const double* beam_part;  // [nslice * kDepBands][rec]
+  const double* beam_part;  // [nslice * kDepParts][rec]
   double* beam_hist;        // [nslice][rec] for this step
   double* field_hist;       // [nfield][nslice][9] for this step
 };
@@ -647,9 +669,9 @@ __global__ void diag_finalize_kernel(const FinalizeArgs a) {
       const int j = i - nf;
       const int s = j / a.rec, k = j - s * a.rec;
       const int op = k < 13 ? 0 : (k < kBeamRec ? ((k - 13) % 2 == 0 ? 1 : 2) : 0);
-      const double* p = a.beam_part + (size_t)s * kDepBands * a.rec + k;
+      const double* p = a.beam_part + (size_t)s * kDepParts * a.rec + k;
       double t = p[0];
-      for (int b = 1; b < kDepBands; ++b) {
+      for (int b = 1; b < kDepParts; ++b) {
         const double u = p[(size_t)b * a.rec];
         t = op == 0 ? t + u : (op == 1 ? fmin(t, u) : fmax(t, u));
       }
@@ -717,7 +739,6 @@ struct g4b_run {
   double* d_beam_part = nullptr;   // deposition CTAs' beam-diagnostic partials
   int hist_steps = 0;
   size_t rec_beam = 0, step_doubles = 0;
-  double fixed_scale = 0, qbound = 0;
   // cached graph
   cudaGraphExec_t gexec = nullptr;
   int g_first = -1, g_n = 0;
@@ -882,7 +903,6 @@ int enqueue_step(g4b_run* r, int i, const StepPlan& p) {
     a.nfield = r->nfield;
     a.nbunch = r->desc.nbunch;
     a.need_aux = 1;
-    a.acc_cells = (int)(kDepAccBytes / 16);
     a.ax = (float)st.ax;
     a.ay = (float)st.ay;
     a.kx = (float)st.kx;
@@ -891,8 +911,7 @@ int enqueue_step(g4b_run* r, int i, const StepPlan& p) {
     a.grady = (float)st.grady;
     a.gref = gbase;
     a.delz = st.delz;
-    a.fixed_scale = r->fixed_scale;
-    a.qbound = r->qbound;
+    a.gref_f = (float)gbase;
     a.beam_part = r->d_beam_part;
     a.err = c->d_error;
     for (int f = 0; f < r->nfield; ++f) {
@@ -917,10 +936,10 @@ int enqueue_step(g4b_run* r, int i, const StepPlan& p) {
     }
     LaunchScope ls(c, "run_deposit_diag");
     if (r->desc.nbunch == 1)
-      deposit_diag_kernel<1><<<r->nslice * kDepBands, kDepThreads, kDepAccBytes, c->stream>>>(a);
+      deposit_diag_kernel<1><<<r->nslice, kDepThreads, kDepSmem, c->stream>>>(a);
     else
       deposit_diag_kernel<kMaxBunch>
-          <<<r->nslice * kDepBands, kDepThreads, kDepAccBytes, c->stream>>>(a);
+          <<<r->nslice, kDepThreads, kDepSmem, c->stream>>>(a);
   }
   if (int rc = check_launch(c, "deposit_diag_kernel")) return rc;
   // K3/K4 per field
@@ -1055,26 +1074,16 @@ int g4b_run_create(g4b_ctx* c, const g4b_run_desc* d, const int64_t* off, g4b_ru
     }
   }
   r->rec_beam = kBeamRec + 2 * d->nbunch;
-  A((void**)&r->d_beam_part, (size_t)d->nslice * kDepBands * r->rec_beam * 8);
+  A((void**)&r->d_beam_part, (size_t)d->nslice * kDepParts * r->rec_beam * 8);
   if (e != cudaSuccess) {
     g4b_run_destroy(r);
     return cuda_fail(e, "g4b_run_create: device allocation");
   }
   r->step_doubles = (size_t)d->nslice * (r->rec_beam + 9 * d->nfield);
-  // fixed point of the deposition: |q| = sqrt(faw2)/gamma <= 4/gamma_ref,
-  // slice sums <= max_np * qbound < 2^46 (split 32-bit accumulation)
-  r->qbound = 4.0 / d->gamma_ref;
-  if (r->max_np > 65536) {
-    g4b_run_destroy(r);
-    return fail(G4B_ERR_RANGE, "g4b_run_create: more than 65536 particles in a slice");
-  }
-  int ex;
-  std::frexp((double)std::max<int64_t>(r->max_np, 1) * r->qbound, &ex);
-  r->fixed_scale = std::ldexp(1.0, 46 - ex);  // slice sums < 2^46
   cudaFuncSetAttribute(deposit_diag_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)kDepAccBytes);
+                       (int)kDepSmem);
   cudaFuncSetAttribute(deposit_diag_kernel<kMaxBunch>,
-                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDepAccBytes);
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDepSmem);
   *out = r;
   return G4B_OK;
 }
