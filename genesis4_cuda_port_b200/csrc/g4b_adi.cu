@@ -280,9 +280,12 @@ __global__ void __launch_bounds__(BandW<T>::value * 32)
     // src/Core/DiagnosticCUDA.cpp:305-363): this warp holds column
     // ix = r0 + warp, rows iy = lane*M + j of the solved plane
     __shared__ double dpart[BandW<T>::value][9];
-    const double shift = -0.5 * (double)(n - 1);
-    const double dx = (double)iy + shift;  // iy is the column index in pass Y
-    double sp = 0, sx1 = 0, sx2 = 0, sy1 = 0, sy2 = 0, sre = 0, sim = 0;
+    // each lane sums its M cells in the state precision T (exact cell
+    // offsets; FP32 partials of <= 33 terms) and the lanes, warps and bands
+    // are then added in FP64
+    const T shift = (T)(-0.5 * (double)(n - 1));
+    const double dx = (double)iy + (double)shift;  // iy is the column index in pass Y
+    T tp = 0, ty1 = 0, ty2 = 0, tre = 0, tim = 0;
     double cre = 0, cim = 0;
     const int ic = (n * n - 1) / 2;
     const int icy = ic / n, icx = ic - icy * n;
@@ -291,23 +294,24 @@ __global__ void __launch_bounds__(BandW<T>::value * 32)
       for (int j = 0; j < M; ++j) {
         const int k = lane * M + j;
         if (k < n) {
-          const double re = (double)v[j].x, im = (double)v[j].y;
-          const double wei = re * re + im * im;
-          const double dy = (double)k + shift;
-          sp += wei;
-          sy1 += dy * wei;
-          sy2 += dy * dy * wei;
-          sre += re;
-          sim += im;
+          const T re = v[j].x, im = v[j].y;
+          const T wei = re * re + im * im;
+          const T dy = (T)k + shift;
+          tp += wei;
+          ty1 += dy * wei;
+          ty2 += dy * dy * wei;
+          tre += re;
+          tim += im;
           if (iy == icx && k == icy) {
-            cre = re;
-            cim = im;
+            cre = (double)re;
+            cim = (double)im;
           }
         }
       }
-      sx1 = dx * sp;
-      sx2 = dx * dx * sp;
     }
+    const double sp = (double)tp, sy1 = (double)ty1, sy2 = (double)ty2;
+    const double sre = (double)tre, sim = (double)tim;
+    const double sx1 = dx * sp, sx2 = dx * dx * sp;
     double vals[9] = {sp, sx1, sx2, sy1, sy2, sre, sim, cre, cim};
 #pragma unroll
     for (int q = 0; q < 9; ++q) {

@@ -208,20 +208,29 @@ __global__ void __launch_bounds__(256) beam_step_kernel(const BeamStepArgs a) {
       }
       sincosf(reduce_angle((double)F.harm * t0), &s0[f], &c0[f]);
     }
-    // btper0 = btpar - (2/ks) Re(c): the field term is ~1e-10 of btpar ~ 2,
-    // far below FP32 resolution, so the sum and eps are formed in FP64 (an
-    // FP32 sum would round up or down with the particle's phase and inject a
-    // spurious phase-correlated detuning)
-    const double ztemp1 = -2.0 / a.xks;
-    const double btpar_d = (double)btpar;
+    // theta' = ks (1 - 1/b0) + ku with b0 = sqrt(1 - eps), eps = btper0 /
+    // gamma^2 ~ 1e-8: the two ~ku terms cancel to the detuning, so the
+    // zero-field, start-of-step value A0 = ku - ks eps0 fe(eps0) (fe =
+    // 1/(b(1+b))) is formed once in FP64.  Within the step eps differs from
+    // eps0 by the relative amount r = (1 + delta/btpar) (g0/gs)^2 - 1, where
+    // delta = -(2/ks) Re(c) is the field term (~1e-10 .. 1e-4 of btpar) and
+    // gs the stage energy; then ks eps fe(eps) = B0 (1 + r) (1 + O(eps0 r))
+    // with B0 = ks eps0 fe(eps0), so theta' = A0 - B0 r to a relative
+    // 1e-8 of the field term, and r is formed in FP32 without cancellation.
+    // The energy derivative Im(c) / (b0 gs) - ez drops b0 = 1 + O(1e-8).
     const double d0 = (double)d;
     const double g0 = a.gref + d0;
-    const double inv_g0 = 1.0 / g0;  // the stage energies differ from g0 by ~1e-9
-    auto ode = [&](float ds, double ts, float& kg, double& kp) {
-      const double del = (double)ds * inv_g0;                // (gs - g0) / g0
-      const double inv_gs = inv_g0 * (1.0 + del * (-1.0 + del));
-      const double inv_g2 = inv_gs * inv_gs;
-      const float dth = (float)(ts - t0);
+    const double inv_g0 = 1.0 / g0;
+    const double eps0 = (double)btpar * inv_g0 * inv_g0;
+    const double fe0 = 0.5 + eps0 * (0.375 + eps0 * 0.3125);
+    const double B0d = a.xks * eps0 * fe0;
+    const float A0 = (float)(a.xku - B0d);
+    const float B0 = (float)B0d;
+    const float inv_btpar = 1.0f / btpar;
+    const float zt = (float)(-2.0 / a.xks) * inv_btpar;  // delta / btpar per unit Re(c)
+    const float ig0 = (float)inv_g0;
+    // stage derivatives at energy offset ds (from g0) and phase offset dth
+    auto ode = [&](float ds, float dth, float& kg, float& kp) {
       float ctr = 0.f, cti = 0.f;
 #pragma unroll
       for (int f = 0; f < kF; ++f) {
@@ -233,54 +242,46 @@ __global__ void __launch_bounds__(256) beam_step_kernel(const BeamStepArgs a) {
         ctr += rr[f] * c + ri[f] * s;
         cti += ri[f] * c - rr[f] * s;
       }
-      const double btper0 = btpar_d + ztemp1 * (double)ctr;
-      const double eps = btper0 * inv_g2;
-      double fe, inv_b0;
-      if (eps < 1e-5) {
-        fe = 0.5 + eps * (0.375 + eps * 0.3125);
-        inv_b0 = 1.0 + eps * (0.5 + eps * 0.375);
-      } else {
-        const double b = sqrt(1.0 - eps);
-        fe = 1.0 / (b * (1.0 + b));
-        inv_b0 = 1.0 / b;
-      }
-      kp += a.xku - a.xks * eps * fe;
-      kg += cti * (float)(inv_b0 * inv_gs) - ez;
+      const float e = ds * ig0;                 // (gs - g0) / g0
+      const float bq = -e / (1.0f + e);         // g0 / gs - 1
+      const float ar = zt * ctr;                // delta / btpar
+      const float r = ar + bq * (2.0f + bq) * (1.0f + ar);
+      kp += A0 - B0 * r;
+      kg += cti * (ig0 * (1.0f + bq)) - ez;
     };
     // Genesis RK4 accumulator form (src/Core/BeamSolverCUDA.cpp:258-299) on
-    // the step's energy increment dd (small, so FP32 keeps its relative
-    // precision); the stored offset is rounded once at the end
-    float dd = 0.f;
-    float k2g = 0.f, k3g;
-    double k2p = 0.0, k3p;
-    ode(dd, t, k2g, k2p);
+    // the step's energy increment dd and phase increment dt (both small, so
+    // FP32 keeps their relative precision); theta and the stored energy
+    // offset are updated once at the end
+    float dd = 0.f, dt = 0.f;
+    float k2g = 0.f, k3g, k2p = 0.f, k3p;
+    ode(dd, dt, k2g, k2p);
     float stf = (float)(0.5 * a.delz);
-    double stp = 0.5 * a.delz;
     dd += stf * k2g;
-    t += stp * k2p;
+    dt += stf * k2p;
     k3g = k2g;
     k3p = k2p;
     k2g = 0.f;
-    k2p = 0.0;
-    ode(dd, t, k2g, k2p);
+    k2p = 0.f;
+    ode(dd, dt, k2g, k2p);
     dd += stf * (k2g - k3g);
-    t += stp * (k2p - k3p);
+    dt += stf * (k2p - k3p);
     k3g /= 6.0f;
-    k3p /= 6.0;
+    k3p /= 6.0f;
     k2g *= -0.5f;
-    k2p *= -0.5;
-    ode(dd, t, k2g, k2p);
+    k2p *= -0.5f;
+    ode(dd, dt, k2g, k2p);
     stf = (float)a.delz;
-    stp = a.delz;
     dd += stf * k2g;
-    t += stp * k2p;
+    dt += stf * k2p;
     k3g -= k2g;
     k3p -= k2p;
     k2g *= 2.0f;
-    k2p *= 2.0;
-    ode(dd, t, k2g, k2p);
+    k2p *= 2.0f;
+    ode(dd, dt, k2g, k2p);
     dd += stf * (k3g + k2g / 6.0f);
-    t += stp * (k3p + k2p / 6.0);
+    dt += stf * (k3p + k2p / 6.0f);
+    t = t0 + (double)dt;
     d = (float)(d0 + (double)dd);
     // applyR56 (src/Core/TrackBeamCUDA.cpp:257-278): theta += R56 (gamma - gamma0)
     if (a.has_r56) t += a.r56 * ((double)d + a.r56_off);
@@ -420,34 +421,52 @@ __global__ void __launch_bounds__(kDepThreads, 2) deposit_diag_kernel(const DepD
     double bre[NB], bim[NB];
 #pragma unroll
     for (int h = 0; h < NB; ++h) bre[h] = bim[h] = 0.0;
-    for (int64_t p = p0 + tid; p < p1; p += kDepThreads) {
-      const float2 xy = a.xy[p], pp = a.pxy[p];
-      const double x = xy.x, y = xy.y, px = pp.x, py = pp.y;
-      const double dgv = a.dg[p];
-      const double g = a.gref + dgv;
-      sdg += dgv;
-      sdg2 += dgv * dgv;
-      v[2] += x; v[3] += x * x; v[4] += y; v[5] += y * y;
-      v[6] += px; v[7] += px * px; v[8] += py; v[9] += py * py;
-      v[10] += x * px; v[11] += y * py; v[12] += 1.0;
-      if (a.need_aux) {
-        v[13] = fmin(v[13], x); v[14] = fmax(v[14], x);
-        v[15] = fmin(v[15], px); v[16] = fmax(v[16], px);
-        v[17] = fmin(v[17], y); v[18] = fmax(v[18], y);
-        v[19] = fmin(v[19], py); v[20] = fmax(v[20], py);
-        v[21] = fmin(v[21], g); v[22] = fmax(v[22], g);
-      }
-      float s1, c1;
-      sincosf(reduce_angle(a.th[p]), &s1, &c1);
-      float ch = c1, sh = s1;
+    // four particles per thread per iteration, loads issued first
+    constexpr int U = 4;
+    for (int64_t pb = p0 + tid; pb < p1; pb += U * kDepThreads) {
+      float2 lxy[U], lpp[U];
+      float ldg[U];
+      double lth[U];
 #pragma unroll
-      for (int h = 0; h < NB; ++h) {
-        if (h >= a.nbunch) break;
-        bre[h] += ch;
-        bim[h] += sh;
-        const float nc = ch * c1 - sh * s1, ns = sh * c1 + ch * s1;
-        ch = nc;
-        sh = ns;
+      for (int u = 0; u < U; ++u) {
+        const int64_t p = pb + u * kDepThreads;
+        if (p < p1) {
+          lxy[u] = a.xy[p];
+          lpp[u] = a.pxy[p];
+          ldg[u] = a.dg[p];
+          lth[u] = a.th[p];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        if (pb + u * kDepThreads >= p1) break;
+        const double x = lxy[u].x, y = lxy[u].y, px = lpp[u].x, py = lpp[u].y;
+        const double dgv = ldg[u];
+        const double g = a.gref + dgv;
+        sdg += dgv;
+        sdg2 += dgv * dgv;
+        v[2] += x; v[3] += x * x; v[4] += y; v[5] += y * y;
+        v[6] += px; v[7] += px * px; v[8] += py; v[9] += py * py;
+        v[10] += x * px; v[11] += y * py; v[12] += 1.0;
+        if (a.need_aux) {
+          v[13] = fmin(v[13], x); v[14] = fmax(v[14], x);
+          v[15] = fmin(v[15], px); v[16] = fmax(v[16], px);
+          v[17] = fmin(v[17], y); v[18] = fmax(v[18], y);
+          v[19] = fmin(v[19], py); v[20] = fmax(v[20], py);
+          v[21] = fmin(v[21], g); v[22] = fmax(v[22], g);
+        }
+        float s1, c1;
+        sincosf(reduce_angle(lth[u]), &s1, &c1);
+        float ch = c1, sh = s1;
+#pragma unroll
+        for (int h = 0; h < NB; ++h) {
+          if (h >= a.nbunch) break;
+          bre[h] += ch;
+          bim[h] += sh;
+          const float nc = ch * c1 - sh * s1, ns = sh * c1 + ch * s1;
+          ch = nc;
+          sh = ns;
+        }
       }
     }
     {
@@ -534,21 +553,51 @@ __global__ void __launch_bounds__(kDepThreads, 2) deposit_diag_kernel(const DepD
       __syncthreads();
       // 1. counts per base cell (ext row iy - ylo + 1) and the largest |q|
       float qmax = 0.f;
-      for (int64_t p = p0 + tid; p < p1; p += kDepThreads) {
-        const float2 xy = a.xy[p];
-        int ix, iy;
-        float wx, wy;
-        if (!cell_f(mf, xy.x, xy.y, ix, iy, wx, wy) || iy + 1 < ylo || iy >= ylo + hb) continue;
-        const int ex = ix - bx0, ey = iy - ylo + 1;
-        if (ex < 0 || ex > bw - 2) {
-          atomicOr(a.err, kErrBadSlice);
-          continue;
+      // (a quad of lanes holding one quiet-start beamlet shares the cell:
+      // one atomic adds its count)
+      for (int64_t pb = p0 + (tid & ~31); pb < p1; pb += 2 * kDepThreads) {
+        float2 lxy[2];
+        float ldg[2];
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          const int64_t p = pb + u * kDepThreads + l;
+          if (p < p1) {
+            lxy[u] = a.xy[p];
+            ldg[u] = a.dg[p];
+          }
         }
-        atomicAdd(&hist[ey * bw + ex], 1);
-        const float dxu = xy.x - a.ax, dyu = xy.y - a.ay;
-        const float faw2 = 1.0f + a.kx * dxu * dxu + a.ky * dyu * dyu +
-                           2.0f * (a.gradx * dxu + a.grady * dyu);
-        qmax = fmaxf(qmax, sqrtf(faw2) / (a.gref_f + a.dg[p]));
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          const int64_t p = pb + u * kDepThreads + l;
+          int cidx = -1;
+          if (p < p1) {
+            int ix, iy;
+            float wx, wy;
+            if (cell_f(mf, lxy[u].x, lxy[u].y, ix, iy, wx, wy) && iy + 1 >= ylo &&
+                iy < ylo + hb) {
+              const int ex = ix - bx0, ey = iy - ylo + 1;
+              if (ex < 0 || ex > bw - 2) {
+                atomicOr(a.err, kErrBadSlice);
+              } else {
+                cidx = ey * bw + ex;
+                const float dxu = lxy[u].x - a.ax, dyu = lxy[u].y - a.ay;
+                const float faw2 = 1.0f + a.kx * dxu * dxu + a.ky * dyu * dyu +
+                                   2.0f * (a.gradx * dxu + a.grady * dyu);
+                qmax = fmaxf(qmax, sqrtf(faw2) / (a.gref_f + ldg[u]));
+              }
+            }
+          }
+          const int c1 = __shfl_xor_sync(0xffffffffu, cidx, 1);
+          const int c2 = __shfl_xor_sync(0xffffffffu, cidx, 2);
+          const int c3 = __shfl_xor_sync(0xffffffffu, cidx, 3);
+          if (cidx >= 0) {
+            if (c1 == cidx && c2 == cidx && c3 == cidx) {
+              if ((l & 3) == 0) atomicAdd(&hist[cidx], 4);
+            } else {
+              atomicAdd(&hist[cidx], 1);
+            }
+          }
+        }
       }
       __syncthreads();
       // 2. M = max over output cells of the contributions it receives
@@ -588,35 +637,85 @@ __global__ void __launch_bounds__(kDepThreads, 2) deposit_diag_kernel(const DepD
       }
       __syncthreads();
       // 3. exact integer accumulation of the bilinear contributions
-      for (int64_t p = p0 + tid; p < p1; p += kDepThreads) {
-        const float2 xy = a.xy[p];
-        int ix, iy;
-        float wx, wy;
-        if (!cell_f(mf, xy.x, xy.y, ix, iy, wx, wy) || iy + 1 < ylo || iy >= ylo + hb) continue;
-        const int ex = ix - bx0, ey = iy - ylo;  // output row of the lower corners
-        if (ex < 0 || ex > bw - 2) continue;
-        const float dxu = xy.x - a.ax, dyu = xy.y - a.ay;
-        const float faw2 = 1.0f + a.kx * dxu * dxu + a.ky * dyu * dyu +
-                           2.0f * (a.gradx * dxu + a.grady * dyu);
-        const float q = fminf(sqrtf(faw2) / (a.gref_f + a.dg[p]), qm) * Sf;
-        float sn, cs;
-        sincosf(reduce_angle((double)fh * a.th[p]), &sn, &cs);
-        const float vre = sn * q, vim = cs * q;
-        const float w00 = wx * wy, w10 = (1.f - wx) * wy, w01 = wx * (1.f - wy),
-                    w11 = (1.f - wx) * (1.f - wy);
-        if (ey >= 0) {
-          const int o = ey * bw + ex;
-          atomicAdd(&are[o], __float2int_rn(vre * w00));
-          atomicAdd(&aim[o], __float2int_rn(vim * w00));
-          atomicAdd(&are[o + 1], __float2int_rn(vre * w10));
-          atomicAdd(&aim[o + 1], __float2int_rn(vim * w10));
+      // (contributions of a quad of lanes with one cell are added as integers
+      // in registers first: exact, so the result is unchanged)
+      for (int64_t pb = p0 + (tid & ~31); pb < p1; pb += 2 * kDepThreads) {
+        float2 lxy[2];
+        float ldg[2];
+        double lth[2];
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          const int64_t p = pb + u * kDepThreads + l;
+          if (p < p1) {
+            lxy[u] = a.xy[p];
+            ldg[u] = a.dg[p];
+            lth[u] = a.th[p];
+          }
         }
-        if (ey + 1 < hb) {
-          const int o = (ey + 1) * bw + ex;
-          atomicAdd(&are[o], __float2int_rn(vre * w01));
-          atomicAdd(&aim[o], __float2int_rn(vim * w01));
-          atomicAdd(&are[o + 1], __float2int_rn(vre * w11));
-          atomicAdd(&aim[o + 1], __float2int_rn(vim * w11));
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          const int64_t p = pb + u * kDepThreads + l;
+          int cidx = -1, ey = 0, ex = 0;
+          int c[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+          if (p < p1) {
+            int ix, iy;
+            float wx, wy;
+            if (cell_f(mf, lxy[u].x, lxy[u].y, ix, iy, wx, wy) && iy + 1 >= ylo &&
+                iy < ylo + hb) {
+              ex = ix - bx0;
+              ey = iy - ylo;  // output row of the lower corners
+              if (ex >= 0 && ex <= bw - 2) {
+                cidx = (ey + 1) * bw + ex;
+                const float dxu = lxy[u].x - a.ax, dyu = lxy[u].y - a.ay;
+                const float faw2 = 1.0f + a.kx * dxu * dxu + a.ky * dyu * dyu +
+                                   2.0f * (a.gradx * dxu + a.grady * dyu);
+                const float q = fminf(sqrtf(faw2) / (a.gref_f + ldg[u]), qm) * Sf;
+                float sn, cs;
+                sincosf(reduce_angle((double)fh * lth[u]), &sn, &cs);
+                const float vre = sn * q, vim = cs * q;
+                const float w00 = wx * wy, w10 = (1.f - wx) * wy, w01 = wx * (1.f - wy),
+                            w11 = (1.f - wx) * (1.f - wy);
+                c[0] = __float2int_rn(vre * w00);
+                c[1] = __float2int_rn(vim * w00);
+                c[2] = __float2int_rn(vre * w10);
+                c[3] = __float2int_rn(vim * w10);
+                c[4] = __float2int_rn(vre * w01);
+                c[5] = __float2int_rn(vim * w01);
+                c[6] = __float2int_rn(vre * w11);
+                c[7] = __float2int_rn(vim * w11);
+              }
+            }
+          }
+          const int c1 = __shfl_xor_sync(0xffffffffu, cidx, 1);
+          const int c2 = __shfl_xor_sync(0xffffffffu, cidx, 2);
+          const int c3 = __shfl_xor_sync(0xffffffffu, cidx, 3);
+          const bool quad = cidx >= 0 && c1 == cidx && c2 == cidx && c3 == cidx;
+          const bool anyquad = __any_sync(0xffffffffu, quad);
+          if (anyquad) {
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+              int t = c[k];
+              t += __shfl_xor_sync(0xffffffffu, t, 1);
+              t += __shfl_xor_sync(0xffffffffu, t, 2);
+              if (quad) c[k] = t;
+            }
+          }
+          if (cidx >= 0 && (!quad || (l & 3) == 0)) {
+            if (ey >= 0) {
+              const int o = ey * bw + ex;
+              atomicAdd(&are[o], c[0]);
+              atomicAdd(&aim[o], c[1]);
+              atomicAdd(&are[o + 1], c[2]);
+              atomicAdd(&aim[o + 1], c[3]);
+            }
+            if (ey + 1 < hb) {
+              const int o = (ey + 1) * bw + ex;
+              atomicAdd(&are[o], c[4]);
+              atomicAdd(&aim[o], c[5]);
+              atomicAdd(&are[o + 1], c[6]);
+              atomicAdd(&aim[o + 1], c[7]);
+            }
+          }
         }
       }
       __syncthreads();
