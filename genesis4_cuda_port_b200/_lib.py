@@ -111,6 +111,15 @@ _SIGS = {
     "g4b_diag_field_static": (C.c_int, [C.c_void_p, c_double_p, c_double_p]),
     "g4b_run_create": (C.c_int, [C.c_void_p, C.POINTER(RunDesc), c_int64_p, c_void_pp]),
     "g4b_run_destroy": (C.c_int, [C.c_void_p]),
+    "g4b_batch_create": (C.c_int, [C.c_void_p, C.c_int, c_void_pp]),
+    "g4b_batch_destroy": (C.c_int, [C.c_void_p]),
+    "g4b_batch_attach": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, c_int_p]),
+    "g4b_batch_detach": (C.c_int, [C.c_void_p, C.c_int]),
+    "g4b_batch_status": (C.c_int, [C.c_void_p, C.c_int, c_int_p, c_int_p]),
+    "g4b_batch_step": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "g4b_batch_tune": (C.c_int, [C.c_void_p]),
+    "g4b_batch_shapes": (C.c_int, [C.c_void_p, c_int_p]),
+    "g4b_ctx_mem_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "g4b_run_upload_beam": (C.c_int, [C.c_void_p] + [c_double_p] * 6),
     "g4b_run_download_beam": (C.c_int, [C.c_void_p] + [c_double_p] * 6),
     "g4b_run_upload_field": (C.c_int, [C.c_void_p, C.c_int, c_double_p, C.c_int]),

@@ -78,40 +78,20 @@ __device__ __forceinline__ C shfl_down_c(C v, int d) {
   return v;
 }
 
-struct AdiPassArgs {
-  const void* in;      // pass X: field (natural); pass Y: R' (transposed)
-  const void* src;     // pass X only: compact per-slice source tiles; nullptr = none
-  const int4* desc;    // per-slice source tile (x0, y0, width, height); width 0 = none
-  size_t src_cap;      // cells reserved per slice in `src`
-  const void* tab;     // lane-minor tables of this precision
-  int n, ld, nband;
-  int out_off;         // byte offset of the output staging tile
-  int bar_off;         // byte offset of the mbarrier
-  int box_rows, nbox;  // TMA store boxes per band
-  double r;
-  int* err;
-  // pass Y extras (fused form): planes [zero_start, zero_start+zero_count)
-  // (mod nslice) are written as zeros (the slippage of this step), and, when
-  // diag is non-null, each CTA writes 9 partial sums of the plane it solved
-  // (power, x1, x2, y1, y2, sum re, sum im, centre re, centre im) to
-  // diag[(slice * nband + band) * 9].
-  int nslice, zero_start, zero_count;
-  double* diag;
-};
 
 template <typename T> struct BandW;
 template <> struct BandW<double> { static constexpr int value = 9; };
 template <> struct BandW<float> { static constexpr int value = 10; };
 
+// One band of W rows (pass X) or W transposed columns (pass Y) of slice s.
+// bar is an initialised mbarrier; parity the phase this band waits on.
 template <typename T, int M, bool PX>
-__global__ void __launch_bounds__(BandW<T>::value * 32)
-    adi_pass_kernel(const AdiPassArgs a, const __grid_constant__ CUtensorMap tm_out) {
+__device__ __forceinline__ void adi_band(const AdiPassArgs& a, const CUtensorMap* tm_out, int s,
+                                         int band, unsigned char* smem, uint64_t* bar,
+                                         uint32_t parity) {
   using C = typename CT<T>::type;
   constexpr int W = BandW<T>::value;
-  extern __shared__ __align__(128) unsigned char smem[];
   const int n = a.n, ld = a.ld;
-  const int band = blockIdx.x % a.nband;
-  const int s = blockIdx.x / a.nband;
   const int r0 = band * W;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   constexpr int kTileRows = PX ? W + 2 : W;
@@ -120,13 +100,6 @@ __global__ void __launch_bounds__(BandW<T>::value * 32)
   C* tile = reinterpret_cast<C*>(smem);
   C* stile = tile + kTileRows * ld;
   C* out = reinterpret_cast<C*>(smem + a.out_off);
-  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + a.bar_off);
-
-  if (tid == 0) {
-    ptx::mbar_init(bar, 1);
-    ptx::fence_mbar_init();
-  }
-  __syncthreads();
 
   const size_t plane = (size_t)n * ld;
   const int lo = PX ? max(r0 - 1, 0) : r0;
@@ -161,7 +134,7 @@ __global__ void __launch_bounds__(BandW<T>::value * 32)
         for (int k = tid; k < ld; k += blockDim.x) tile[t * ld + k] = C{0, 0};
     }
   }
-  ptx::mbar_wait_bounded(bar, 0, a.err);
+  ptx::mbar_wait_bounded(bar, parity, a.err);
   __syncthreads();
 
   const T r = (T)a.r;
@@ -337,10 +310,48 @@ __global__ void __launch_bounds__(BandW<T>::value * 32)
   __syncthreads();
   if (tid == 0) {
     for (int i = 0; i < a.nbox; ++i)
-      ptx::tma_store_3d(&tm_out, out + (size_t)i * a.box_rows * W, 2 * r0,
+      ptx::tma_store_3d(tm_out, out + (size_t)i * a.box_rows * W, 2 * r0,
                         i * a.box_rows, s);
     ptx::bulk_commit();
     ptx::bulk_wait_read0();
+  }
+}
+
+template <typename T, int M, bool PX>
+__global__ void __launch_bounds__(BandW<T>::value * 32)
+    adi_pass_kernel(const __grid_constant__ AdiPassArgs a,
+                    const __grid_constant__ CUtensorMap tm_out) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ uint64_t bar;
+  if (threadIdx.x == 0) {
+    ptx::mbar_init(&bar, 1);
+    ptx::fence_mbar_init();
+  }
+  __syncthreads();
+  adi_band<T, M, PX>(a, &tm_out, blockIdx.x / a.nband, blockIdx.x % a.nband, smem, &bar, 0u);
+}
+
+// Persistent form over a work list of (run, slice, band) items of many runs
+// (one mbarrier, one phase per item; tensor maps read from global memory).
+template <typename T, int M, bool PX>
+__global__ void __launch_bounds__(BandW<T>::value * 32)
+    adi_batch_kernel(const __grid_constant__ AdiBatchArgs b) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ uint64_t bar;
+  if (threadIdx.x == 0) {
+    ptx::mbar_init(&bar, 1);
+    ptx::fence_mbar_init();
+  }
+  __syncthreads();
+  const int nitems = *b.nitems;
+  uint32_t parity = 0;
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const int4 w = b.items[it];
+    const CUtensorMap* tm = b.maps + w.x;
+    if (threadIdx.x == 0) ptx::fence_tensormap_acquire(tm);
+    adi_band<T, M, PX>(b.args[w.x], tm, w.y, w.z, smem, &bar, parity);
+    parity ^= 1u;
+    __syncthreads();
   }
 }
 
@@ -608,8 +619,8 @@ static int launch_pass_m(int M, g4b_field* f, const AdiPassArgs& args,
   return fail(G4B_ERR_RANGE, "adi: unsupported elements per lane");
 }
 
-int adi_run(g4b_adi* adi, g4b_field* f, const void* src, const int4* desc,
-            const AdiYExtras* ex) {
+int adi_plan(g4b_adi* adi, g4b_field* f, const void* src, const int4* desc,
+             const AdiYExtras* ex, AdiPlan& P) {
   const int n = f->ngrid, ld = f->ld, W = f->band_rows;
   AdiPassArgs args{};
   args.n = n;
@@ -622,27 +633,28 @@ int adi_run(g4b_adi* adi, g4b_field* f, const void* src, const int4* desc,
   args.tab = f->precision == G4B_FP64 ? (const void*)adi->d_tab64 : (const void*)adi->d_tab32;
   const size_t cb = f->cell_bytes;
   const size_t out_bytes = (size_t)f->store_nbox * f->store_box_rows * W * cb;
-  auto smem_for = [&](bool px, bool src) {
+  auto smem_for = [&](bool px, bool with_src) {
     size_t tile = (size_t)((px ? W + 2 : W) * ld) * cb;
-    if (px && src) tile += (size_t)W * ld * cb;
+    if (px && with_src) tile += (size_t)W * ld * cb;
     const size_t out_off = (tile + 127) / 128 * 128;
-    const size_t bar_off = (out_off + out_bytes + 15) / 16 * 16;
     args.out_off = (int)out_off;
-    args.bar_off = (int)bar_off;
-    return bar_off + 16;
+    return out_off + out_bytes;
   };
-  int rc;
+  P.M = adi->M;
+  P.precision = f->precision;
+  P.grid = (unsigned)(f->nslice * args.nband);
+  P.tm_x = &f->tm_store_b;
+  P.tm_y = &f->tm_store_a;
   // pass X: a -> b (transposed R')
   args.in = f->a;
   args.src = src;
   args.desc = desc;
   args.src_cap = (size_t)f->ngrid * f->ld;
-  size_t smem = smem_for(true, src != nullptr);
-  if (smem + 2048 > 227 * 1024) return fail(G4B_ERR_RANGE, "adi: pass X tile exceeds shared memory");
-  rc = f->precision == G4B_FP64
-           ? launch_pass_m<double, true>(adi->M, f, args, f->tm_store_b, smem)
-           : launch_pass_m<float, true>(adi->M, f, args, f->tm_store_b, smem);
-  if (rc) return rc;
+  P.smem_x_max = smem_for(true, true);
+  P.smem_x = smem_for(true, src != nullptr);
+  if (P.smem_x + 2048 > 227 * 1024)
+    return fail(G4B_ERR_RANGE, "adi: pass X tile exceeds shared memory");
+  P.x = args;
   // pass Y: b -> a (natural)
   args.in = f->b;
   args.src = nullptr;
@@ -652,11 +664,69 @@ int adi_run(g4b_adi* adi, g4b_field* f, const void* src, const int4* desc,
     args.zero_count = ex->zero_count;
     args.diag = ex->diag;
   }
-  smem = smem_for(false, false);
-  rc = f->precision == G4B_FP64
-           ? launch_pass_m<double, false>(adi->M, f, args, f->tm_store_a, smem)
-           : launch_pass_m<float, false>(adi->M, f, args, f->tm_store_a, smem);
-  return rc;
+  P.smem_y = smem_for(false, false);
+  P.y = args;
+  return G4B_OK;
+}
+
+int adi_launch(g4b_field* f, const AdiPlan& P) {
+  int rc = P.precision == G4B_FP64
+               ? launch_pass_m<double, true>(P.M, f, P.x, *P.tm_x, P.smem_x)
+               : launch_pass_m<float, true>(P.M, f, P.x, *P.tm_x, P.smem_x);
+  if (rc) return rc;
+  return P.precision == G4B_FP64
+             ? launch_pass_m<double, false>(P.M, f, P.y, *P.tm_y, P.smem_y)
+             : launch_pass_m<float, false>(P.M, f, P.y, *P.tm_y, P.smem_y);
+}
+
+int adi_run(g4b_adi* adi, g4b_field* f, const void* src, const int4* desc,
+            const AdiYExtras* ex) {
+  AdiPlan P;
+  if (int rc = adi_plan(adi, f, src, desc, ex, P)) return rc;
+  return adi_launch(f, P);
+}
+
+template <int M, bool PX>
+static int batch_launch_t(g4b_ctx* c, const AdiBatchArgs& b, size_t smem, int grid) {
+  static uint64_t configured = 0;
+  auto kern = adi_batch_kernel<float, M, PX>;
+  if (c->device >= 64 || !((configured >> c->device) & 1)) {
+    cudaFuncAttributes fa;
+    cudaError_t e = cudaFuncGetAttributes(&fa, kern);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaFuncGetAttributes(adi_batch)");
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             227 * 1024 - (int)fa.sharedSizeBytes);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(adi_batch)");
+    if (c->device < 64) configured |= 1ull << c->device;
+  }
+  {
+    LaunchScope ls(c, PX ? "batch_adi_x" : "batch_adi_y");
+    kern<<<grid, BandW<float>::value * 32, smem, c->stream>>>(b);
+  }
+  return check_launch(c, "adi_batch_kernel");
+}
+
+int adi_batch_launch(g4b_ctx* c, int M, bool px, const AdiBatchArgs& b, size_t smem, int grid) {
+#define G4B_BATCH_CASE(m)                                                      \
+  case m:                                                                      \
+    return px ? batch_launch_t<m, true>(c, b, smem, grid)                      \
+              : batch_launch_t<m, false>(c, b, smem, grid);
+  switch (M) {
+    G4B_BATCH_CASE(1)
+    G4B_BATCH_CASE(3)
+    G4B_BATCH_CASE(5)
+    G4B_BATCH_CASE(7)
+    G4B_BATCH_CASE(9)
+    G4B_BATCH_CASE(11)
+    G4B_BATCH_CASE(13)
+    G4B_BATCH_CASE(15)
+    G4B_BATCH_CASE(17)
+    G4B_BATCH_CASE(21)
+    G4B_BATCH_CASE(25)
+    G4B_BATCH_CASE(33)
+  }
+#undef G4B_BATCH_CASE
+  return fail(G4B_ERR_RANGE, "adi: unsupported elements per lane");
 }
 
 }  // namespace g4b

@@ -238,6 +238,16 @@ int g4b_ctx_synchronize(g4b_ctx* c) {
   return read_device_error(c, "g4b_ctx_synchronize");
 }
 
+int g4b_ctx_mem_info(g4b_ctx* c, uint64_t* free_bytes, uint64_t* total_bytes) {
+  if (!c || !free_bytes || !total_bytes) return fail(G4B_ERR_ARG, "g4b_ctx_mem_info: null arg");
+  G4B_CUDA_TRY(cudaSetDevice(c->device));
+  size_t f = 0, t = 0;
+  G4B_CUDA_TRY(cudaMemGetInfo(&f, &t));
+  *free_bytes = f;
+  *total_bytes = t;
+  return G4B_OK;
+}
+
 int g4b_ctx_launch_count(g4b_ctx* c, uint64_t* count) {
   if (!c || !count) return fail(G4B_ERR_ARG, "g4b_ctx_launch_count: null arg");
   *count = c->launches.load();

@@ -150,6 +150,26 @@ struct LaunchScope {
 int check_launch(g4b_ctx* ctx, const char* what);
 int read_device_error(g4b_ctx* ctx, const char* what);
 
+struct AdiPassArgs {
+  const void* in;      // pass X: field (natural); pass Y: R' (transposed)
+  const void* src;     // pass X only: compact per-slice source tiles; nullptr = none
+  const int4* desc;    // per-slice source tile (x0, y0, width, height); width 0 = none
+  size_t src_cap;      // cells reserved per slice in `src`
+  const void* tab;     // lane-minor tables of this precision
+  int n, ld, nband;
+  int out_off;         // byte offset of the output staging tile
+  int box_rows, nbox;  // TMA store boxes per band
+  double r;
+  int* err;
+  // pass Y extras (fused form): planes [zero_start, zero_start+zero_count)
+  // (mod nslice) are written as zeros (the slippage of this step), and, when
+  // diag is non-null, each CTA writes 9 partial sums of the plane it solved
+  // (power, x1, x2, y1, y2, sum re, sum im, centre re, centre im) to
+  // diag[(slice * nband + band) * 9].
+  int nslice, zero_start, zero_count;
+  double* diag;
+};
+
 // Shared ADI entry used by the drop-in and the fused path.  The extras of the
 // fused form (may be null): zero the planes the step's slippage zeroes, and
 // write per-band field-diagnostic partial sums (9 per band).
@@ -159,6 +179,29 @@ struct AdiYExtras {
 };
 int adi_run(g4b_adi* adi, g4b_field* f, const void* src, const int4* desc,
             const AdiYExtras* ex);
+// The two passes of one field step, resolved but not launched.
+struct AdiPlan {
+  AdiPassArgs x, y;
+  const CUtensorMap* tm_x;  // host copies of the field's store maps
+  const CUtensorMap* tm_y;
+  size_t smem_x, smem_y;
+  size_t smem_x_max;        // pass X with a source tile (the largest)
+  int M, precision;
+  unsigned grid;            // CTAs per pass: nslice * nband
+};
+int adi_plan(g4b_adi* adi, g4b_field* f, const void* src, const int4* desc,
+             const AdiYExtras* ex, AdiPlan& plan);
+int adi_launch(g4b_field* f, const AdiPlan& plan);
+// Batched passes (mixed precision): items[i] = (run, slice, band, 0) of the
+// runs whose ADI uses M elements per lane; args / maps indexed by run.
+struct AdiBatchArgs {
+  const AdiPassArgs* args;
+  const CUtensorMap* maps;
+  const int4* items;
+  const int* nitems;
+};
+int adi_batch_launch(g4b_ctx* c, int M, bool px, const AdiBatchArgs& b, size_t smem,
+                     int grid);
 // Sets the launch attributes of the ADI kernels for this field's grid (done
 // before any stream capture).
 int adi_configure(g4b_field* f);
@@ -249,6 +292,12 @@ __device__ __forceinline__ void tma_store_3d(const CUtensorMap* map,
       "[%0, {%2, %3, %4}], [%1];" ::"l"(map),
       "r"(smem_u32(src_smem)), "r"(x), "r"(y), "r"(z)
       : "memory");
+}
+
+// Make a tensor map written through the generic proxy (host copy into
+// global memory) visible to the tensor-map proxy before its first use.
+__device__ __forceinline__ void fence_tensormap_acquire(const void* map) {
+  asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(map) : "memory");
 }
 
 __device__ __forceinline__ void bulk_commit() {

@@ -138,11 +138,10 @@ __device__ __forceinline__ bool cell_f(const MixField& f, float x, float y, int&
 
 // NF: number of fields when known at compile time (1, 2), 0 = up to 8.
 template <int NF>
-__global__ void __launch_bounds__(256) beam_step_kernel(const BeamStepArgs a) {
+__device__ __forceinline__ void beam_chunk(const BeamStepArgs& a, const int4 ch) {
   constexpr int kF = NF > 0 ? NF : kRunFields;
   const int nfield = NF > 0 ? NF : a.nfield;
   __shared__ int sbb[kRunFields][4][8];
-  const int4 ch = a.chunks[blockIdx.x];
   const int slice = ch.x;
   const int tid = threadIdx.x;
   const bool live = tid < ch.z;
@@ -345,6 +344,29 @@ __global__ void __launch_bounds__(256) beam_step_kernel(const BeamStepArgs a) {
   }
 }
 
+template <int NF>
+__global__ void __launch_bounds__(256) beam_step_kernel(const __grid_constant__ BeamStepArgs a) {
+  beam_chunk<NF>(a, a.chunks[blockIdx.x]);
+}
+
+// Batched form: items[i] = (run, chunk of that run), per-run arguments.
+struct BeamBatchArgs {
+  const BeamStepArgs* args;
+  const int2* items;
+  const int* nitems;
+};
+
+template <int NF>
+__global__ void __launch_bounds__(256) beam_batch_kernel(const __grid_constant__ BeamBatchArgs b) {
+  const int nitems = *b.nitems;
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const int2 w = b.items[it];
+    const BeamStepArgs& a = b.args[w.x];
+    beam_chunk<NF>(a, a.chunks[w.y]);
+    __syncthreads();
+  }
+}
+
 // ------------------------------------------------------ deposit + beam diag --
 struct DepField {
   float2* src;        // compact tiles, cap cells per slice
@@ -396,13 +418,12 @@ constexpr size_t kDepSmem = (size_t)kDepMaxCells * 8;
 
 // NB: bunching harmonics accumulated (1, or up to kMaxBunch)
 template <int NB>
-__global__ void __launch_bounds__(kDepThreads, 2) deposit_diag_kernel(const DepDiagArgs a) {
-  extern __shared__ __align__(128) unsigned char smem[];
+__device__ __forceinline__ void deposit_slice(const DepDiagArgs& a, const int bs,
+                                              unsigned char* smem) {
   __shared__ double dpart[kDepThreads / 32][kBeamRec + 2 * kMaxBunch];
   __shared__ int4 sbox[kRunFields];
   __shared__ int wsum[kDepThreads / 32];
   __shared__ float wmax[kDepThreads / 32];
-  const int bs = blockIdx.x;
   const int tid = threadIdx.x, w = tid >> 5, l = tid & 31;
   const int64_t p0 = a.off[bs], p1 = a.off[bs + 1];
   const int64_t np = p1 - p0;
@@ -726,6 +747,32 @@ __global__ void __launch_bounds__(kDepThreads, 2) deposit_diag_kernel(const DepD
   }
 }
 
+template <int NB>
+__global__ void __launch_bounds__(kDepThreads, 2)
+    deposit_diag_kernel(const __grid_constant__ DepDiagArgs a) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  deposit_slice<NB>(a, blockIdx.x, smem);
+}
+
+// Batched form: items[i] = (run, slice of that run).
+struct DepBatchArgs {
+  const DepDiagArgs* args;
+  const int2* items;
+  const int* nitems;
+};
+
+template <int NB>
+__global__ void __launch_bounds__(kDepThreads, 2)
+    deposit_batch_kernel(const __grid_constant__ DepBatchArgs b) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  const int nitems = *b.nitems;
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const int2 w = b.items[it];
+    deposit_slice<NB>(b.args[w.x], w.y, smem);
+    __syncthreads();
+  }
+}
+
 // Resets the per-slice boxes after the deposition has read them.
 __global__ void bbox_reset_kernel(int4* bbox, int n) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -750,11 +797,10 @@ struct FinalizeArgs {
 // is = (nslice + storage - first) % nslice (src/Core/DiagnosticCUDA.cpp:320)
 // from the pass-Y band partials, the beam diagnostics from the deposition
 // CTAs' quarters; also resets the deposition boxes for the next step.
-__global__ void diag_finalize_kernel(const FinalizeArgs a) {
+__device__ __forceinline__ void finalize_range(const FinalizeArgs& a, int i0, int stride) {
   const int nf = a.nfield * a.nslice;
   const int nb = a.nslice * a.rec;
-  const int stride = gridDim.x * blockDim.x;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nf + nb + nf; i += stride) {
+  for (int i = i0; i < nf + nb + nf; i += stride) {
     if (i < nf) {
       const int f = i / a.nslice, s = i - f * a.nslice;
       const double* p = a.part[f] + (size_t)s * a.nband[f] * 9;
@@ -781,6 +827,16 @@ __global__ void diag_finalize_kernel(const FinalizeArgs a) {
       a.bbox[f][s] = make_int4(1 << 30, 1 << 30, -1, -1);
     }
   }
+}
+
+__global__ void diag_finalize_kernel(const __grid_constant__ FinalizeArgs a) {
+  finalize_range(a, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+}
+
+// Batched form: one CTA per run at a time.
+__global__ void finalize_batch_kernel(const FinalizeArgs* args, const int* nruns) {
+  const int n = *nruns;
+  for (int r = blockIdx.x; r < n; r += gridDim.x) finalize_range(args[r], threadIdx.x, blockDim.x);
 }
 
 static PlaneMapF plane_map_f(double strength, double offset) {
@@ -852,6 +908,16 @@ namespace {
 
 constexpr int kRunChunk = 256;
 
+// Every argument of one lattice step of one run.
+struct StepArgs {
+  bool has_beam;
+  BeamStepArgs bs;
+  DepDiagArgs dd;
+  AdiPlan adi[kRunFields];
+  FinalizeArgs fa;
+  int nfin;
+};
+
 int plan_step(g4b_run* r, int i, StepPlan& p) {
   p.st = r->steps[i];
   for (int f = 0; f < r->nfield; ++f) {
@@ -898,8 +964,11 @@ int plan_step(g4b_run* r, int i, StepPlan& p) {
   return G4B_OK;
 }
 
-int enqueue_step(g4b_run* r, int i, const StepPlan& p) {
+// Resolves every kernel argument of lattice step i (plan p) without
+// launching anything; the single-run path and the batch engine launch them.
+int build_step(g4b_run* r, int i, const StepPlan& p, StepArgs& L) {
   g4b_ctx* c = r->ctx;
+  L = StepArgs{};
   const g4b_step& st = p.st;
   const double gref = r->desc.gamma_ref;
   // particles store dg = gamma - (float)gamma_ref; every kernel rebuilds gamma
@@ -980,15 +1049,9 @@ int enqueue_step(g4b_run* r, int i, const StepPlan& p) {
       a.cy = (float)(st.cy * gref);
     }
     a.err = c->d_error;
-    LaunchScope ls(c, "run_beam_step");
-    if (r->nfield == 1)
-      beam_step_kernel<1><<<r->nchunk, kRunChunk, 0, c->stream>>>(a);
-    else if (r->nfield == 2)
-      beam_step_kernel<2><<<r->nchunk, kRunChunk, 0, c->stream>>>(a);
-    else
-      beam_step_kernel<0><<<r->nchunk, kRunChunk, 0, c->stream>>>(a);
+    L.has_beam = true;
+    L.bs = a;
   }
-  if (int rc = check_launch(c, "beam_step_kernel")) return rc;
   // K2
   double* step_hist = r->d_hist + (size_t)(i % r->hist_steps) * r->step_doubles;
   {
@@ -1033,21 +1096,16 @@ int enqueue_step(g4b_run* r, int i, const StepPlan& p) {
       d.fc = p.fc[f];
       d.xks = F.f->xks;
     }
-    LaunchScope ls(c, "run_deposit_diag");
-    if (r->desc.nbunch == 1)
-      deposit_diag_kernel<1><<<r->nslice, kDepThreads, kDepSmem, c->stream>>>(a);
-    else
-      deposit_diag_kernel<kMaxBunch>
-          <<<r->nslice, kDepThreads, kDepSmem, c->stream>>>(a);
+    L.dd = a;
   }
-  if (int rc = check_launch(c, "deposit_diag_kernel")) return rc;
   // K3/K4 per field
   for (int f = 0; f < r->nfield; ++f) {
     RunFieldState& F = r->fs[f];
     F.f->first = p.first_before[f];
     const bool src = st.in_undulator && (F.harm % 2) == 1 && p.fc[f] != 0.0 && r->npart > 0;
     AdiYExtras ex{p.zero_start[f], p.zero_count[f], F.d_part};
-    if (int rc = adi_run(F.adis[p.adi_index[f]], F.f, src ? F.f->src : nullptr, F.f->desc, &ex))
+    if (int rc = adi_plan(F.adis[p.adi_index[f]], F.f, src ? F.f->src : nullptr, F.f->desc, &ex,
+                          L.adi[f]))
       return rc;
     F.f->first = p.first_after[f];
   }
@@ -1066,11 +1124,46 @@ int enqueue_step(g4b_run* r, int i, const StepPlan& p) {
       a.nband[f] = r->fs[f].nband;
       a.first_after[f] = p.first_after[f];
     }
-    const int n = 2 * r->nfield * r->nslice + r->nslice * (int)r->rec_beam;
+    L.nfin = 2 * r->nfield * r->nslice + r->nslice * (int)r->rec_beam;
+    L.fa = a;
+  }
+  return G4B_OK;
+}
+
+// Launches one step of one run from its resolved arguments.
+int launch_single(g4b_run* r, const StepArgs& L) {
+  g4b_ctx* c = r->ctx;
+  if (L.has_beam) {
+    LaunchScope ls(c, "run_beam_step");
+    if (r->nfield == 1)
+      beam_step_kernel<1><<<r->nchunk, kRunChunk, 0, c->stream>>>(L.bs);
+    else if (r->nfield == 2)
+      beam_step_kernel<2><<<r->nchunk, kRunChunk, 0, c->stream>>>(L.bs);
+    else
+      beam_step_kernel<0><<<r->nchunk, kRunChunk, 0, c->stream>>>(L.bs);
+  }
+  if (int rc = check_launch(c, "beam_step_kernel")) return rc;
+  {
+    LaunchScope ls(c, "run_deposit_diag");
+    if (r->desc.nbunch == 1)
+      deposit_diag_kernel<1><<<r->nslice, kDepThreads, kDepSmem, c->stream>>>(L.dd);
+    else
+      deposit_diag_kernel<kMaxBunch><<<r->nslice, kDepThreads, kDepSmem, c->stream>>>(L.dd);
+  }
+  if (int rc = check_launch(c, "deposit_diag_kernel")) return rc;
+  for (int f = 0; f < r->nfield; ++f)
+    if (int rc = adi_launch(r->fs[f].f, L.adi[f])) return rc;
+  {
     LaunchScope ls(c, "run_diag_finalize");
-    diag_finalize_kernel<<<(n + 255) / 256, 256, 0, c->stream>>>(a);
+    diag_finalize_kernel<<<(L.nfin + 255) / 256, 256, 0, c->stream>>>(L.fa);
   }
   return check_launch(c, "diag_finalize_kernel");
+}
+
+int enqueue_step(g4b_run* r, int i, const StepPlan& p) {
+  StepArgs L;
+  if (int rc = build_step(r, i, p, L)) return rc;
+  return launch_single(r, L);
 }
 
 std::vector<int> state_key(g4b_run* r) {
@@ -1340,6 +1433,8 @@ int g4b_run_set_lattice(g4b_run* r, int nstep, const g4b_step* steps, const doub
 static int run_capture(g4b_run* r, int first_step, int nsteps, cudaGraphExec_t* out) {
   g4b_ctx* c = r->ctx;
   cudaGraph_t g = nullptr;
+  const bool prof = c->prof.on;  // no profiler events inside a graph
+  c->prof.on = false;
   G4B_CUDA_TRY(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
   int rc = G4B_OK;
   for (int k = 0; k < nsteps && rc == G4B_OK; ++k) {
@@ -1349,6 +1444,7 @@ static int run_capture(g4b_run* r, int first_step, int nsteps, cudaGraphExec_t* 
     if (rc == G4B_OK) rc = enqueue_step(r, first_step + k, p);
   }
   cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+  c->prof.on = prof;
   if (rc) {
     if (g) cudaGraphDestroy(g);
     return rc;
@@ -1449,6 +1545,455 @@ int g4b_run_history(g4b_run* r, int step, double* beam, double* field) {
 int g4b_run_device_bytes(g4b_run* r, uint64_t* bytes) {
   if (!r || !bytes) return fail(G4B_ERR_ARG, "g4b_run_device_bytes: null arg");
   *bytes = r->bytes + (uint64_t)r->hist_steps * r->step_doubles * 8;
+  return G4B_OK;
+}
+
+}  // extern "C"
+
+// =========================================================== batched runs ===
+// Many independent runs advanced together: per step one persistent launch
+// per kernel phase covers every attached run.  Each run keeps its own state
+// (a g4b_run); the engine resolves every run's step arguments on the host
+// (build_step, the same code the single-run path uses), uploads them with
+// one copy, and the batch kernels walk work lists of (run, chunk / slice /
+// band) items.  Every item is computed exactly as in the single-run kernels,
+// so a run's results do not depend on what else is in the batch.
+
+namespace {
+
+constexpr int kNumM = 12;
+const int kMList[kNumM] = {1, 3, 5, 7, 9, 11, 13, 15, 17, 21, 25, 33};
+int m_index(int M) {
+  for (int i = 0; i < kNumM; ++i)
+    if (kMList[i] == M) return i;
+  return -1;
+}
+
+// counts block at the head of the staging area
+struct BatchCounts {
+  int beam, dep, fin, pad;
+  int adi[kNumM];
+};
+
+template <typename T>
+size_t align_up(size_t x) {
+  const size_t a = alignof(T) < 128 ? 128 : alignof(T);
+  return (x + a - 1) / a * a;
+}
+
+}  // namespace
+
+struct g4b_batch {
+  g4b_ctx* ctx = nullptr;
+  int max_runs = 0;
+  std::vector<g4b_run*> runs;   // per slot (nullptr = free)
+  std::vector<int> next, last;  // per slot: next lattice step, end (exclusive)
+  bool dirty = true;            // composition changed since the last upload
+  // staging (pinned host, double-buffered) and device mirror
+  size_t off_bs = 0, off_dd = 0, off_fa = 0, off_ax = 0, off_ay = 0, off_mx = 0, off_my = 0,
+         args_bytes = 0;
+  unsigned char* h_args[2] = {nullptr, nullptr};
+  unsigned char* d_args = nullptr;
+  cudaEvent_t copied[2] = {nullptr, nullptr};
+  int buf = 0;
+  // work lists
+  std::vector<int2> beam_items, dep_items;
+  std::vector<int4> adi_items[kNumM];
+  size_t items_cap = 0;
+  unsigned char* d_items = nullptr;
+  size_t off_beam = 0, off_dep = 0, off_adi[kNumM] = {};
+  BatchCounts counts{};
+  size_t smem_x[kNumM] = {}, smem_y[kNumM] = {};
+  int nf_kind = 1, nb_kind = 1;  // beam kernel fields (1 or 0 = any), bunch kinds
+  // launch shapes (CTAs per kernel), chosen by the tuner
+  int grid[4] = {0, 0, 0, 0};    // beam, deposit, adi, finalize
+  int tune_left = 0, tune_idx = 0;
+  std::vector<float> tune_ms[4];
+  cudaEvent_t ev[5] = {};
+  // graph of one step for the current composition and shapes
+  cudaGraphExec_t gexec = nullptr;
+  bool graph_valid = false;
+  uint64_t steps_done = 0;
+};
+
+namespace {
+
+// The tuner's candidates per kernel, in units of SMs.
+const int kTuneBeam[4] = {2, 4, 8, 16};
+const int kTuneDep[4] = {2, 4, 6, 8};
+const int kTuneAdi[4] = {2, 4, 6, 8};
+
+int batch_layout(g4b_batch* b) {
+  size_t o = align_up<BatchCounts>(sizeof(BatchCounts));
+  const size_t nr = b->max_runs, nf = (size_t)b->max_runs * kRunFields;
+  b->off_bs = o;
+  o = align_up<BeamStepArgs>(o + nr * sizeof(BeamStepArgs));
+  b->off_dd = o;
+  o = align_up<DepDiagArgs>(o + nr * sizeof(DepDiagArgs));
+  b->off_fa = o;
+  o = align_up<FinalizeArgs>(o + nr * sizeof(FinalizeArgs));
+  b->off_ax = o;
+  o = align_up<AdiPassArgs>(o + nf * sizeof(AdiPassArgs));
+  b->off_ay = o;
+  o = align_up<AdiPassArgs>(o + nf * sizeof(AdiPassArgs));
+  b->off_mx = o;
+  o = align_up<CUtensorMap>(o + nf * sizeof(CUtensorMap));
+  b->off_my = o;
+  o = align_up<CUtensorMap>(o + nf * sizeof(CUtensorMap));
+  b->args_bytes = o;
+  for (int k = 0; k < 2; ++k) {
+    G4B_CUDA_TRY(cudaMallocHost(&b->h_args[k], o));
+    std::memset(b->h_args[k], 0, o);
+    G4B_CUDA_TRY(cudaEventCreateWithFlags(&b->copied[k], cudaEventDisableTiming));
+  }
+  G4B_CUDA_TRY(cudaMalloc(&b->d_args, o));
+  for (auto& e : b->ev) G4B_CUDA_TRY(cudaEventCreate(&e));
+  return G4B_OK;
+}
+
+// Rebuild the work lists after the set of attached, unfinished runs changed.
+int batch_rebuild(g4b_batch* b) {
+  b->beam_items.clear();
+  b->dep_items.clear();
+  for (auto& v : b->adi_items) v.clear();
+  std::memset(b->smem_x, 0, sizeof b->smem_x);
+  std::memset(b->smem_y, 0, sizeof b->smem_y);
+  b->nf_kind = 1;
+  b->nb_kind = 1;
+  int nactive = 0;
+  for (int s = 0; s < b->max_runs; ++s) {
+    g4b_run* r = b->runs[s];
+    if (!r || b->next[s] >= b->last[s]) continue;
+    ++nactive;
+    if (r->nfield != 1) b->nf_kind = 0;
+    if (r->desc.nbunch != 1) b->nb_kind = 0;
+    for (int k = 0; k < r->nchunk; ++k) b->beam_items.push_back(make_int2(s, k));
+    for (int sl = 0; sl < r->nslice; ++sl) b->dep_items.push_back(make_int2(s, sl));
+    for (int f = 0; f < r->nfield; ++f) {
+      g4b_field* F = r->fs[f].f;
+      const int mi = m_index(r->fs[f].adis.empty() ? pick_M(F->ngrid) : r->fs[f].adis[0]->M);
+      if (mi < 0) return fail(G4B_ERR_RANGE, "g4b_batch: unsupported grid");
+      const int nband = (F->ngrid + F->band_rows - 1) / F->band_rows;
+      for (int sl = 0; sl < r->nslice; ++sl)
+        for (int bd = 0; bd < nband; ++bd)
+          b->adi_items[mi].push_back(make_int4(s * kRunFields + f, sl, bd, 0));
+      // shared memory of the largest band in this group
+      const int W = F->band_rows, ld = F->ld;
+      const size_t cb = F->cell_bytes;
+      const size_t out_bytes = (size_t)F->store_nbox * F->store_box_rows * W * cb;
+      const size_t tx = (size_t)((W + 2) * ld + W * ld) * cb, ty = (size_t)(W * ld) * cb;
+      b->smem_x[mi] = std::max(b->smem_x[mi], (tx + 127) / 128 * 128 + out_bytes);
+      b->smem_y[mi] = std::max(b->smem_y[mi], (ty + 127) / 128 * 128 + out_bytes);
+    }
+  }
+  b->counts = BatchCounts{};
+  b->counts.beam = (int)b->beam_items.size();
+  b->counts.dep = (int)b->dep_items.size();
+  b->counts.fin = nactive;
+  size_t need = 0;
+  b->off_beam = 0;
+  need = align_up<int2>(b->beam_items.size() * sizeof(int2));
+  b->off_dep = need;
+  need = align_up<int2>(need + b->dep_items.size() * sizeof(int2));
+  for (int m = 0; m < kNumM; ++m) {
+    b->counts.adi[m] = (int)b->adi_items[m].size();
+    b->off_adi[m] = need;
+    need = align_up<int4>(need + b->adi_items[m].size() * sizeof(int4));
+  }
+  need = std::max<size_t>(need, 256);
+  if (need > b->items_cap) {
+    if (b->d_items) cudaFree(b->d_items);
+    b->d_items = nullptr;
+    G4B_CUDA_TRY(cudaMalloc(&b->d_items, need));
+    b->items_cap = need;
+  }
+  std::vector<unsigned char> h(need, 0);
+  std::memcpy(h.data() + b->off_beam, b->beam_items.data(), b->beam_items.size() * sizeof(int2));
+  std::memcpy(h.data() + b->off_dep, b->dep_items.data(), b->dep_items.size() * sizeof(int2));
+  for (int m = 0; m < kNumM; ++m)
+    std::memcpy(h.data() + b->off_adi[m], b->adi_items[m].data(),
+                b->adi_items[m].size() * sizeof(int4));
+  G4B_CUDA_TRY(cudaMemcpyAsync(b->d_items, h.data(), need, cudaMemcpyHostToDevice,
+                               b->ctx->stream));
+  G4B_CUDA_TRY(cudaStreamSynchronize(b->ctx->stream));
+  b->dirty = false;
+  b->graph_valid = false;
+  return G4B_OK;
+}
+
+// Resolve this step's arguments of every active run into the staging buffer.
+int batch_stage(g4b_batch* b) {
+  const int k = b->buf;
+  G4B_CUDA_TRY(cudaEventSynchronize(b->copied[k]));  // the copy of two steps ago
+  unsigned char* h = b->h_args[k];
+  std::memcpy(h, &b->counts, sizeof(BatchCounts));
+  auto* bs = reinterpret_cast<BeamStepArgs*>(h + b->off_bs);
+  auto* dd = reinterpret_cast<DepDiagArgs*>(h + b->off_dd);
+  auto* fa = reinterpret_cast<FinalizeArgs*>(h + b->off_fa);
+  auto* ax = reinterpret_cast<AdiPassArgs*>(h + b->off_ax);
+  auto* ay = reinterpret_cast<AdiPassArgs*>(h + b->off_ay);
+  auto* mx = reinterpret_cast<CUtensorMap*>(h + b->off_mx);
+  auto* my = reinterpret_cast<CUtensorMap*>(h + b->off_my);
+  int nfin = 0;
+  for (int s = 0; s < b->max_runs; ++s) {
+    g4b_run* r = b->runs[s];
+    if (!r || b->next[s] >= b->last[s]) continue;
+    const int i = b->next[s];
+    StepPlan p;
+    if (int rc = plan_step(r, i % (int)r->steps.size(), p)) return rc;
+    StepArgs L;
+    if (int rc = build_step(r, i, p, L)) return rc;
+    bs[s] = L.bs;
+    dd[s] = L.dd;
+    fa[nfin++] = L.fa;
+    for (int f = 0; f < r->nfield; ++f) {
+      ax[s * kRunFields + f] = L.adi[f].x;
+      ay[s * kRunFields + f] = L.adi[f].y;
+      mx[s * kRunFields + f] = *L.adi[f].tm_x;
+      my[s * kRunFields + f] = *L.adi[f].tm_y;
+    }
+    b->next[s] = i + 1;
+    if (b->next[s] >= b->last[s]) b->dirty = true;  // leaves the lists next step
+  }
+  G4B_CUDA_TRY(cudaMemcpyAsync(b->d_args, h, b->args_bytes, cudaMemcpyHostToDevice,
+                               b->ctx->stream));
+  G4B_CUDA_TRY(cudaEventRecord(b->copied[k], b->ctx->stream));
+  b->buf ^= 1;
+  return G4B_OK;
+}
+
+// The kernels of one batch step (capturable: no host synchronisation).
+int batch_launch(g4b_batch* b, bool timed) {
+  g4b_ctx* c = b->ctx;
+  const int* counts = reinterpret_cast<const int*>(b->d_args);
+  auto ev = [&](int i) {
+    if (timed) cudaEventRecord(b->ev[i], c->stream);
+  };
+  ev(0);
+  if (b->counts.beam > 0) {
+    BeamBatchArgs a{reinterpret_cast<const BeamStepArgs*>(b->d_args + b->off_bs),
+                    reinterpret_cast<const int2*>(b->d_items + b->off_beam), counts + 0};
+    LaunchScope ls(c, "batch_beam_step");
+    if (b->nf_kind == 1)
+      beam_batch_kernel<1><<<b->grid[0], kRunChunk, 0, c->stream>>>(a);
+    else
+      beam_batch_kernel<0><<<b->grid[0], kRunChunk, 0, c->stream>>>(a);
+  }
+  if (int rc = check_launch(c, "beam_batch_kernel")) return rc;
+  ev(1);
+  {
+    DepBatchArgs a{reinterpret_cast<const DepDiagArgs*>(b->d_args + b->off_dd),
+                   reinterpret_cast<const int2*>(b->d_items + b->off_dep), counts + 1};
+    LaunchScope ls(c, "batch_deposit_diag");
+    if (b->nb_kind == 1)
+      deposit_batch_kernel<1><<<b->grid[1], kDepThreads, kDepSmem, c->stream>>>(a);
+    else
+      deposit_batch_kernel<kMaxBunch><<<b->grid[1], kDepThreads, kDepSmem, c->stream>>>(a);
+  }
+  if (int rc = check_launch(c, "deposit_batch_kernel")) return rc;
+  ev(2);
+  for (int pass = 0; pass < 2; ++pass) {
+    for (int m = 0; m < kNumM; ++m) {
+      if (b->counts.adi[m] == 0) continue;
+      AdiBatchArgs a;
+      a.args = reinterpret_cast<const AdiPassArgs*>(b->d_args + (pass ? b->off_ay : b->off_ax));
+      a.maps = reinterpret_cast<const CUtensorMap*>(b->d_args + (pass ? b->off_my : b->off_mx));
+      a.items = reinterpret_cast<const int4*>(b->d_items + b->off_adi[m]);
+      a.nitems = reinterpret_cast<const int*>(b->d_args) + 4 + m;
+      const int g = std::min(b->grid[2], b->counts.adi[m]);
+      if (int rc = adi_batch_launch(c, kMList[m], pass == 0, a, pass ? b->smem_y[m] : b->smem_x[m],
+                                    g))
+        return rc;
+    }
+    ev(3 + pass);
+  }
+  {
+    LaunchScope ls(c, "batch_diag_finalize");
+    finalize_batch_kernel<<<b->grid[3], 256, 0, c->stream>>>(
+        reinterpret_cast<const FinalizeArgs*>(b->d_args + b->off_fa), counts + 2);
+  }
+  return check_launch(c, "finalize_batch_kernel");
+}
+
+void batch_default_grids(g4b_batch* b) {
+  const int sm = b->ctx->sm_count;
+  b->grid[0] = 8 * sm;
+  b->grid[1] = 2 * sm;
+  b->grid[2] = 4 * sm;
+  b->grid[3] = sm;
+}
+
+}  // namespace
+
+extern "C" {
+
+int g4b_batch_create(g4b_ctx* c, int max_runs, g4b_batch** out) {
+  if (!c || !out || max_runs < 1) return fail(G4B_ERR_ARG, "g4b_batch_create: bad arg");
+  *out = nullptr;
+  G4B_CUDA_TRY(cudaSetDevice(c->device));
+  auto b = new (std::nothrow) g4b_batch();
+  if (!b) return fail(G4B_ERR_NOMEM, "g4b_batch_create: host allocation");
+  b->ctx = c;
+  ctx_retain(c);
+  b->max_runs = max_runs;
+  b->runs.assign(max_runs, nullptr);
+  b->next.assign(max_runs, 0);
+  b->last.assign(max_runs, 0);
+  batch_default_grids(b);
+  cudaFuncSetAttribute(deposit_batch_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)kDepSmem);
+  cudaFuncSetAttribute(deposit_batch_kernel<kMaxBunch>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDepSmem);
+  if (int rc = batch_layout(b)) {
+    g4b_batch_destroy(b);
+    return rc;
+  }
+  *out = b;
+  return G4B_OK;
+}
+
+int g4b_batch_destroy(g4b_batch* b) {
+  if (!b) return G4B_OK;
+  ctx_quiesce(b->ctx);
+  if (b->gexec) cudaGraphExecDestroy(b->gexec);
+  for (int k = 0; k < 2; ++k) {
+    if (b->h_args[k]) cudaFreeHost(b->h_args[k]);
+    if (b->copied[k]) cudaEventDestroy(b->copied[k]);
+  }
+  for (auto e : b->ev)
+    if (e) cudaEventDestroy(e);
+  if (b->d_args) cudaFree(b->d_args);
+  if (b->d_items) cudaFree(b->d_items);
+  ctx_release(b->ctx);
+  delete b;
+  return G4B_OK;
+}
+
+// Attach a prepared run (created, uploaded, lattice set): it takes part in
+// the batch's steps from lattice step `first_step` for `nsteps` steps.
+int g4b_batch_attach(g4b_batch* b, g4b_run* r, int first_step, int nsteps, int* slot) {
+  if (!b || !r || !slot || nsteps < 0 || first_step < 0)
+    return fail(G4B_ERR_ARG, "g4b_batch_attach: bad arg");
+  if (r->ctx != b->ctx) return fail(G4B_ERR_ARG, "g4b_batch_attach: run on another context");
+  if (r->steps.empty()) return fail(G4B_ERR_STATE, "g4b_batch_attach: run has no lattice");
+  for (int f = 0; f < r->nfield; ++f)
+    if (r->fs[f].f->precision != G4B_MIXED)
+      return fail(G4B_ERR_ARG, "g4b_batch_attach: mixed-precision runs only");
+  for (int s = 0; s < b->max_runs; ++s)
+    if (b->runs[s] == r) return fail(G4B_ERR_STATE, "g4b_batch_attach: run already attached");
+  for (int s = 0; s < b->max_runs; ++s) {
+    if (b->runs[s]) continue;
+    b->runs[s] = r;
+    b->next[s] = first_step;
+    b->last[s] = first_step + nsteps;
+    b->dirty = true;
+    *slot = s;
+    return G4B_OK;
+  }
+  return fail(G4B_ERR_RANGE, "g4b_batch_attach: no free slot");
+}
+
+// Detach the run in `slot` (the run itself is not destroyed).  Waits for the
+// batch's queued work first.
+int g4b_batch_detach(g4b_batch* b, int slot) {
+  if (!b || slot < 0 || slot >= b->max_runs || !b->runs[slot])
+    return fail(G4B_ERR_ARG, "g4b_batch_detach: bad slot");
+  G4B_CUDA_TRY(cudaStreamSynchronize(b->ctx->stream));
+  b->runs[slot] = nullptr;
+  b->dirty = true;
+  return G4B_OK;
+}
+
+int g4b_batch_status(g4b_batch* b, int slot, int* next_step, int* remaining) {
+  if (!b || slot < 0 || slot >= b->max_runs || !b->runs[slot])
+    return fail(G4B_ERR_ARG, "g4b_batch_status: bad slot");
+  if (next_step) *next_step = b->next[slot];
+  if (remaining) *remaining = std::max(0, b->last[slot] - b->next[slot]);
+  return G4B_OK;
+}
+
+// Start the tuner: the next 4 batch steps run with candidate launch shapes
+// (per kernel: CTAs per SM) and time each kernel; the fastest shape of every
+// kernel is kept.  Results do not depend on the shapes.
+int g4b_batch_tune(g4b_batch* b) {
+  if (!b) return fail(G4B_ERR_ARG, "g4b_batch_tune: null batch");
+  b->tune_left = 4;
+  b->tune_idx = 0;
+  for (auto& v : b->tune_ms) v.assign(4, 0.f);
+  return G4B_OK;
+}
+
+// Launch shapes in use: CTAs of the beam, deposition, ADI and finalize kernels.
+int g4b_batch_shapes(g4b_batch* b, int* grids) {
+  if (!b || !grids) return fail(G4B_ERR_ARG, "g4b_batch_shapes: null arg");
+  for (int k = 0; k < 4; ++k) grids[k] = b->grid[k];
+  return G4B_OK;
+}
+
+// Advance every attached, unfinished run by `nsteps` lattice steps (runs that
+// reach their end drop out).  With use_graph the kernels of a step are
+// replayed from a CUDA graph captured for the current composition.
+int g4b_batch_step(g4b_batch* b, int nsteps, int use_graph) {
+  if (!b || nsteps < 0) return fail(G4B_ERR_ARG, "g4b_batch_step: bad arg");
+  g4b_ctx* c = b->ctx;
+  G4B_CUDA_TRY(cudaSetDevice(c->device));
+  for (int k = 0; k < nsteps; ++k) {
+    if (b->dirty)
+      if (int rc = batch_rebuild(b)) return rc;
+    if (b->counts.fin == 0) return G4B_OK;
+    if (int rc = batch_stage(b)) return rc;
+    if (b->tune_left > 0) {
+      const int sm = c->sm_count, t = b->tune_idx;
+      b->grid[0] = kTuneBeam[t] * sm;
+      b->grid[1] = kTuneDep[t] * sm;
+      b->grid[2] = kTuneAdi[t] * sm;
+      if (int rc = batch_launch(b, true)) return rc;
+      G4B_CUDA_TRY(cudaEventSynchronize(b->ev[4]));
+      for (int q = 0; q < 3; ++q) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, b->ev[q], b->ev[q + 1]);
+        b->tune_ms[q][t] = ms;
+      }
+      {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, b->ev[3], b->ev[4]);
+        b->tune_ms[2][t] += ms;  // both ADI passes
+      }
+      b->tune_idx++;
+      if (--b->tune_left == 0) {
+        const int* cand[3] = {kTuneBeam, kTuneDep, kTuneAdi};
+        for (int q = 0; q < 3; ++q) {
+          int best = 0;
+          for (int j = 1; j < 4; ++j)
+            if (b->tune_ms[q][j] < b->tune_ms[q][best]) best = j;
+          b->grid[q] = cand[q][best] * sm;
+        }
+        b->graph_valid = false;
+      }
+    } else if (use_graph) {
+      if (!b->graph_valid) {
+        if (b->gexec) cudaGraphExecDestroy(b->gexec);
+        b->gexec = nullptr;
+        cudaGraph_t g;
+        const bool prof = c->prof.on;  // no profiler events inside a graph
+        c->prof.on = false;
+        G4B_CUDA_TRY(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        const int rc = batch_launch(b, false);
+        cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+        c->prof.on = prof;
+        if (rc) return rc;
+        if (e != cudaSuccess) return cuda_fail(e, "g4b_batch_step: capture");
+        e = cudaGraphInstantiate(&b->gexec, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return cuda_fail(e, "g4b_batch_step: instantiate");
+        b->graph_valid = true;
+      }
+      G4B_CUDA_TRY(cudaGraphLaunch(b->gexec, c->stream));
+    } else {
+      if (int rc = batch_launch(b, false)) return rc;
+    }
+    b->steps_done++;
+  }
   return G4B_OK;
 }
 

@@ -349,3 +349,62 @@ class Run:
             self.close()
         except Exception:
             pass
+
+
+class Batch:
+    """Many independent mixed-precision runs advanced together by one
+    persistent launch per kernel phase (g4b_batch_* in include/g4b.h).  Runs
+    are attached as prepared `Run` objects and leave on reaching their last
+    step; their state and diagnostics stay readable through the `Run`."""
+
+    def __init__(self, ctx: Context, max_runs: int):
+        self.ctx, self.lib = ctx, ctx.lib
+        h = C.c_void_p()
+        check(self.lib.g4b_batch_create(ctx.h, max_runs, C.byref(h)))
+        self.h = h
+        self.runs = {}
+
+    def attach(self, run: Run, first_step: int, nsteps: int) -> int:
+        slot = C.c_int()
+        check(self.lib.g4b_batch_attach(self.h, run.h, first_step, nsteps, C.byref(slot)))
+        self.runs[slot.value] = run
+        return slot.value
+
+    def detach(self, slot: int) -> None:
+        check(self.lib.g4b_batch_detach(self.h, slot))
+        self.runs.pop(slot, None)
+
+    def status(self, slot: int):
+        """(next lattice step, steps remaining)."""
+        nxt, rem = C.c_int(), C.c_int()
+        check(self.lib.g4b_batch_status(self.h, slot, C.byref(nxt), C.byref(rem)))
+        return nxt.value, rem.value
+
+    def step(self, nsteps: int = 1, graph: bool = True) -> None:
+        check(self.lib.g4b_batch_step(self.h, nsteps, int(graph)))
+
+    def tune(self) -> None:
+        check(self.lib.g4b_batch_tune(self.h))
+
+    def shapes(self):
+        g = (C.c_int * 4)()
+        check(self.lib.g4b_batch_shapes(self.h, g))
+        return dict(zip(("beam", "deposit", "adi", "finalize"), list(g)))
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.g4b_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def mem_info(ctx: Context):
+    """(free, total) device bytes."""
+    f, t = C.c_uint64(), C.c_uint64()
+    check(ctx.lib.g4b_ctx_mem_info(ctx.h, C.byref(f), C.byref(t)))
+    return int(f.value), int(t.value)

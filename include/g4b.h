@@ -259,6 +259,34 @@ int g4b_run_prepare(g4b_run* run, int first_step, int nsteps);
 int g4b_run_history(g4b_run* run, int step, double* beam, double* field);
 int g4b_run_device_bytes(g4b_run* run, uint64_t* bytes);
 
+/* ---- batched runs ---------------------------------------------------------
+ * No counterpart in the reference (it advances one simulation per process).
+ * Many independent mixed-precision runs (each a g4b_run: own slice count,
+ * grid, particle count, lattice and slippage) advance together: per step one
+ * persistent launch per kernel phase covers every attached run, driven by
+ * work lists of (run, chunk / slice / band) items.  A run's results are the
+ * same alone and in any mix (every item is computed as in the single-run
+ * kernels).  Runs join (attach) and leave (detach, or on reaching their last
+ * step) between steps. */
+typedef struct g4b_batch g4b_batch;
+int g4b_batch_create(g4b_ctx* ctx, int max_runs, g4b_batch** out);
+int g4b_batch_destroy(g4b_batch* batch);
+/* The run takes part in lattice steps [first_step, first_step + nsteps). */
+int g4b_batch_attach(g4b_batch* batch, g4b_run* run, int first_step, int nsteps,
+                     int* slot);
+int g4b_batch_detach(g4b_batch* batch, int slot);
+int g4b_batch_status(g4b_batch* batch, int slot, int* next_step, int* remaining);
+/* Advance every attached, unfinished run by nsteps steps (asynchronous);
+ * use_graph replays each step's kernels from a CUDA graph. */
+int g4b_batch_step(g4b_batch* batch, int nsteps, int use_graph);
+/* Autotuner: the next 4 steps try candidate launch shapes (CTAs per SM) for
+ * each kernel, timed with CUDA events; the fastest shape per kernel stays. */
+int g4b_batch_tune(g4b_batch* batch);
+/* CTAs of the beam, deposition, ADI and finalize launches in use. */
+int g4b_batch_shapes(g4b_batch* batch, int* grids4);
+/* Free and total device memory (cudaMemGetInfo) for admission decisions. */
+int g4b_ctx_mem_info(g4b_ctx* ctx, uint64_t* free_bytes, uint64_t* total_bytes);
+
 #ifdef __cplusplus
 }
 #endif

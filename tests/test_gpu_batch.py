@@ -1,0 +1,114 @@
+"""Batched runs: runs of different grids, particle counts, slice counts,
+tapers and lengths advanced together give exactly the results they give
+alone (every work item is computed as in the single-run kernels)."""
+import numpy as np
+import pytest
+
+from genesis4_cuda_port_b200 import device as dev
+from tests import synth
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = dev.Context(0)
+    yield c
+    c.synchronize()
+
+
+CONFIGS = [
+    # nslice, npart/slice, ngrid, taper, detuning, time_run, nsteps
+    dict(nslice=1, npart=1024, ngrid=45, taper=0.02, dgam=0.0, time_run=False, nsteps=8),
+    dict(nslice=1, npart=2048, ngrid=71, taper=0.0, dgam=3e-4, time_run=False, nsteps=8),
+    dict(nslice=3, npart=512, ngrid=33, taper=0.01, dgam=-2e-4, time_run=True, nsteps=6),
+    dict(nslice=2, npart=768, ngrid=101, taper=0.0, dgam=0.0, time_run=True, nsteps=7),
+]
+
+
+def _inputs(k, cfg):
+    off, parts = synth.beam(cfg["nslice"], cfg["npart"], seed=200 + k)
+    parts["gamma"] = parts["gamma"] * (1 + cfg["dgam"])
+    cells = synth.field(cfg["nslice"], cfg["ngrid"], 160e-6, seed=300 + k, amplitude=2e12)
+    n = cfg["nsteps"]
+    steps = [synth.und_step(aw=synth.AW * (1 - cfg["taper"] * i / n)) for i in range(n - 1)]
+    steps.append(synth.drift_step(delz=0.05, qf=1.0))
+    fc = [[synth.coupling(st.aw) if st.in_undulator else 0.0] for st in steps]
+    slip = [st.delz * (1 + st.aw ** 2) / (2 * synth.GAMMA0 ** 2) / synth.LAMBDA0 for st in steps]
+    return off, parts, cells, steps, fc, slip
+
+
+def _make(ctx, k, cfg):
+    off, parts, cells, steps, fc, slip = _inputs(k, cfg)
+    run = dev.Run(ctx, off, fields=[(1, cfg["ngrid"], 160e-6)], lambda0=synth.LAMBDA0,
+                  gamma_ref=synth.GAMMA0, sample=1.0, time_run=cfg["time_run"], nbunch=1)
+    run.upload_beam(parts)
+    run.upload_field(0, cells, 0)
+    run.set_current(np.full(cfg["nslice"], synth.CURRENT))
+    run.set_lattice(steps, fc, slip)
+    return run
+
+
+def _result(run, nsteps):
+    beam = run.download_beam()
+    cells, first = run.download_field(0)
+    hist = [run.history(i) for i in range(nsteps)]
+    return beam, cells, first, hist
+
+
+def _same(a, b):
+    for k in a[0]:
+        assert np.array_equal(a[0][k], b[0][k]), k
+    assert np.array_equal(a[1], b[1])
+    assert a[2] == b[2]
+    for (hb1, hf1), (hb2, hf2) in zip(a[3], b[3]):
+        assert np.array_equal(hb1, hb2) and np.array_equal(hf1, hf2)
+
+
+def _alone(ctx):
+    out = []
+    for k, cfg in enumerate(CONFIGS):
+        run = _make(ctx, k, cfg)
+        run.advance(0, cfg["nsteps"], graph=False)
+        out.append(_result(run, cfg["nsteps"]))
+        run.close()
+    return out
+
+
+@pytest.mark.parametrize("graph, tune", [(False, False), (True, False), (True, True)])
+def test_batch_equals_runs_alone(ctx, graph, tune):
+    alone = _alone(ctx)
+    batch = dev.Batch(ctx, 8)
+    runs = [_make(ctx, k, cfg) for k, cfg in enumerate(CONFIGS)]
+    slots = [batch.attach(r, 0, cfg["nsteps"]) for r, cfg in zip(runs, CONFIGS)]
+    if tune:
+        batch.tune()
+    longest = max(cfg["nsteps"] for cfg in CONFIGS)
+    batch.step(longest + 2, graph=graph)  # runs leave at their own end
+    ctx.synchronize()
+    for s, r, cfg, ref in zip(slots, runs, CONFIGS, alone):
+        assert batch.status(s) == (cfg["nsteps"], 0)
+        _same(_result(r, cfg["nsteps"]), ref)
+    if tune:
+        g = batch.shapes()
+        assert all(v > 0 for v in g.values())
+    batch.close()
+
+
+def test_run_joins_a_batch_in_progress(ctx):
+    """A run attached while others are mid-way (continuous batching) ends
+    with the results it has alone."""
+    alone = _alone(ctx)
+    batch = dev.Batch(ctx, 4)
+    runs = [_make(ctx, k, cfg) for k, cfg in enumerate(CONFIGS)]
+    batch.attach(runs[0], 0, CONFIGS[0]["nsteps"])
+    batch.attach(runs[1], 0, CONFIGS[1]["nsteps"])
+    batch.step(3, graph=True)
+    batch.attach(runs[2], 0, CONFIGS[2]["nsteps"])
+    batch.step(2, graph=True)
+    batch.attach(runs[3], 0, CONFIGS[3]["nsteps"])
+    batch.step(12, graph=True)
+    ctx.synchronize()
+    for r, cfg, ref in zip(runs, CONFIGS, alone):
+        _same(_result(r, cfg["nsteps"]), ref)
+    batch.close()
