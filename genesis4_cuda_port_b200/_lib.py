@@ -119,6 +119,8 @@ _SIGS = {
     "g4b_batch_step": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
     "g4b_batch_tune": (C.c_int, [C.c_void_p]),
     "g4b_batch_shapes": (C.c_int, [C.c_void_p, c_int_p]),
+    "g4b_ctx_mark": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64)]),
+    "g4b_ctx_mark_query": (C.c_int, [C.c_void_p, C.c_uint64, C.c_int, c_int_p]),
     "g4b_ctx_mem_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "g4b_run_upload_beam": (C.c_int, [C.c_void_p] + [c_double_p] * 6),
     "g4b_run_download_beam": (C.c_int, [C.c_void_p] + [c_double_p] * 6),

@@ -203,6 +203,8 @@ int g4b_ctx_destroy(g4b_ctx* c) {
     cudaEventDestroy(q.b);
   }
   c->prof.pending.clear();
+  for (auto e : c->marks) cudaEventDestroy(e);
+  c->marks.clear();
   for (auto e : c->prof.pool) cudaEventDestroy(e);
   c->prof.pool.clear();
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
@@ -236,6 +238,41 @@ int g4b_ctx_synchronize(g4b_ctx* c) {
   if (!c) return fail(G4B_ERR_ARG, "g4b_ctx_synchronize: null ctx");
   G4B_CUDA_TRY(cudaStreamSynchronize(c->stream));
   return read_device_error(c, "g4b_ctx_synchronize");
+}
+
+static constexpr size_t kMarkRing = 256;
+
+int g4b_ctx_mark(g4b_ctx* c, uint64_t* ticket) {
+  if (!c || !ticket) return fail(G4B_ERR_ARG, "g4b_ctx_mark: null arg");
+  G4B_CUDA_TRY(cudaSetDevice(c->device));
+  if (c->marks.empty()) {
+    c->marks.resize(kMarkRing, nullptr);
+    for (auto& e : c->marks) G4B_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  }
+  const uint64_t t = c->mark_next++;
+  G4B_CUDA_TRY(cudaEventRecord(c->marks[t % kMarkRing], c->stream));
+  *ticket = t;
+  return G4B_OK;
+}
+
+int g4b_ctx_mark_query(g4b_ctx* c, uint64_t ticket, int wait, int* done) {
+  if (!c || !done) return fail(G4B_ERR_ARG, "g4b_ctx_mark_query: null arg");
+  if (ticket >= c->mark_next || c->mark_next - ticket > kMarkRing)
+    return fail(G4B_ERR_ARG, "g4b_ctx_mark_query: unknown or recycled ticket");
+  cudaEvent_t e = c->marks[ticket % kMarkRing];
+  if (wait) {
+    G4B_CUDA_TRY(cudaEventSynchronize(e));
+    *done = 1;
+    return G4B_OK;
+  }
+  const cudaError_t q = cudaEventQuery(e);
+  if (q == cudaErrorNotReady) {
+    *done = 0;
+    return G4B_OK;
+  }
+  if (q != cudaSuccess) return cuda_fail(q, "g4b_ctx_mark_query");
+  *done = 1;
+  return G4B_OK;
 }
 
 int g4b_ctx_mem_info(g4b_ctx* c, uint64_t* free_bytes, uint64_t* total_bytes) {

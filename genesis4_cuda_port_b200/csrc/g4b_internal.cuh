@@ -71,6 +71,9 @@ struct g4b_ctx {
   // their context (the struct lives until the last reference goes)
   std::atomic<int> refs{1};
   bool destroyed = false;
+  // stream marks (g4b_ctx_mark): a ring of events, ticket % size
+  std::vector<cudaEvent_t> marks;
+  uint64_t mark_next = 0;
 };
 
 struct g4b_field {

@@ -240,3 +240,95 @@ class Result:
                 self.h = None
         except Exception:
             pass
+
+
+# ---- many runs on one GPU: batched scan and served stream -------------------
+
+class Job(C.Structure):
+    """Mirror of ``g4h_job``: one mixed-precision FEL run."""
+
+    _fields_ = [("nslice", C.c_int), ("npart", C.c_int), ("ngrid", C.c_int),
+                ("nsteps", C.c_int), ("shotnoise", C.c_int), ("time_run", C.c_int),
+                ("seed", C.c_uint64), ("gridmax", C.c_double), ("gamma", C.c_double),
+                ("delgam", C.c_double), ("emit", C.c_double), ("beta", C.c_double),
+                ("current", C.c_double), ("seed_power", C.c_double), ("waist", C.c_double),
+                ("taper", C.c_double)]
+
+
+class EngineConfig(C.Structure):
+    """Mirror of ``g4h_engine_config``."""
+
+    _fields_ = [("lattice", C.c_char_p), ("beamline", C.c_char_p), ("delz", C.c_double),
+                ("gamma_ref", C.c_double), ("lambda0", C.c_double), ("max_runs", C.c_int),
+                ("use_graph", C.c_int), ("tune", C.c_int), ("mode", C.c_int),
+                ("threads", C.c_int), ("reserve_bytes", C.c_double)]
+
+
+class ScanResult(C.Structure):
+    _fields_ = [("value", C.c_double), ("seconds", C.c_double), ("slice_steps", C.c_double),
+                ("device_bytes", C.c_double), ("njobs", C.c_int), ("grids", C.c_int * 4)]
+
+
+class ServeStats(C.Structure):
+    _fields_ = [("seconds", C.c_double), ("p50", C.c_double), ("p99", C.c_double),
+                ("mean", C.c_double), ("requests_per_s", C.c_double),
+                ("slice_steps", C.c_double), ("slice_steps_per_s", C.c_double),
+                ("batch_steps", C.c_double), ("peak_concurrency", C.c_int),
+                ("reserved", C.c_int)]
+
+
+def _bind_engine(h):
+    h.g4h_scan.argtypes = [C.POINTER(EngineConfig), C.POINTER(Job), C.c_int,
+                           C.POINTER(ScanResult), _lib.c_double_p, _lib.c_double_p]
+    h.g4h_serve.argtypes = [C.POINTER(EngineConfig), C.POINTER(Job), _lib.c_double_p, C.c_int,
+                            _lib.c_double_p, _lib.c_double_p, _lib.c_double_p,
+                            C.POINTER(ServeStats)]
+
+
+def engine_config(lattice: str, beamline: str, delz: float, gamma_ref: float, lambda0: float,
+                  max_runs: int = 256, graph: bool = True, tune: bool = True, mode: int = 0,
+                  threads: int = 0, reserve_bytes: float = 4e9) -> EngineConfig:
+    c = EngineConfig()
+    c._keep = (lattice.encode(), beamline.encode())
+    c.lattice, c.beamline = c._keep
+    c.delz, c.gamma_ref, c.lambda0 = delz, gamma_ref, lambda0
+    c.max_runs, c.use_graph, c.tune, c.mode = max_runs, int(graph), int(tune), mode
+    c.threads, c.reserve_bytes = threads, reserve_bytes
+    return c
+
+
+def _jobs_array(jobs):
+    arr = (Job * len(jobs))()
+    for i, j in enumerate(jobs):
+        arr[i] = j
+    return arr
+
+
+def scan(cfg: EngineConfig, jobs, records: bool = False):
+    """Run every job to its end (batched for cfg.mode 0); returns
+    (ScanResult, final power per job [W], raw last-step records or None)."""
+    h = load()
+    _bind_engine(h)
+    arr = _jobs_array(jobs)
+    res = ScanResult()
+    power = np.empty(len(jobs))
+    rec = np.empty(sum(j.nslice for j in jobs) * 34) if records else None
+    _check(h.g4h_scan(C.byref(cfg), arr, len(jobs), C.byref(res), dptr(power),
+                      dptr(rec) if rec is not None else None))
+    return res, power, rec
+
+
+def serve(cfg: EngineConfig, jobs, arrival, records: bool = False):
+    """Served stream: returns (ServeStats, latency [s], final power [W],
+    raw last-step records or None)."""
+    h = load()
+    _bind_engine(h)
+    arr = _jobs_array(jobs)
+    arrival = np.ascontiguousarray(arrival, np.float64)
+    lat = np.empty(len(jobs))
+    power = np.empty(len(jobs))
+    rec = np.empty(sum(j.nslice for j in jobs) * 34) if records else None
+    st = ServeStats()
+    _check(h.g4h_serve(C.byref(cfg), arr, dptr(arrival), len(jobs), dptr(lat), dptr(power),
+                       dptr(rec) if rec is not None else None, C.byref(st)))
+    return st, lat, power, rec

@@ -118,6 +118,67 @@ def large_sase_h3(nslice=8192, npart=16384, ngrid=255):
 WORKLOADS = {"steady": steady_state, "sase": sase, "sase_h3": large_sase_h3}
 
 
+def _job(wl: Workload, **kw):
+    from .host import Job
+    j = Job()
+    base = dict(nslice=1, npart=wl.npart, ngrid=wl.ngrid, nsteps=10 ** 6, shotnoise=1,
+                time_run=0, seed=wl.seed, gridmax=wl.gridmax, gamma=wl.gamma0,
+                delgam=wl.rel_spread * wl.gamma0, emit=wl.emit_n, beta=wl.beta,
+                current=wl.current, seed_power=0.0, waist=wl.waist, taper=0.0)
+    base.update(kw)
+    for k, v in base.items():
+        setattr(j, k, v)
+    return j
+
+
+def engine(wl: Workload, **kw):
+    """Engine configuration of the shared SASE lattice at the workload's
+    reference energy."""
+    from .host import engine_config
+    return engine_config(wl.lattice, wl.beamline, wl.delz, wl.gamma0, wl.lambda0, **kw)
+
+
+def batched_scan(nruns=256, seed=1):
+    """Steady-state scan: nruns single-slice runs with ngrid ~ U[101,301],
+    npart ~ U[2048,32768] (multiple of 4), linear taper d(aw)/aw ~ U[0,2%],
+    detuning dgamma/gamma ~ U[-5e-4,5e-4], seed power log-U[100 W, 10 kW];
+    every run takes the whole lattice.  Returns (workload, jobs, params)."""
+    wl = steady_state()
+    rng = np.random.default_rng(seed)
+    params = []
+    jobs = []
+    for i in range(nruns):
+        p = dict(ngrid=int(rng.integers(101, 302)),
+                 npart=int(rng.integers(2048 // 4, 32768 // 4 + 1)) * 4,
+                 taper=float(rng.uniform(0.0, 0.02)),
+                 detune=float(rng.uniform(-5e-4, 5e-4)),
+                 seed_power=float(10 ** rng.uniform(2.0, 4.0)))
+        params.append(p)
+        jobs.append(_job(wl, ngrid=p["ngrid"], npart=p["npart"], taper=p["taper"],
+                         gamma=wl.gamma0 * (1 + p["detune"]), seed_power=p["seed_power"],
+                         shotnoise=0, seed=seed + i))
+    return wl, jobs, params
+
+
+def served_stream(nreq=2000, rate=200.0, seed=1):
+    """Served stream: Poisson arrivals (rate per second) of runs with
+    nslice ~ U{1..64}, ngrid ~ U[101,255], npart ~ U[2048,16384] (multiple of
+    4), nsteps ~ U[110,330]; SASE from shot noise, slippage on for nslice > 1.
+    Returns (workload, jobs, arrival times [s], params)."""
+    wl = sase()
+    rng = np.random.default_rng(seed)
+    arrival = np.cumsum(rng.exponential(1.0 / rate, nreq))
+    jobs, params = [], []
+    for i in range(nreq):
+        p = dict(nslice=int(rng.integers(1, 65)), ngrid=int(rng.integers(101, 256)),
+                 npart=int(rng.integers(2048 // 4, 16384 // 4 + 1)) * 4,
+                 nsteps=int(rng.integers(110, 331)))
+        params.append(p)
+        jobs.append(_job(wl, nslice=p["nslice"], ngrid=p["ngrid"], npart=p["npart"],
+                         nsteps=p["nsteps"], time_run=int(p["nslice"] > 1), seed=seed + i))
+    return wl, jobs, arrival, params
+
+
 def lambda_res(lambdau, aw, gamma):
     return lambdau * (1 + aw * aw) / (2 * gamma * gamma)
 

@@ -284,6 +284,12 @@ int g4b_batch_step(g4b_batch* batch, int nsteps, int use_graph);
 int g4b_batch_tune(g4b_batch* batch);
 /* CTAs of the beam, deposition, ADI and finalize launches in use. */
 int g4b_batch_shapes(g4b_batch* batch, int* grids4);
+/* Stream marks: g4b_ctx_mark records a point in the context's stream and
+ * returns its ticket; g4b_ctx_mark_query reports (or with wait, waits for)
+ * the completion of everything enqueued before it.  The last 256 tickets
+ * stay valid. */
+int g4b_ctx_mark(g4b_ctx* ctx, uint64_t* ticket);
+int g4b_ctx_mark_query(g4b_ctx* ctx, uint64_t ticket, int wait, int* done);
 /* Free and total device memory (cudaMemGetInfo) for admission decisions. */
 int g4b_ctx_mem_info(g4b_ctx* ctx, uint64_t* free_bytes, uint64_t* total_bytes);
 

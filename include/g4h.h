@@ -118,6 +118,55 @@ int g4h_result_get(g4h_result* res, int group, const char* key, double* out,
 /* Final cells of field i (2*nslice*ngrid^2 doubles) and its `first`. */
 int g4h_result_field(g4h_result* res, int ifield, double* cells, int* first);
 
+/* ---- many runs on one GPU: batched scan and served stream ----------------
+ * A job is one mixed-precision FEL run on the shared lattice of the engine
+ * configuration: its own slice count, grid, particles per slice, taper
+ * (linear d(aw)/aw over the run), beam energy (detuning from gamma_ref),
+ * seed power and number of lattice steps.  Inputs are prepared by host
+ * worker threads (quiet start + shot noise, Gaussian seed); runs execute on
+ * the g4b_batch engine of g4b.h. */
+typedef struct g4h_job {
+  int nslice, npart, ngrid, nsteps;
+  int shotnoise, time_run;
+  uint64_t seed;
+  double gridmax, gamma, delgam, emit, beta, current, seed_power, waist, taper;
+} g4h_job;
+
+typedef struct g4h_engine_config {
+  const char* lattice;   /* .lat text and the beamline to expand            */
+  const char* beamline;
+  double delz, gamma_ref, lambda0;
+  int max_runs;          /* batch slots                                      */
+  int use_graph, tune;
+  int mode;              /* scan: 0 batched, 1 one run after another         */
+  int threads;           /* input-preparation threads (0 = cores - 2)        */
+  double reserve_bytes;  /* serve: device memory kept free at admission      */
+} g4h_engine_config;
+
+typedef struct g4h_scan_result {
+  double value;          /* slice-steps/s of the timed stepping loop         */
+  double seconds, slice_steps, device_bytes;
+  int njobs;
+  int grids[4];          /* launch shapes the batch used                     */
+} g4h_scan_result;
+
+typedef struct g4h_serve_stats {
+  double seconds, p50, p99, mean, requests_per_s;
+  double slice_steps, slice_steps_per_s, batch_steps;
+  int peak_concurrency, reserved;
+} g4h_serve_stats;
+
+/* final_power[njobs] (W, last step) and records[sum nslice*34] (the last
+ * step's raw beam record [nslice][25] then field record [nslice][9]) may be
+ * null. */
+int g4h_scan(const g4h_engine_config* cfg, const g4h_job* jobs, int njobs,
+             g4h_scan_result* result, double* final_power, double* records);
+/* arrival[njobs] in seconds from the start, non-decreasing; latency[njobs]
+ * receives completion - arrival. */
+int g4h_serve(const g4h_engine_config* cfg, const g4h_job* jobs, const double* arrival,
+              int njobs, double* latency, double* final_power, double* records,
+              g4h_serve_stats* stats);
+
 #ifdef __cplusplus
 }
 #endif
