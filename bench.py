@@ -52,6 +52,14 @@ def parse_args(argv=None):
     p.add_argument("--cpu-steps", type=int, default=8)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-accuracy", action="store_true")
+    p.add_argument("--workload", choices=["sase", "scan", "serve", "sase_h3", "steady"],
+                   default="sase",
+                   help="sase: the headline line; the others measure the batched scan, "
+                        "the served stream, the large SASE with h=1 and h=3, steady state")
+    p.add_argument("--runs", type=int, default=256, help="scan: runs in the batch")
+    p.add_argument("--requests", type=int, default=400, help="serve: requests in the stream")
+    p.add_argument("--rate", type=float, default=200.0, help="serve: arrivals per second")
     return p.parse_args(argv)
 
 
@@ -257,6 +265,196 @@ def _stats(prof, alg, steps):
     return per
 
 
+def accuracy():
+    """P(z) and |b1|(z) of the mixed form against the FP64 oracle on the
+    steady-state FEL (1 slice, 8192 particles, ngrid 151, 1 kW seed, whole
+    lattice): max relative power error and max absolute bunching error."""
+    from genesis4_cuda_port_b200 import device as dev, workloads
+    from oracle import pyoracle as orc
+    wl = workloads.steady_state()
+    off, parts = wl.make_beam()
+    cells = wl.make_field()
+    lat = wl.make_lattice()
+    n = lat.nstep
+    p = {k: v.copy() for k, v in parts.items()}
+    f = dict(cells=cells.copy(), gridmax=wl.gridmax, xlambda=wl.lambda0, fc=0.0, first=0,
+             accuslip=0.0)
+    cur = np.full(1, wl.current)
+    pz, bz = [], []
+    for i in range(n):
+        f["fc"] = lat.fc(i, 1)
+        orc.step(off, cur, lat.steps[i], wl.lambda0, lat.slip[i], 1.0, False, False, [f], p)
+        pz.append(orc.diag_field(f["cells"], 0)[0][0, 0])
+        s_, bre, bim = orc.diag_beam(off, p, 1)
+        bz.append(abs(bre[0, 0] + 1j * bim[0, 0]) / s_[0, 12])
+    ctx = dev.Context(int(os.environ.get("LOCAL_RANK", "0")))
+    run = dev.Run(ctx, off, fields=[(1, wl.ngrid, wl.gridmax)], lambda0=wl.lambda0,
+                  gamma_ref=wl.gamma0, sample=1.0, time_run=False, nbunch=1)
+    run.upload_beam(parts)
+    run.upload_field(0, cells, 0)
+    run.set_current(cur)
+    run.set_lattice(lat.steps, [[lat.fc(i, 1)] for i in range(n)], lat.slip)
+    run.advance(0, n, graph=True)
+    hb, hf = run.history_range(0, n)
+    pm = hf[:, 0, 0, 0]
+    bm = np.abs(hb[:, 0, 23] + 1j * hb[:, 0, 24]) / hb[:, 0, 12]
+    pz, bz = np.array(pz), np.array(bz)
+    return {"workload": wl.name, "pz_rel_err_max": float(np.max(np.abs(pm - pz) / pz)),
+            "b1_abs_err_max": float(np.max(np.abs(bm - bz))),
+            "power_gain": float(pz[-1] / pz[0]), "gates": {"pz_rel": 1e-3, "b1_abs": 1e-3}}
+
+
+def _engine_clocks():
+    return Clocks(int(os.environ.get("LOCAL_RANK", "0")))
+
+
+def run_scan(args):
+    """Batched steady-state scan: every run resident, one persistent launch
+    per phase per step (tuned shapes, graph), against the same runs one after
+    another through the single-run graph path."""
+    from genesis4_cuda_port_b200 import host, workloads
+    wl, jobs, params = workloads.batched_scan(args.runs)
+    clk = _engine_clocks()
+    clk.start()
+    time.sleep(0.5)
+    rb, _, _ = host.scan(workloads.engine(wl, max_runs=len(jobs), tune=True, mode=0), jobs)
+    c = clk.stop()
+    rs, _, _ = host.scan(workloads.engine(wl, max_runs=len(jobs), mode=1), jobs)
+    line = {"metric": "slice-steps/s, batched steady-state scan", "value": rb.value,
+            "unit": UNIT, "n_gpus": 1, "steps": int(rb.slice_steps / len(jobs)),
+            "higher_is_better": True, "dtype": "f32 state, f64 theta", "data": "synthetic",
+            "config": {"workload": f"batched steady-state scan, {len(jobs)} runs",
+                       "ngrid": "U[101,301]", "npart": "U[2048,32768]", "taper": "U[0,2%]",
+                       "detuning": "U[-5e-4,5e-4]", "seed_power": "logU[100 W,10 kW]",
+                       "prng_seed": 1, "params": params},
+            "seconds": rb.seconds, "slice_steps": rb.slice_steps,
+            "device_bytes": rb.device_bytes, "launch_shapes": list(rb.grids),
+            "one_at_a_time": {"value": rs.value, "seconds": rs.seconds},
+            "batched_over_one_at_a_time": rb.value / rs.value, "clocks": c}
+    print(json.dumps(line), flush=True)
+
+
+def run_serve(args):
+    """Served stream with continuous batching; p50/p99 latency beside the
+    throughput."""
+    from genesis4_cuda_port_b200 import host, workloads
+    wl, jobs, arrival, params = workloads.served_stream(args.requests, args.rate)
+    clk = _engine_clocks()
+    clk.start()
+    time.sleep(0.5)
+    st, lat, power, _ = host.serve(workloads.engine(wl, max_runs=256), jobs, arrival)
+    c = clk.stop()
+    line = {"metric": "p99 latency, served stream", "value": st.p99, "unit": "s",
+            "higher_is_better": False, "n_gpus": 1, "dtype": "f32 state, f64 theta",
+            "data": "synthetic",
+            "config": {"workload": f"served stream, {len(jobs)} requests, Poisson "
+                                   f"{args.rate}/s", "nslice": "U{1..64}",
+                       "ngrid": "U[101,255]", "npart": "U[2048,16384]",
+                       "nsteps": "U[110,330]", "admission": "free HBM - 4 GB reserve, "
+                                                           "256 batch slots"},
+            "p50_s": st.p50, "p99_s": st.p99, "mean_s": st.mean,
+            "throughput": {"requests_per_s": st.requests_per_s,
+                           "slice_steps_per_s": st.slice_steps_per_s},
+            "seconds": st.seconds, "peak_concurrency": st.peak_concurrency,
+            "batch_steps": st.batch_steps, "clocks": c}
+    print(json.dumps(line), flush=True)
+
+
+def _load_beam_parallel(wl, threads=12):
+    """Quiet-start beam of a large workload, slices loaded by worker threads."""
+    from concurrent.futures import ThreadPoolExecutor
+    from genesis4_cuda_port_b200 import host
+    n = wl.nslice * wl.npart
+    parts = {k: np.empty(n) for k in ("x", "y", "px", "py", "gamma", "theta")}
+    per = max(1, wl.nslice // threads)
+
+    def load(s0):
+        s1 = min(wl.nslice, s0 + per)
+        sub = type(wl)(**{**wl.__dict__, "nslice": s1 - s0, "seed": wl.seed * 1000003 + s0})
+        o, pp = host.load_beam(sub.beam_spec(), np.full(s1 - s0, wl.current))
+        for k in parts:
+            parts[k][s0 * wl.npart:s1 * wl.npart] = pp[k]
+
+    with ThreadPoolExecutor(threads) as ex:
+        list(ex.map(load, range(0, wl.nslice, per)))
+    off = np.arange(wl.nslice + 1, dtype=np.int64) * wl.npart
+    return off, parts
+
+
+def run_h3(args):
+    """Large time-dependent SASE, fundamental and 3rd harmonic fields."""
+    import torch
+    from genesis4_cuda_port_b200 import device as dev, workloads
+    wl = workloads.large_sase_h3()
+    ctx = dev.Context(int(os.environ.get("LOCAL_RANK", "0")))
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    off, parts = _load_beam_parallel(wl)
+    lat = wl.make_lattice()
+    run = dev.Run(ctx, off, fields=[(1, wl.ngrid, wl.gridmax), (3, wl.ngrid, wl.gridmax)],
+                  lambda0=wl.lambda0, gamma_ref=wl.gamma0, sample=wl.sample, time_run=True,
+                  nbunch=3)
+    run.upload_beam(parts)
+    del parts
+    run.upload_field(0, None, 0)  # SASE: no seed field
+    run.upload_field(1, None, 0)
+    run.set_current(np.full(wl.nslice, wl.current))
+    run.set_lattice(lat.steps, [[lat.fc(i, 1), lat.fc(i, 3)] for i in range(lat.nstep)],
+                    lat.slip, hist_steps=4)
+    K, W = args.steps, args.warmup
+    run.advance(0, W, graph=False)
+    ctx.synchronize()
+    run.prepare(W, K)
+    clk = Clocks(int(os.environ.get("LOCAL_RANK", "0")))
+    clk.start()
+    time.sleep(0.5)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    run.advance(W, K, graph=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    c = clk.stop()
+    line = {"metric": "slice-steps/s, large SASE h=1 and h=3", "value": wl.nslice * K / (ms / 1e3),
+            "unit": UNIT, "n_gpus": 1, "steps": K, "warmup": W, "ms_per_step": ms / K,
+            "higher_is_better": True, "dtype": "f32 state, f64 theta", "data": "synthetic",
+            "config": {"workload": wl.name, "nslice": wl.nslice, "npart": wl.npart,
+                       "ngrid": wl.ngrid, "fields": "h=1, h=3", "nbunch": 3},
+            "device_bytes": run.device_bytes(), "clocks": c}
+    print(json.dumps(line), flush=True)
+
+
+def run_steady(args):
+    """Steady state (1 slice, 8192 particles, ngrid 151): latency per step."""
+    import torch
+    from genesis4_cuda_port_b200 import device as dev, workloads
+    wl = workloads.steady_state()
+    ctx = dev.Context(int(os.environ.get("LOCAL_RANK", "0")))
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    off, parts = wl.make_beam()
+    lat = wl.make_lattice()
+    run = dev.Run(ctx, off, fields=[(1, wl.ngrid, wl.gridmax)], lambda0=wl.lambda0,
+                  gamma_ref=wl.gamma0, sample=1.0, time_run=False, nbunch=1)
+    run.upload_beam(parts)
+    run.upload_field(0, wl.make_field(), 0)
+    run.set_current(np.full(1, wl.current))
+    run.set_lattice(lat.steps, [[lat.fc(i, 1)] for i in range(lat.nstep)], lat.slip)
+    run.advance(0, args.warmup, graph=False)
+    n = lat.nstep
+    run.prepare(0, n)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    run.advance(0, n, graph=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    line = {"metric": "us per step, steady state", "value": 1e3 * ms / n, "unit": "us/step",
+            "higher_is_better": False, "n_gpus": 1, "steps": n, "dtype": "f32 state, f64 theta",
+            "data": "synthetic", "config": {"workload": wl.name}}
+    print(json.dumps(line), flush=True)
+
+
 def run_ours(args, wl, rank, world):
     import torch
 
@@ -334,8 +532,7 @@ def run_ours(args, wl, rank, world):
         def e2e_run():
             mx.upload(pin, pcells)
             mx.run.advance(0, K, graph=False)
-            for i in range(K):
-                hist.append(mx.run.history(i))
+            hist.append(mx.run.history_range(0, K))
             mx.run.download_beam()
             mx.run.download_field(0)
 
@@ -370,6 +567,10 @@ def run_ours(args, wl, rank, world):
             "timing": "CUDA events around each launch on the launching stream, "
                       f"{kp} direct-launch steps following the graph-timed region"}
 
+    acc = None
+    if rank == 0 and not args.no_accuracy:
+        acc = accuracy()
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_sample(wl, args.cpu_slices, args.cpu_steps, lat)
@@ -391,6 +592,7 @@ def run_ours(args, wl, rank, world):
                            "form": "FP64 drop-in, per-phase C-ABI calls, host sync per step",
                            "kernels": fp64_k},
             "mixed_over_fp64_plain": value / value64,
+            "accuracy": acc,
         }
         print(json.dumps(line), flush=True)
     ctx.synchronize()
@@ -407,6 +609,11 @@ def main(argv=None):
     wl = workloads.sase(args.nslice, args.npart, args.ngrid)
     if args.impl == "reference":
         run_reference(args, wl, rank)
+        return
+    if args.workload != "sase":
+        if rank == 0:
+            {"scan": run_scan, "serve": run_serve, "sase_h3": run_h3,
+             "steady": run_steady}[args.workload](args)
         return
     run_ours(args, wl, rank, world)
 

@@ -111,6 +111,7 @@ _SIGS = {
     "g4b_diag_field_static": (C.c_int, [C.c_void_p, c_double_p, c_double_p]),
     "g4b_run_create": (C.c_int, [C.c_void_p, C.POINTER(RunDesc), c_int64_p, c_void_pp]),
     "g4b_run_destroy": (C.c_int, [C.c_void_p]),
+    "g4b_run_history_range": (C.c_int, [C.c_void_p, C.c_int, C.c_int, c_double_p]),
     "g4b_batch_create": (C.c_int, [C.c_void_p, C.c_int, c_void_pp]),
     "g4b_batch_destroy": (C.c_int, [C.c_void_p]),
     "g4b_batch_attach": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, c_int_p]),

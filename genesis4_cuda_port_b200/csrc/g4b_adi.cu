@@ -28,6 +28,8 @@
 #include <complex>
 #include <new>
 
+#include <atomic>
+
 #include "g4b_internal.cuh"
 
 namespace g4b {
@@ -542,8 +544,8 @@ static constexpr double kEev = 510998.95;          // upstream `eev`
 
 template <typename T, int M, bool PX>
 static int configure_pass_t(int device) {
-  static uint64_t configured = 0;  // per instantiation, one bit per device
-  if (device < 64 && (configured >> device) & 1) return G4B_OK;
+  static std::atomic<uint64_t> configured{0};  // per instantiation, one bit per device
+  if (device < 64 && (configured.load() >> device) & 1) return G4B_OK;
   // static + dynamic shared memory must fit the 227 KB a CTA may use
   cudaFuncAttributes fa;
   cudaError_t e = cudaFuncGetAttributes(&fa, adi_pass_kernel<T, M, PX>);
@@ -551,7 +553,7 @@ static int configure_pass_t(int device) {
   e = cudaFuncSetAttribute(adi_pass_kernel<T, M, PX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            227 * 1024 - (int)fa.sharedSizeBytes);
   if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(adi_pass)");
-  if (device < 64) configured |= 1ull << device;
+  if (device < 64) configured.fetch_or(1ull << device);
   return G4B_OK;
 }
 
@@ -688,16 +690,16 @@ int adi_run(g4b_adi* adi, g4b_field* f, const void* src, const int4* desc,
 
 template <int M, bool PX>
 static int batch_launch_t(g4b_ctx* c, const AdiBatchArgs& b, size_t smem, int grid) {
-  static uint64_t configured = 0;
+  static std::atomic<uint64_t> configured{0};
   auto kern = adi_batch_kernel<float, M, PX>;
-  if (c->device >= 64 || !((configured >> c->device) & 1)) {
+  if (c->device >= 64 || !((configured.load() >> c->device) & 1)) {
     cudaFuncAttributes fa;
     cudaError_t e = cudaFuncGetAttributes(&fa, kern);
     if (e != cudaSuccess) return cuda_fail(e, "cudaFuncGetAttributes(adi_batch)");
     e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              227 * 1024 - (int)fa.sharedSizeBytes);
     if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(adi_batch)");
-    if (c->device < 64) configured |= 1ull << c->device;
+    if (c->device < 64) configured.fetch_or(1ull << c->device);
   }
   {
     LaunchScope ls(c, PX ? "batch_adi_x" : "batch_adi_y");
@@ -748,8 +750,8 @@ int g4b_adi_create(g4b_ctx* c, g4b_adi** out) {
 int g4b_adi_destroy(g4b_adi* a) {
   if (!a) return G4B_OK;
   ctx_quiesce(a->ctx);
-  if (a->d_tab64) cudaFree(a->d_tab64);
-  if (a->d_tab32) cudaFree(a->d_tab32);
+  dev_free(a->ctx, a->d_tab64);
+  dev_free(a->ctx, a->d_tab32);
   ctx_release(a->ctx);
   delete a;
   return G4B_OK;
@@ -843,13 +845,13 @@ int g4b_adi_init(g4b_adi* a, double delz, double dgrid, double xks, int ngrid) {
   G4B_CUDA_TRY(cudaSetDevice(ctx->device));
   if (a->d_tab64) {
     cudaStreamSynchronize(ctx->stream);
-    cudaFree(a->d_tab64);
-    cudaFree(a->d_tab32);
+    dev_free(a->ctx, a->d_tab64);
+    dev_free(a->ctx, a->d_tab32);
     a->d_tab64 = nullptr;
     a->d_tab32 = nullptr;
   }
-  G4B_CUDA_TRY(cudaMalloc(&a->d_tab64, tot * sizeof(double2)));
-  G4B_CUDA_TRY(cudaMalloc(&a->d_tab32, tot * sizeof(float2)));
+  G4B_CUDA_TRY(dev_alloc(a->ctx, (void**)&a->d_tab64, tot * sizeof(double2)));
+  G4B_CUDA_TRY(dev_alloc(a->ctx, (void**)&a->d_tab32, tot * sizeof(float2)));
   G4B_CUDA_TRY(cudaMemcpyAsync(a->d_tab64, t64.data(), tot * sizeof(double2),
                                cudaMemcpyHostToDevice, ctx->stream));
   G4B_CUDA_TRY(cudaMemcpyAsync(a->d_tab32, t32.data(), tot * sizeof(float2),
@@ -916,13 +918,9 @@ int g4b_adi_advance(g4b_adi* adi, g4b_field* f, g4b_beam* b, const g4b_step* st,
     da.err = c->d_error;
     const size_t acc_bytes = 96 * 1024;
     da.acc_cells = (int)(acc_bytes / 16);
-    static bool configured = false;
-    if (!configured) {
-      G4B_CUDA_TRY(cudaFuncSetAttribute(deposit_slice_kernel,
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)acc_bytes));
-      configured = true;
-    }
+    G4B_CUDA_TRY(cudaFuncSetAttribute(deposit_slice_kernel,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)acc_bytes));  // per device, cheap
     {
       LaunchScope ls(c, "deposit");
       deposit_slice_kernel<<<f->nslice, 512, acc_bytes, c->stream>>>(da);

@@ -25,6 +25,16 @@ int cuda_fail(cudaError_t e, const char* where) {
   return e == cudaErrorMemoryAllocation ? G4B_ERR_NOMEM : G4B_ERR_CUDA;
 }
 
+cudaError_t dev_alloc(g4b_ctx* c, void** p, size_t bytes) {
+  *p = nullptr;
+  if (bytes == 0) bytes = 16;
+  return cudaMallocAsync(p, bytes, c->stream);
+}
+
+void dev_free(g4b_ctx* c, void* p) {
+  if (p) cudaFreeAsync(p, c->stream);
+}
+
 int check_launch(g4b_ctx* ctx, const char* what) {
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, what);
@@ -103,13 +113,37 @@ void prof_end(g4b_ctx* c) {
   if (p.pending.size() > 8192) prof_resolve(c);
 }
 
+// The context's device resources (stream, error flag, events) live until the
+// last reference goes: objects created on a context keep working after
+// g4b_ctx_destroy released the handle.
+static void ctx_teardown(g4b_ctx* c) {
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->d_error) cudaFree(c->d_error);
+  c->d_error = nullptr;
+  for (auto& q : c->prof.pending) {
+    cudaEventDestroy(q.a);
+    cudaEventDestroy(q.b);
+  }
+  c->prof.pending.clear();
+  for (auto e : c->marks) cudaEventDestroy(e);
+  c->marks.clear();
+  for (auto e : c->prof.pool) cudaEventDestroy(e);
+  c->prof.pool.clear();
+  if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+  c->stream = nullptr;
+}
+
 void ctx_release(g4b_ctx* c) {
-  if (--c->refs == 0) delete c;
+  if (--c->refs == 0) {
+    ctx_teardown(c);
+    delete c;
+  }
 }
 
 void ctx_quiesce(g4b_ctx* c) {
   cudaSetDevice(c->device);
-  if (!c->destroyed && c->stream) cudaStreamSynchronize(c->stream);
+  if (c->stream) cudaStreamSynchronize(c->stream);
 }
 
 int pick_M(int n) {
@@ -177,6 +211,14 @@ int g4b_ctx_create(int device, g4b_ctx** out) {
     return cuda_fail(e, "cudaStreamCreateWithFlags");
   }
   c->own_stream = true;
+  {
+    // keep released stream-ordered blocks in the pool (process-local setting)
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+      uint64_t thr = ~0ull;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+  }
   e = cudaMalloc(&c->d_error, sizeof(int));
   if (e == cudaSuccess) e = cudaMemset(c->d_error, 0, sizeof(int));
   if (e != cudaSuccess) {
@@ -194,21 +236,6 @@ int g4b_ctx_create(int device, g4b_ctx** out) {
 
 int g4b_ctx_destroy(g4b_ctx* c) {
   if (!c || c->destroyed) return G4B_OK;
-  cudaSetDevice(c->device);
-  if (c->stream) cudaStreamSynchronize(c->stream);
-  if (c->d_error) cudaFree(c->d_error);
-  c->d_error = nullptr;
-  for (auto& q : c->prof.pending) {
-    cudaEventDestroy(q.a);
-    cudaEventDestroy(q.b);
-  }
-  c->prof.pending.clear();
-  for (auto e : c->marks) cudaEventDestroy(e);
-  c->marks.clear();
-  for (auto e : c->prof.pool) cudaEventDestroy(e);
-  c->prof.pool.clear();
-  if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
-  c->stream = nullptr;
   c->destroyed = true;
   ctx_release(c);
   return G4B_OK;
@@ -280,6 +307,14 @@ int g4b_ctx_mem_info(g4b_ctx* c, uint64_t* free_bytes, uint64_t* total_bytes) {
   G4B_CUDA_TRY(cudaSetDevice(c->device));
   size_t f = 0, t = 0;
   G4B_CUDA_TRY(cudaMemGetInfo(&f, &t));
+  // blocks released to the default pool are free for this process too
+  cudaMemPool_t pool;
+  uint64_t reserved = 0, used = 0;
+  if (cudaDeviceGetDefaultMemPool(&pool, c->device) == cudaSuccess &&
+      cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved) == cudaSuccess &&
+      cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used) == cudaSuccess &&
+      reserved > used)
+    f += reserved - used;
   *free_bytes = f;
   *total_bytes = t;
   return G4B_OK;
@@ -365,10 +400,10 @@ int g4b_field_create(g4b_ctx* c, int nslice, int ngrid, double gridmax,
   f->store_nbox = (ngrid + 255) / 256;
   f->store_box_rows = ((ngrid + f->store_nbox - 1) / f->store_nbox + 7) / 8 * 8;
   const size_t bytes = (size_t)nslice * ngrid * f->ld * f->cell_bytes + 256;
-  cudaError_t e = cudaMalloc(&f->a, bytes);
-  if (e == cudaSuccess) e = cudaMalloc(&f->b, bytes);
-  if (e == cudaSuccess) e = cudaMalloc(&f->src, bytes);
-  if (e == cudaSuccess) e = cudaMalloc(&f->desc, nslice * sizeof(int4));
+  cudaError_t e = dev_alloc(c, &f->a, bytes);
+  if (e == cudaSuccess) e = dev_alloc(c, &f->b, bytes);
+  if (e == cudaSuccess) e = dev_alloc(c, &f->src, bytes);
+  if (e == cudaSuccess) e = dev_alloc(c, (void**)&f->desc, nslice * sizeof(int4));
   if (e == cudaSuccess) e = cudaMemsetAsync(f->desc, 0, nslice * sizeof(int4), c->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(f->a, 0, bytes, c->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(f->b, 0, bytes, c->stream);
@@ -393,16 +428,38 @@ int g4b_field_create(g4b_ctx* c, int nslice, int ngrid, double gridmax,
 int g4b_field_destroy(g4b_field* f) {
   if (!f) return G4B_OK;
   ctx_quiesce(f->ctx);
-  if (f->a) cudaFree(f->a);
-  if (f->b) cudaFree(f->b);
-  if (f->src) cudaFree(f->src);
-  if (f->desc) cudaFree(f->desc);
+  dev_free(f->ctx, f->a);
+  dev_free(f->ctx, f->b);
+  dev_free(f->ctx, f->src);
+  dev_free(f->ctx, f->desc);
   ctx_release(f->ctx);
   delete f;
   return G4B_OK;
 }
 
 // Host (re,im) doubles [slice][iy][ix] <-> device cells [slice][iy][ld].
+// Row-wise conversions between FP64 cells (rows of n, unpadded) and the
+// mixed form's complex64 rows (pitch ld).
+__global__ void cells_f64_to_f32(const double2* src, float2* dst, int n, int ld, size_t rows) {
+  const size_t total = rows * (size_t)n;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const size_t r = i / n, k = i - r * n;
+    const double2 v = src[i];
+    dst[r * ld + k] = make_float2((float)v.x, (float)v.y);
+  }
+}
+
+__global__ void cells_f32_to_f64(const float2* src, double2* dst, int n, int ld, size_t rows) {
+  const size_t total = rows * (size_t)n;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const size_t r = i / n, k = i - r * n;
+    const float2 v = src[r * ld + k];
+    dst[i] = make_double2((double)v.x, (double)v.y);
+  }
+}
+
 static int field_copy(g4b_field* f, double* host, bool upload) {
   g4b_ctx* c = f->ctx;
   G4B_CUDA_TRY(cudaSetDevice(c->device));
@@ -418,21 +475,33 @@ static int field_copy(g4b_field* f, double* host, bool upload) {
     G4B_CUDA_TRY(cudaStreamSynchronize(c->stream));
     return G4B_OK;
   }
-  // mixed: convert through a host staging buffer of pitched float2 rows
-  std::vector<float> stage(rows * f->ld * 2, 0.0f);
-  if (upload) {
-    for (size_t r = 0; r < rows; ++r)
-      for (size_t i = 0; i < 2 * n; ++i) stage[r * 2 * f->ld + i] = (float)host[r * 2 * n + i];
-    G4B_CUDA_TRY(cudaMemcpyAsync(f->a, stage.data(), stage.size() * 4,
-                                 cudaMemcpyHostToDevice, c->stream));
-    G4B_CUDA_TRY(cudaStreamSynchronize(c->stream));
-  } else {
-    G4B_CUDA_TRY(cudaMemcpyAsync(stage.data(), f->a, stage.size() * 4,
-                                 cudaMemcpyDeviceToHost, c->stream));
-    G4B_CUDA_TRY(cudaStreamSynchronize(c->stream));
-    for (size_t r = 0; r < rows; ++r)
-      for (size_t i = 0; i < 2 * n; ++i) host[r * 2 * n + i] = stage[r * 2 * f->ld + i];
+  // mixed: FP64 rows cross the bus and are converted on the device, in
+  // chunks of whole rows through a staging buffer
+  const size_t row_bytes = n * 16;
+  const size_t chunk_rows = std::max<size_t>(1, std::min(rows, (size_t)(64u << 20) / row_bytes));
+  double2* stage = nullptr;
+  G4B_CUDA_TRY(dev_alloc(c, (void**)&stage, chunk_rows * row_bytes));
+  cudaError_t e = cudaSuccess;
+  float2* a = static_cast<float2*>(f->a);
+  for (size_t r0 = 0; r0 < rows && e == cudaSuccess; r0 += chunk_rows) {
+    const size_t nr = std::min(chunk_rows, rows - r0);
+    const unsigned grid = (unsigned)std::min<size_t>((nr * n + 255) / 256, 65535u * 32u);
+    if (upload) {
+      e = cudaMemcpyAsync(stage, host + r0 * 2 * n, nr * row_bytes, cudaMemcpyHostToDevice,
+                          c->stream);
+      if (e == cudaSuccess)
+        cells_f64_to_f32<<<grid, 256, 0, c->stream>>>(stage, a + r0 * f->ld, (int)n, f->ld, nr);
+    } else {
+      cells_f32_to_f64<<<grid, 256, 0, c->stream>>>(a + r0 * f->ld, stage, (int)n, f->ld, nr);
+      e = cudaMemcpyAsync(host + r0 * 2 * n, stage, nr * row_bytes, cudaMemcpyDeviceToHost,
+                          c->stream);
+    }
+    if (e == cudaSuccess) e = cudaGetLastError();
   }
+  dev_free(c, stage);
+  const cudaError_t es = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "field copy");
+  if (es != cudaSuccess) return cuda_fail(es, "field copy");
   return G4B_OK;
 }
 
@@ -504,13 +573,13 @@ int g4b_beam_create(g4b_ctx* c, int nslice, const int64_t* off, int precision,
   cudaError_t e = cudaSuccess;
   double** arrs[6] = {&b->x, &b->y, &b->px, &b->py, &b->gamma, &b->theta};
   for (double** a : arrs)
-    if (e == cudaSuccess) e = cudaMalloc(a, np * sizeof(double));
-  if (e == cudaSuccess) e = cudaMalloc(&b->d_off, (nslice + 1) * sizeof(int64_t));
-  if (e == cudaSuccess) e = cudaMalloc(&b->d_current, nslice * sizeof(double));
-  if (e == cudaSuccess) e = cudaMalloc(&b->d_eloss, nslice * sizeof(double));
-  if (e == cudaSuccess) e = cudaMalloc(&b->d_scl, nslice * sizeof(double));
+    if (e == cudaSuccess) e = dev_alloc(c, (void**)a, np * sizeof(double));
+  if (e == cudaSuccess) e = dev_alloc(c, (void**)&b->d_off, (nslice + 1) * sizeof(int64_t));
+  if (e == cudaSuccess) e = dev_alloc(c, (void**)&b->d_current, nslice * sizeof(double));
+  if (e == cudaSuccess) e = dev_alloc(c, (void**)&b->d_eloss, nslice * sizeof(double));
+  if (e == cudaSuccess) e = dev_alloc(c, (void**)&b->d_scl, nslice * sizeof(double));
   if (e == cudaSuccess)
-    e = cudaMalloc(&b->d_chunks, std::max(1, b->nchunk) * sizeof(int4));
+    e = dev_alloc(c, (void**)&b->d_chunks, std::max(1, b->nchunk) * sizeof(int4));
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(b->d_off, off, (nslice + 1) * sizeof(int64_t),
                         cudaMemcpyHostToDevice, c->stream);
@@ -535,8 +604,7 @@ int g4b_beam_destroy(g4b_beam* b) {
   ctx_quiesce(b->ctx);
   void* ptrs[] = {b->x, b->y, b->px, b->py, b->gamma, b->theta, b->d_off,
                   b->d_current, b->d_eloss, b->d_scl, b->d_chunks};
-  for (void* p : ptrs)
-    if (p) cudaFree(p);
+  for (void* p : ptrs) dev_free(b->ctx, p);
   ctx_release(b->ctx);
   delete b;
   return G4B_OK;

@@ -150,6 +150,13 @@ struct LaunchScope {
   }
 };
 
+// Stream-ordered device memory from the device's default pool: allocation and
+// release are ordered on the context's stream, so neither waits for other
+// streams' work (cudaFree would synchronise the whole device); released
+// blocks stay in the pool for reuse.
+cudaError_t dev_alloc(g4b_ctx* ctx, void** p, size_t bytes);
+void dev_free(g4b_ctx* ctx, void* p);
+
 int check_launch(g4b_ctx* ctx, const char* what);
 int read_device_error(g4b_ctx* ctx, const char* what);
 

@@ -839,6 +839,31 @@ __global__ void finalize_batch_kernel(const FinalizeArgs* args, const int* nruns
   for (int r = blockIdx.x; r < n; r += gridDim.x) finalize_range(args[r], threadIdx.x, blockDim.x);
 }
 
+// Particle conversions between FP64 host arrays (x, y, px, py, gamma, each
+// `stride` apart in the staging buffer) and the mixed form's state.
+__global__ void beam_f64_to_mixed(const double* stage, size_t stride, size_t m, float gf,
+                                  float2* xy, float2* pxy, float* dg) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < m;
+       i += (size_t)gridDim.x * blockDim.x) {
+    xy[i] = make_float2((float)stage[i], (float)stage[stride + i]);
+    pxy[i] = make_float2((float)stage[2 * stride + i], (float)stage[3 * stride + i]);
+    dg[i] = (float)(stage[4 * stride + i] - (double)gf);
+  }
+}
+
+__global__ void beam_mixed_to_f64(const float2* xy, const float2* pxy, const float* dg,
+                                  double gf, size_t m, double* stage, size_t stride) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < m;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const float2 a = xy[i], b = pxy[i];
+    stage[i] = a.x;
+    stage[stride + i] = a.y;
+    stage[2 * stride + i] = b.x;
+    stage[3 * stride + i] = b.y;
+    stage[4 * stride + i] = gf + (double)dg[i];
+  }
+}
+
 static PlaneMapF plane_map_f(double strength, double offset) {
   PlaneMapF m{0, (float)strength, 0.f};
   if (strength == 0.0) return m;
@@ -1217,7 +1242,7 @@ int g4b_run_create(g4b_ctx* c, const g4b_run_desc* d, const int64_t* off, g4b_ru
   const size_t np = (size_t)std::max<int64_t>(r->npart, 1);
   cudaError_t e = cudaSuccess;
   auto A = [&](void** p, size_t b) {
-    if (e == cudaSuccess) e = cudaMalloc(p, b);
+    if (e == cudaSuccess) e = dev_alloc(c, p, b);
     if (e == cudaSuccess) r->bytes += b;
   };
   A((void**)&r->xy, np * 8);
@@ -1286,42 +1311,50 @@ int g4b_run_destroy(g4b_run* r) {
   if (r->gexec) cudaGraphExecDestroy(r->gexec);
   void* ptrs[] = {r->xy, r->pxy, r->dg, r->th, r->d_off, r->d_chunks, r->d_current,
                   r->d_eloss, r->d_hist, r->d_beam_part};
-  for (void* p : ptrs)
-    if (p) cudaFree(p);
+  for (void* p : ptrs) dev_free(r->ctx, p);
   for (int f = 0; f < kRunFields; ++f) {
     RunFieldState& F = r->fs[f];
     for (g4b_adi* a : F.adis) g4b_adi_destroy(a);
     if (F.f) g4b_field_destroy(F.f);
-    if (F.d_bbox) cudaFree(F.d_bbox);
-    if (F.d_part) cudaFree(F.d_part);
+    dev_free(r->ctx, F.d_bbox);
+    dev_free(r->ctx, F.d_part);
   }
   ctx_release(r->ctx);
   delete r;
   return G4B_OK;
 }
 
+// FP64 particle arrays cross the bus and are converted on the device, in
+// chunks through a staging buffer (theta stays FP64 and is copied directly).
 int g4b_run_upload_beam(g4b_run* r, const double* x, const double* y, const double* px,
                         const double* py, const double* gamma, const double* theta) {
   if (!r || !x || !y || !px || !py || !gamma || !theta)
     return fail(G4B_ERR_ARG, "g4b_run_upload_beam: null arg");
   G4B_CUDA_TRY(cudaSetDevice(r->ctx->device));
   const size_t n = (size_t)r->npart;
-  std::vector<float2> xy(n), pp(n);
-  std::vector<float> dg(n);
-  const float gf = (float)r->desc.gamma_ref;
-  for (size_t i = 0; i < n; ++i) {
-    xy[i] = make_float2((float)x[i], (float)y[i]);
-    pp[i] = make_float2((float)px[i], (float)py[i]);
-    dg[i] = (float)(gamma[i] - (double)gf);
-  }
   cudaStream_t s = r->ctx->stream;
-  if (n) {
-    G4B_CUDA_TRY(cudaMemcpyAsync(r->xy, xy.data(), n * 8, cudaMemcpyHostToDevice, s));
-    G4B_CUDA_TRY(cudaMemcpyAsync(r->pxy, pp.data(), n * 8, cudaMemcpyHostToDevice, s));
-    G4B_CUDA_TRY(cudaMemcpyAsync(r->dg, dg.data(), n * 4, cudaMemcpyHostToDevice, s));
-    G4B_CUDA_TRY(cudaMemcpyAsync(r->th, theta, n * 8, cudaMemcpyHostToDevice, s));
+  if (n == 0) return G4B_OK;
+  const size_t chunk = std::min(n, (size_t)(64u << 20) / 40);
+  double* stage = nullptr;
+  G4B_CUDA_TRY(dev_alloc(r->ctx, (void**)&stage, chunk * 40));
+  const double* src[5] = {x, y, px, py, gamma};
+  cudaError_t e = cudaMemcpyAsync(r->th, theta, n * 8, cudaMemcpyHostToDevice, s);
+  const float gf = (float)r->desc.gamma_ref;
+  for (size_t p0 = 0; p0 < n && e == cudaSuccess; p0 += chunk) {
+    const size_t m = std::min(chunk, n - p0);
+    for (int k = 0; k < 5 && e == cudaSuccess; ++k)
+      e = cudaMemcpyAsync(stage + k * chunk, src[k] + p0, m * 8, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) {
+      const unsigned grid = (unsigned)std::min<size_t>((m + 255) / 256, 1u << 20);
+      beam_f64_to_mixed<<<grid, 256, 0, s>>>(stage, chunk, m, gf, r->xy + p0, r->pxy + p0,
+                                             r->dg + p0);
+      e = cudaGetLastError();
+    }
   }
-  G4B_CUDA_TRY(cudaStreamSynchronize(s));
+  dev_free(r->ctx, stage);
+  const cudaError_t es = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_fail(e, "g4b_run_upload_beam");
+  if (es != cudaSuccess) return cuda_fail(es, "g4b_run_upload_beam");
   return G4B_OK;
 }
 
@@ -1330,32 +1363,44 @@ int g4b_run_download_beam(g4b_run* r, double* x, double* y, double* px, double* 
   if (!r) return fail(G4B_ERR_ARG, "g4b_run_download_beam: null run");
   G4B_CUDA_TRY(cudaSetDevice(r->ctx->device));
   const size_t n = (size_t)r->npart;
-  std::vector<float2> xy(n), pp(n);
-  std::vector<float> dg(n);
   cudaStream_t s = r->ctx->stream;
-  if (n) {
-    G4B_CUDA_TRY(cudaMemcpyAsync(xy.data(), r->xy, n * 8, cudaMemcpyDeviceToHost, s));
-    G4B_CUDA_TRY(cudaMemcpyAsync(pp.data(), r->pxy, n * 8, cudaMemcpyDeviceToHost, s));
-    G4B_CUDA_TRY(cudaMemcpyAsync(dg.data(), r->dg, n * 4, cudaMemcpyDeviceToHost, s));
-    if (theta) G4B_CUDA_TRY(cudaMemcpyAsync(theta, r->th, n * 8, cudaMemcpyDeviceToHost, s));
-  }
-  G4B_CUDA_TRY(cudaStreamSynchronize(s));
+  if (n == 0) return read_device_error(r->ctx, "g4b_run_download_beam");
+  const size_t chunk = std::min(n, (size_t)(64u << 20) / 40);
+  double* stage = nullptr;
+  G4B_CUDA_TRY(dev_alloc(r->ctx, (void**)&stage, chunk * 40));
+  double* dst[5] = {x, y, px, py, gamma};
+  cudaError_t e = theta ? cudaMemcpyAsync(theta, r->th, n * 8, cudaMemcpyDeviceToHost, s)
+                        : cudaSuccess;
   const double gf = (double)(float)r->desc.gamma_ref;
-  for (size_t i = 0; i < n; ++i) {
-    if (x) x[i] = xy[i].x;
-    if (y) y[i] = xy[i].y;
-    if (px) px[i] = pp[i].x;
-    if (py) py[i] = pp[i].y;
-    if (gamma) gamma[i] = gf + (double)dg[i];
+  for (size_t p0 = 0; p0 < n && e == cudaSuccess; p0 += chunk) {
+    const size_t m = std::min(chunk, n - p0);
+    const unsigned grid = (unsigned)std::min<size_t>((m + 255) / 256, 1u << 20);
+    beam_mixed_to_f64<<<grid, 256, 0, s>>>(r->xy + p0, r->pxy + p0, r->dg + p0, gf, m, stage,
+                                           chunk);
+    e = cudaGetLastError();
+    for (int k = 0; k < 5 && e == cudaSuccess; ++k)
+      if (dst[k]) e = cudaMemcpyAsync(dst[k] + p0, stage + k * chunk, m * 8,
+                                      cudaMemcpyDeviceToHost, s);
   }
+  dev_free(r->ctx, stage);
+  const cudaError_t es = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_fail(e, "g4b_run_download_beam");
+  if (es != cudaSuccess) return cuda_fail(es, "g4b_run_download_beam");
   return read_device_error(r->ctx, "g4b_run_download_beam");
 }
 
 int g4b_run_upload_field(g4b_run* r, int fi, const double* cells, int first) {
-  if (!r || fi < 0 || fi >= r->nfield || !cells)
+  if (!r || fi < 0 || fi >= r->nfield || first < 0 || first >= r->nslice)
     return fail(G4B_ERR_ARG, "g4b_run_upload_field: bad argument");
   RunFieldState& F = r->fs[fi];
-  if (int rc = g4b_field_upload(F.f, cells)) return rc;
+  if (cells) {
+    if (int rc = g4b_field_upload(F.f, cells)) return rc;
+  } else {  // a zero field (no seed)
+    G4B_CUDA_TRY(cudaSetDevice(r->ctx->device));
+    G4B_CUDA_TRY(cudaMemsetAsync(F.f->a, 0, (size_t)F.f->nslice * F.f->ngrid * F.f->ld *
+                                                F.f->cell_bytes, r->ctx->stream));
+    G4B_CUDA_TRY(cudaStreamSynchronize(r->ctx->stream));
+  }
   if (int rc = g4b_field_set_first(F.f, first)) return rc;
   F.first = first;
   F.accuslip = 0.0;
@@ -1418,9 +1463,9 @@ int g4b_run_set_lattice(g4b_run* r, int nstep, const g4b_step* steps, const doub
     if (int rc = adi_configure(F.f)) return rc;
   }
   const int hs = hist_steps > 0 ? hist_steps : nstep;
-  if (r->d_hist) cudaFree(r->d_hist);
+  dev_free(r->ctx, r->d_hist);
   r->d_hist = nullptr;
-  G4B_CUDA_TRY(cudaMalloc(&r->d_hist, (size_t)hs * r->step_doubles * 8));
+  G4B_CUDA_TRY(dev_alloc(r->ctx, (void**)&r->d_hist, (size_t)hs * r->step_doubles * 8));
   G4B_CUDA_TRY(cudaMemsetAsync(r->d_hist, 0, (size_t)hs * r->step_doubles * 8, r->ctx->stream));
   r->hist_steps = hs;
   if (r->gexec) {
@@ -1542,6 +1587,27 @@ int g4b_run_history(g4b_run* r, int step, double* beam, double* field) {
   return read_device_error(r->ctx, "g4b_run_history");
 }
 
+// Diagnostics of steps [first, first + n) in one read: out[n][step record],
+// a step record being beam [nslice][23 + 2 nbunch] then field [nfield][nslice][9].
+int g4b_run_history_range(g4b_run* r, int first, int n, double* out) {
+  if (!r || first < 0 || n < 0 || !out) return fail(G4B_ERR_ARG, "g4b_run_history_range: bad arg");
+  if (!r->d_hist) return fail(G4B_ERR_STATE, "g4b_run_history_range: no lattice");
+  if (n > r->hist_steps)
+    return fail(G4B_ERR_RANGE, "g4b_run_history_range: more steps than the history keeps");
+  G4B_CUDA_TRY(cudaSetDevice(r->ctx->device));
+  const size_t sd = r->step_doubles;
+  int done = 0;
+  while (done < n) {
+    const int slot = (first + done) % r->hist_steps;
+    const int cnt = std::min(n - done, r->hist_steps - slot);
+    G4B_CUDA_TRY(cudaMemcpyAsync(out + (size_t)done * sd, r->d_hist + (size_t)slot * sd,
+                                 (size_t)cnt * sd * 8, cudaMemcpyDeviceToHost, r->ctx->stream));
+    done += cnt;
+  }
+  G4B_CUDA_TRY(cudaStreamSynchronize(r->ctx->stream));
+  return read_device_error(r->ctx, "g4b_run_history_range");
+}
+
 int g4b_run_device_bytes(g4b_run* r, uint64_t* bytes) {
   if (!r || !bytes) return fail(G4B_ERR_ARG, "g4b_run_device_bytes: null arg");
   *bytes = r->bytes + (uint64_t)r->hist_steps * r->step_doubles * 8;
@@ -1599,8 +1665,12 @@ struct g4b_batch {
   // work lists
   std::vector<int2> beam_items, dep_items;
   std::vector<int4> adi_items[kNumM];
-  size_t items_cap = 0;
+  size_t items_cap = 0, h_items_cap[2] = {0, 0};
   unsigned char* d_items = nullptr;
+  unsigned char* h_items[2] = {nullptr, nullptr};  // pinned, alternating
+  cudaEvent_t items_copied[2] = {nullptr, nullptr};
+  int ibuf = 0;
+  int stable = 0;               // steps since the composition last changed
   size_t off_beam = 0, off_dep = 0, off_adi[kNumM] = {};
   BatchCounts counts{};
   size_t smem_x[kNumM] = {}, smem_y[kNumM] = {};
@@ -1701,21 +1771,36 @@ int batch_rebuild(g4b_batch* b) {
     need = align_up<int4>(need + b->adi_items[m].size() * sizeof(int4));
   }
   need = std::max<size_t>(need, 256);
-  if (need > b->items_cap) {
-    if (b->d_items) cudaFree(b->d_items);
+  if (need > b->items_cap) {  // stream-ordered: the old lists' readers finish first
+    dev_free(b->ctx, b->d_items);
     b->d_items = nullptr;
-    G4B_CUDA_TRY(cudaMalloc(&b->d_items, need));
-    b->items_cap = need;
+    b->items_cap = 0;
+    G4B_CUDA_TRY(dev_alloc(b->ctx, (void**)&b->d_items, need * 2));
+    b->items_cap = need * 2;
   }
-  std::vector<unsigned char> h(need, 0);
-  std::memcpy(h.data() + b->off_beam, b->beam_items.data(), b->beam_items.size() * sizeof(int2));
-  std::memcpy(h.data() + b->off_dep, b->dep_items.data(), b->dep_items.size() * sizeof(int2));
+  // pinned staging, alternating buffers: wait only for the copy that used
+  // this buffer two rebuilds ago
+  const int k = b->ibuf;
+  if (!b->items_copied[k])
+    G4B_CUDA_TRY(cudaEventCreateWithFlags(&b->items_copied[k], cudaEventDisableTiming));
+  G4B_CUDA_TRY(cudaEventSynchronize(b->items_copied[k]));
+  if (need > b->h_items_cap[k]) {
+    if (b->h_items[k]) cudaFreeHost(b->h_items[k]);
+    b->h_items[k] = nullptr;
+    b->h_items_cap[k] = 0;
+    G4B_CUDA_TRY(cudaMallocHost(&b->h_items[k], need * 2));
+    b->h_items_cap[k] = need * 2;
+  }
+  unsigned char* h = b->h_items[k];
+  std::memcpy(h + b->off_beam, b->beam_items.data(), b->beam_items.size() * sizeof(int2));
+  std::memcpy(h + b->off_dep, b->dep_items.data(), b->dep_items.size() * sizeof(int2));
   for (int m = 0; m < kNumM; ++m)
-    std::memcpy(h.data() + b->off_adi[m], b->adi_items[m].data(),
+    std::memcpy(h + b->off_adi[m], b->adi_items[m].data(),
                 b->adi_items[m].size() * sizeof(int4));
-  G4B_CUDA_TRY(cudaMemcpyAsync(b->d_items, h.data(), need, cudaMemcpyHostToDevice,
-                               b->ctx->stream));
-  G4B_CUDA_TRY(cudaStreamSynchronize(b->ctx->stream));
+  G4B_CUDA_TRY(cudaMemcpyAsync(b->d_items, h, need, cudaMemcpyHostToDevice, b->ctx->stream));
+  G4B_CUDA_TRY(cudaEventRecord(b->items_copied[k], b->ctx->stream));
+  b->ibuf ^= 1;
+  b->stable = 0;
   b->dirty = false;
   b->graph_valid = false;
   return G4B_OK;
@@ -1863,7 +1948,11 @@ int g4b_batch_destroy(g4b_batch* b) {
   for (auto e : b->ev)
     if (e) cudaEventDestroy(e);
   if (b->d_args) cudaFree(b->d_args);
-  if (b->d_items) cudaFree(b->d_items);
+  dev_free(b->ctx, b->d_items);
+  for (int k = 0; k < 2; ++k) {
+    if (b->h_items[k]) cudaFreeHost(b->h_items[k]);
+    if (b->items_copied[k]) cudaEventDestroy(b->items_copied[k]);
+  }
   ctx_release(b->ctx);
   delete b;
   return G4B_OK;
@@ -1874,7 +1963,8 @@ int g4b_batch_destroy(g4b_batch* b) {
 int g4b_batch_attach(g4b_batch* b, g4b_run* r, int first_step, int nsteps, int* slot) {
   if (!b || !r || !slot || nsteps < 0 || first_step < 0)
     return fail(G4B_ERR_ARG, "g4b_batch_attach: bad arg");
-  if (r->ctx != b->ctx) return fail(G4B_ERR_ARG, "g4b_batch_attach: run on another context");
+  if (r->ctx->device != b->ctx->device)
+    return fail(G4B_ERR_ARG, "g4b_batch_attach: run on another device");
   if (r->steps.empty()) return fail(G4B_ERR_STATE, "g4b_batch_attach: run has no lattice");
   for (int f = 0; f < r->nfield; ++f)
     if (r->fs[f].f->precision != G4B_MIXED)
@@ -1893,12 +1983,12 @@ int g4b_batch_attach(g4b_batch* b, g4b_run* r, int first_step, int nsteps, int* 
   return fail(G4B_ERR_RANGE, "g4b_batch_attach: no free slot");
 }
 
-// Detach the run in `slot` (the run itself is not destroyed).  Waits for the
-// batch's queued work first.
+// Detach the run in `slot` (the run itself is not destroyed); later steps
+// leave it out.  Steps already enqueued may still use it: destroy it only
+// after they completed (a g4b_ctx_mark after its last step).
 int g4b_batch_detach(g4b_batch* b, int slot) {
   if (!b || slot < 0 || slot >= b->max_runs || !b->runs[slot])
     return fail(G4B_ERR_ARG, "g4b_batch_detach: bad slot");
-  G4B_CUDA_TRY(cudaStreamSynchronize(b->ctx->stream));
   b->runs[slot] = nullptr;
   b->dirty = true;
   return G4B_OK;
@@ -1970,7 +2060,8 @@ int g4b_batch_step(g4b_batch* b, int nsteps, int use_graph) {
         }
         b->graph_valid = false;
       }
-    } else if (use_graph) {
+    } else if (use_graph && b->stable >= 2) {
+      // a graph pays once the composition holds for a few steps
       if (!b->graph_valid) {
         if (b->gexec) cudaGraphExecDestroy(b->gexec);
         b->gexec = nullptr;
@@ -1993,6 +2084,7 @@ int g4b_batch_step(g4b_batch* b, int nsteps, int use_graph) {
       if (int rc = batch_launch(b, false)) return rc;
     }
     b->steps_done++;
+    b->stable++;
   }
   return G4B_OK;
 }

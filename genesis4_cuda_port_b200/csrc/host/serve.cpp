@@ -14,6 +14,7 @@
 #include <deque>
 #include <memory>
 #include <mutex>
+#include <string>
 #include <thread>
 #include <vector>
 
@@ -336,12 +337,14 @@ int g4h_scan(const g4h_engine_config* cfg, const g4h_job* jobs, int njobs,
 }
 
 // Served request stream with continuous batching.  Request i arrives at
-// arrival[i] seconds after the start; it is admitted between steps once it
-// has arrived, its inputs are prepared, a batch slot is free and the free
-// device memory minus the reserve covers its estimated footprint.  Every
-// admitted request advances one lattice step per batch step; when its last
-// step has completed on the device its final diagnostics are read back and
-// its state is freed.  latency[i] = completion - arrival (seconds).
+// arrival[i] seconds after the start.  Admission threads (each with its own
+// context and stream) prepare a request's inputs ahead of time; once it has
+// arrived, a batch slot is free and the free device memory minus the reserve
+// covers its estimated footprint, they create and upload its device state.
+// The step loop attaches admitted requests between steps, advances every
+// admitted request by one lattice step per batch step (one step kept in
+// flight), and when a request's last step has completed on the device reads
+// its final diagnostics back and frees it.  latency[i] = completion - arrival.
 int g4h_serve(const g4h_engine_config* cfg, const g4h_job* jobs, const double* arrival,
               int njobs, double* latency, double* final_power, double* records,
               g4h_serve_stats* stats) {
@@ -356,53 +359,130 @@ int g4h_serve(const g4h_engine_config* cfg, const g4h_job* jobs, const double* a
     const int max_runs = std::max(1, cfg->max_runs);
     g4b_batch* batch = nullptr;
     if (int rc = g4b_batch_create(ctx, max_runs, &batch)) return rc;
+    struct Ready {
+      int job;
+      g4b_run* run;
+      std::unique_ptr<JobInputs> in;
+    };
+    std::mutex m;
+    std::condition_variable cv;
+    std::deque<Ready> ready;
+    int claimed = 0, slots_used = 0;
+    double reserved = 0;  // bytes promised to requests being created
+    bool stop = false, failed = false;
+    std::string err;
+    const double t0 = now_s();
+    auto worker = [&]() {
+     try {
+      g4b_ctx* wc = nullptr;
+      if (g4b_ctx_create(0, &wc) != G4B_OK) {
+        std::lock_guard<std::mutex> l(m);
+        failed = true;
+        err = g4b_last_error();
+        cv.notify_all();
+        return;
+      }
+      for (;;) {
+        int i;
+        {
+          std::unique_lock<std::mutex> l(m);
+          if (stop || failed || claimed >= njobs) break;
+          i = claimed++;
+        }
+        auto in = std::make_unique<JobInputs>();
+        if (!prepare(*cfg, lat, jobs[i], i, *in)) {
+          std::lock_guard<std::mutex> l(m);
+          failed = true;
+          err = "input preparation failed";
+          cv.notify_all();
+          break;
+        }
+        // wait for the arrival, then for a slot and memory
+        const double wait = arrival[i] - (now_s() - t0);
+        if (wait > 0) std::this_thread::sleep_for(std::chrono::duration<double>(wait));
+        const double need = estimate_bytes(jobs[i]);
+        {
+          std::unique_lock<std::mutex> l(m);
+          for (;;) {
+            if (stop || failed) break;
+            if (slots_used < max_runs) {
+              uint64_t fb = 0, tb = 0;
+              g4b_ctx_mem_info(wc, &fb, &tb);
+              if ((double)fb - reserved - cfg->reserve_bytes >= need) break;
+            }
+            cv.wait_for(l, std::chrono::milliseconds(1));
+          }
+          if (stop || failed) break;
+          ++slots_used;
+          reserved += need;
+        }
+        g4b_run* r = nullptr;
+        const int rc = create_run(wc, *cfg, jobs[i], *in, &r);
+        std::lock_guard<std::mutex> l(m);
+        reserved -= need;
+        if (rc != G4B_OK) {
+          failed = true;
+          err = g4b_last_error();
+          --slots_used;
+          cv.notify_all();
+          break;
+        }
+        ready.push_back(Ready{i, r, std::move(in)});
+        cv.notify_all();
+      }
+      g4b_ctx_destroy(wc);  // released once its runs are destroyed
+     } catch (const std::exception& e) {
+      std::lock_guard<std::mutex> l(m);
+      failed = true;
+      err = e.what();
+      cv.notify_all();
+     }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 0; t < threads_for(cfg); ++t) pool.emplace_back(worker);
     struct Active {
-      int job = -1, slot = -1, last_step = 0;
+      int job = -1, slot = -1;
       g4b_run* run = nullptr;
       std::unique_ptr<JobInputs> in;
-      uint64_t done_ticket = 0;
-      bool launched_last = false;
+      uint64_t done_ticket = 0;  // mark after the last step, + 1 (0 = none yet)
+      bool last_launched = false;
     };
     std::vector<Active> act;
     std::vector<size_t> rec_off(njobs + 1, 0);
     for (int i = 0; i < njobs; ++i) rec_off[i + 1] = rec_off[i] + (size_t)jobs[i].nslice * 34;
-    Producer prod(*cfg, lat, jobs, njobs, threads_for(cfg), std::max(8, max_runs));
-    int next = 0, finished = 0, peak = 0;
-    double slice_steps = 0, busy_steps = 0;
-    const double t0 = now_s();
+    int finished = 0, peak = 0;
+    double slice_steps = 0, batch_steps = 0;
     uint64_t last_ticket = 0;
     bool have_ticket = false;
+    int rc_loop = G4B_OK;
+    try {
     while (finished < njobs) {
-      const double t = now_s() - t0;
-      // admission
-      while (next < njobs && arrival[next] <= t && (int)act.size() < max_runs) {
-        uint64_t fb = 0, tb = 0;
-        g4b_ctx_mem_info(ctx, &fb, &tb);
-        if ((double)fb - cfg->reserve_bytes < estimate_bytes(jobs[next])) break;
-        auto in = prod.take(next, false);
-        if (!in) {
-          if (prod.failed()) {
-            set_error("g4h_serve: input preparation failed");
-            g4b_batch_destroy(batch);
-            return G4B_ERR_ARG;
+      {  // attach admitted requests
+        std::unique_lock<std::mutex> l(m);
+        if (failed) {
+          set_error("g4h_serve: " + err);
+          rc_loop = G4B_ERR_CUDA;
+          break;
+        }
+        if (act.empty() && ready.empty())
+          cv.wait_for(l, std::chrono::milliseconds(1));
+        while (!ready.empty()) {
+          Ready rd = std::move(ready.front());
+          ready.pop_front();
+          Active a;
+          a.job = rd.job;
+          a.run = rd.run;
+          a.in = std::move(rd.in);
+          const int nst = (int)a.in->steps.size();
+          if (g4b_batch_attach(batch, a.run, 0, nst, &a.slot) != G4B_OK) {
+            rc_loop = G4B_ERR_STATE;
+            break;
           }
-          break;  // not prepared yet
+          act.push_back(std::move(a));
         }
-        Active a;
-        a.job = next;
-        if (int rc = create_run(ctx, *cfg, jobs[next], *in, &a.run)) {
-          g4b_batch_destroy(batch);
-          return rc;
-        }
-        a.last_step = (int)in->steps.size();
-        check(g4b_batch_attach(batch, a.run, 0, a.last_step, &a.slot), "g4h_serve");
-        a.in = std::move(in);
-        act.push_back(std::move(a));
-        ++next;
+        if (rc_loop) break;
       }
       peak = std::max(peak, (int)act.size());
-      // one step of everything on the device
-      bool stepped = false;
       int running = 0;
       for (auto& a : act) {
         int nxt = 0, rem = 0;
@@ -410,7 +490,7 @@ int g4h_serve(const g4h_engine_config* cfg, const g4h_job* jobs, const double* a
         if (rem > 0) {
           ++running;
           slice_steps += jobs[a.job].nslice;
-          if (rem == 1) a.launched_last = true;
+          if (rem == 1) a.last_launched = true;
         }
       }
       if (running > 0) {
@@ -418,28 +498,25 @@ int g4h_serve(const g4h_engine_config* cfg, const g4h_job* jobs, const double* a
         uint64_t tk;
         check(g4b_ctx_mark(ctx, &tk), "g4h_serve");
         for (auto& a : act)
-          if (a.launched_last && a.done_ticket == 0) a.done_ticket = tk + 1;  // +1: 0 = none
-        // keep one step in flight: wait for the previous one
-        if (have_ticket) {
+          if (a.last_launched && a.done_ticket == 0) a.done_ticket = tk + 1;
+        if (have_ticket) {  // keep one step in flight
           int d;
           check(g4b_ctx_mark_query(ctx, last_ticket, 1, &d), "g4h_serve");
         }
         last_ticket = tk;
         have_ticket = true;
-        stepped = true;
-        busy_steps += 1;
+        batch_steps += 1;
       }
-      // completions
       for (size_t k = 0; k < act.size();) {
         Active& a = act[k];
         int done = 0;
-        if (a.done_ticket) check(g4b_ctx_mark_query(ctx, a.done_ticket - 1, 0, &done), "g4h_serve");
+        if (a.done_ticket)
+          check(g4b_ctx_mark_query(ctx, a.done_ticket - 1, 0, &done), "g4h_serve");
         if (!done) {
           ++k;
           continue;
         }
-        const double tc = now_s() - t0;
-        latency[a.job] = tc - arrival[a.job];
+        latency[a.job] = (now_s() - t0) - arrival[a.job];
         double p;
         std::vector<double> rec;
         collect(a.run, jobs[a.job], *a.in, &p, rec);
@@ -449,19 +526,31 @@ int g4h_serve(const g4h_engine_config* cfg, const g4h_job* jobs, const double* a
         g4b_run_destroy(a.run);
         act.erase(act.begin() + k);
         ++finished;
-      }
-      if (!stepped && finished < njobs) {
-        // idle: wait for the next arrival (or for inputs being prepared)
-        if (next < njobs) {
-          const double wait = arrival[next] - (now_s() - t0);
-          if (wait > 0) std::this_thread::sleep_for(std::chrono::duration<double>(std::min(wait, 0.002)));
-          else std::this_thread::sleep_for(std::chrono::microseconds(100));
-        }
+        std::lock_guard<std::mutex> l(m);
+        --slots_used;
+        cv.notify_all();
       }
     }
+    } catch (const std::exception& e) {
+      set_error(std::string("g4h_serve: ") + e.what());
+      rc_loop = G4B_ERR_CUDA;
+    }
+    {
+      std::lock_guard<std::mutex> l(m);
+      stop = true;
+      cv.notify_all();
+    }
+    for (auto& t : pool) t.join();
+    for (auto& rd : ready) g4b_run_destroy(rd.run);
+    for (auto& a : act) g4b_run_destroy(a.run);
     const double t1 = now_s();
-    check(g4b_ctx_synchronize(ctx), "g4h_serve");
+    g4b_ctx_synchronize(ctx);
     g4b_batch_destroy(batch);
+    if (rc_loop) {
+      const std::string msg = g4h::last_error();
+      g4h::set_error(msg);
+      return rc_loop;
+    }
     std::vector<double> l(latency, latency + njobs);
     std::sort(l.begin(), l.end());
     auto pct = [&](double q) {
@@ -478,7 +567,7 @@ int g4h_serve(const g4h_engine_config* cfg, const g4h_job* jobs, const double* a
     stats->slice_steps = slice_steps;
     stats->slice_steps_per_s = slice_steps / stats->seconds;
     stats->peak_concurrency = peak;
-    stats->batch_steps = busy_steps;
+    stats->batch_steps = batch_steps;
     return G4B_OK;
   } catch (const std::exception& e) {
     set_error(e.what());

@@ -292,6 +292,10 @@ class Run:
         return out
 
     def upload_field(self, i: int, cells, first: int = 0) -> None:
+        """cells None: a zero field."""
+        if cells is None:
+            check(self.lib.g4b_run_upload_field(self.h, i, None, first))
+            return
         a = np.ascontiguousarray(cells, dtype=np.complex128).reshape(-1)
         check(self.lib.g4b_run_upload_field(self.h, i, dptr(a.view(np.float64)), first))
 
@@ -332,6 +336,17 @@ class Run:
         field = np.empty((len(self.fields), self.nslice, 9))
         check(self.lib.g4b_run_history(self.h, step, dptr(beam.reshape(-1)),
                                        dptr(field.reshape(-1))))
+        return beam, field
+
+    def history_range(self, first: int, n: int):
+        """Diagnostics of steps [first, first+n) in one read: (beam [n, nslice,
+        23+2*nbunch], field [n, nfield, nslice, 9])."""
+        rb = self.nslice * (23 + 2 * self.nbunch)
+        rf = len(self.fields) * self.nslice * 9
+        out = np.empty((n, rb + rf))
+        check(self.lib.g4b_run_history_range(self.h, first, n, dptr(out.reshape(-1))))
+        beam = out[:, :rb].reshape(n, self.nslice, 23 + 2 * self.nbunch)
+        field = out[:, rb:].reshape(n, len(self.fields), self.nslice, 9)
         return beam, field
 
     def device_bytes(self) -> int:

@@ -238,6 +238,7 @@ int g4b_run_upload_beam(g4b_run* run, const double* x, const double* y,
                         const double* theta);
 int g4b_run_download_beam(g4b_run* run, double* x, double* y, double* px,
                           double* py, double* gamma, double* theta);
+/* cells = NULL uploads a zero field. */
 int g4b_run_upload_field(g4b_run* run, int ifield, const double* cells, int first);
 int g4b_run_download_field(g4b_run* run, int ifield, double* cells, int* first);
 int g4b_run_set_current(g4b_run* run, const double* current);
@@ -257,6 +258,10 @@ int g4b_run_prepare(g4b_run* run, int first_step, int nsteps);
  * order of g4b_diag_beam, bunching interleaved re,im), field[nfield*nslice*9]
  * (the 7 sums of g4b_diag_field, then the centre cell re, im). */
 int g4b_run_history(g4b_run* run, int step, double* beam, double* field);
+/* Diagnostics of steps [first, first+n) with one read: out[n][step record],
+ * a step record being the beam and field blocks of g4b_run_history
+ * back to back (n <= the steps the history keeps). */
+int g4b_run_history_range(g4b_run* run, int first, int n, double* out);
 int g4b_run_device_bytes(g4b_run* run, uint64_t* bytes);
 
 /* ---- batched runs ---------------------------------------------------------
