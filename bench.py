@@ -116,6 +116,24 @@ class Clocks:
                 "samples": len(sm), "reasons": sorted(reasons)}
 
 
+def profile_traffic(kernel, wl):
+    """DRAM bytes per launch of a mixed kernel from the committed ncu summary
+    (captured on 1024 slices x 8192 particles, ngrid 201), scaled by the
+    particles or cells of this workload; None if not profiled."""
+    path = ROOT / "profiles" / "mixed_step_sase1024x8192_n201.md"
+    if not path.exists():
+        return None
+    for line in path.read_text().splitlines():
+        f = line.split()
+        if len(f) == 3 and f[0] == "traffic" and f[1] == kernel:
+            if kernel.startswith("adi"):
+                scale = wl.nslice * wl.ngrid ** 2 / (1024 * 201 ** 2)
+            else:
+                scale = wl.nslice * wl.npart / (1024 * 8192)
+            return int(float(f[2]) * scale)
+    return None
+
+
 def measured_peak():
     path = ROOT / "MEASURED_PEAKS.json"
     if path.exists():
@@ -563,7 +581,9 @@ def run_ours(args, wl, rank, world):
     d = mixed_k[dom]
     roof = {"bound": "hbm", "kernel": dom, "achieved": d["gbs"], "peak": peak,
             "peak_source": peak_kind, "unit": "GB/s", "frac": d["gbs"] / peak,
-            "traffic": None, "alg_bytes_per_launch": d["alg_bytes"],
+            "traffic": profile_traffic(dom, wl), "alg_bytes_per_launch": d["alg_bytes"],
+            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch, "
+                              "profiles/mixed_step_sase1024x8192_n201.md",
             "timing": "CUDA events around each launch on the launching stream, "
                       f"{kp} direct-launch steps following the graph-timed region"}
 
