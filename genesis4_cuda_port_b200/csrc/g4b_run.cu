@@ -241,8 +241,8 @@ __device__ __forceinline__ void beam_chunk(const BeamStepArgs& a, const int4 ch)
         ctr += rr[f] * c + ri[f] * s;
         cti += ri[f] * c - rr[f] * s;
       }
-      const float e = ds * ig0;                 // (gs - g0) / g0
-      const float bq = -e / (1.0f + e);         // g0 / gs - 1
+      const float e = ds * ig0;                 // (gs - g0) / g0, |e| <~ 1e-3
+      const float bq = e * (e - 1.0f);          // g0 / gs - 1, error O(e^3)
       const float ar = zt * ctr;                // delta / btpar
       const float r = ar + bq * (2.0f + bq) * (1.0f + ar);
       kp += A0 - B0 * r;
@@ -320,11 +320,8 @@ __device__ __forceinline__ void beam_chunk(const BeamStepArgs& a, const int4 ch)
     if (f >= nfield) break;
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-      int v = bb[f][q];
-      for (int o = 16; o > 0; o >>= 1) {
-        const int u = __shfl_xor_sync(0xffffffffu, v, o);
-        v = q < 2 ? min(v, u) : max(v, u);
-      }
+      const int v = q < 2 ? __reduce_min_sync(0xffffffffu, bb[f][q])
+                          : __reduce_max_sync(0xffffffffu, bb[f][q]);
       if (l == 0) sbb[f][q][w] = v;
     }
   }
