@@ -82,8 +82,8 @@ __device__ __forceinline__ C shfl_down_c(C v, int d) {
 
 
 template <typename T> struct BandW;
-template <> struct BandW<double> { static constexpr int value = 9; };
-template <> struct BandW<float> { static constexpr int value = 10; };
+template <> struct BandW<double> { static constexpr int value = 9; static constexpr int blocks = 2; };
+template <> struct BandW<float> { static constexpr int value = 10; static constexpr int blocks = 4; };
 
 // One band of W rows (pass X) or W transposed columns (pass Y) of slice s.
 // bar is an initialised mbarrier; parity the phase this band waits on.
@@ -284,15 +284,31 @@ __device__ __forceinline__ void adi_band(const AdiPassArgs& a, const CUtensorMap
         }
       }
     }
-    const double sp = (double)tp, sy1 = (double)ty1, sy2 = (double)ty2;
-    const double sre = (double)tre, sim = (double)tim;
-    const double sx1 = dx * sp, sx2 = dx * dx * sp;
-    double vals[9] = {sp, sx1, sx2, sy1, sy2, sre, sim, cre, cim};
+    // power over the column in FP64; the moments and sums over the column's
+    // lanes in the state precision; the x moments follow from the column's
+    // power (x is the column); the centre cell comes from the one lane that
+    // holds it
+    double sp = (double)tp;
+    for (int o = 16; o > 0; o >>= 1) sp += __shfl_xor_sync(0xffffffffu, sp, o);
+    T vals[4] = {ty1, ty2, tre, tim};
 #pragma unroll
-    for (int q = 0; q < 9; ++q) {
-      double t = vals[q];
-      for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
-      if (lane == 0) dpart[warp][q] = t;
+    for (int q = 0; q < 4; ++q)
+      for (int o = 16; o > 0; o >>= 1) vals[q] += __shfl_xor_sync(0xffffffffu, vals[q], o);
+    if (lane == 0) {
+      dpart[warp][0] = sp;
+      dpart[warp][1] = dx * sp;
+      dpart[warp][2] = dx * dx * sp;
+      dpart[warp][3] = (double)vals[0];
+      dpart[warp][4] = (double)vals[1];
+      dpart[warp][5] = (double)vals[2];
+      dpart[warp][6] = (double)vals[3];
+      dpart[warp][7] = 0.0;
+      dpart[warp][8] = 0.0;
+    }
+    __syncwarp();
+    if (cre != 0.0 || cim != 0.0) {  // the lane holding the centre cell
+      dpart[warp][7] = cre;
+      dpart[warp][8] = cim;
     }
     __syncthreads();
     if (tid < 9) {
@@ -320,7 +336,7 @@ __device__ __forceinline__ void adi_band(const AdiPassArgs& a, const CUtensorMap
 }
 
 template <typename T, int M, bool PX>
-__global__ void __launch_bounds__(BandW<T>::value * 32)
+__global__ void __launch_bounds__(BandW<T>::value * 32, (M <= 9 ? BandW<T>::blocks : 2))
     adi_pass_kernel(const __grid_constant__ AdiPassArgs a,
                     const __grid_constant__ CUtensorMap tm_out) {
   extern __shared__ __align__(128) unsigned char smem[];
@@ -336,7 +352,7 @@ __global__ void __launch_bounds__(BandW<T>::value * 32)
 // Persistent form over a work list of (run, slice, band) items of many runs
 // (one mbarrier, one phase per item; tensor maps read from global memory).
 template <typename T, int M, bool PX>
-__global__ void __launch_bounds__(BandW<T>::value * 32)
+__global__ void __launch_bounds__(BandW<T>::value * 32, (M <= 9 ? BandW<T>::blocks : 2))
     adi_batch_kernel(const __grid_constant__ AdiBatchArgs b) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ uint64_t bar;
