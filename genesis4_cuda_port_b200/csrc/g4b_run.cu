@@ -410,6 +410,8 @@ struct DepDiagArgs {
 // (from K1); tiles larger than kDepMaxCells are processed in row bands.
 constexpr int kDepParts = 1;          // beam-diagnostic partial records per slice
 constexpr int kDepThreads = 256;
+constexpr int kDepHistU = 4;          // particles in flight per thread: count pass
+constexpr int kDepAccU = 4;           // accumulation pass
 constexpr int kDepMaxCells = 12288;   // output cells per band
 constexpr size_t kDepSmem = (size_t)kDepMaxCells * 8;
 
@@ -573,11 +575,11 @@ __device__ __forceinline__ void deposit_slice(const DepDiagArgs& a, const int bs
       float qmax = 0.f;
       // (a quad of lanes holding one quiet-start beamlet shares the cell:
       // one atomic adds its count)
-      for (int64_t pb = p0 + (tid & ~31); pb < p1; pb += 2 * kDepThreads) {
-        float2 lxy[2];
-        float ldg[2];
+      for (int64_t pb = p0 + (tid & ~31); pb < p1; pb += kDepHistU * kDepThreads) {
+        float2 lxy[kDepHistU];
+        float ldg[kDepHistU];
 #pragma unroll
-        for (int u = 0; u < 2; ++u) {
+        for (int u = 0; u < kDepHistU; ++u) {
           const int64_t p = pb + u * kDepThreads + l;
           if (p < p1) {
             lxy[u] = a.xy[p];
@@ -585,7 +587,7 @@ __device__ __forceinline__ void deposit_slice(const DepDiagArgs& a, const int bs
           }
         }
 #pragma unroll
-        for (int u = 0; u < 2; ++u) {
+        for (int u = 0; u < kDepHistU; ++u) {
           const int64_t p = pb + u * kDepThreads + l;
           int cidx = -1;
           if (p < p1) {
@@ -657,12 +659,12 @@ __device__ __forceinline__ void deposit_slice(const DepDiagArgs& a, const int bs
       // 3. exact integer accumulation of the bilinear contributions
       // (contributions of a quad of lanes with one cell are added as integers
       // in registers first: exact, so the result is unchanged)
-      for (int64_t pb = p0 + (tid & ~31); pb < p1; pb += 2 * kDepThreads) {
-        float2 lxy[2];
-        float ldg[2];
-        double lth[2];
+      for (int64_t pb = p0 + (tid & ~31); pb < p1; pb += kDepAccU * kDepThreads) {
+        float2 lxy[kDepAccU];
+        float ldg[kDepAccU];
+        double lth[kDepAccU];
 #pragma unroll
-        for (int u = 0; u < 2; ++u) {
+        for (int u = 0; u < kDepAccU; ++u) {
           const int64_t p = pb + u * kDepThreads + l;
           if (p < p1) {
             lxy[u] = a.xy[p];
@@ -671,7 +673,7 @@ __device__ __forceinline__ void deposit_slice(const DepDiagArgs& a, const int bs
           }
         }
 #pragma unroll
-        for (int u = 0; u < 2; ++u) {
+        for (int u = 0; u < kDepAccU; ++u) {
           const int64_t p = pb + u * kDepThreads + l;
           int cidx = -1, ey = 0, ex = 0;
           int c[8] = {0, 0, 0, 0, 0, 0, 0, 0};
