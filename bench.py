@@ -545,14 +545,18 @@ def run_ours(args, wl, rank, world):
     if not args.no_e2e:
         pin = {k: torch.from_numpy(v).pin_memory().numpy() for k, v in parts.items()}
         pcells = torch.from_numpy(cells.view(np.float64)).pin_memory().numpy().view(np.complex128)
+        pout = {k: torch.empty(v.shape, dtype=torch.float64).pin_memory().numpy()
+                for k, v in parts.items()}
+        pcout = torch.empty(cells.view(np.float64).shape,
+                            dtype=torch.float64).pin_memory().numpy().view(np.complex128)
         hist = []
 
         def e2e_run():
             mx.upload(pin, pcells)
             mx.run.advance(0, K, graph=False)
             hist.append(mx.run.history_range(0, K))
-            mx.run.download_beam()
-            mx.run.download_field(0)
+            mx.run.download_beam(pout)
+            mx.run.download_field(0, pcout)
 
         ems = timed(e2e_run)
         state_bytes = sum(v.nbytes for v in parts.values()) + cells.nbytes

@@ -286,8 +286,10 @@ class Run:
         arrs = [np.ascontiguousarray(parts[k], dtype=np.float64) for k in BeamState.NAMES]
         check(self.lib.g4b_run_upload_beam(self.h, *[dptr(a) for a in arrs]))
 
-    def download_beam(self) -> dict:
-        out = {k: np.empty(self.npart) for k in BeamState.NAMES}
+    def download_beam(self, out: dict | None = None) -> dict:
+        """out: optional preallocated (e.g. pinned) float64 arrays by name."""
+        if out is None:
+            out = {k: np.empty(self.npart) for k in BeamState.NAMES}
         check(self.lib.g4b_run_download_beam(self.h, *[dptr(out[k]) for k in BeamState.NAMES]))
         return out
 
@@ -299,9 +301,11 @@ class Run:
         a = np.ascontiguousarray(cells, dtype=np.complex128).reshape(-1)
         check(self.lib.g4b_run_upload_field(self.h, i, dptr(a.view(np.float64)), first))
 
-    def download_field(self, i: int):
+    def download_field(self, i: int, out=None):
+        """out: optional preallocated (e.g. pinned) complex128 [nslice, n, n]."""
         n = self.fields[i][1]
-        out = np.empty((self.nslice, n, n), np.complex128)
+        if out is None:
+            out = np.empty((self.nslice, n, n), np.complex128)
         first = C.c_int()
         check(self.lib.g4b_run_download_field(self.h, i, dptr(out.reshape(-1).view(np.float64)),
                                               C.byref(first)))
