@@ -116,6 +116,23 @@ class Clocks:
                 "samples": len(sm), "reasons": sorted(reasons)}
 
 
+def max_over_ranks(ms, dist=None, device="cuda"):
+    """Device time of a step range as the max over ranks (the slowest replica
+    bounds the job)."""
+    if dist is None:
+        return ms
+    import torch
+    t = torch.tensor([ms], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(world, nslice, steps, ms):
+    """Whole-job slice-steps/s of `world` independent replicas of an
+    nslice-slice workload that all took `steps` steps in at most `ms`."""
+    return world * nslice * steps / (ms / 1e3)
+
+
 def profile_traffic(kernel, wl):
     """DRAM bytes per launch of a mixed kernel from the committed ncu summary
     (captured on 1024 slices x 8192 particles, ngrid 201), scaled by the
@@ -492,12 +509,6 @@ def run_ours(args, wl, rank, world):
         if dist is not None:
             dist.barrier()
 
-    def max_over_ranks(ms):
-        if dist is None:
-            return ms
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
 
     ctx = dev.Context(local)
     stream = torch.cuda.ExternalStream(ctx.stream)
@@ -517,7 +528,7 @@ def run_ours(args, wl, rank, world):
         e1.record(stream)
         torch.cuda.synchronize()
         barrier()
-        return max_over_ranks(e0.elapsed_time(e1))
+        return max_over_ranks(e0.elapsed_time(e1), dist)
 
     # ---------------- mixed fused form: the headline ----------------
     mx = MixedRun(ctx, wl, off, lat)
@@ -532,7 +543,7 @@ def run_ours(args, wl, rank, world):
     ms = timed(lambda: mx.run.advance(W, K, graph=True))
     launches = ctx.launch_count() - launches0
     clk = clocks.stop()
-    value = world * wl.nslice * K / (ms / 1e3)
+    value = replica_throughput(world, wl.nslice, K, ms)
     # per-kernel CUDA-event timing of the same kernels (direct launches)
     ctx.profile(True)
     kp = min(K, 30)
@@ -577,7 +588,7 @@ def run_ours(args, wl, rank, world):
     ms64 = timed(lambda: [eng.step(lat, (W + k) % nstep) for k in range(K)])
     fp64_k = _stats(ctx.profile_read(), kernel_alg_bytes(wl, False), K)
     ctx.profile(False)
-    value64 = world * wl.nslice * K / (ms64 / 1e3)
+    value64 = replica_throughput(world, wl.nslice, K, ms64)
     del eng
 
     dom = max(mixed_k, key=lambda n: mixed_k[n]["ms_per_step"])
