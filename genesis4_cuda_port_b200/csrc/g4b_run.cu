@@ -116,7 +116,9 @@ __device__ __forceinline__ void sincos_small(float a, float& s, float& c) {
   }
 }
 
-// Reduce an FP64 angle to [-pi, pi) before FP32 trigonometry.
+// Reduce an FP64 angle to [-pi, pi) before FP32 trigonometry (the
+// hardware sine / cosine, __sincosf, has an absolute error below 2^-21.4 on
+// that interval).
 __device__ __forceinline__ float reduce_angle(double a) {
   const double twopi = 6.283185307179586476925287;
   return (float)(a - twopi * rint(a * (1.0 / twopi)));
@@ -205,7 +207,7 @@ __device__ __forceinline__ void beam_chunk(const BeamStepArgs& a, const int4 ch)
         rr[f] = sc * cre;
         ri[f] = -sc * cim;
       }
-      sincosf(reduce_angle((double)F.harm * t0), &s0[f], &c0[f]);
+      __sincosf(reduce_angle((double)F.harm * t0), &s0[f], &c0[f]);
     }
     // theta' = ks (1 - 1/b0) + ku with b0 = sqrt(1 - eps), eps = btper0 /
     // gamma^2 ~ 1e-8: the two ~ku terms cancel to the detuning, so the
@@ -391,29 +393,46 @@ struct DepDiagArgs {
 
 // Deposition + beam diagnostics, one CTA per slice.
 //
-// The beam diagnostics are FP64 sums over the slice's particles (one pass).
-// The deposition (adi_deposit_source_atomic, FieldSolverADICUDA.cpp:98-174)
-// is a deterministic per-cell reduction in exact integer arithmetic:
-//   1. a first pass counts the particles per base cell (ix, iy) of the tile
-//      and finds the slice's largest charge |q|;
+// A first pass reads every particle of the slice once for the beam
+// diagnostics (FP64 sums; the minima and maxima are taken in FP32, which is
+// exact for FP32 state) and for the slice's largest charge weight
+// qmax = max sqrt(faw2) / gamma.  The deposition (adi_deposit_source_atomic,
+// FieldSolverADICUDA.cpp:98-174) is then a deterministic per-cell reduction
+// in exact integer arithmetic:
+//   1. a count pass gives the number of particles per base cell (ix, iy) of
+//      the tile;
 //   2. the largest number M of contributions any output cell receives (the
 //      sum of the counts of its four base cells) fixes the slice's scale
 //      S = 2^30 / (M qmax), so every contribution rounds to an int32 with
 //      |c| <= 2^30 / M and no cell sum can overflow;
-//   3. a second pass adds each particle's four bilinear contributions
+//   3. an accumulation pass adds each particle's four bilinear contributions
 //      c = rint(S q w (sin h theta, cos h theta)) with 32-bit shared-memory
 //      integer atomics (re and im in separate planes, so the 32 lanes of a
 //      warp spread over the banks).
 // Integer addition is associative, so the source does not depend on the
 // order in which threads add, and each contribution keeps FP32 resolution
-// (2^-24 relative).  The tile is the slice's bounding box of touched cells
-// (from K1); tiles larger than kDepMaxCells are processed in row bands.
+// (2^-24 relative).  Phases are reduced to [-pi, pi) in FP64 and their sine
+// and cosine taken with the hardware approximation (absolute error below
+// 2^-21.4 on that interval).  The tile is the slice's bounding box of
+// touched cells (from K1); tiles larger than kDepMaxCells are processed in
+// row bands.
 constexpr int kDepParts = 1;          // beam-diagnostic partial records per slice
 constexpr int kDepThreads = 256;
-constexpr int kDepHistU = 4;          // particles in flight per thread: count pass
+constexpr int kDepDiagU = 4;          // particles in flight per thread: diagnostics pass
+constexpr int kDepHistU = 4;          // count pass
 constexpr int kDepAccU = 4;           // accumulation pass
-constexpr int kDepMaxCells = 12288;   // output cells per band
+constexpr int kDepMaxCells = 12288;   // output cells per band (a multiple of 4)
 constexpr size_t kDepSmem = (size_t)kDepMaxCells * 8;
+
+// Charge weight sqrt(faw2) / gamma of one particle (FP32), the same
+// expression for the slice maximum and for the contributions.
+__device__ __forceinline__ float dep_charge(const DepDiagArgs& a, const float2 xy,
+                                            const float dg) {
+  const float dxu = xy.x - a.ax, dyu = xy.y - a.ay;
+  const float faw2 = 1.0f + a.kx * dxu * dxu + a.ky * dyu * dyu +
+                     2.0f * (a.gradx * dxu + a.grady * dyu);
+  return __fdividef(sqrtf(faw2), a.gref_f + dg);
+}
 
 // NB: bunching harmonics accumulated (1, or up to kMaxBunch)
 template <int NB>
@@ -424,59 +443,62 @@ __device__ __forceinline__ void deposit_slice(const DepDiagArgs& a, const int bs
   __shared__ int wsum[kDepThreads / 32];
   __shared__ float wmax[kDepThreads / 32];
   const int tid = threadIdx.x, w = tid >> 5, l = tid & 31;
-  const int64_t p0 = a.off[bs], p1 = a.off[bs + 1];
-  const int64_t np = p1 - p0;
+  const int64_t p0 = a.off[bs];
+  const int np = (int)(a.off[bs + 1] - p0);  // at most 65536 particles per slice
+  const float2* xyp = a.xy + p0;
+  const float2* pxyp = a.pxy + p0;
+  const float* dgp = a.dg + p0;
+  const double* thp = a.th + p0;
   const int rec = kBeamRec + 2 * a.nbunch;
+  bool want_q = false;
+  for (int fi = 0; fi < a.nfield; ++fi) want_q |= a.f[fi].do_source != 0;
   if (tid < a.nfield) sbox[tid] = a.f[tid].bbox[bs];
 
-  // ---- beam diagnostics of the slice (FP64 sums) ----
+  // ---- beam diagnostics of the slice (FP64 sums) and the largest charge ----
   {
-    double v[kBeamRec];
+    double sm[12];  // sums of x, x^2, y, y^2, px, px^2, py, py^2, x px, y py, dg, dg^2
 #pragma unroll
-    for (int k = 0; k < 13; ++k) v[k] = 0.0;
-    v[13] = 1.0e5; v[14] = -1.0e5; v[15] = 1.0e5; v[16] = -1.0e5;
-    v[17] = 1.0e5; v[18] = -1.0e5; v[19] = 1.0e5; v[20] = -1.0e5;
-    v[21] = 1.0e7; v[22] = 1.0;
-    double sdg = 0.0, sdg2 = 0.0;
+    for (int k = 0; k < 12; ++k) sm[k] = 0.0;
+    // minima / maxima of x, px, y, py (reference start values -+1e5) and dg
+    float mn[5] = {1.0e5f, 1.0e5f, 1.0e5f, 1.0e5f, INFINITY};
+    float mx[5] = {-1.0e5f, -1.0e5f, -1.0e5f, -1.0e5f, -INFINITY};
+    float qmax = 0.f;
     double bre[NB], bim[NB];
 #pragma unroll
     for (int h = 0; h < NB; ++h) bre[h] = bim[h] = 0.0;
-    // four particles per thread per iteration, loads issued first
-    constexpr int U = 4;
-    for (int64_t pb = p0 + tid; pb < p1; pb += U * kDepThreads) {
-      float2 lxy[U], lpp[U];
-      float ldg[U];
-      double lth[U];
+    for (int pb = tid; pb < np; pb += kDepDiagU * kDepThreads) {
+      float2 lxy[kDepDiagU], lpp[kDepDiagU];
+      float ldg[kDepDiagU];
+      double lth[kDepDiagU];
 #pragma unroll
-      for (int u = 0; u < U; ++u) {
-        const int64_t p = pb + u * kDepThreads;
-        if (p < p1) {
-          lxy[u] = a.xy[p];
-          lpp[u] = a.pxy[p];
-          ldg[u] = a.dg[p];
-          lth[u] = a.th[p];
+      for (int u = 0; u < kDepDiagU; ++u) {
+        const int p = pb + u * kDepThreads;
+        if (p < np) {
+          lxy[u] = xyp[p];
+          lpp[u] = pxyp[p];
+          ldg[u] = dgp[p];
+          lth[u] = thp[p];
         }
       }
 #pragma unroll
-      for (int u = 0; u < U; ++u) {
-        if (pb + u * kDepThreads >= p1) break;
+      for (int u = 0; u < kDepDiagU; ++u) {
+        if (pb + u * kDepThreads >= np) break;
         const double x = lxy[u].x, y = lxy[u].y, px = lpp[u].x, py = lpp[u].y;
-        const double dgv = ldg[u];
-        const double g = a.gref + dgv;
-        sdg += dgv;
-        sdg2 += dgv * dgv;
-        v[2] += x; v[3] += x * x; v[4] += y; v[5] += y * y;
-        v[6] += px; v[7] += px * px; v[8] += py; v[9] += py * py;
-        v[10] += x * px; v[11] += y * py; v[12] += 1.0;
+        const double d = ldg[u];
+        sm[0] += x; sm[1] += x * x; sm[2] += y; sm[3] += y * y;
+        sm[4] += px; sm[5] += px * px; sm[6] += py; sm[7] += py * py;
+        sm[8] += x * px; sm[9] += y * py; sm[10] += d; sm[11] += d * d;
         if (a.need_aux) {
-          v[13] = fmin(v[13], x); v[14] = fmax(v[14], x);
-          v[15] = fmin(v[15], px); v[16] = fmax(v[16], px);
-          v[17] = fmin(v[17], y); v[18] = fmax(v[18], y);
-          v[19] = fmin(v[19], py); v[20] = fmax(v[20], py);
-          v[21] = fmin(v[21], g); v[22] = fmax(v[22], g);
+          const float f[5] = {lxy[u].x, lpp[u].x, lxy[u].y, lpp[u].y, ldg[u]};
+#pragma unroll
+          for (int i = 0; i < 5; ++i) {
+            mn[i] = fminf(mn[i], f[i]);
+            mx[i] = fmaxf(mx[i], f[i]);
+          }
         }
+        if (want_q) qmax = fmaxf(qmax, dep_charge(a, lxy[u], ldg[u]));
         float s1, c1;
-        sincosf(reduce_angle(lth[u]), &s1, &c1);
+        __sincosf(reduce_angle(lth[u]), &s1, &c1);
         float ch = c1, sh = s1;
 #pragma unroll
         for (int h = 0; h < NB; ++h) {
@@ -489,21 +511,29 @@ __device__ __forceinline__ void deposit_slice(const DepDiagArgs& a, const int bs
         }
       }
     }
-    {
-      const double N = v[12];
-      v[0] = N * a.gref + sdg;
-      v[1] = N * a.gref * a.gref + 2.0 * a.gref * sdg + sdg2;
+    // per-warp records in the layout of the final one: [0] sum dg,
+    // [1] sum dg^2, [2..11] the sums of x .. y py, [13..22] minima / maxima
+    // of x, px, y, py, dg
+#pragma unroll
+    for (int k = 0; k < 12; ++k) {
+      double t = sm[k];
+      for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+      if (l == 0) dpart[w][k < 10 ? k + 2 : k - 10] = t;
     }
 #pragma unroll
-    for (int k = 0; k < kBeamRec; ++k) {
-      double t = v[k];
-      const int op = k < 13 ? 0 : ((k - 13) % 2 == 0 ? 1 : 2);
+    for (int i = 0; i < 5; ++i) {
+      float lo = mn[i], hi = mx[i];
       for (int o = 16; o > 0; o >>= 1) {
-        const double u = __shfl_xor_sync(0xffffffffu, t, o);
-        t = op == 0 ? t + u : (op == 1 ? fmin(t, u) : fmax(t, u));
+        lo = fminf(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+        hi = fmaxf(hi, __shfl_xor_sync(0xffffffffu, hi, o));
       }
-      if (l == 0) dpart[w][k] = t;
+      if (l == 0) {
+        dpart[w][13 + 2 * i] = lo;
+        dpart[w][14 + 2 * i] = hi;
+      }
     }
+    for (int o = 16; o > 0; o >>= 1) qmax = fmaxf(qmax, __shfl_xor_sync(0xffffffffu, qmax, o));
+    if (l == 0) wmax[w] = qmax;
 #pragma unroll
     for (int h = 0; h < NB; ++h) {
       if (h >= a.nbunch) break;
@@ -519,16 +549,33 @@ __device__ __forceinline__ void deposit_slice(const DepDiagArgs& a, const int bs
     }
     __syncthreads();
     if (tid < rec) {
+      // record (DiagnosticCUDA.cpp:102-125): [0] sum gamma, [1] sum gamma^2,
+      // [12] count, [21] / [22] min / max gamma from the dg extremes (gamma
+      // = gref + dg is monotonic in dg)
+      const double N = (double)np;
       const int op = tid < 13 ? 0 : (tid < kBeamRec ? ((tid - 13) % 2 == 0 ? 1 : 2) : 0);
-      double t = dpart[0][tid];
-      for (int i = 1; i < kDepThreads / 32; ++i) {
-        const double u = dpart[i][tid];
-        t = op == 0 ? t + u : (op == 1 ? fmin(t, u) : fmax(t, u));
+      double t = N;
+      if (tid != 12) {
+        t = dpart[0][tid];
+        for (int i = 1; i < kDepThreads / 32; ++i) {
+          const double u = dpart[i][tid];
+          t = op == 0 ? t + u : (op == 1 ? fmin(t, u) : fmax(t, u));
+        }
       }
+      if (tid == 0) t += N * a.gref;
+      if (tid == 1) {
+        double sd = dpart[0][0];
+        for (int i = 1; i < kDepThreads / 32; ++i) sd += dpart[i][0];
+        t += N * a.gref * a.gref + 2.0 * a.gref * sd;
+      }
+      if (tid == 21) t = fmin(1.0e7, a.gref + t);
+      if (tid == 22) t = fmax(1.0, a.gref + t);
       if (tid >= 13 && tid < kBeamRec && !a.need_aux) t = 0.0;
       a.beam_part[(size_t)bs * rec + tid] = t;
     }
   }
+  float qm = wmax[0];
+  for (int i = 1; i < kDepThreads / 32; ++i) qm = fmaxf(qm, wmax[i]);
 
   // ---- deposition of every field with a source this step ----
   int* are = reinterpret_cast<int*>(smem);        // [hb * bw] real parts
@@ -557,8 +604,11 @@ __device__ __forceinline__ void deposit_slice(const DepDiagArgs& a, const int bs
       if (bx0 + bw > F.ld) --bx0;
     }
     if (tid == 0) F.desc[target] = make_int4(bx0, by0, bw, bh);
-    const int hband = max(1, kDepMaxCells / bw);
+    const int hband = max(1, kDepMaxCells / bw);  // bw <= ngrid + 1 < kDepMaxCells
     const float fh = (float)F.harm;
+    // row of output cell o: (o + 1/2) / bw in FP32 is never within
+    // nout 2^-23 / bw of an integer boundary, so the truncation is exact
+    const float inv_bw = 1.0f / (float)bw;
     MixField mf;
     mf.gridmax = F.gridmax;
     mf.dgrid = F.dgrid;
@@ -569,42 +619,35 @@ __device__ __forceinline__ void deposit_slice(const DepDiagArgs& a, const int bs
       const int ylo = by0 + yb;  // first grid row of this band
       const int nout = hb * bw, nbase = (hb + 1) * bw;
       __syncthreads();
-      for (int i = tid; i < nbase; i += kDepThreads) hist[i] = 0;
+      {
+        int4* h4 = reinterpret_cast<int4*>(hist);
+        for (int i = tid; i < (nbase + 3) >> 2; i += kDepThreads) h4[i] = make_int4(0, 0, 0, 0);
+      }
       __syncthreads();
-      // 1. counts per base cell (ext row iy - ylo + 1) and the largest |q|
-      float qmax = 0.f;
+      // 1. counts per base cell (ext row iy - ylo + 1)
       // (a quad of lanes holding one quiet-start beamlet shares the cell:
       // one atomic adds its count)
-      for (int64_t pb = p0 + (tid & ~31); pb < p1; pb += kDepHistU * kDepThreads) {
+      for (int pb = tid & ~31; pb < np; pb += kDepHistU * kDepThreads) {
         float2 lxy[kDepHistU];
-        float ldg[kDepHistU];
 #pragma unroll
         for (int u = 0; u < kDepHistU; ++u) {
-          const int64_t p = pb + u * kDepThreads + l;
-          if (p < p1) {
-            lxy[u] = a.xy[p];
-            ldg[u] = a.dg[p];
-          }
+          const int p = pb + u * kDepThreads + l;
+          if (p < np) lxy[u] = xyp[p];
         }
 #pragma unroll
         for (int u = 0; u < kDepHistU; ++u) {
-          const int64_t p = pb + u * kDepThreads + l;
+          const int p = pb + u * kDepThreads + l;
           int cidx = -1;
-          if (p < p1) {
+          if (p < np) {
             int ix, iy;
             float wx, wy;
             if (cell_f(mf, lxy[u].x, lxy[u].y, ix, iy, wx, wy) && iy + 1 >= ylo &&
                 iy < ylo + hb) {
               const int ex = ix - bx0, ey = iy - ylo + 1;
-              if (ex < 0 || ex > bw - 2) {
+              if (ex < 0 || ex > bw - 2)
                 atomicOr(a.err, kErrBadSlice);
-              } else {
+              else
                 cidx = ey * bw + ex;
-                const float dxu = lxy[u].x - a.ax, dyu = lxy[u].y - a.ay;
-                const float faw2 = 1.0f + a.kx * dxu * dxu + a.ky * dyu * dyu +
-                                   2.0f * (a.gradx * dxu + a.grady * dyu);
-                qmax = fmaxf(qmax, sqrtf(faw2) / (a.gref_f + ldg[u]));
-              }
             }
           }
           const int c1 = __shfl_xor_sync(0xffffffffu, cidx, 1);
@@ -623,26 +666,16 @@ __device__ __forceinline__ void deposit_slice(const DepDiagArgs& a, const int bs
       // 2. M = max over output cells of the contributions it receives
       int mloc = 0;
       for (int o = tid; o < nout; o += kDepThreads) {
-        const int r = o / bw, x = o - r * bw;
+        const int r = (int)(((float)o + 0.5f) * inv_bw), x = o - r * bw;
         int m = hist[(r + 1) * bw + x] + hist[r * bw + x];
         if (x > 0) m += hist[(r + 1) * bw + x - 1] + hist[r * bw + x - 1];
         mloc = max(mloc, m);
       }
-      for (int o = 16; o > 0; o >>= 1) {
-        mloc = max(mloc, __shfl_xor_sync(0xffffffffu, mloc, o));
-        qmax = fmaxf(qmax, __shfl_xor_sync(0xffffffffu, qmax, o));
-      }
-      if (l == 0) {
-        wsum[w] = mloc;
-        wmax[w] = qmax;
-      }
+      for (int o = 16; o > 0; o >>= 1) mloc = max(mloc, __shfl_xor_sync(0xffffffffu, mloc, o));
+      if (l == 0) wsum[w] = mloc;
       __syncthreads();
       int M = wsum[0];
-      float qm = wmax[0];
-      for (int i = 1; i < kDepThreads / 32; ++i) {
-        M = max(M, wsum[i]);
-        qm = fmaxf(qm, wmax[i]);
-      }
+      for (int i = 1; i < kDepThreads / 32; ++i) M = max(M, wsum[i]);
       float2* out = F.src + (size_t)target * F.cap + (size_t)yb * bw;
       if (M == 0 || !(qm > 0.f) || !(qm < 3.0e38f)) {
         if (M > 0) atomicOr(a.err, kErrFixedRange);  // non-finite charge
@@ -651,33 +684,37 @@ __device__ __forceinline__ void deposit_slice(const DepDiagArgs& a, const int bs
       }
       const double S = 1073741824.0 / ((double)M * (double)qm);  // 2^30 / (M qmax)
       const float Sf = (float)S;
-      for (int i = tid; i < nout; i += kDepThreads) {
-        are[i] = 0;
-        aim[i] = 0;
+      {
+        int4* r4 = reinterpret_cast<int4*>(are);
+        int4* i4 = reinterpret_cast<int4*>(aim);
+        for (int i = tid; i < (nout + 3) >> 2; i += kDepThreads) {
+          r4[i] = make_int4(0, 0, 0, 0);
+          i4[i] = make_int4(0, 0, 0, 0);
+        }
       }
       __syncthreads();
       // 3. exact integer accumulation of the bilinear contributions
       // (contributions of a quad of lanes with one cell are added as integers
       // in registers first: exact, so the result is unchanged)
-      for (int64_t pb = p0 + (tid & ~31); pb < p1; pb += kDepAccU * kDepThreads) {
+      for (int pb = tid & ~31; pb < np; pb += kDepAccU * kDepThreads) {
         float2 lxy[kDepAccU];
         float ldg[kDepAccU];
         double lth[kDepAccU];
 #pragma unroll
         for (int u = 0; u < kDepAccU; ++u) {
-          const int64_t p = pb + u * kDepThreads + l;
-          if (p < p1) {
-            lxy[u] = a.xy[p];
-            ldg[u] = a.dg[p];
-            lth[u] = a.th[p];
+          const int p = pb + u * kDepThreads + l;
+          if (p < np) {
+            lxy[u] = xyp[p];
+            ldg[u] = dgp[p];
+            lth[u] = thp[p];
           }
         }
 #pragma unroll
         for (int u = 0; u < kDepAccU; ++u) {
-          const int64_t p = pb + u * kDepThreads + l;
+          const int p = pb + u * kDepThreads + l;
           int cidx = -1, ey = 0, ex = 0;
           int c[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-          if (p < p1) {
+          if (p < np) {
             int ix, iy;
             float wx, wy;
             if (cell_f(mf, lxy[u].x, lxy[u].y, ix, iy, wx, wy) && iy + 1 >= ylo &&
@@ -686,12 +723,9 @@ __device__ __forceinline__ void deposit_slice(const DepDiagArgs& a, const int bs
               ey = iy - ylo;  // output row of the lower corners
               if (ex >= 0 && ex <= bw - 2) {
                 cidx = (ey + 1) * bw + ex;
-                const float dxu = lxy[u].x - a.ax, dyu = lxy[u].y - a.ay;
-                const float faw2 = 1.0f + a.kx * dxu * dxu + a.ky * dyu * dyu +
-                                   2.0f * (a.gradx * dxu + a.grady * dyu);
-                const float q = fminf(sqrtf(faw2) / (a.gref_f + ldg[u]), qm) * Sf;
+                const float q = fminf(dep_charge(a, lxy[u], ldg[u]), qm) * Sf;
                 float sn, cs;
-                sincosf(reduce_angle((double)fh * lth[u]), &sn, &cs);
+                __sincosf(reduce_angle((double)fh * lth[u]), &sn, &cs);
                 const float vre = sn * q, vim = cs * q;
                 const float w00 = wx * wy, w10 = (1.f - wx) * wy, w01 = wx * (1.f - wy),
                             w11 = (1.f - wx) * (1.f - wy);
