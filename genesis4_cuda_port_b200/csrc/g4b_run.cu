@@ -58,6 +58,7 @@ struct BeamStepArgs {
   MixField f[kRunFields];
   int nfield;
   float gref_f, aw, aw2, ax, ay, kx, ky, gradx, grady, half;
+  float zt0;          // -2 / xks (FP32)
   double gref, xks, xku, delz, autophase;
   PlaneMapF xm, ym;
   int pre;            // 1 chicane before the first half step
@@ -130,11 +131,12 @@ __device__ __forceinline__ bool cell_f(const MixField& f, float x, float y, int&
   const float gm = f.gridmax;
   if (!(x > -gm && x < gm && y > -gm && y < gm)) return false;
   const float wxr = (x + gm) * f.inv_dgrid, wyr = (y + gm) * f.inv_dgrid;
-  ix = (int)floorf(wxr);
-  iy = (int)floorf(wyr);
+  const float fx = floorf(wxr), fy = floorf(wyr);  // integers below 2^24: exact
+  ix = (int)fx;
+  iy = (int)fy;
   if (ix < 0 || ix >= f.n - 1 || iy < 0 || iy >= f.n - 1) return false;
-  wx = 1.0f + (float)ix - wxr;
-  wy = 1.0f + (float)iy - wyr;
+  wx = 1.0f + fx - wxr;
+  wy = 1.0f + fy - wyr;
   return true;
 }
 
@@ -195,7 +197,8 @@ __device__ __forceinline__ void beam_chunk(const BeamStepArgs& a, const int4 ch)
       int ix, iy;
       float wx, wy;
       if (cell_f(F, x, y, ix, iy, wx, wy)) {
-        const int islice = (slice + F.first) % F.nslice;
+        int islice = slice + F.first;  // both in [0, nslice)
+        if (islice >= F.nslice) islice -= F.nslice;
         const float2* c = F.cells + (size_t)islice * F.n * F.ld + (size_t)iy * F.ld + ix;
         const float2 c00 = __ldg(c), c10 = __ldg(c + 1), c01 = __ldg(c + F.ld),
                      c11 = __ldg(c + F.ld + 1);
@@ -221,14 +224,16 @@ __device__ __forceinline__ void beam_chunk(const BeamStepArgs& a, const int4 ch)
     // The energy derivative Im(c) / (b0 gs) - ez drops b0 = 1 + O(1e-8).
     const double d0 = (double)d;
     const double g0 = a.gref + d0;
-    const double inv_g0 = 1.0 / g0;
+    // 1/g0: one Newton step from the FP32 reciprocal (relative error ~2^-44,
+    // far below what the FP32 results keep)
+    double inv_g0 = (double)__fdividef(1.0f, (float)g0);
+    inv_g0 = fma(inv_g0, fma(-g0, inv_g0, 1.0), inv_g0);
     const double eps0 = (double)btpar * inv_g0 * inv_g0;
     const double fe0 = 0.5 + eps0 * (0.375 + eps0 * 0.3125);
     const double B0d = a.xks * eps0 * fe0;
     const float A0 = (float)(a.xku - B0d);
     const float B0 = (float)B0d;
-    const float inv_btpar = 1.0f / btpar;
-    const float zt = (float)(-2.0 / a.xks) * inv_btpar;  // delta / btpar per unit Re(c)
+    const float zt = __fdividef(a.zt0, btpar);  // delta / btpar per unit Re(c)
     const float ig0 = (float)inv_g0;
     // stage derivatives at energy offset ds (from g0) and phase offset dth
     auto ode = [&](float ds, float dth, float& kg, float& kp) {
@@ -267,8 +272,9 @@ __device__ __forceinline__ void beam_chunk(const BeamStepArgs& a, const int4 ch)
     ode(dd, dt, k2g, k2p);
     dd += stf * (k2g - k3g);
     dt += stf * (k2p - k3p);
-    k3g /= 6.0f;
-    k3p /= 6.0f;
+    constexpr float kSixth = 1.0f / 6.0f;
+    k3g *= kSixth;
+    k3p *= kSixth;
     k2g *= -0.5f;
     k2p *= -0.5f;
     ode(dd, dt, k2g, k2p);
@@ -280,8 +286,8 @@ __device__ __forceinline__ void beam_chunk(const BeamStepArgs& a, const int4 ch)
     k2g *= 2.0f;
     k2p *= 2.0f;
     ode(dd, dt, k2g, k2p);
-    dd += stf * (k3g + k2g / 6.0f);
-    dt += stf * (k3p + k2p / 6.0f);
+    dd += stf * (k3g + k2g * kSixth);
+    dt += stf * (k3p + k2p * kSixth);
     t = t0 + (double)dt;
     d = (float)(d0 + (double)dd);
     // applyR56 (src/Core/TrackBeamCUDA.cpp:257-278): theta += R56 (gamma - gamma0)
@@ -828,23 +834,23 @@ struct FinalizeArgs {
 
 // Per-slice reductions in fixed order: field diagnostics per beam slice
 // is = (nslice + storage - first) % nslice (src/Core/DiagnosticCUDA.cpp:320)
-// from the pass-Y band partials, the beam diagnostics from the deposition
-// CTAs' quarters; also resets the deposition boxes for the next step.
+// from the pass-Y band partials (one thread per slice and quantity, adding
+// the bands in order), the beam diagnostics from the deposition CTAs'
+// records; also resets the deposition boxes for the next step.
 __device__ __forceinline__ void finalize_range(const FinalizeArgs& a, int i0, int stride) {
   const int nf = a.nfield * a.nslice;
   const int nb = a.nslice * a.rec;
-  for (int i = i0; i < nf + nb + nf; i += stride) {
-    if (i < nf) {
-      const int f = i / a.nslice, s = i - f * a.nslice;
-      const double* p = a.part[f] + (size_t)s * a.nband[f] * 9;
-      double v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-      for (int b = 0; b < a.nband[f]; ++b)
-        for (int q = 0; q < 9; ++q) v[q] += p[b * 9 + q];
+  for (int i = i0; i < 9 * nf + nb + nf; i += stride) {
+    if (i < 9 * nf) {
+      const int j = i / 9, q = i - 9 * j;
+      const int f = j / a.nslice, s = j - f * a.nslice;
+      const double* p = a.part[f] + (size_t)s * a.nband[f] * 9 + q;
+      double v = 0.0;
+      for (int b = 0; b < a.nband[f]; ++b) v += p[b * 9];
       const int is = (a.nslice + s - a.first_after[f]) % a.nslice;
-      double* o = a.field_hist + ((size_t)f * a.nslice + is) * 9;
-      for (int q = 0; q < 9; ++q) o[q] = v[q];
-    } else if (i < nf + nb) {
-      const int j = i - nf;
+      a.field_hist[((size_t)f * a.nslice + is) * 9 + q] = v;
+    } else if (i < 9 * nf + nb) {
+      const int j = i - 9 * nf;
       const int s = j / a.rec, k = j - s * a.rec;
       const int op = k < 13 ? 0 : (k < kBeamRec ? ((k - 13) % 2 == 0 ? 1 : 2) : 0);
       const double* p = a.beam_part + (size_t)s * kDepParts * a.rec + k;
@@ -855,7 +861,7 @@ __device__ __forceinline__ void finalize_range(const FinalizeArgs& a, int i0, in
       }
       a.beam_hist[(size_t)s * a.rec + k] = t;
     } else {
-      const int j = i - nf - nb;
+      const int j = i - 9 * nf - nb;
       const int f = j / a.nslice, s = j - f * a.nslice;
       a.bbox[f][s] = make_int4(1 << 30, 1 << 30, -1, -1);
     }
@@ -1063,6 +1069,7 @@ int build_step(g4b_run* r, int i, const StepPlan& p, StepArgs& L) {
     a.gref = gbase;
     a.gref_f = (float)gref;
     a.xks = xks_local;
+    a.zt0 = (float)(-2.0 / xks_local);
     a.xku = st.ku != 0.0 ? st.ku : xks_local * 0.5 / gref / gref;
     a.delz = st.delz;
     a.half = (float)(0.5 * st.delz);
@@ -1182,7 +1189,7 @@ int build_step(g4b_run* r, int i, const StepPlan& p, StepArgs& L) {
       a.nband[f] = r->fs[f].nband;
       a.first_after[f] = p.first_after[f];
     }
-    L.nfin = 2 * r->nfield * r->nslice + r->nslice * (int)r->rec_beam;
+    L.nfin = 10 * r->nfield * r->nslice + r->nslice * (int)r->rec_beam;
     L.fa = a;
   }
   return G4B_OK;
