@@ -122,7 +122,7 @@ __device__ __forceinline__ void sincos_small(float a, float& s, float& c) {
 // that interval).
 __device__ __forceinline__ float reduce_angle(double a) {
   const double twopi = 6.283185307179586476925287;
-  return (float)(a - twopi * rint(a * (1.0 / twopi)));
+  return (float)__fma_rn(-twopi, rint(a * (1.0 / twopi)), a);
 }
 
 // cell of the deposit / gather in FP32 (the same arithmetic in K1 and K2)
@@ -130,7 +130,8 @@ __device__ __forceinline__ bool cell_f(const MixField& f, float x, float y, int&
                                        float& wx, float& wy) {
   const float gm = f.gridmax;
   if (!(x > -gm && x < gm && y > -gm && y < gm)) return false;
-  const float wxr = (x + gm) * f.inv_dgrid, wyr = (y + gm) * f.inv_dgrid;
+  // explicit roundings: every kernel computes the same cell and weights
+  const float wxr = __fmul_rn(x + gm, f.inv_dgrid), wyr = __fmul_rn(y + gm, f.inv_dgrid);
   const float fx = floorf(wxr), fy = floorf(wyr);  // integers below 2^24: exact
   ix = (int)fx;
   iy = (int)fy;
@@ -377,6 +378,7 @@ struct DepField {
   float2* src;        // compact tiles, cap cells per slice
   int4* desc;
   int4* bbox;
+  int* mpred;         // [nslice] M of the slice's previous deposition (0: none)
   size_t cap;
   int first, n, ld, nslice, harm, do_source;
   float gridmax, dgrid, inv_dgrid;
@@ -404,39 +406,44 @@ struct DepDiagArgs {
 // exact for FP32 state) and for the slice's largest charge weight
 // qmax = max sqrt(faw2) / gamma.  The deposition (adi_deposit_source_atomic,
 // FieldSolverADICUDA.cpp:98-174) is then a deterministic per-cell reduction
-// in exact integer arithmetic:
-//   1. a count pass gives the number of particles per base cell (ix, iy) of
-//      the tile;
-//   2. the largest number M of contributions any output cell receives (the
-//      sum of the counts of its four base cells) fixes the slice's scale
-//      S = 2^30 / (M qmax), so every contribution rounds to an int32 with
-//      |c| <= 2^30 / M and no cell sum can overflow;
-//   3. an accumulation pass adds each particle's four bilinear contributions
-//      c = rint(S q w (sin h theta, cos h theta)) with 32-bit shared-memory
-//      integer atomics (re and im in separate planes, so the 32 lanes of a
-//      warp spread over the banks).
+// in exact integer arithmetic.  With M the largest number of contributions
+// any output cell receives (the sum of the particle counts of its four base
+// cells), the scale S = 2^30 / (M' qmax) for any M' >= M rounds every
+// contribution c = rint(S q w (sin h theta, cos h theta)) to an int32 with
+// |c| <= 2^30 / M', so no cell sum of 32-bit shared-memory integer atomics
+// can overflow (re and im in separate planes, so the 32 lanes of a warp
+// spread over the banks).  M' is the slice's M of the previous step plus a
+// quarter plus 4: one pass counts the particles per base cell and adds the
+// contributions at that scale, and the band is redone at the exact scale
+// S = 2^30 / (M qmax) in the rare case that the counted M exceeds M'.  The
+// first deposition after a beam upload counts first (exact M).
 // Integer addition is associative, so the source does not depend on the
 // order in which threads add, and each contribution keeps FP32 resolution
-// (2^-24 relative).  Phases are reduced to [-pi, pi) in FP64 and their sine
-// and cosine taken with the hardware approximation (absolute error below
-// 2^-21.4 on that interval).  The tile is the slice's bounding box of
-// touched cells (from K1); tiles larger than kDepMaxCells are processed in
-// row bands.
+// (2^-24 relative, times at most 1.25 M / M').  Phases are reduced to
+// [-pi, pi) in FP64 and their sine and cosine taken with the hardware
+// approximation (absolute error below 2^-21.4 on that interval).  Every
+// rounding that could be fused differently is written out with intrinsics,
+// so the single-run and the batched kernels give the same bits.  The tile is
+// the slice's bounding box of touched cells (from K1); tiles larger than
+// kDepMaxCells are processed in row bands.
 constexpr int kDepParts = 1;          // beam-diagnostic partial records per slice
 constexpr int kDepThreads = 256;
 constexpr int kDepDiagU = 4;          // particles in flight per thread: diagnostics pass
-constexpr int kDepHistU = 4;          // count pass
-constexpr int kDepAccU = 4;           // accumulation pass
-constexpr int kDepMaxCells = 12288;   // output cells per band (a multiple of 4)
-constexpr size_t kDepSmem = (size_t)kDepMaxCells * 8;
+constexpr int kDepAccU = 4;           // count / accumulation passes
+constexpr int kDepMaxCells = 8192;    // output cells per band (a multiple of 4)
+constexpr int kDepMaxWidth = 896;     // tile width bound: mixed ngrid <= 880
+// re and im planes, then the counts per base cell ((hb + 1) bw <= cells + width)
+constexpr size_t kDepSmem = (size_t)(3 * kDepMaxCells + kDepMaxWidth) * 4;
 
 // Charge weight sqrt(faw2) / gamma of one particle (FP32), the same
 // expression for the slice maximum and for the contributions.
 __device__ __forceinline__ float dep_charge(const DepDiagArgs& a, const float2 xy,
                                             const float dg) {
   const float dxu = xy.x - a.ax, dyu = xy.y - a.ay;
-  const float faw2 = 1.0f + a.kx * dxu * dxu + a.ky * dyu * dyu +
-                     2.0f * (a.gradx * dxu + a.grady * dyu);
+  // 1 + kx dx^2 + ky dy^2 + 2 (gradx dx + grady dy), every rounding explicit
+  const float lin = __fmaf_rn(a.grady, dyu, __fmul_rn(a.gradx, dxu));
+  const float faw2 = __fmaf_rn(__fmul_rn(a.kx, dxu), dxu,
+                               __fmaf_rn(__fmul_rn(a.ky, dyu), dyu, __fmaf_rn(2.0f, lin, 1.0f)));
   return __fdividef(sqrtf(faw2), a.gref_f + dg);
 }
 
@@ -491,9 +498,12 @@ __device__ __forceinline__ void deposit_slice(const DepDiagArgs& a, const int bs
         if (pb + u * kDepThreads >= np) break;
         const double x = lxy[u].x, y = lxy[u].y, px = lpp[u].x, py = lpp[u].y;
         const double d = ldg[u];
-        sm[0] += x; sm[1] += x * x; sm[2] += y; sm[3] += y * y;
-        sm[4] += px; sm[5] += px * px; sm[6] += py; sm[7] += py * py;
-        sm[8] += x * px; sm[9] += y * py; sm[10] += d; sm[11] += d * d;
+        sm[0] += x; sm[1] = __fma_rn(x, x, sm[1]);
+        sm[2] += y; sm[3] = __fma_rn(y, y, sm[3]);
+        sm[4] += px; sm[5] = __fma_rn(px, px, sm[5]);
+        sm[6] += py; sm[7] = __fma_rn(py, py, sm[7]);
+        sm[8] = __fma_rn(x, px, sm[8]); sm[9] = __fma_rn(y, py, sm[9]);
+        sm[10] += d; sm[11] = __fma_rn(d, d, sm[11]);
         if (a.need_aux) {
           const float f[5] = {lxy[u].x, lpp[u].x, lxy[u].y, lpp[u].y, ldg[u]};
 #pragma unroll
@@ -511,7 +521,8 @@ __device__ __forceinline__ void deposit_slice(const DepDiagArgs& a, const int bs
           if (h >= a.nbunch) break;
           bre[h] += ch;
           bim[h] += sh;
-          const float nc = ch * c1 - sh * s1, ns = sh * c1 + ch * s1;
+          const float nc = __fmaf_rn(ch, c1, -__fmul_rn(sh, s1));
+          const float ns = __fmaf_rn(sh, c1, __fmul_rn(ch, s1));
           ch = nc;
           sh = ns;
         }
@@ -568,11 +579,11 @@ __device__ __forceinline__ void deposit_slice(const DepDiagArgs& a, const int bs
           t = op == 0 ? t + u : (op == 1 ? fmin(t, u) : fmax(t, u));
         }
       }
-      if (tid == 0) t += N * a.gref;
+      if (tid == 0) t = __fma_rn(N, a.gref, t);
       if (tid == 1) {
         double sd = dpart[0][0];
         for (int i = 1; i < kDepThreads / 32; ++i) sd += dpart[i][0];
-        t += N * a.gref * a.gref + 2.0 * a.gref * sd;
+        t = __fma_rn(__dmul_rn(N, a.gref), a.gref, __fma_rn(__dmul_rn(2.0, a.gref), sd, t));
       }
       if (tid == 21) t = fmin(1.0e7, a.gref + t);
       if (tid == 22) t = fmax(1.0, a.gref + t);
@@ -586,7 +597,7 @@ __device__ __forceinline__ void deposit_slice(const DepDiagArgs& a, const int bs
   // ---- deposition of every field with a source this step ----
   int* are = reinterpret_cast<int*>(smem);        // [hb * bw] real parts
   int* aim = are + kDepMaxCells;                  // [hb * bw] imaginary parts
-  int* hist = are;  // step 1: counts per base cell, (hb + 1) * bw <= 2 kDepMaxCells
+  int* hist = aim + kDepMaxCells;                 // [(hb + 1) * bw] counts per base cell
   const double npd = (double)np;
   for (int fi = 0; fi < a.nfield; ++fi) {
     const DepField& F = a.f[fi];
@@ -609,6 +620,13 @@ __device__ __forceinline__ void deposit_slice(const DepDiagArgs& a, const int bs
       ++bw;
       if (bx0 + bw > F.ld) --bx0;
     }
+    if (bw > kDepMaxWidth) {  // excluded by g4b_run_create's ngrid limit
+      if (tid == 0) {
+        atomicOr(a.err, kErrBadSlice);
+        F.desc[target] = make_int4(0, 0, 0, 0);
+      }
+      continue;
+    }
     if (tid == 0) F.desc[target] = make_int4(bx0, by0, bw, bh);
     const int hband = max(1, kDepMaxCells / bw);  // bw <= ngrid + 1 < kDepMaxCells
     const float fh = (float)F.harm;
@@ -620,56 +638,135 @@ __device__ __forceinline__ void deposit_slice(const DepDiagArgs& a, const int bs
     mf.dgrid = F.dgrid;
     mf.inv_dgrid = F.inv_dgrid;
     mf.n = F.n;
+    // M of this slice's previous deposition of this field (0: none yet)
+    // bounds the contributions of the single-pass form below
+    const int mprev = F.mpred[bs];
+    const int m_use = mprev > 0 ? mprev + (mprev >> 2) + 4 : 0;
+    const bool q_ok = qm > 0.f && qm < 3.0e38f;
+    int m_seen = 0;
     for (int yb = 0; yb < bh; yb += hband) {
       const int hb = min(hband, bh - yb);
       const int ylo = by0 + yb;  // first grid row of this band
       const int nout = hb * bw, nbase = (hb + 1) * bw;
+      // counts per base cell (ext row iy - ylo + 1) and, with `add`, the
+      // contributions at scale Sf; a quad of lanes holding one quiet-start
+      // beamlet in one cell adds its count with one atomic and its
+      // contributions as integers summed in registers (exact)
+      auto pass = [&](const bool count, const bool add, const float Sf) {
+        for (int pb = tid & ~31; pb < np; pb += kDepAccU * kDepThreads) {
+          float2 lxy[kDepAccU];
+          float ldg[kDepAccU];
+          double lth[kDepAccU];
+#pragma unroll
+          for (int u = 0; u < kDepAccU; ++u) {
+            const int p = pb + u * kDepThreads + l;
+            if (p < np) {
+              lxy[u] = xyp[p];
+              if (add) {
+                ldg[u] = dgp[p];
+                lth[u] = thp[p];
+              }
+            }
+          }
+#pragma unroll
+          for (int u = 0; u < kDepAccU; ++u) {
+            const int p = pb + u * kDepThreads + l;
+            int cidx = -1, ey = 0, ex = 0;
+            int c[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+            if (p < np) {
+              int ix, iy;
+              float wx, wy;
+              if (cell_f(mf, lxy[u].x, lxy[u].y, ix, iy, wx, wy) && iy + 1 >= ylo &&
+                  iy < ylo + hb) {
+                ex = ix - bx0;
+                ey = iy - ylo;  // output row of the lower corners
+                if (ex < 0 || ex > bw - 2) {
+                  if (count) atomicOr(a.err, kErrBadSlice);
+                } else {
+                  cidx = (ey + 1) * bw + ex;
+                  if (add) {
+                    const float q = fminf(dep_charge(a, lxy[u], ldg[u]), qm) * Sf;
+                    float sn, cs;
+                    __sincosf(reduce_angle((double)fh * lth[u]), &sn, &cs);
+                    const float vre = sn * q, vim = cs * q;
+                    const float w00 = wx * wy, w10 = (1.f - wx) * wy, w01 = wx * (1.f - wy),
+                                w11 = (1.f - wx) * (1.f - wy);
+                    c[0] = __float2int_rn(vre * w00);
+                    c[1] = __float2int_rn(vim * w00);
+                    c[2] = __float2int_rn(vre * w10);
+                    c[3] = __float2int_rn(vim * w10);
+                    c[4] = __float2int_rn(vre * w01);
+                    c[5] = __float2int_rn(vim * w01);
+                    c[6] = __float2int_rn(vre * w11);
+                    c[7] = __float2int_rn(vim * w11);
+                  }
+                }
+              }
+            }
+            const int c1 = __shfl_xor_sync(0xffffffffu, cidx, 1);
+            const int c2 = __shfl_xor_sync(0xffffffffu, cidx, 2);
+            const int c3 = __shfl_xor_sync(0xffffffffu, cidx, 3);
+            const bool quad = cidx >= 0 && c1 == cidx && c2 == cidx && c3 == cidx;
+            if (add && __any_sync(0xffffffffu, quad)) {
+#pragma unroll
+              for (int k = 0; k < 8; ++k) {
+                int t = c[k];
+                t += __shfl_xor_sync(0xffffffffu, t, 1);
+                t += __shfl_xor_sync(0xffffffffu, t, 2);
+                if (quad) c[k] = t;
+              }
+            }
+            if (cidx >= 0 && (!quad || (l & 3) == 0)) {
+              if (count) atomicAdd(&hist[cidx], quad ? 4 : 1);
+              if (add) {
+                if (ey >= 0) {
+                  const int o = ey * bw + ex;
+                  atomicAdd(&are[o], c[0]);
+                  atomicAdd(&aim[o], c[1]);
+                  atomicAdd(&are[o + 1], c[2]);
+                  atomicAdd(&aim[o + 1], c[3]);
+                }
+                if (ey + 1 < hb) {
+                  const int o = (ey + 1) * bw + ex;
+                  atomicAdd(&are[o], c[4]);
+                  atomicAdd(&aim[o], c[5]);
+                  atomicAdd(&are[o + 1], c[6]);
+                  atomicAdd(&aim[o + 1], c[7]);
+                }
+              }
+            }
+          }
+        }
+      };
+      auto zero_acc = [&]() {
+        int4* r4 = reinterpret_cast<int4*>(are);
+        int4* i4 = reinterpret_cast<int4*>(aim);
+        for (int i = tid; i < (nout + 3) >> 2; i += kDepThreads) {
+          r4[i] = make_int4(0, 0, 0, 0);
+          i4[i] = make_int4(0, 0, 0, 0);
+        }
+      };
       __syncthreads();
       {
         int4* h4 = reinterpret_cast<int4*>(hist);
         for (int i = tid; i < (nbase + 3) >> 2; i += kDepThreads) h4[i] = make_int4(0, 0, 0, 0);
       }
-      __syncthreads();
-      // 1. counts per base cell (ext row iy - ylo + 1)
-      // (a quad of lanes holding one quiet-start beamlet shares the cell:
-      // one atomic adds its count)
-      for (int pb = tid & ~31; pb < np; pb += kDepHistU * kDepThreads) {
-        float2 lxy[kDepHistU];
-#pragma unroll
-        for (int u = 0; u < kDepHistU; ++u) {
-          const int p = pb + u * kDepThreads + l;
-          if (p < np) lxy[u] = xyp[p];
-        }
-#pragma unroll
-        for (int u = 0; u < kDepHistU; ++u) {
-          const int p = pb + u * kDepThreads + l;
-          int cidx = -1;
-          if (p < np) {
-            int ix, iy;
-            float wx, wy;
-            if (cell_f(mf, lxy[u].x, lxy[u].y, ix, iy, wx, wy) && iy + 1 >= ylo &&
-                iy < ylo + hb) {
-              const int ex = ix - bx0, ey = iy - ylo + 1;
-              if (ex < 0 || ex > bw - 2)
-                atomicOr(a.err, kErrBadSlice);
-              else
-                cidx = ey * bw + ex;
-            }
-          }
-          const int c1 = __shfl_xor_sync(0xffffffffu, cidx, 1);
-          const int c2 = __shfl_xor_sync(0xffffffffu, cidx, 2);
-          const int c3 = __shfl_xor_sync(0xffffffffu, cidx, 3);
-          if (cidx >= 0) {
-            if (c1 == cidx && c2 == cidx && c3 == cidx) {
-              if ((l & 3) == 0) atomicAdd(&hist[cidx], 4);
-            } else {
-              atomicAdd(&hist[cidx], 1);
-            }
-          }
-        }
+      const bool single = m_use > 0 && q_ok;
+      double S = 0.0;
+      if (single) {
+        // one pass: counts and contributions at the scale of the predicted
+        // bound; kept if the counted M does not exceed it (then no cell sum
+        // can have overflowed), else redone below at the exact scale
+        S = 1073741824.0 / ((double)m_use * (double)qm);  // 2^30 / (M qmax)
+        zero_acc();
+        __syncthreads();
+        pass(true, true, (float)S);
+      } else {
+        __syncthreads();
+        pass(true, false, 0.f);
       }
       __syncthreads();
-      // 2. M = max over output cells of the contributions it receives
+      // the largest number M of contributions any output cell receives
       int mloc = 0;
       for (int o = tid; o < nout; o += kDepThreads) {
         const int r = (int)(((float)o + 0.5f) * inv_bw), x = o - r * bw;
@@ -682,107 +779,25 @@ __device__ __forceinline__ void deposit_slice(const DepDiagArgs& a, const int bs
       __syncthreads();
       int M = wsum[0];
       for (int i = 1; i < kDepThreads / 32; ++i) M = max(M, wsum[i]);
+      m_seen = max(m_seen, M);
       float2* out = F.src + (size_t)target * F.cap + (size_t)yb * bw;
-      if (M == 0 || !(qm > 0.f) || !(qm < 3.0e38f)) {
+      if (M == 0 || !q_ok) {
         if (M > 0) atomicOr(a.err, kErrFixedRange);  // non-finite charge
         for (int i = tid; i < nout; i += kDepThreads) out[i] = make_float2(0.f, 0.f);
         continue;
       }
-      const double S = 1073741824.0 / ((double)M * (double)qm);  // 2^30 / (M qmax)
-      const float Sf = (float)S;
-      {
-        int4* r4 = reinterpret_cast<int4*>(are);
-        int4* i4 = reinterpret_cast<int4*>(aim);
-        for (int i = tid; i < (nout + 3) >> 2; i += kDepThreads) {
-          r4[i] = make_int4(0, 0, 0, 0);
-          i4[i] = make_int4(0, 0, 0, 0);
-        }
-      }
-      __syncthreads();
-      // 3. exact integer accumulation of the bilinear contributions
-      // (contributions of a quad of lanes with one cell are added as integers
-      // in registers first: exact, so the result is unchanged)
-      for (int pb = tid & ~31; pb < np; pb += kDepAccU * kDepThreads) {
-        float2 lxy[kDepAccU];
-        float ldg[kDepAccU];
-        double lth[kDepAccU];
-#pragma unroll
-        for (int u = 0; u < kDepAccU; ++u) {
-          const int p = pb + u * kDepThreads + l;
-          if (p < np) {
-            lxy[u] = xyp[p];
-            ldg[u] = dgp[p];
-            lth[u] = thp[p];
-          }
-        }
-#pragma unroll
-        for (int u = 0; u < kDepAccU; ++u) {
-          const int p = pb + u * kDepThreads + l;
-          int cidx = -1, ey = 0, ex = 0;
-          int c[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-          if (p < np) {
-            int ix, iy;
-            float wx, wy;
-            if (cell_f(mf, lxy[u].x, lxy[u].y, ix, iy, wx, wy) && iy + 1 >= ylo &&
-                iy < ylo + hb) {
-              ex = ix - bx0;
-              ey = iy - ylo;  // output row of the lower corners
-              if (ex >= 0 && ex <= bw - 2) {
-                cidx = (ey + 1) * bw + ex;
-                const float q = fminf(dep_charge(a, lxy[u], ldg[u]), qm) * Sf;
-                float sn, cs;
-                __sincosf(reduce_angle((double)fh * lth[u]), &sn, &cs);
-                const float vre = sn * q, vim = cs * q;
-                const float w00 = wx * wy, w10 = (1.f - wx) * wy, w01 = wx * (1.f - wy),
-                            w11 = (1.f - wx) * (1.f - wy);
-                c[0] = __float2int_rn(vre * w00);
-                c[1] = __float2int_rn(vim * w00);
-                c[2] = __float2int_rn(vre * w10);
-                c[3] = __float2int_rn(vim * w10);
-                c[4] = __float2int_rn(vre * w01);
-                c[5] = __float2int_rn(vim * w01);
-                c[6] = __float2int_rn(vre * w11);
-                c[7] = __float2int_rn(vim * w11);
-              }
-            }
-          }
-          const int c1 = __shfl_xor_sync(0xffffffffu, cidx, 1);
-          const int c2 = __shfl_xor_sync(0xffffffffu, cidx, 2);
-          const int c3 = __shfl_xor_sync(0xffffffffu, cidx, 3);
-          const bool quad = cidx >= 0 && c1 == cidx && c2 == cidx && c3 == cidx;
-          const bool anyquad = __any_sync(0xffffffffu, quad);
-          if (anyquad) {
-#pragma unroll
-            for (int k = 0; k < 8; ++k) {
-              int t = c[k];
-              t += __shfl_xor_sync(0xffffffffu, t, 1);
-              t += __shfl_xor_sync(0xffffffffu, t, 2);
-              if (quad) c[k] = t;
-            }
-          }
-          if (cidx >= 0 && (!quad || (l & 3) == 0)) {
-            if (ey >= 0) {
-              const int o = ey * bw + ex;
-              atomicAdd(&are[o], c[0]);
-              atomicAdd(&aim[o], c[1]);
-              atomicAdd(&are[o + 1], c[2]);
-              atomicAdd(&aim[o + 1], c[3]);
-            }
-            if (ey + 1 < hb) {
-              const int o = (ey + 1) * bw + ex;
-              atomicAdd(&are[o], c[4]);
-              atomicAdd(&aim[o], c[5]);
-              atomicAdd(&are[o + 1], c[6]);
-              atomicAdd(&aim[o + 1], c[7]);
-            }
-          }
-        }
+      if (!single || M > m_use) {
+        S = 1073741824.0 / ((double)M * (double)qm);
+        zero_acc();
+        __syncthreads();
+        pass(false, true, (float)S);
       }
       __syncthreads();
       const double unscale = scl / S;
       for (int i = tid; i < nout; i += kDepThreads)
         out[i] = make_float2((float)((double)are[i] * unscale), (float)((double)aim[i] * unscale));
     }
+    if (tid == 0) F.mpred[bs] = m_seen;
   }
 }
 
@@ -929,6 +944,7 @@ struct RunFieldState {
   std::vector<double> adi_delz;
   int harm = 1;
   int4* d_bbox = nullptr;
+  int* d_mpred = nullptr;       // [nslice] deposition contribution bound per slice
   double* d_part = nullptr;
   int nband = 0;
   double accuslip = 0.0;        // host slippage model
@@ -1147,6 +1163,7 @@ int build_step(g4b_run* r, int i, const StepPlan& p, StepArgs& L) {
       d.src = static_cast<float2*>(F.f->src);
       d.desc = F.f->desc;
       d.bbox = F.d_bbox;
+      d.mpred = F.d_mpred;
       d.cap = (size_t)F.f->ngrid * F.f->ld;
       d.first = p.first_before[f];
       d.n = F.f->ngrid;
@@ -1256,6 +1273,9 @@ int g4b_run_create(g4b_ctx* c, const g4b_run_desc* d, const int64_t* off, g4b_ru
     return fail(G4B_ERR_ARG, "g4b_run_create: bad descriptor");
   if (d->precision != G4B_MIXED)
     return fail(G4B_ERR_ARG, "g4b_run_create: the fused run holds mixed-precision state");
+  for (int f = 0; f < d->nfield; ++f)
+    if (d->ngrid[f] + 2 > kDepMaxWidth)
+      return fail(G4B_ERR_ARG, "g4b_run_create: ngrid above the mixed form's limit (880)");
   if (off[0] != 0) return fail(G4B_ERR_ARG, "g4b_run_create: slice_offsets[0] != 0");
   G4B_CUDA_TRY(cudaSetDevice(c->device));
   auto r = new (std::nothrow) g4b_run();
@@ -1316,6 +1336,7 @@ int g4b_run_create(g4b_ctx* c, const g4b_run_desc* d, const int64_t* off, g4b_ru
     r->bytes += F.f->bytes;
     F.nband = (F.f->ngrid + F.f->band_rows - 1) / F.f->band_rows;
     A((void**)&F.d_bbox, d->nslice * sizeof(int4));
+    A((void**)&F.d_mpred, d->nslice * sizeof(int));
     A((void**)&F.d_part, (size_t)d->nslice * F.nband * 9 * 8);
     if (e != cudaSuccess) {
       g4b_run_destroy(r);
@@ -1324,6 +1345,7 @@ int g4b_run_create(g4b_ctx* c, const g4b_run_desc* d, const int64_t* off, g4b_ru
     std::vector<int4> init(d->nslice, make_int4(1 << 30, 1 << 30, -1, -1));
     e = cudaMemcpyAsync(F.d_bbox, init.data(), init.size() * sizeof(int4),
                         cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(F.d_mpred, 0, d->nslice * sizeof(int), c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) {
       g4b_run_destroy(r);
@@ -1357,6 +1379,7 @@ int g4b_run_destroy(g4b_run* r) {
     for (g4b_adi* a : F.adis) g4b_adi_destroy(a);
     if (F.f) g4b_field_destroy(F.f);
     dev_free(r->ctx, F.d_bbox);
+    dev_free(r->ctx, F.d_mpred);
     dev_free(r->ctx, F.d_part);
   }
   ctx_release(r->ctx);
@@ -1392,6 +1415,9 @@ int g4b_run_upload_beam(g4b_run* r, const double* x, const double* y, const doub
     }
   }
   dev_free(r->ctx, stage);
+  // a new beam: the next deposition counts before it accumulates
+  for (int f = 0; f < r->nfield && e == cudaSuccess; ++f)
+    e = cudaMemsetAsync(r->fs[f].d_mpred, 0, r->nslice * sizeof(int), s);
   const cudaError_t es = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return cuda_fail(e, "g4b_run_upload_beam");
   if (es != cudaSuccess) return cuda_fail(es, "g4b_run_upload_beam");
@@ -1714,7 +1740,9 @@ struct g4b_batch {
   size_t off_beam = 0, off_dep = 0, off_adi[kNumM] = {};
   BatchCounts counts{};
   size_t smem_x[kNumM] = {}, smem_y[kNumM] = {};
-  int nf_kind = 1, nb_kind = 1;  // beam kernel fields (1 or 0 = any), bunch kinds
+  // push kernel field count (1 or 2 when every run has it, else 0 = any:
+  // the single-run kernel of the same count), deposition bunching kind
+  int nf_kind = 1, nb_kind = 1;
   // launch shapes (CTAs per kernel), chosen by the tuner
   int grid[4] = {0, 0, 0, 0};    // beam, deposit, adi, finalize
   int tune_left = 0, tune_idx = 0;
@@ -1768,14 +1796,16 @@ int batch_rebuild(g4b_batch* b) {
   for (auto& v : b->adi_items) v.clear();
   std::memset(b->smem_x, 0, sizeof b->smem_x);
   std::memset(b->smem_y, 0, sizeof b->smem_y);
-  b->nf_kind = 1;
+  b->nf_kind = -1;
   b->nb_kind = 1;
   int nactive = 0;
   for (int s = 0; s < b->max_runs; ++s) {
     g4b_run* r = b->runs[s];
     if (!r || b->next[s] >= b->last[s]) continue;
     ++nactive;
-    if (r->nfield != 1) b->nf_kind = 0;
+    const int kind = r->nfield <= 2 ? r->nfield : 0;
+    if (b->nf_kind < 0) b->nf_kind = kind;
+    else if (b->nf_kind != kind) b->nf_kind = 0;
     if (r->desc.nbunch != 1) b->nb_kind = 0;
     for (int k = 0; k < r->nchunk; ++k) b->beam_items.push_back(make_int2(s, k));
     for (int sl = 0; sl < r->nslice; ++sl) b->dep_items.push_back(make_int2(s, sl));
@@ -1901,6 +1931,8 @@ int batch_launch(g4b_batch* b, bool timed) {
     LaunchScope ls(c, "batch_beam_step");
     if (b->nf_kind == 1)
       beam_batch_kernel<1><<<b->grid[0], kRunChunk, 0, c->stream>>>(a);
+    else if (b->nf_kind == 2)
+      beam_batch_kernel<2><<<b->grid[0], kRunChunk, 0, c->stream>>>(a);
     else
       beam_batch_kernel<0><<<b->grid[0], kRunChunk, 0, c->stream>>>(a);
   }
