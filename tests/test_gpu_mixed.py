@@ -4,6 +4,8 @@ Per-step tolerances follow from FP32 state (relative ~1e-6 after a few
 steps); the end-to-end gates are the ones the mixed form is held to:
 P(z) within 1e-3 relative before saturation and |b1|(z) within 1e-3 absolute
 of the FP64 oracle on identical seeded inputs, slippage bit-exact."""
+import math
+
 import numpy as np
 import pytest
 
@@ -82,6 +84,62 @@ def test_mixed_steps_track_the_oracle(ctx, harms):
         cf, first = run.download_field(i)
         assert first == flds[i]["first"]
         assert synth.rel_err(cf, flds[i]["cells"]) < 1e-4
+
+
+def _max_contrib(x, y, ngrid, gridmax):
+    """The deposition's M from positions (FP32 cell arithmetic): the largest
+    number of bilinear contributions any output cell receives, the sum of the
+    particle counts of its four base cells."""
+    x = x.astype(np.float32)
+    y = y.astype(np.float32)
+    gm = np.float32(gridmax)
+    inv = np.float32(1.0 / (2 * gridmax / (ngrid - 1)))
+    ok = (x > -gm) & (x < gm) & (y > -gm) & (y < gm)
+    ix = np.floor((x[ok] + gm) * inv).astype(np.int64)
+    iy = np.floor((y[ok] + gm) * inv).astype(np.int64)
+    ok = (ix >= 0) & (ix < ngrid - 1) & (iy >= 0) & (iy < ngrid - 1)
+    h = np.zeros((ngrid + 1, ngrid + 1), np.int64)
+    np.add.at(h, (iy[ok] + 1, ix[ok] + 1), 1)
+    m = h[1:, 1:] + h[:-1, 1:] + h[1:, :-1] + h[:-1, :-1]
+    return int(m.max())
+
+
+def test_recount_when_the_contribution_bound_is_exceeded(ctx):
+    """A quadrupole that images the beam's angles onto the grid (phase advance
+    pi/2 over one step) concentrates the particles in x: that step's
+    deposition counts more contributions per cell than the bound taken from
+    the step before (M + M/4 + 4) and is redone at the exact scale.  The
+    result is the one a fresh run gives from the same state, whose first
+    deposition counts before it accumulates: bit-identical."""
+    nslice, ngrid, gridmax = 2, 65, 160e-6
+    off, parts = synth.beam(nslice, 2048, seed=70)
+    cells = [synth.field(nslice, ngrid, gridmax, seed=71, amplitude=3e13)]
+    k = (math.pi / (2 * synth.LAMBDA_U)) ** 2
+    steps = [synth.und_step(), synth.und_step(qf=k)]
+    cur = np.full(nslice, synth.CURRENT)
+
+    def m_of(b):
+        return [_max_contrib(b["x"][off[s]:off[s + 1]], b["y"][off[s]:off[s + 1]], ngrid,
+                             gridmax) for s in range(nslice)]
+
+    run, _, _ = _mk_run(ctx, off, parts, cells, (1,), ngrid, gridmax, steps, cur, time_run=False)
+    run.advance(0, 1, graph=False)
+    b0 = run.download_beam()
+    f0, first0 = run.download_field(0)
+    run.advance(1, 1, graph=False)
+    b1 = run.download_beam()
+    f1, _ = run.download_field(0)
+    m0, m1 = m_of(b0), m_of(b1)
+    assert all(m1[s] > m0[s] + m0[s] // 4 + 4 for s in range(nslice)), (m0, m1)
+    assert first0 == 0
+    fresh, _, _ = _mk_run(ctx, off, b0, [f0], (1,), ngrid, gridmax, steps, cur, time_run=False)
+    fresh.advance(1, 1, graph=False)
+    b2 = fresh.download_beam()
+    f2, _ = fresh.download_field(0)
+    for key in b1:
+        assert np.array_equal(b1[key], b2[key]), key
+    assert np.array_equal(f1, f2)
+    assert np.abs(f1 - f0).max() > 0  # the step deposited a source
 
 
 def test_graph_replay_equals_direct_launches_and_is_deterministic(ctx):
