@@ -50,20 +50,13 @@ __device__ __forceinline__ C cfma(C b, C c, C a) {
   return r;
 }
 
+// b*c with the fused roundings written out (the same bits in every kernel)
 template <typename C>
 __device__ __forceinline__ C cmul(C b, C c) {
   C r;
-  r.x = b.x * c.x - b.y * c.y;
-  r.y = b.x * c.y + b.y * c.x;
+  r.x = fma(b.x, c.x, -(b.y * c.y));
+  r.y = fma(b.x, c.y, b.y * c.x);
   return r;
-}
-
-template <typename C, typename T>
-__device__ __forceinline__ C cmul_ir(T r, C c) {  // (i r) * c
-  C o;
-  o.x = -r * c.y;
-  o.y = r * c.x;
-  return o;
 }
 
 template <typename C>
@@ -146,6 +139,7 @@ __device__ __forceinline__ void adi_band(const AdiPassArgs& a, const CUtensorMap
   const C* tH = tab + 2 * M * 32;    // suffix prod [M][32]
   const C* tF = tab + 3 * M * 32;    // fwd scan    [5][32]
   const C* tB = tF + 5 * 32;         // bwd scan    [5][32]
+  const C* tS = tB + 5 * 32;         // s_k = i r cbet_k (0 at the last row) [M][32]
   const int iy = r0 + warp;
   const bool active = iy < n;
   const bool row_src = band_src && iy >= srow_lo && iy < srow_hi;
@@ -162,10 +156,10 @@ __device__ __forceinline__ void adi_band(const AdiPassArgs& a, const CUtensorMap
           const C u = tile[(warp + 1) * ld + k];
           const C up = tile[(warp + 2) * ld + k];
           const C dn = tile[warp * ld + k];
-          const T lr = up.x + dn.x - u.x * (T)2;
-          const T li = up.y + dn.y - u.y * (T)2;
-          R.x = u.x + (-r * li);
-          R.y = u.y + r * lr;
+          const T lr = fma((T)-2, u.x, up.x + dn.x);
+          const T li = fma((T)-2, u.y, up.y + dn.y);
+          R.x = fma(-r, li, u.x);
+          R.y = fma(r, lr, u.y);
           if (row_src && k >= sx0 && k < sx0 + sbw) R = cadd(R, srow[k]);
         } else {
           R = tile[warp * ld + k];
@@ -173,14 +167,16 @@ __device__ __forceinline__ void adi_band(const AdiPassArgs& a, const CUtensorMap
       }
       v[j] = R;
     }
-    // forward recurrence, local part
+    // forward recurrence, local part: y_k = cbet_k (R_k + i r y_{k-1})
     {
-      C cb = __ldg(&tcb[lane]);
-      v[0] = cmul(cb, v[0]);
+      v[0] = cmul(__ldg(&tcb[lane]), v[0]);
 #pragma unroll
       for (int j = 1; j < M; ++j) {
-        cb = __ldg(&tcb[j * 32 + lane]);
-        v[j] = cfma(cmul_ir(r, cb), v[j - 1], cmul(cb, v[j]));
+        const C cb = __ldg(&tcb[j * 32 + lane]);
+        C t;
+        t.x = fma(-r, v[j - 1].y, v[j].x);
+        t.y = fma(r, v[j - 1].x, v[j].y);
+        v[j] = cmul(cb, t);
       }
     }
     // forward carry scan across lanes
@@ -195,12 +191,9 @@ __device__ __forceinline__ void adi_band(const AdiPassArgs& a, const CUtensorMap
     if (lane == 0) yin = C{0, 0};
 #pragma unroll
     for (int j = 0; j < M; ++j) v[j] = cfma(__ldg(&tG[j * 32 + lane]), yin, v[j]);
-    // backward recurrence, local part
+    // backward recurrence, local part: u_k = y_k + s_k u_{k+1}
 #pragma unroll
-    for (int j = M - 2; j >= 0; --j) {
-      const C cb = __ldg(&tcb[j * 32 + lane]);
-      v[j] = cfma(cmul_ir(r, cb), v[j + 1], v[j]);
-    }
+    for (int j = M - 2; j >= 0; --j) v[j] = cfma(__ldg(&tS[j * 32 + lane]), v[j + 1], v[j]);
     b = v[0];
 #pragma unroll
     for (int t = 0; t < 5; ++t) {
@@ -231,11 +224,11 @@ __device__ __forceinline__ void adi_band(const AdiPassArgs& a, const CUtensorMap
       const int k = lane * M + j;
       const C um = j > 0 ? v[j - 1] : left;
       const C upp = j < M - 1 ? v[j + 1] : right;
-      const T lr = upp.x + um.x - v[j].x * (T)2;
-      const T li = upp.y + um.y - v[j].y * (T)2;
+      const T lr = fma((T)-2, v[j].x, upp.x + um.x);
+      const T li = fma((T)-2, v[j].y, upp.y + um.y);
       C R;
-      R.x = v[j].x + (-r * li);
-      R.y = v[j].y + r * lr;
+      R.x = fma(-r, li, v[j].x);
+      R.y = fma(r, lr, v[j].y);
       if (row_src && k >= sx0 && k < sx0 + sbw) R = cadd(R, srow[k]);
       w2[j] = R;
     }
@@ -839,6 +832,7 @@ int g4b_adi_init(g4b_adi* a, double delz, double dgrid, double xks, int ngrid) {
       put(tab_cbet(M) + j * 32 + L, cb[k]);
       put(tab_G(M) + j * 32 + L, G[k]);
       put(tab_H(M) + j * 32 + L, H[k]);
+      put(tab_S(M) + j * 32 + L, sv[k]);
     }
   std::vector<cd> af = A, ab = B;
   for (int t = 0; t < 5; ++t) {

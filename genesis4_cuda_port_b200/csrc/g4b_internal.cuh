@@ -222,7 +222,8 @@ inline size_t tab_G(int M) { return (size_t)M * 32; }
 inline size_t tab_H(int M) { return (size_t)2 * M * 32; }
 inline size_t tab_scanF(int M) { return (size_t)3 * M * 32; }
 inline size_t tab_scanB(int M) { return (size_t)3 * M * 32 + 5 * 32; }
-inline size_t tab_total(int M) { return (size_t)3 * M * 32 + 10 * 32; }
+inline size_t tab_S(int M) { return (size_t)3 * M * 32 + 10 * 32; }
+inline size_t tab_total(int M) { return (size_t)4 * M * 32 + 10 * 32; }
 
 int pick_M(int n);
 

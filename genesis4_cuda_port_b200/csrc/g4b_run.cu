@@ -466,6 +466,7 @@ __device__ __forceinline__ void deposit_slice(const DepDiagArgs& a, const int bs
   bool want_q = false;
   for (int fi = 0; fi < a.nfield; ++fi) want_q |= a.f[fi].do_source != 0;
   if (tid < a.nfield) sbox[tid] = a.f[tid].bbox[bs];
+  __syncthreads();  // sbox is read by every thread below
 
   // ---- beam diagnostics of the slice (FP64 sums) and the largest charge ----
   {
