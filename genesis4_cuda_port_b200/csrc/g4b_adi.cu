@@ -258,23 +258,27 @@ __device__ __forceinline__ void adi_band(const AdiPassArgs& a, const CUtensorMap
     const int ic = (n * n - 1) / 2;
     const int icy = ic / n, icx = ic - icy * n;
     if (active) {
+      // cells past the row end hold exact zeros (their coefficients are 0)
+      const T dy0 = (T)(lane * M) + shift;  // exact: small integers and halves
 #pragma unroll
       for (int j = 0; j < M; ++j) {
-        const int k = lane * M + j;
-        if (k < n) {
-          const T re = v[j].x, im = v[j].y;
-          const T wei = re * re + im * im;
-          const T dy = (T)k + shift;
-          tp += wei;
-          ty1 += dy * wei;
-          ty2 += dy * dy * wei;
-          tre += re;
-          tim += im;
-          if (iy == icx && k == icy) {
-            cre = (double)re;
-            cim = (double)im;
+        const T re = v[j].x, im = v[j].y;
+        const T wei = fma(re, re, im * im);
+        const T dy = dy0 + (T)j;
+        tp += wei;
+        ty1 = fma(dy, wei, ty1);
+        ty2 = fma(dy * dy, wei, ty2);
+        tre += re;
+        tim += im;
+      }
+      const int jc = iy == icx ? icy - lane * M : -1;
+      if (jc >= 0 && jc < M) {
+#pragma unroll
+        for (int j = 0; j < M; ++j)
+          if (j == jc) {
+            cre = (double)v[j].x;
+            cim = (double)v[j].y;
           }
-        }
       }
     }
     // power over the column in FP64; the moments and sums over the column's
