@@ -144,6 +144,13 @@ __device__ __forceinline__ void adi_band(const AdiPassArgs& a, const CUtensorMap
   const bool active = iy < n;
   const bool row_src = band_src && iy >= srow_lo && iy < srow_hi;
   const C* srow = stile + warp * sbw - sx0;  // srow[k] for k in [sx0, sx0+sbw)
+  // bit j set: this lane's element j lies in the source tile's columns
+  unsigned long long smask = 0ull;
+  if (row_src) {
+    const int jlo = min(max(sx0 - lane * M, 0), M), jhi = min(max(sx0 + sbw - lane * M, 0), M);
+    smask = ((1ull << jhi) - 1ull) & ~((1ull << jlo) - 1ull);
+  }
+  const int jn = min(max(n - lane * M, 0), M);  // elements j < jn lie in the row
   C v[M];
 
   if (active) {
@@ -151,7 +158,7 @@ __device__ __forceinline__ void adi_band(const AdiPassArgs& a, const CUtensorMap
     for (int j = 0; j < M; ++j) {
       const int k = lane * M + j;
       C R = C{0, 0};
-      if (k < n) {
+      if (j < jn) {
         if (PX) {
           const C u = tile[(warp + 1) * ld + k];
           const C up = tile[(warp + 2) * ld + k];
@@ -160,7 +167,7 @@ __device__ __forceinline__ void adi_band(const AdiPassArgs& a, const CUtensorMap
           const T li = fma((T)-2, u.y, up.y + dn.y);
           R.x = fma(-r, li, u.x);
           R.y = fma(r, lr, u.y);
-          if (row_src && k >= sx0 && k < sx0 + sbw) R = cadd(R, srow[k]);
+          if ((smask >> j) & 1ull) R = cadd(R, srow[k]);
         } else {
           R = tile[warp * ld + k];
         }
@@ -229,7 +236,7 @@ __device__ __forceinline__ void adi_band(const AdiPassArgs& a, const CUtensorMap
       C R;
       R.x = fma(-r, li, v[j].x);
       R.y = fma(r, lr, v[j].y);
-      if (row_src && k >= sx0 && k < sx0 + sbw) R = cadd(R, srow[k]);
+      if ((smask >> j) & 1ull) R = cadd(R, srow[k]);
       w2[j] = R;
     }
 #pragma unroll
@@ -318,7 +325,7 @@ __device__ __forceinline__ void adi_band(const AdiPassArgs& a, const CUtensorMap
 #pragma unroll
     for (int j = 0; j < M; ++j) {
       const int k = lane * M + j;
-      if (k < n) out[k * W + warp] = v[j];
+      if (j < jn) out[k * W + warp] = v[j];
     }
   }
   ptx::fence_proxy_async();
