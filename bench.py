@@ -264,7 +264,7 @@ def kernel_alg_bytes(wl, mixed: bool):
     N = wl.nslice * wl.npart
     C = wl.nslice * wl.ngrid ** 2
     if mixed:
-        return {"run_beam_step": 56 * N, "run_deposit_diag": 28 * N,
+        return {"run_beam_step": 56 * N, "run_deposit": 20 * N, "run_beam_diag": 28 * N,
                 "adi_pass_x": 16 * C, "adi_pass_y": 16 * C, "run_diag_finalize": 0}
     return {"track": 72 * N, "push": 64 * N, "r56": 24 * N, "deposit": 32 * N,
             "adi_pass_x": 32 * C, "adi_pass_y": 32 * C, "diag_beam": 48 * N,

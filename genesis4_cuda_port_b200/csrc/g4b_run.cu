@@ -397,60 +397,231 @@ struct DepField {
   double fc, xks, dgrid_d;
 };
 
-struct DepDiagArgs {
-  const float2 *xy, *pxy;
+struct DepArgs {
+  const float2* xy;
   const float* dg;
   const double* th;
   const int64_t* off;
   const double* current;
+  float* qpred;       // [nslice] largest charge weight of the previous deposition (0: none)
   DepField f[kRunFields];
-  int nfield, nbunch, need_aux;
+  int nfield;
   float ax, ay, kx, ky, gradx, grady, gref_f;
-  double gref, delz;
-  double* beam_part;  // [nslice * kDepParts][23 + 2*nbunch] partial sums
+  double delz;
   int* err;
 };
 
-// Deposition + beam diagnostics, one CTA per slice.
-//
-// A first pass reads every particle of the slice once for the beam
-// diagnostics (FP64 sums; the minima and maxima are taken in FP32, which is
-// exact for FP32 state) and for the slice's largest charge weight
-// qmax = max sqrt(faw2) / gamma.  The deposition (adi_deposit_source_atomic,
-// FieldSolverADICUDA.cpp:98-174) is then a deterministic per-cell reduction
-// in exact integer arithmetic.  With M the largest number of contributions
-// any output cell receives (the sum of the particle counts of its four base
-// cells), the scale S = 2^30 / (M' qmax) for any M' >= M rounds every
-// contribution c = rint(S q w (sin h theta, cos h theta)) to an int32 with
+struct BeamDiagArgs {
+  const float2 *xy, *pxy;
+  const float* dg;
+  const double* th;
+  const int64_t* off;
+  int nbunch, need_aux;
+  double gref;
+  double* beam_part;  // [nslice * kDepParts][23 + 2*nbunch] records
+};
+
+// Beam diagnostics (DiagnosticCUDA.cpp:102-125), kDepParts CTAs per slice,
+// each over a quarter of the slice's particles: one pass with FP64 sums (the
+// minima and maxima in FP32, exact for FP32 state) into a record of the
+// final layout; the finalize combines a slice's records in a fixed order
+// (sums, minima and maxima of records are the record of the union).
+// Independent of the deposition, so it can run beside it and the ADI
+// passes.
+constexpr int kDepParts = 1;          // beam-diagnostic records per slice
+constexpr int kDiagThreads = 256;
+constexpr int kDepDiagU = 8;          // particles in flight per thread
+
+template <int NB>
+__device__ __forceinline__ void diag_slice(const BeamDiagArgs& a, const int bs, const int part) {
+  __shared__ double dpart[kDiagThreads / 32][kBeamRec + 2 * kMaxBunch];
+  const int tid = threadIdx.x, w = tid >> 5, l = tid & 31;
+  const int nall = (int)(a.off[bs + 1] - a.off[bs]);  // at most 65536 per slice
+  const int per = (nall + kDepParts - 1) / kDepParts;
+  const int first = min(part * per, nall);
+  const int64_t p0 = a.off[bs] + first;
+  const int np = min(per, nall - first);
+  const float2* xyp = a.xy + p0;
+  const float2* pxyp = a.pxy + p0;
+  const float* dgp = a.dg + p0;
+  const double* thp = a.th + p0;
+  const int rec = kBeamRec + 2 * a.nbunch;
+  double sm[12];  // sums of x, x^2, y, y^2, px, px^2, py, py^2, x px, y py, dg, dg^2
+#pragma unroll
+  for (int k = 0; k < 12; ++k) sm[k] = 0.0;
+  // minima / maxima of x, px, y, py (reference start values -+1e5) and dg
+  float mn[5] = {1.0e5f, 1.0e5f, 1.0e5f, 1.0e5f, INFINITY};
+  float mx[5] = {-1.0e5f, -1.0e5f, -1.0e5f, -1.0e5f, -INFINITY};
+  double bre[NB], bim[NB];
+#pragma unroll
+  for (int h = 0; h < NB; ++h) bre[h] = bim[h] = 0.0;
+  for (int pb = tid; pb < np; pb += kDepDiagU * kDiagThreads) {
+    float2 lxy[kDepDiagU], lpp[kDepDiagU];
+    float ldg[kDepDiagU];
+    double lth[kDepDiagU];
+#pragma unroll
+    for (int u = 0; u < kDepDiagU; ++u) {
+      const int p = pb + u * kDiagThreads;
+      if (p < np) {
+        lxy[u] = xyp[p];
+        lpp[u] = pxyp[p];
+        ldg[u] = dgp[p];
+        lth[u] = thp[p];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kDepDiagU; ++u) {
+      if (pb + u * kDiagThreads >= np) break;
+      const double x = lxy[u].x, y = lxy[u].y, px = lpp[u].x, py = lpp[u].y;
+      const double d = ldg[u];
+      sm[0] += x; sm[1] = __fma_rn(x, x, sm[1]);
+      sm[2] += y; sm[3] = __fma_rn(y, y, sm[3]);
+      sm[4] += px; sm[5] = __fma_rn(px, px, sm[5]);
+      sm[6] += py; sm[7] = __fma_rn(py, py, sm[7]);
+      sm[8] = __fma_rn(x, px, sm[8]); sm[9] = __fma_rn(y, py, sm[9]);
+      sm[10] += d; sm[11] = __fma_rn(d, d, sm[11]);
+      if (a.need_aux) {
+        const float f[5] = {lxy[u].x, lpp[u].x, lxy[u].y, lpp[u].y, ldg[u]};
+#pragma unroll
+        for (int i = 0; i < 5; ++i) {
+          mn[i] = fminf(mn[i], f[i]);
+          mx[i] = fmaxf(mx[i], f[i]);
+        }
+      }
+      float s1, c1;
+      __sincosf(reduce_angle(lth[u]), &s1, &c1);
+      float ch = c1, sh = s1;
+#pragma unroll
+      for (int h = 0; h < NB; ++h) {
+        if (h >= a.nbunch) break;
+        bre[h] += ch;
+        bim[h] += sh;
+        const float nc = __fmaf_rn(ch, c1, -__fmul_rn(sh, s1));
+        const float ns = __fmaf_rn(sh, c1, __fmul_rn(ch, s1));
+        ch = nc;
+        sh = ns;
+      }
+    }
+  }
+  // per-warp records in the layout of the final one: [0] sum dg,
+  // [1] sum dg^2, [2..11] the sums of x .. y py, [13..22] minima / maxima
+  // of x, px, y, py, dg
+#pragma unroll
+  for (int k = 0; k < 12; ++k) {
+    double t = sm[k];
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    if (l == 0) dpart[w][k < 10 ? k + 2 : k - 10] = t;
+  }
+#pragma unroll
+  for (int i = 0; i < 5; ++i) {
+    float lo = mn[i], hi = mx[i];
+    for (int o = 16; o > 0; o >>= 1) {
+      lo = fminf(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+      hi = fmaxf(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    }
+    if (l == 0) {
+      dpart[w][13 + 2 * i] = lo;
+      dpart[w][14 + 2 * i] = hi;
+    }
+  }
+#pragma unroll
+  for (int h = 0; h < NB; ++h) {
+    if (h >= a.nbunch) break;
+    double tr = bre[h], ti = bim[h];
+    for (int o = 16; o > 0; o >>= 1) {
+      tr += __shfl_xor_sync(0xffffffffu, tr, o);
+      ti += __shfl_xor_sync(0xffffffffu, ti, o);
+    }
+    if (l == 0) {
+      dpart[w][kBeamRec + 2 * h] = tr;
+      dpart[w][kBeamRec + 2 * h + 1] = ti;
+    }
+  }
+  __syncthreads();
+  if (tid < rec) {
+    // record (DiagnosticCUDA.cpp:102-125): [0] sum gamma, [1] sum gamma^2,
+    // [12] count, [21] / [22] min / max gamma from the dg extremes (gamma
+    // = gref + dg is monotonic in dg)
+    const double N = (double)np;
+    const int op = tid < 13 ? 0 : (tid < kBeamRec ? ((tid - 13) % 2 == 0 ? 1 : 2) : 0);
+    double t = N;
+    if (tid != 12) {
+      t = dpart[0][tid];
+      for (int i = 1; i < kDiagThreads / 32; ++i) {
+        const double u = dpart[i][tid];
+        t = op == 0 ? t + u : (op == 1 ? fmin(t, u) : fmax(t, u));
+      }
+    }
+    if (tid == 0) t = __fma_rn(N, a.gref, t);
+    if (tid == 1) {
+      double sd = dpart[0][0];
+      for (int i = 1; i < kDiagThreads / 32; ++i) sd += dpart[i][0];
+      t = __fma_rn(__dmul_rn(N, a.gref), a.gref, __fma_rn(__dmul_rn(2.0, a.gref), sd, t));
+    }
+    if (tid == 21) t = fmin(1.0e7, a.gref + t);
+    if (tid == 22) t = fmax(1.0, a.gref + t);
+    if (tid >= 13 && tid < kBeamRec && !a.need_aux) t = 0.0;
+    a.beam_part[((size_t)bs * kDepParts + part) * rec + tid] = t;
+  }
+}
+
+template <int NB>
+__global__ void __launch_bounds__(kDiagThreads, 2)
+    beam_diag_kernel(const __grid_constant__ BeamDiagArgs a) {
+  diag_slice<NB>(a, blockIdx.x / kDepParts, blockIdx.x % kDepParts);
+}
+
+// Batched form: items[i] = (run, slice of that run).
+struct DiagBatchArgs {
+  const BeamDiagArgs* args;
+  const int2* items;
+  const int* nitems;
+};
+
+template <int NB>
+__global__ void __launch_bounds__(kDiagThreads, 2)
+    beam_diag_batch_kernel(const __grid_constant__ DiagBatchArgs b) {
+  const int nitems = *b.nitems * kDepParts;
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const int2 w = b.items[it / kDepParts];
+    diag_slice<NB>(b.args[w.x], w.y, it % kDepParts);
+    __syncthreads();
+  }
+}
+
+// Deposition (adi_deposit_source_atomic, FieldSolverADICUDA.cpp:98-174),
+// one CTA per slice: a deterministic per-cell reduction in exact integer
+// arithmetic.  With M the largest number of contributions any output cell
+// receives (the sum of the particle counts of its four base cells) and
+// qmax the largest charge weight sqrt(faw2) / gamma, the scale
+// S = 2^30 / (M' q') for any M' >= M, q' >= qmax rounds every contribution
+// c = rint(S q w (sin h theta, cos h theta)) to an int32 with
 // |c| <= 2^30 / M', so no cell sum of 32-bit shared-memory integer atomics
 // can overflow (re and im in separate planes, so the 32 lanes of a warp
-// spread over the banks).  M' is the slice's M of the previous step plus a
-// quarter plus 4: one pass counts the particles per base cell and adds the
-// contributions at that scale, and the band is redone at the exact scale
-// S = 2^30 / (M qmax) in the rare case that the counted M exceeds M'.  The
-// first deposition after a beam upload counts first (exact M).
+// spread over the banks).  M' and q' come from the slice's previous
+// deposition (M + M/4 + 4 and qmax (1 + 2^-6)): one pass counts the
+// particles per base cell, takes qmax and adds the contributions at that
+// scale, and the band is redone at the exact scale S = 2^30 / (M qmax) in
+// the rare case that the counted M or qmax exceeds its bound.  The first
+// deposition after a beam upload counts first.
 // Integer addition is associative, so the source does not depend on the
 // order in which threads add, and each contribution keeps FP32 resolution
-// (2^-24 relative, times at most 1.25 M / M').  Phases are reduced to
-// [-pi, pi) in FP64 and their sine and cosine taken with the hardware
+// (2^-24 relative, times at most 1.25 M qmax / (M' q')).  Phases are reduced
+// to [-pi, pi) in FP64 and their sine and cosine taken with the hardware
 // approximation (absolute error below 2^-21.4 on that interval).  Every
 // rounding that could be fused differently is written out with intrinsics,
 // so the single-run and the batched kernels give the same bits.  The tile is
 // the slice's bounding box of touched cells (from K1); tiles larger than
 // kDepMaxCells are processed in row bands.
-constexpr int kDepParts = 1;          // beam-diagnostic partial records per slice
 constexpr int kDepThreads = 256;
-constexpr int kDepDiagU = 4;          // particles in flight per thread: diagnostics pass
-constexpr int kDepAccU = 4;           // count / accumulation passes
+constexpr int kDepAccU = 4;           // particles in flight per thread
 constexpr int kDepMaxCells = 8192;    // output cells per band (a multiple of 4)
 constexpr int kDepMaxWidth = 896;     // tile width bound: mixed ngrid <= 880
 // re and im planes, then the counts per base cell ((hb + 1) bw <= cells + width)
 constexpr size_t kDepSmem = (size_t)(3 * kDepMaxCells + kDepMaxWidth) * 4;
 
-// Charge weight sqrt(faw2) / gamma of one particle (FP32), the same
-// expression for the slice maximum and for the contributions.
-__device__ __forceinline__ float dep_charge(const DepDiagArgs& a, const float2 xy,
-                                            const float dg) {
+// Charge weight sqrt(faw2) / gamma of one particle (FP32).
+__device__ __forceinline__ float dep_charge(const DepArgs& a, const float2 xy, const float dg) {
   const float dxu = xy.x - a.ax, dyu = xy.y - a.ay;
   // 1 + kx dx^2 + ky dy^2 + 2 (gradx dx + grady dy), every rounding explicit
   const float lin = __fmaf_rn(a.grady, dyu, __fmul_rn(a.gradx, dxu));
@@ -459,11 +630,7 @@ __device__ __forceinline__ float dep_charge(const DepDiagArgs& a, const float2 x
   return __fdividef(sqrtf(faw2), a.gref_f + dg);
 }
 
-// NB: bunching harmonics accumulated (1, or up to kMaxBunch)
-template <int NB>
-__device__ __forceinline__ void deposit_slice(const DepDiagArgs& a, const int bs,
-                                              unsigned char* smem) {
-  __shared__ double dpart[kDepThreads / 32][kBeamRec + 2 * kMaxBunch];
+__device__ __forceinline__ void deposit_slice(const DepArgs& a, const int bs, unsigned char* smem) {
   __shared__ int4 sbox[kRunFields];
   __shared__ int wsum[kDepThreads / 32];
   __shared__ float wmax[kDepThreads / 32];
@@ -471,141 +638,14 @@ __device__ __forceinline__ void deposit_slice(const DepDiagArgs& a, const int bs
   const int64_t p0 = a.off[bs];
   const int np = (int)(a.off[bs + 1] - p0);  // at most 65536 particles per slice
   const float2* xyp = a.xy + p0;
-  const float2* pxyp = a.pxy + p0;
   const float* dgp = a.dg + p0;
   const double* thp = a.th + p0;
-  const int rec = kBeamRec + 2 * a.nbunch;
-  bool want_q = false;
-  for (int fi = 0; fi < a.nfield; ++fi) want_q |= a.f[fi].do_source != 0;
   if (tid < a.nfield) sbox[tid] = a.f[tid].bbox[bs];
+  const float qprev = a.qpred[bs];
+  const float q_use = qprev * 1.015625f;  // 0 without a previous deposition
+  float q_seen = 0.f;
+  bool deposited = false;
   __syncthreads();  // sbox is read by every thread below
-
-  // ---- beam diagnostics of the slice (FP64 sums) and the largest charge ----
-  {
-    double sm[12];  // sums of x, x^2, y, y^2, px, px^2, py, py^2, x px, y py, dg, dg^2
-#pragma unroll
-    for (int k = 0; k < 12; ++k) sm[k] = 0.0;
-    // minima / maxima of x, px, y, py (reference start values -+1e5) and dg
-    float mn[5] = {1.0e5f, 1.0e5f, 1.0e5f, 1.0e5f, INFINITY};
-    float mx[5] = {-1.0e5f, -1.0e5f, -1.0e5f, -1.0e5f, -INFINITY};
-    float qmax = 0.f;
-    double bre[NB], bim[NB];
-#pragma unroll
-    for (int h = 0; h < NB; ++h) bre[h] = bim[h] = 0.0;
-    for (int pb = tid; pb < np; pb += kDepDiagU * kDepThreads) {
-      float2 lxy[kDepDiagU], lpp[kDepDiagU];
-      float ldg[kDepDiagU];
-      double lth[kDepDiagU];
-#pragma unroll
-      for (int u = 0; u < kDepDiagU; ++u) {
-        const int p = pb + u * kDepThreads;
-        if (p < np) {
-          lxy[u] = xyp[p];
-          lpp[u] = pxyp[p];
-          ldg[u] = dgp[p];
-          lth[u] = thp[p];
-        }
-      }
-#pragma unroll
-      for (int u = 0; u < kDepDiagU; ++u) {
-        if (pb + u * kDepThreads >= np) break;
-        const double x = lxy[u].x, y = lxy[u].y, px = lpp[u].x, py = lpp[u].y;
-        const double d = ldg[u];
-        sm[0] += x; sm[1] = __fma_rn(x, x, sm[1]);
-        sm[2] += y; sm[3] = __fma_rn(y, y, sm[3]);
-        sm[4] += px; sm[5] = __fma_rn(px, px, sm[5]);
-        sm[6] += py; sm[7] = __fma_rn(py, py, sm[7]);
-        sm[8] = __fma_rn(x, px, sm[8]); sm[9] = __fma_rn(y, py, sm[9]);
-        sm[10] += d; sm[11] = __fma_rn(d, d, sm[11]);
-        if (a.need_aux) {
-          const float f[5] = {lxy[u].x, lpp[u].x, lxy[u].y, lpp[u].y, ldg[u]};
-#pragma unroll
-          for (int i = 0; i < 5; ++i) {
-            mn[i] = fminf(mn[i], f[i]);
-            mx[i] = fmaxf(mx[i], f[i]);
-          }
-        }
-        if (want_q) qmax = fmaxf(qmax, dep_charge(a, lxy[u], ldg[u]));
-        float s1, c1;
-        __sincosf(reduce_angle(lth[u]), &s1, &c1);
-        float ch = c1, sh = s1;
-#pragma unroll
-        for (int h = 0; h < NB; ++h) {
-          if (h >= a.nbunch) break;
-          bre[h] += ch;
-          bim[h] += sh;
-          const float nc = __fmaf_rn(ch, c1, -__fmul_rn(sh, s1));
-          const float ns = __fmaf_rn(sh, c1, __fmul_rn(ch, s1));
-          ch = nc;
-          sh = ns;
-        }
-      }
-    }
-    // per-warp records in the layout of the final one: [0] sum dg,
-    // [1] sum dg^2, [2..11] the sums of x .. y py, [13..22] minima / maxima
-    // of x, px, y, py, dg
-#pragma unroll
-    for (int k = 0; k < 12; ++k) {
-      double t = sm[k];
-      for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
-      if (l == 0) dpart[w][k < 10 ? k + 2 : k - 10] = t;
-    }
-#pragma unroll
-    for (int i = 0; i < 5; ++i) {
-      float lo = mn[i], hi = mx[i];
-      for (int o = 16; o > 0; o >>= 1) {
-        lo = fminf(lo, __shfl_xor_sync(0xffffffffu, lo, o));
-        hi = fmaxf(hi, __shfl_xor_sync(0xffffffffu, hi, o));
-      }
-      if (l == 0) {
-        dpart[w][13 + 2 * i] = lo;
-        dpart[w][14 + 2 * i] = hi;
-      }
-    }
-    for (int o = 16; o > 0; o >>= 1) qmax = fmaxf(qmax, __shfl_xor_sync(0xffffffffu, qmax, o));
-    if (l == 0) wmax[w] = qmax;
-#pragma unroll
-    for (int h = 0; h < NB; ++h) {
-      if (h >= a.nbunch) break;
-      double tr = bre[h], ti = bim[h];
-      for (int o = 16; o > 0; o >>= 1) {
-        tr += __shfl_xor_sync(0xffffffffu, tr, o);
-        ti += __shfl_xor_sync(0xffffffffu, ti, o);
-      }
-      if (l == 0) {
-        dpart[w][kBeamRec + 2 * h] = tr;
-        dpart[w][kBeamRec + 2 * h + 1] = ti;
-      }
-    }
-    __syncthreads();
-    if (tid < rec) {
-      // record (DiagnosticCUDA.cpp:102-125): [0] sum gamma, [1] sum gamma^2,
-      // [12] count, [21] / [22] min / max gamma from the dg extremes (gamma
-      // = gref + dg is monotonic in dg)
-      const double N = (double)np;
-      const int op = tid < 13 ? 0 : (tid < kBeamRec ? ((tid - 13) % 2 == 0 ? 1 : 2) : 0);
-      double t = N;
-      if (tid != 12) {
-        t = dpart[0][tid];
-        for (int i = 1; i < kDepThreads / 32; ++i) {
-          const double u = dpart[i][tid];
-          t = op == 0 ? t + u : (op == 1 ? fmin(t, u) : fmax(t, u));
-        }
-      }
-      if (tid == 0) t = __fma_rn(N, a.gref, t);
-      if (tid == 1) {
-        double sd = dpart[0][0];
-        for (int i = 1; i < kDepThreads / 32; ++i) sd += dpart[i][0];
-        t = __fma_rn(__dmul_rn(N, a.gref), a.gref, __fma_rn(__dmul_rn(2.0, a.gref), sd, t));
-      }
-      if (tid == 21) t = fmin(1.0e7, a.gref + t);
-      if (tid == 22) t = fmax(1.0, a.gref + t);
-      if (tid >= 13 && tid < kBeamRec && !a.need_aux) t = 0.0;
-      a.beam_part[(size_t)bs * rec + tid] = t;
-    }
-  }
-  float qm = wmax[0];
-  for (int i = 1; i < kDepThreads / 32; ++i) qm = fmaxf(qm, wmax[i]);
 
   // ---- deposition of every field with a source this step ----
   int* are = reinterpret_cast<int*>(smem);        // [hb * bw] real parts
@@ -655,17 +695,18 @@ __device__ __forceinline__ void deposit_slice(const DepDiagArgs& a, const int bs
     // bounds the contributions of the single-pass form below
     const int mprev = F.mpred[bs];
     const int m_use = mprev > 0 ? mprev + (mprev >> 2) + 4 : 0;
-    const bool q_ok = qm > 0.f && qm < 3.0e38f;
     int m_seen = 0;
     for (int yb = 0; yb < bh; yb += hband) {
       const int hb = min(hband, bh - yb);
       const int ylo = by0 + yb;  // first grid row of this band
       const int nout = hb * bw, nbase = (hb + 1) * bw;
-      // counts per base cell (ext row iy - ylo + 1) and, with `add`, the
-      // contributions at scale Sf; a quad of lanes holding one quiet-start
-      // beamlet in one cell adds its count with one atomic and its
+      // with `count` the counts per base cell (ext row iy - ylo + 1) and the
+      // largest charge weight (qloc), with `add` the contributions at scale
+      // Sf of charge weights capped at qc; a quad of lanes holding one
+      // quiet-start beamlet in one cell adds its count with one atomic and its
       // contributions as integers summed in registers (exact)
-      auto pass = [&](const bool count, const bool add, const float Sf) {
+      float qloc = 0.f;
+      auto pass = [&](const bool count, const bool add, const float Sf, const float qc) {
         for (int pb = tid & ~31; pb < np; pb += kDepAccU * kDepThreads) {
           float2 lxy[kDepAccU];
           float ldg[kDepAccU];
@@ -675,10 +716,8 @@ __device__ __forceinline__ void deposit_slice(const DepDiagArgs& a, const int bs
             const int p = pb + u * kDepThreads + l;
             if (p < np) {
               lxy[u] = xyp[p];
-              if (add) {
-                ldg[u] = dgp[p];
-                lth[u] = thp[p];
-              }
+              ldg[u] = dgp[p];
+              if (add) lth[u] = thp[p];
             }
           }
 #pragma unroll
@@ -697,8 +736,10 @@ __device__ __forceinline__ void deposit_slice(const DepDiagArgs& a, const int bs
                   if (count) atomicOr(a.err, kErrBadSlice);
                 } else {
                   cidx = (ey + 1) * bw + ex;
+                  const float qraw = dep_charge(a, lxy[u], ldg[u]);
+                  if (count) qloc = fmaxf(qloc, qraw);
                   if (add) {
-                    const float q = fminf(dep_charge(a, lxy[u], ldg[u]), qm) * Sf;
+                    const float q = fminf(qraw, qc) * Sf;
                     float sn, cs;
                     __sincosf(reduce_angle((double)fh * lth[u]), &sn, &cs);
                     const float vre = sn * q, vim = cs * q;
@@ -764,19 +805,20 @@ __device__ __forceinline__ void deposit_slice(const DepDiagArgs& a, const int bs
         int4* h4 = reinterpret_cast<int4*>(hist);
         for (int i = tid; i < (nbase + 3) >> 2; i += kDepThreads) h4[i] = make_int4(0, 0, 0, 0);
       }
-      const bool single = m_use > 0 && q_ok;
+      const bool single = m_use > 0 && q_use > 0.f && q_use < 3.0e38f;
       double S = 0.0;
       if (single) {
-        // one pass: counts and contributions at the scale of the predicted
-        // bound; kept if the counted M does not exceed it (then no cell sum
-        // can have overflowed), else redone below at the exact scale
-        S = 1073741824.0 / ((double)m_use * (double)qm);  // 2^30 / (M qmax)
+        // one pass: counts, qmax and contributions at the scale of the
+        // predicted bounds; kept if neither counted bound exceeds its
+        // prediction (then no cell sum can have overflowed and no charge was
+        // capped), else redone below at the exact scale
+        S = 1073741824.0 / ((double)m_use * (double)q_use);  // 2^30 / (M' q')
         zero_acc();
         __syncthreads();
-        pass(true, true, (float)S);
+        pass(true, true, (float)S, q_use);
       } else {
         __syncthreads();
-        pass(true, false, 0.f);
+        pass(true, false, 0.f, 0.f);
       }
       __syncthreads();
       // the largest number M of contributions any output cell receives
@@ -787,23 +829,35 @@ __device__ __forceinline__ void deposit_slice(const DepDiagArgs& a, const int bs
         if (x > 0) m += hist[(r + 1) * bw + x - 1] + hist[r * bw + x - 1];
         mloc = max(mloc, m);
       }
-      for (int o = 16; o > 0; o >>= 1) mloc = max(mloc, __shfl_xor_sync(0xffffffffu, mloc, o));
-      if (l == 0) wsum[w] = mloc;
+      for (int o = 16; o > 0; o >>= 1) {
+        mloc = max(mloc, __shfl_xor_sync(0xffffffffu, mloc, o));
+        qloc = fmaxf(qloc, __shfl_xor_sync(0xffffffffu, qloc, o));
+      }
+      if (l == 0) {
+        wsum[w] = mloc;
+        wmax[w] = qloc;
+      }
       __syncthreads();
       int M = wsum[0];
-      for (int i = 1; i < kDepThreads / 32; ++i) M = max(M, wsum[i]);
+      float qm = wmax[0];
+      for (int i = 1; i < kDepThreads / 32; ++i) {
+        M = max(M, wsum[i]);
+        qm = fmaxf(qm, wmax[i]);
+      }
       m_seen = max(m_seen, M);
       float2* out = F.src + (size_t)target * F.cap + (size_t)yb * bw;
-      if (M == 0 || !q_ok) {
+      if (M == 0 || !(qm > 0.f) || !(qm < 3.0e38f)) {
         if (M > 0) atomicOr(a.err, kErrFixedRange);  // non-finite charge
         for (int i = tid; i < nout; i += kDepThreads) out[i] = make_float2(0.f, 0.f);
         continue;
       }
-      if (!single || M > m_use) {
-        S = 1073741824.0 / ((double)M * (double)qm);
+      q_seen = fmaxf(q_seen, qm);
+      deposited = true;
+      if (!single || M > m_use || qm > q_use) {
+        S = 1073741824.0 / ((double)M * (double)qm);  // 2^30 / (M qmax)
         zero_acc();
         __syncthreads();
-        pass(false, true, (float)S);
+        pass(false, true, (float)S, qm);
       }
       __syncthreads();
       const double unscale = scl / S;
@@ -812,30 +866,28 @@ __device__ __forceinline__ void deposit_slice(const DepDiagArgs& a, const int bs
     }
     if (tid == 0) F.mpred[bs] = m_seen;
   }
+  if (tid == 0 && deposited) a.qpred[bs] = q_seen;
 }
 
-template <int NB>
-__global__ void __launch_bounds__(kDepThreads, 2)
-    deposit_diag_kernel(const __grid_constant__ DepDiagArgs a) {
+__global__ void __launch_bounds__(kDepThreads, 2) deposit_kernel(const __grid_constant__ DepArgs a) {
   extern __shared__ __align__(128) unsigned char smem[];
-  deposit_slice<NB>(a, blockIdx.x, smem);
+  deposit_slice(a, blockIdx.x, smem);
 }
 
 // Batched form: items[i] = (run, slice of that run).
 struct DepBatchArgs {
-  const DepDiagArgs* args;
+  const DepArgs* args;
   const int2* items;
   const int* nitems;
 };
 
-template <int NB>
 __global__ void __launch_bounds__(kDepThreads, 2)
     deposit_batch_kernel(const __grid_constant__ DepBatchArgs b) {
   extern __shared__ __align__(128) unsigned char smem[];
   const int nitems = *b.nitems;
   for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
     const int2 w = b.items[it];
-    deposit_slice<NB>(b.args[w.x], w.y, smem);
+    deposit_slice(b.args[w.x], w.y, smem);
     __syncthreads();
   }
 }
@@ -984,7 +1036,12 @@ struct g4b_run {
   std::vector<double> slip;
   // history of diagnostics: per step beam [nslice][rec] then fields
   double* d_hist = nullptr;
-  double* d_beam_part = nullptr;   // deposition CTAs' beam-diagnostic partials
+  double* d_beam_part = nullptr;   // beam-diagnostic records per slice
+  float* d_qpred = nullptr;        // [nslice] largest charge weight of the last deposition
+  // second stream and fork / join events of a captured step (diagnostics branch)
+  cudaStream_t aux = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  bool capturing = false;
   int hist_steps = 0;
   size_t rec_beam = 0, step_doubles = 0;
   // cached graph
@@ -1005,7 +1062,8 @@ constexpr int kRunChunk = 256;
 struct StepArgs {
   bool has_beam;
   BeamStepArgs bs;
-  DepDiagArgs dd;
+  DepArgs dd;
+  BeamDiagArgs bd;
   AdiPlan adi[kRunFields];
   FinalizeArgs fa;
   int nfin;
@@ -1149,26 +1207,33 @@ int build_step(g4b_run* r, int i, const StepPlan& p, StepArgs& L) {
   // K2
   double* step_hist = r->d_hist + (size_t)(i % r->hist_steps) * r->step_doubles;
   {
-    DepDiagArgs a{};
+    BeamDiagArgs b{};
+    b.xy = r->xy;
+    b.pxy = r->pxy;
+    b.dg = r->dg;
+    b.th = r->th;
+    b.off = r->d_off;
+    b.nbunch = r->desc.nbunch;
+    b.need_aux = 1;
+    b.gref = gbase;
+    b.beam_part = r->d_beam_part;
+    L.bd = b;
+    DepArgs a{};
     a.xy = r->xy;
-    a.pxy = r->pxy;
     a.dg = r->dg;
     a.th = r->th;
     a.off = r->d_off;
     a.current = r->d_current;
+    a.qpred = r->d_qpred;
     a.nfield = r->nfield;
-    a.nbunch = r->desc.nbunch;
-    a.need_aux = 1;
     a.ax = (float)st.ax;
     a.ay = (float)st.ay;
     a.kx = (float)st.kx;
     a.ky = (float)st.ky;
     a.gradx = (float)st.gradx;
     a.grady = (float)st.grady;
-    a.gref = gbase;
     a.delz = st.delz;
     a.gref_f = (float)gbase;
-    a.beam_part = r->d_beam_part;
     a.err = c->d_error;
     for (int f = 0; f < r->nfield; ++f) {
       const RunFieldState& F = r->fs[f];
@@ -1238,16 +1303,33 @@ int launch_single(g4b_run* r, const StepArgs& L) {
       beam_step_kernel<0><<<r->nchunk, kRunChunk, 0, c->stream>>>(L.bs);
   }
   if (int rc = check_launch(c, "beam_step_kernel")) return rc;
-  {
-    LaunchScope ls(c, "run_deposit_diag");
+  // The beam diagnostics depend only on K1; in a captured graph they form a
+  // branch of their own beside the deposition and the ADI passes (filling
+  // the SMs those leave idle), joined before the finalize.
+  auto diag = [&](cudaStream_t st) {
+    LaunchScope ls(c, "run_beam_diag");
     if (r->desc.nbunch == 1)
-      deposit_diag_kernel<1><<<r->nslice, kDepThreads, kDepSmem, c->stream>>>(L.dd);
+      beam_diag_kernel<1><<<r->nslice * kDepParts, kDiagThreads, 0, st>>>(L.bd);
     else
-      deposit_diag_kernel<kMaxBunch><<<r->nslice, kDepThreads, kDepSmem, c->stream>>>(L.dd);
+      beam_diag_kernel<kMaxBunch><<<r->nslice * kDepParts, kDiagThreads, 0, st>>>(L.bd);
+    return check_launch(c, "beam_diag_kernel");
+  };
+  if (r->capturing) {
+    G4B_CUDA_TRY(cudaEventRecord(r->ev_fork, c->stream));
+    G4B_CUDA_TRY(cudaStreamWaitEvent(r->aux, r->ev_fork, 0));
+    if (int rc = diag(r->aux)) return rc;
+    G4B_CUDA_TRY(cudaEventRecord(r->ev_join, r->aux));
   }
-  if (int rc = check_launch(c, "deposit_diag_kernel")) return rc;
+  {
+    LaunchScope ls(c, "run_deposit");
+    deposit_kernel<<<r->nslice, kDepThreads, kDepSmem, c->stream>>>(L.dd);
+  }
+  if (int rc = check_launch(c, "deposit_kernel")) return rc;
+  if (!r->capturing)
+    if (int rc = diag(c->stream)) return rc;
   for (int f = 0; f < r->nfield; ++f)
     if (int rc = adi_launch(r->fs[f].f, L.adi[f])) return rc;
+  if (r->capturing) G4B_CUDA_TRY(cudaStreamWaitEvent(c->stream, r->ev_join, 0));
   {
     LaunchScope ls(c, "run_diag_finalize");
     diag_finalize_kernel<<<(L.nfin + 255) / 256, 256, 0, c->stream>>>(L.fa);
@@ -1367,15 +1449,16 @@ int g4b_run_create(g4b_ctx* c, const g4b_run_desc* d, const int64_t* off, g4b_ru
   }
   r->rec_beam = kBeamRec + 2 * d->nbunch;
   A((void**)&r->d_beam_part, (size_t)d->nslice * kDepParts * r->rec_beam * 8);
+  A((void**)&r->d_qpred, d->nslice * sizeof(float));
+  if (e == cudaSuccess) e = cudaMemsetAsync(r->d_qpred, 0, d->nslice * sizeof(float), c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) {
     g4b_run_destroy(r);
     return cuda_fail(e, "g4b_run_create: device allocation");
   }
   r->step_doubles = (size_t)d->nslice * (r->rec_beam + 9 * d->nfield);
-  cudaFuncSetAttribute(deposit_diag_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaFuncSetAttribute(deposit_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)kDepSmem);
-  cudaFuncSetAttribute(deposit_diag_kernel<kMaxBunch>,
-                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDepSmem);
   *out = r;
   return G4B_OK;
 }
@@ -1384,8 +1467,11 @@ int g4b_run_destroy(g4b_run* r) {
   if (!r) return G4B_OK;
   ctx_quiesce(r->ctx);
   if (r->gexec) cudaGraphExecDestroy(r->gexec);
+  if (r->ev_fork) cudaEventDestroy(r->ev_fork);
+  if (r->ev_join) cudaEventDestroy(r->ev_join);
+  if (r->aux) cudaStreamDestroy(r->aux);
   void* ptrs[] = {r->xy, r->pxy, r->dg, r->th, r->d_off, r->d_chunks, r->d_current,
-                  r->d_eloss, r->d_hist, r->d_beam_part};
+                  r->d_eloss, r->d_hist, r->d_beam_part, r->d_qpred};
   for (void* p : ptrs) dev_free(r->ctx, p);
   for (int f = 0; f < kRunFields; ++f) {
     RunFieldState& F = r->fs[f];
@@ -1431,6 +1517,7 @@ int g4b_run_upload_beam(g4b_run* r, const double* x, const double* y, const doub
   // a new beam: the next deposition counts before it accumulates
   for (int f = 0; f < r->nfield && e == cudaSuccess; ++f)
     e = cudaMemsetAsync(r->fs[f].d_mpred, 0, r->nslice * sizeof(int), s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(r->d_qpred, 0, r->nslice * sizeof(float), s);
   const cudaError_t es = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return cuda_fail(e, "g4b_run_upload_beam");
   if (es != cudaSuccess) return cuda_fail(es, "g4b_run_upload_beam");
@@ -1557,9 +1644,15 @@ int g4b_run_set_lattice(g4b_run* r, int nstep, const g4b_step* steps, const doub
 static int run_capture(g4b_run* r, int first_step, int nsteps, cudaGraphExec_t* out) {
   g4b_ctx* c = r->ctx;
   cudaGraph_t g = nullptr;
+  if (!r->aux) {
+    G4B_CUDA_TRY(cudaStreamCreateWithFlags(&r->aux, cudaStreamNonBlocking));
+    G4B_CUDA_TRY(cudaEventCreateWithFlags(&r->ev_fork, cudaEventDisableTiming));
+    G4B_CUDA_TRY(cudaEventCreateWithFlags(&r->ev_join, cudaEventDisableTiming));
+  }
   const bool prof = c->prof.on;  // no profiler events inside a graph
   c->prof.on = false;
   G4B_CUDA_TRY(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+  r->capturing = true;
   int rc = G4B_OK;
   for (int k = 0; k < nsteps && rc == G4B_OK; ++k) {
     const int i = (first_step + k) % (int)r->steps.size();
@@ -1567,6 +1660,7 @@ static int run_capture(g4b_run* r, int first_step, int nsteps, cudaGraphExec_t* 
     rc = plan_step(r, i, p);
     if (rc == G4B_OK) rc = enqueue_step(r, first_step + k, p);
   }
+  r->capturing = false;
   cudaError_t e = cudaStreamEndCapture(c->stream, &g);
   c->prof.on = prof;
   if (rc) {
@@ -1636,7 +1730,7 @@ int g4b_run_advance(g4b_run* r, int first_step, int nsteps, int use_graph) {
     return G4B_OK;
   }
   if (int rc = run_prepare(r, first_step, nsteps)) return rc;
-  r->ctx->launches += (uint64_t)nsteps * (3 + 2 * r->nfield);
+  r->ctx->launches += (uint64_t)nsteps * (4 + 2 * r->nfield);
   G4B_CUDA_TRY(cudaGraphLaunch(r->gexec, r->ctx->stream));
   // advance the host model exactly as the captured steps did
   for (int k = 0; k < nsteps; ++k) {
@@ -1735,7 +1829,7 @@ struct g4b_batch {
   std::vector<int> next, last;  // per slot: next lattice step, end (exclusive)
   bool dirty = true;            // composition changed since the last upload
   // staging (pinned host, double-buffered) and device mirror
-  size_t off_bs = 0, off_dd = 0, off_fa = 0, off_ax = 0, off_ay = 0, off_mx = 0, off_my = 0,
+  size_t off_bs = 0, off_dd = 0, off_bd = 0, off_fa = 0, off_ax = 0, off_ay = 0, off_mx = 0, off_my = 0,
          args_bytes = 0;
   unsigned char* h_args[2] = {nullptr, nullptr};
   unsigned char* d_args = nullptr;
@@ -1780,7 +1874,9 @@ int batch_layout(g4b_batch* b) {
   b->off_bs = o;
   o = align_up<BeamStepArgs>(o + nr * sizeof(BeamStepArgs));
   b->off_dd = o;
-  o = align_up<DepDiagArgs>(o + nr * sizeof(DepDiagArgs));
+  o = align_up<DepArgs>(o + nr * sizeof(DepArgs));
+  b->off_bd = o;
+  o = align_up<BeamDiagArgs>(o + nr * sizeof(BeamDiagArgs));
   b->off_fa = o;
   o = align_up<FinalizeArgs>(o + nr * sizeof(FinalizeArgs));
   b->off_ax = o;
@@ -1896,7 +1992,8 @@ int batch_stage(g4b_batch* b) {
   unsigned char* h = b->h_args[k];
   std::memcpy(h, &b->counts, sizeof(BatchCounts));
   auto* bs = reinterpret_cast<BeamStepArgs*>(h + b->off_bs);
-  auto* dd = reinterpret_cast<DepDiagArgs*>(h + b->off_dd);
+  auto* dd = reinterpret_cast<DepArgs*>(h + b->off_dd);
+  auto* bd = reinterpret_cast<BeamDiagArgs*>(h + b->off_bd);
   auto* fa = reinterpret_cast<FinalizeArgs*>(h + b->off_fa);
   auto* ax = reinterpret_cast<AdiPassArgs*>(h + b->off_ax);
   auto* ay = reinterpret_cast<AdiPassArgs*>(h + b->off_ay);
@@ -1913,6 +2010,7 @@ int batch_stage(g4b_batch* b) {
     if (int rc = build_step(r, i, p, L)) return rc;
     bs[s] = L.bs;
     dd[s] = L.dd;
+    bd[s] = L.bd;
     fa[nfin++] = L.fa;
     for (int f = 0; f < r->nfield; ++f) {
       ax[s * kRunFields + f] = L.adi[f].x;
@@ -1952,15 +2050,22 @@ int batch_launch(g4b_batch* b, bool timed) {
   if (int rc = check_launch(c, "beam_batch_kernel")) return rc;
   ev(1);
   {
-    DepBatchArgs a{reinterpret_cast<const DepDiagArgs*>(b->d_args + b->off_dd),
+    DepBatchArgs a{reinterpret_cast<const DepArgs*>(b->d_args + b->off_dd),
                    reinterpret_cast<const int2*>(b->d_items + b->off_dep), counts + 1};
-    LaunchScope ls(c, "batch_deposit_diag");
-    if (b->nb_kind == 1)
-      deposit_batch_kernel<1><<<b->grid[1], kDepThreads, kDepSmem, c->stream>>>(a);
-    else
-      deposit_batch_kernel<kMaxBunch><<<b->grid[1], kDepThreads, kDepSmem, c->stream>>>(a);
+    LaunchScope ls(c, "batch_deposit");
+    deposit_batch_kernel<<<b->grid[1], kDepThreads, kDepSmem, c->stream>>>(a);
   }
   if (int rc = check_launch(c, "deposit_batch_kernel")) return rc;
+  {
+    DiagBatchArgs a{reinterpret_cast<const BeamDiagArgs*>(b->d_args + b->off_bd),
+                    reinterpret_cast<const int2*>(b->d_items + b->off_dep), counts + 1};
+    LaunchScope ls(c, "batch_beam_diag");
+    if (b->nb_kind == 1)
+      beam_diag_batch_kernel<1><<<3 * c->sm_count, kDiagThreads, 0, c->stream>>>(a);
+    else
+      beam_diag_batch_kernel<kMaxBunch><<<3 * c->sm_count, kDiagThreads, 0, c->stream>>>(a);
+  }
+  if (int rc = check_launch(c, "beam_diag_batch_kernel")) return rc;
   ev(2);
   for (int pass = 0; pass < 2; ++pass) {
     for (int m = 0; m < kNumM; ++m) {
@@ -2010,10 +2115,8 @@ int g4b_batch_create(g4b_ctx* c, int max_runs, g4b_batch** out) {
   b->next.assign(max_runs, 0);
   b->last.assign(max_runs, 0);
   batch_default_grids(b);
-  cudaFuncSetAttribute(deposit_batch_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaFuncSetAttribute(deposit_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)kDepSmem);
-  cudaFuncSetAttribute(deposit_batch_kernel<kMaxBunch>,
-                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDepSmem);
   if (int rc = batch_layout(b)) {
     g4b_batch_destroy(b);
     return rc;
