@@ -13,8 +13,8 @@ quiet-start beam with shot noise, no seed field.
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 Multi-GPU (torchrun, one process per GPU): every rank runs an independent
-replica of the workload (the path is slice-local; SURVEY-level decision:
-replicas only), value = total slice-steps/s of all ranks over the max-over-ranks
+replica of the workload (the path is slice-local and has no exchange step, so
+ranks run replicas), value = total slice-steps/s of all ranks over the max-over-ranks
 device time.
 """
 from __future__ import annotations
