@@ -1303,9 +1303,11 @@ int launch_single(g4b_run* r, const StepArgs& L) {
       beam_step_kernel<0><<<r->nchunk, kRunChunk, 0, c->stream>>>(L.bs);
   }
   if (int rc = check_launch(c, "beam_step_kernel")) return rc;
-  // The beam diagnostics depend only on K1; in a captured graph they form a
-  // branch of their own beside the deposition and the ADI passes (filling
-  // the SMs those leave idle), joined before the finalize.
+  // The beam diagnostics depend only on K1; in a captured graph of a run
+  // with slices enough to fill the GPU twice they form a branch of their own
+  // beside the deposition and the ADI passes (filling the SMs those leave
+  // idle), joined before the finalize.  Smaller runs keep one chain: their
+  // kernels are short and a smaller graph instantiates faster.
   auto diag = [&](cudaStream_t st) {
     LaunchScope ls(c, "run_beam_diag");
     if (r->desc.nbunch == 1)
@@ -1314,7 +1316,8 @@ int launch_single(g4b_run* r, const StepArgs& L) {
       beam_diag_kernel<kMaxBunch><<<r->nslice * kDepParts, kDiagThreads, 0, st>>>(L.bd);
     return check_launch(c, "beam_diag_kernel");
   };
-  if (r->capturing) {
+  const bool branch = r->capturing && r->nslice >= 2 * c->sm_count;
+  if (branch) {
     G4B_CUDA_TRY(cudaEventRecord(r->ev_fork, c->stream));
     G4B_CUDA_TRY(cudaStreamWaitEvent(r->aux, r->ev_fork, 0));
     if (int rc = diag(r->aux)) return rc;
@@ -1325,11 +1328,11 @@ int launch_single(g4b_run* r, const StepArgs& L) {
     deposit_kernel<<<r->nslice, kDepThreads, kDepSmem, c->stream>>>(L.dd);
   }
   if (int rc = check_launch(c, "deposit_kernel")) return rc;
-  if (!r->capturing)
+  if (!branch)
     if (int rc = diag(c->stream)) return rc;
   for (int f = 0; f < r->nfield; ++f)
     if (int rc = adi_launch(r->fs[f].f, L.adi[f])) return rc;
-  if (r->capturing) G4B_CUDA_TRY(cudaStreamWaitEvent(c->stream, r->ev_join, 0));
+  if (branch) G4B_CUDA_TRY(cudaStreamWaitEvent(c->stream, r->ev_join, 0));
   {
     LaunchScope ls(c, "run_diag_finalize");
     diag_finalize_kernel<<<(L.nfin + 255) / 256, 256, 0, c->stream>>>(L.fa);
