@@ -59,17 +59,18 @@ __device__ __forceinline__ C cmul(C b, C c) {
   return r;
 }
 
-template <typename C>
+// shuffles within groups of L lanes (L = 32: the warp; L = 16: its halves)
+template <int L, typename C>
 __device__ __forceinline__ C shfl_up_c(C v, int d) {
-  v.x = __shfl_up_sync(0xffffffffu, v.x, d);
-  v.y = __shfl_up_sync(0xffffffffu, v.y, d);
+  v.x = __shfl_up_sync(0xffffffffu, v.x, d, L);
+  v.y = __shfl_up_sync(0xffffffffu, v.y, d, L);
   return v;
 }
 
-template <typename C>
+template <int L, typename C>
 __device__ __forceinline__ C shfl_down_c(C v, int d) {
-  v.x = __shfl_down_sync(0xffffffffu, v.x, d);
-  v.y = __shfl_down_sync(0xffffffffu, v.y, d);
+  v.x = __shfl_down_sync(0xffffffffu, v.x, d, L);
+  v.y = __shfl_down_sync(0xffffffffu, v.y, d, L);
   return v;
 }
 
@@ -79,16 +80,23 @@ template <> struct BandW<double> { static constexpr int value = 9; static conste
 template <> struct BandW<float> { static constexpr int value = 10; static constexpr int blocks = 4; };
 
 // One band of W rows (pass X) or W transposed columns (pass Y) of slice s.
-// bar is an initialised mbarrier; parity the phase this band waits on.
-template <typename T, int M, bool PX>
+// A row is solved by L lanes holding M elements each: L = 32, one row per
+// warp; L = 16, two rows per warp (one per half), for rows that fit 16 M
+// slots more closely than 32 M.  bar is an initialised mbarrier; parity the
+// phase this band waits on.
+template <typename T, int M, bool PX, int L>
 __device__ __forceinline__ void adi_band(const AdiPassArgs& a, const CUtensorMap* tm_out, int s,
                                          int band, unsigned char* smem, uint64_t* bar,
                                          uint32_t parity) {
   using C = typename CT<T>::type;
-  constexpr int W = BandW<T>::value;
+  constexpr int R = 32 / L;                     // rows per warp
+  constexpr int W = BandW<T>::value * R;        // rows per band
+  constexpr int kScan = L == 32 ? 5 : 4;        // log2 L
   const int n = a.n, ld = a.ld;
   const int r0 = band * W;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int gl = lane & (L - 1);                // lane within the row's group
+  const int row = warp * R + (lane >> 4) * (R - 1);  // row within the band
   constexpr int kTileRows = PX ? W + 2 : W;
   const bool has_src = PX && a.src != nullptr;
 
@@ -134,113 +142,113 @@ __device__ __forceinline__ void adi_band(const AdiPassArgs& a, const CUtensorMap
 
   const T r = (T)a.r;
   const C* tab = reinterpret_cast<const C*>(a.tab);
-  const C* tcb = tab;                // cbet        [M][32]
-  const C* tG = tab + M * 32;        // prefix prod [M][32]
-  const C* tH = tab + 2 * M * 32;    // suffix prod [M][32]
-  const C* tF = tab + 3 * M * 32;    // fwd scan    [5][32]
-  const C* tB = tF + 5 * 32;         // bwd scan    [5][32]
-  const C* tS = tB + 5 * 32;         // s_k = i r cbet_k (0 at the last row) [M][32]
-  const int iy = r0 + warp;
+  const C* tcb = tab;                // cbet        [M][L]
+  const C* tG = tab + M * L;         // prefix prod [M][L]
+  const C* tH = tab + 2 * M * L;     // suffix prod [M][L]
+  const C* tF = tab + 3 * M * L;     // fwd scan    [5][L]
+  const C* tB = tF + 5 * L;          // bwd scan    [5][L]
+  const C* tS = tB + 5 * L;          // s_k = i r cbet_k (0 at the last row) [M][L]
+  const int iy = r0 + row;
   const bool active = iy < n;
   const bool row_src = band_src && iy >= srow_lo && iy < srow_hi;
-  const C* srow = stile + warp * sbw - sx0;  // srow[k] for k in [sx0, sx0+sbw)
+  const C* srow = stile + row * sbw - sx0;  // srow[k] for k in [sx0, sx0+sbw)
   // bit j set: this lane's element j lies in the source tile's columns
   unsigned long long smask = 0ull;
   if (row_src) {
-    const int jlo = min(max(sx0 - lane * M, 0), M), jhi = min(max(sx0 + sbw - lane * M, 0), M);
+    const int jlo = min(max(sx0 - gl * M, 0), M), jhi = min(max(sx0 + sbw - gl * M, 0), M);
     smask = ((1ull << jhi) - 1ull) & ~((1ull << jlo) - 1ull);
   }
-  const int jn = min(max(n - lane * M, 0), M);  // elements j < jn lie in the row
+  // elements j < jn lie in the row (none for a row past the plane)
+  const int jn = active ? min(max(n - gl * M, 0), M) : 0;
   C v[M];
 
-  if (active) {
+  // a warp with any row in the plane solves both (a row past the plane is
+  // all zeros), so that every lane takes part in the group shuffles
+  if (__any_sync(0xffffffffu, active)) {
 #pragma unroll
     for (int j = 0; j < M; ++j) {
-      const int k = lane * M + j;
+      const int k = gl * M + j;
       C R = C{0, 0};
       if (j < jn) {
         if (PX) {
-          const C u = tile[(warp + 1) * ld + k];
-          const C up = tile[(warp + 2) * ld + k];
-          const C dn = tile[warp * ld + k];
+          const C u = tile[(row + 1) * ld + k];
+          const C up = tile[(row + 2) * ld + k];
+          const C dn = tile[row * ld + k];
           const T lr = fma((T)-2, u.x, up.x + dn.x);
           const T li = fma((T)-2, u.y, up.y + dn.y);
           R.x = fma(-r, li, u.x);
           R.y = fma(r, lr, u.y);
           if ((smask >> j) & 1ull) R = cadd(R, srow[k]);
         } else {
-          R = tile[warp * ld + k];
+          R = tile[row * ld + k];
         }
       }
       v[j] = R;
     }
     // forward recurrence, local part: y_k = cbet_k (R_k + i r y_{k-1})
     {
-      v[0] = cmul(__ldg(&tcb[lane]), v[0]);
+      v[0] = cmul(__ldg(&tcb[gl]), v[0]);
 #pragma unroll
       for (int j = 1; j < M; ++j) {
-        const C cb = __ldg(&tcb[j * 32 + lane]);
+        const C cb = __ldg(&tcb[j * L + gl]);
         C t;
         t.x = fma(-r, v[j - 1].y, v[j].x);
         t.y = fma(r, v[j - 1].x, v[j].y);
         v[j] = cmul(cb, t);
       }
     }
-    // forward carry scan across lanes
+    // forward carry scan across the row's lanes
     C b = v[M - 1];
 #pragma unroll
-    for (int t = 0; t < 5; ++t) {
+    for (int t = 0; t < kScan; ++t) {
       const int d = 1 << t;
-      const C o = shfl_up_c(b, d);
-      if (lane >= d) b = cfma(__ldg(&tF[t * 32 + lane]), o, b);
+      const C o = shfl_up_c<L>(b, d);
+      if (gl >= d) b = cfma(__ldg(&tF[t * L + gl]), o, b);
     }
-    C yin = shfl_up_c(b, 1);
-    if (lane == 0) yin = C{0, 0};
+    C yin = shfl_up_c<L>(b, 1);
+    if (gl == 0) yin = C{0, 0};
 #pragma unroll
-    for (int j = 0; j < M; ++j) v[j] = cfma(__ldg(&tG[j * 32 + lane]), yin, v[j]);
+    for (int j = 0; j < M; ++j) v[j] = cfma(__ldg(&tG[j * L + gl]), yin, v[j]);
     // backward recurrence, local part: u_k = y_k + s_k u_{k+1}
 #pragma unroll
-    for (int j = M - 2; j >= 0; --j) v[j] = cfma(__ldg(&tS[j * 32 + lane]), v[j + 1], v[j]);
+    for (int j = M - 2; j >= 0; --j) v[j] = cfma(__ldg(&tS[j * L + gl]), v[j + 1], v[j]);
     b = v[0];
 #pragma unroll
-    for (int t = 0; t < 5; ++t) {
+    for (int t = 0; t < kScan; ++t) {
       const int d = 1 << t;
-      const C o = shfl_down_c(b, d);
-      if (lane + d < 32) b = cfma(__ldg(&tB[t * 32 + lane]), o, b);
+      const C o = shfl_down_c<L>(b, d);
+      if (gl + d < L) b = cfma(__ldg(&tB[t * L + gl]), o, b);
     }
-    C uin = shfl_down_c(b, 1);
-    if (lane == 31) uin = C{0, 0};
+    C uin = shfl_down_c<L>(b, 1);
+    if (gl == L - 1) uin = C{0, 0};
 #pragma unroll
-    for (int j = 0; j < M; ++j) v[j] = cfma(__ldg(&tH[j * 32 + lane]), uin, v[j]);
+    for (int j = 0; j < M; ++j) v[j] = cfma(__ldg(&tH[j * L + gl]), uin, v[j]);
+
+    if (PX) {
+      // R' = u' + i r d2x(u') + S  (src/Core/FieldSolverADICUDA.cpp:279-323),
+      // in place with the original left neighbour carried along
+      C prev = shfl_up_c<L>(v[M - 1], 1);
+      if (gl == 0) prev = C{0, 0};
+      C right = shfl_down_c<L>(v[0], 1);
+      if (gl == L - 1) right = C{0, 0};
+#pragma unroll
+      for (int j = 0; j < M; ++j) {
+        const int k = gl * M + j;
+        const C cur = v[j];
+        const C upp = j < M - 1 ? v[j + 1] : right;
+        const T lr = fma((T)-2, cur.x, upp.x + prev.x);
+        const T li = fma((T)-2, cur.y, upp.y + prev.y);
+        C R;
+        R.x = fma(-r, li, cur.x);
+        R.y = fma(r, lr, cur.y);
+        if ((smask >> j) & 1ull) R = cadd(R, srow[k]);
+        v[j] = R;
+        prev = cur;
+      }
+    }
   } else {
 #pragma unroll
     for (int j = 0; j < M; ++j) v[j] = C{0, 0};
-    // keep the warp's shuffles matched with nothing: inactive warps do not
-    // take part in any warp-level exchange
-  }
-
-  if (PX && active) {
-    // R' = u' + i r d2x(u') + S  (src/Core/FieldSolverADICUDA.cpp:279-323)
-    C left = shfl_up_c(v[M - 1], 1);
-    if (lane == 0) left = C{0, 0};
-    C right = shfl_down_c(v[0], 1);
-    if (lane == 31) right = C{0, 0};
-    C w2[M];
-#pragma unroll
-    for (int j = 0; j < M; ++j) {
-      const int k = lane * M + j;
-      const C um = j > 0 ? v[j - 1] : left;
-      const C upp = j < M - 1 ? v[j + 1] : right;
-      const T lr = fma((T)-2, v[j].x, upp.x + um.x);
-      const T li = fma((T)-2, v[j].y, upp.y + um.y);
-      C R;
-      R.x = fma(-r, li, v[j].x);
-      R.y = fma(r, lr, v[j].y);
-      if ((smask >> j) & 1ull) R = cadd(R, srow[k]);
-      w2[j] = R;
-    }
-#pragma unroll
-    for (int j = 0; j < M; ++j) v[j] = w2[j];
   }
 
   if (!PX && a.zero_count > 0) {
@@ -252,9 +260,9 @@ __device__ __forceinline__ void adi_band(const AdiPassArgs& a, const CUtensorMap
   }
   if (!PX && a.diag != nullptr) {
     // field diagnostics of this band (g4_field_slice_reduce_kernel,
-    // src/Core/DiagnosticCUDA.cpp:305-363): this warp holds column
-    // ix = r0 + warp, rows iy = lane*M + j of the solved plane
-    __shared__ double dpart[BandW<T>::value][9];
+    // src/Core/DiagnosticCUDA.cpp:305-363): this lane group holds column
+    // ix = r0 + row, rows iy = gl*M + j of the solved plane
+    __shared__ double dpart[W][9];
     // each lane sums its M cells in the state precision T (exact cell
     // offsets; FP32 partials of <= 33 terms) and the lanes, warps and bands
     // are then added in FP64
@@ -266,7 +274,7 @@ __device__ __forceinline__ void adi_band(const AdiPassArgs& a, const CUtensorMap
     const int icy = ic / n, icx = ic - icy * n;
     if (active) {
       // cells past the row end hold exact zeros (their coefficients are 0)
-      const T dy0 = (T)(lane * M) + shift;  // exact: small integers and halves
+      const T dy0 = (T)(gl * M) + shift;  // exact: small integers and halves
 #pragma unroll
       for (int j = 0; j < M; ++j) {
         const T re = v[j].x, im = v[j].y;
@@ -278,7 +286,7 @@ __device__ __forceinline__ void adi_band(const AdiPassArgs& a, const CUtensorMap
         tre += re;
         tim += im;
       }
-      const int jc = iy == icx ? icy - lane * M : -1;
+      const int jc = iy == icx ? icy - gl * M : -1;
       if (jc >= 0 && jc < M) {
 #pragma unroll
         for (int j = 0; j < M; ++j)
@@ -293,26 +301,26 @@ __device__ __forceinline__ void adi_band(const AdiPassArgs& a, const CUtensorMap
     // power (x is the column); the centre cell comes from the one lane that
     // holds it
     double sp = (double)tp;
-    for (int o = 16; o > 0; o >>= 1) sp += __shfl_xor_sync(0xffffffffu, sp, o);
+    for (int o = L / 2; o > 0; o >>= 1) sp += __shfl_xor_sync(0xffffffffu, sp, o);
     T vals[4] = {ty1, ty2, tre, tim};
 #pragma unroll
     for (int q = 0; q < 4; ++q)
-      for (int o = 16; o > 0; o >>= 1) vals[q] += __shfl_xor_sync(0xffffffffu, vals[q], o);
-    if (lane == 0) {
-      dpart[warp][0] = sp;
-      dpart[warp][1] = dx * sp;
-      dpart[warp][2] = dx * dx * sp;
-      dpart[warp][3] = (double)vals[0];
-      dpart[warp][4] = (double)vals[1];
-      dpart[warp][5] = (double)vals[2];
-      dpart[warp][6] = (double)vals[3];
-      dpart[warp][7] = 0.0;
-      dpart[warp][8] = 0.0;
+      for (int o = L / 2; o > 0; o >>= 1) vals[q] += __shfl_xor_sync(0xffffffffu, vals[q], o);
+    if (gl == 0) {
+      dpart[row][0] = sp;
+      dpart[row][1] = dx * sp;
+      dpart[row][2] = dx * dx * sp;
+      dpart[row][3] = (double)vals[0];
+      dpart[row][4] = (double)vals[1];
+      dpart[row][5] = (double)vals[2];
+      dpart[row][6] = (double)vals[3];
+      dpart[row][7] = 0.0;
+      dpart[row][8] = 0.0;
     }
     __syncwarp();
     if (cre != 0.0 || cim != 0.0) {  // the lane holding the centre cell
-      dpart[warp][7] = cre;
-      dpart[warp][8] = cim;
+      dpart[row][7] = cre;
+      dpart[row][8] = cim;
     }
     __syncthreads();
     if (tid < 9) {
@@ -321,12 +329,11 @@ __device__ __forceinline__ void adi_band(const AdiPassArgs& a, const CUtensorMap
       a.diag[((size_t)s * a.nband + band) * 9 + tid] = t;
     }
   }
-  if (active) {
+  if (PX) __syncthreads();  // out overlays the input tile
 #pragma unroll
-    for (int j = 0; j < M; ++j) {
-      const int k = lane * M + j;
-      if (j < jn) out[k * W + warp] = v[j];
-    }
+  for (int j = 0; j < M; ++j) {
+    const int k = gl * M + j;
+    if (j < jn) out[k * W + row] = v[j];
   }
   ptx::fence_proxy_async();
   __syncthreads();
@@ -339,8 +346,14 @@ __device__ __forceinline__ void adi_band(const AdiPassArgs& a, const CUtensorMap
   }
 }
 
-template <typename T, int M, bool PX>
-__global__ void __launch_bounds__(BandW<T>::value * 32, (M <= 9 ? BandW<T>::blocks : 2))
+template <int M, int L> struct AdiBlocks {
+  static constexpr int value = M <= 9 ? 4 : (L == 16 && M <= 17 ? 3 : 2);
+};
+
+template <typename T, int M, bool PX, int L>
+__global__ void __launch_bounds__(BandW<T>::value * 32,
+                                  (sizeof(T) == 8 ? (M <= 9 ? BandW<T>::blocks : 2)
+                                                  : AdiBlocks<M, L>::value))
     adi_pass_kernel(const __grid_constant__ AdiPassArgs a,
                     const __grid_constant__ CUtensorMap tm_out) {
   extern __shared__ __align__(128) unsigned char smem[];
@@ -350,13 +363,13 @@ __global__ void __launch_bounds__(BandW<T>::value * 32, (M <= 9 ? BandW<T>::bloc
     ptx::fence_mbar_init();
   }
   __syncthreads();
-  adi_band<T, M, PX>(a, &tm_out, blockIdx.x / a.nband, blockIdx.x % a.nband, smem, &bar, 0u);
+  adi_band<T, M, PX, L>(a, &tm_out, blockIdx.x / a.nband, blockIdx.x % a.nband, smem, &bar, 0u);
 }
 
 // Persistent form over a work list of (run, slice, band) items of many runs
 // (one mbarrier, one phase per item; tensor maps read from global memory).
-template <typename T, int M, bool PX>
-__global__ void __launch_bounds__(BandW<T>::value * 32, (M <= 9 ? BandW<T>::blocks : 2))
+template <typename T, int M, bool PX, int L>
+__global__ void __launch_bounds__(BandW<T>::value * 32, AdiBlocks<M, L>::value)
     adi_batch_kernel(const __grid_constant__ AdiBatchArgs b) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ uint64_t bar;
@@ -371,7 +384,7 @@ __global__ void __launch_bounds__(BandW<T>::value * 32, (M <= 9 ? BandW<T>::bloc
     const int4 w = b.items[it];
     const CUtensorMap* tm = b.maps + w.x;
     if (threadIdx.x == 0) ptx::fence_tensormap_acquire(tm);
-    adi_band<T, M, PX>(b.args[w.x], tm, w.y, w.z, smem, &bar, parity);
+    adi_band<T, M, PX, L>(b.args[w.x], tm, w.y, w.z, smem, &bar, parity);
     parity ^= 1u;
     __syncthreads();
   }
@@ -562,27 +575,27 @@ __global__ void slice_scl_kernel(int nslice, const int64_t* off, const double* c
 static constexpr double kVacimp = 376.73031346177;  // upstream `vacimp`
 static constexpr double kEev = 510998.95;          // upstream `eev`
 
-template <typename T, int M, bool PX>
+template <typename T, int M, bool PX, int L>
 static int configure_pass_t(int device) {
   static std::atomic<uint64_t> configured{0};  // per instantiation, one bit per device
   if (device < 64 && (configured.load() >> device) & 1) return G4B_OK;
   // static + dynamic shared memory must fit the 227 KB a CTA may use
   cudaFuncAttributes fa;
-  cudaError_t e = cudaFuncGetAttributes(&fa, adi_pass_kernel<T, M, PX>);
+  cudaError_t e = cudaFuncGetAttributes(&fa, adi_pass_kernel<T, M, PX, L>);
   if (e != cudaSuccess) return cuda_fail(e, "cudaFuncGetAttributes(adi_pass)");
-  e = cudaFuncSetAttribute(adi_pass_kernel<T, M, PX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  e = cudaFuncSetAttribute(adi_pass_kernel<T, M, PX, L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            227 * 1024 - (int)fa.sharedSizeBytes);
   if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(adi_pass)");
   if (device < 64) configured.fetch_or(1ull << device);
   return G4B_OK;
 }
 
-template <typename T, int M, bool PX>
+template <typename T, int M, bool PX, int L>
 static int launch_pass_t(g4b_field* f, const AdiPassArgs& args, const CUtensorMap& tm,
                          size_t smem) {
-  constexpr int W = BandW<T>::value;
-  auto kern = adi_pass_kernel<T, M, PX>;
-  if (int rc = configure_pass_t<T, M, PX>(f->ctx->device)) return rc;
+  constexpr int W = BandW<T>::value;  // warps per CTA
+  auto kern = adi_pass_kernel<T, M, PX, L>;
+  if (int rc = configure_pass_t<T, M, PX, L>(f->ctx->device)) return rc;
   const unsigned grid = (unsigned)(f->nslice * args.nband);
   {
     LaunchScope ls(f->ctx, PX ? "adi_pass_x" : "adi_pass_y");
@@ -591,27 +604,28 @@ static int launch_pass_t(g4b_field* f, const AdiPassArgs& args, const CUtensorMa
   return check_launch(f->ctx, "adi_pass_kernel");
 }
 
+// Kernel modes: M (odd elements per lane) with 32-lane rows, 100 + M with
+// 16-lane rows (FP32 only).
+#define G4B_MODES32(X) X(1, 32) X(3, 32) X(5, 32) X(7, 32) X(9, 32) X(11, 32) X(13, 32) \
+  X(15, 32) X(17, 32) X(21, 32) X(25, 32) X(33, 32)
+#define G4B_MODES16(X) X(5, 16) X(7, 16) X(9, 16) X(11, 16) X(13, 16) X(15, 16) X(17, 16) \
+  X(21, 16) X(25, 16) X(33, 16)
+
 template <typename T, bool PX>
-static int configure_pass_m(int M, int device) {
-  switch (M) {
-    case 1: return configure_pass_t<T, 1, PX>(device);
-    case 3: return configure_pass_t<T, 3, PX>(device);
-    case 5: return configure_pass_t<T, 5, PX>(device);
-    case 7: return configure_pass_t<T, 7, PX>(device);
-    case 9: return configure_pass_t<T, 9, PX>(device);
-    case 11: return configure_pass_t<T, 11, PX>(device);
-    case 13: return configure_pass_t<T, 13, PX>(device);
-    case 15: return configure_pass_t<T, 15, PX>(device);
-    case 17: return configure_pass_t<T, 17, PX>(device);
-    case 21: return configure_pass_t<T, 21, PX>(device);
-    case 25: return configure_pass_t<T, 25, PX>(device);
-    case 33: return configure_pass_t<T, 33, PX>(device);
+static int configure_pass_m(int mode, int device) {
+#define G4B_CFG(m, l) \
+  case (l == 16 ? 100 : 0) + m: return configure_pass_t<T, m, PX, l>(device);
+  if constexpr (sizeof(T) == 8) {
+    switch (mode) { G4B_MODES32(G4B_CFG) }
+  } else {
+    switch (mode) { G4B_MODES32(G4B_CFG) G4B_MODES16(G4B_CFG) }
   }
+#undef G4B_CFG
   return fail(G4B_ERR_RANGE, "adi: unsupported elements per lane");
 }
 
 int adi_configure(g4b_field* f) {
-  const int M = pick_M(f->ngrid);
+  const int M = f->mode;
   const int d = f->ctx->device;
   if (f->precision == G4B_FP64) {
     if (int rc = configure_pass_m<double, true>(M, d)) return rc;
@@ -622,22 +636,16 @@ int adi_configure(g4b_field* f) {
 }
 
 template <typename T, bool PX>
-static int launch_pass_m(int M, g4b_field* f, const AdiPassArgs& args,
+static int launch_pass_m(int mode, g4b_field* f, const AdiPassArgs& args,
                          const CUtensorMap& tm, size_t smem) {
-  switch (M) {
-    case 1: return launch_pass_t<T, 1, PX>(f, args, tm, smem);
-    case 3: return launch_pass_t<T, 3, PX>(f, args, tm, smem);
-    case 5: return launch_pass_t<T, 5, PX>(f, args, tm, smem);
-    case 7: return launch_pass_t<T, 7, PX>(f, args, tm, smem);
-    case 9: return launch_pass_t<T, 9, PX>(f, args, tm, smem);
-    case 11: return launch_pass_t<T, 11, PX>(f, args, tm, smem);
-    case 13: return launch_pass_t<T, 13, PX>(f, args, tm, smem);
-    case 15: return launch_pass_t<T, 15, PX>(f, args, tm, smem);
-    case 17: return launch_pass_t<T, 17, PX>(f, args, tm, smem);
-    case 21: return launch_pass_t<T, 21, PX>(f, args, tm, smem);
-    case 25: return launch_pass_t<T, 25, PX>(f, args, tm, smem);
-    case 33: return launch_pass_t<T, 33, PX>(f, args, tm, smem);
+#define G4B_LAUNCH(m, l) \
+  case (l == 16 ? 100 : 0) + m: return launch_pass_t<T, m, PX, l>(f, args, tm, smem);
+  if constexpr (sizeof(T) == 8) {
+    switch (mode) { G4B_MODES32(G4B_LAUNCH) }
+  } else {
+    switch (mode) { G4B_MODES32(G4B_LAUNCH) G4B_MODES16(G4B_LAUNCH) }
   }
+#undef G4B_LAUNCH
   return fail(G4B_ERR_RANGE, "adi: unsupported elements per lane");
 }
 
@@ -658,11 +666,19 @@ int adi_plan(g4b_adi* adi, g4b_field* f, const void* src, const int4* desc,
   auto smem_for = [&](bool px, bool with_src) {
     size_t tile = (size_t)((px ? W + 2 : W) * ld) * cb;
     if (px && with_src) tile += (size_t)W * ld * cb;
+    // pass X: the output staging tile reuses the input tile's memory
+    // (written after a barrier that ends every read of the input), which
+    // keeps three CTAs of 16-lane rows on an SM; pass Y: after the input
+    if (px) {
+      args.out_off = 0;
+      return std::max(tile, out_bytes);
+    }
     const size_t out_off = (tile + 127) / 128 * 128;
     args.out_off = (int)out_off;
     return out_off + out_bytes;
   };
-  P.M = adi->M;
+  P.M = f->precision == G4B_FP64 ? adi->M : adi->mode32;
+  if (P.M != f->mode) return fail(G4B_ERR_STATE, "adi: solver and field row layouts differ");
   P.precision = f->precision;
   P.grid = (unsigned)(f->nslice * args.nband);
   P.tm_x = &f->tm_store_b;
@@ -708,10 +724,10 @@ int adi_run(g4b_adi* adi, g4b_field* f, const void* src, const int4* desc,
   return adi_launch(f, P);
 }
 
-template <int M, bool PX>
+template <int M, bool PX, int L>
 static int batch_launch_t(g4b_ctx* c, const AdiBatchArgs& b, size_t smem, int grid) {
   static std::atomic<uint64_t> configured{0};
-  auto kern = adi_batch_kernel<float, M, PX>;
+  auto kern = adi_batch_kernel<float, M, PX, L>;
   if (c->device >= 64 || !((configured.load() >> c->device) & 1)) {
     cudaFuncAttributes fa;
     cudaError_t e = cudaFuncGetAttributes(&fa, kern);
@@ -728,25 +744,13 @@ static int batch_launch_t(g4b_ctx* c, const AdiBatchArgs& b, size_t smem, int gr
   return check_launch(c, "adi_batch_kernel");
 }
 
-int adi_batch_launch(g4b_ctx* c, int M, bool px, const AdiBatchArgs& b, size_t smem, int grid) {
-#define G4B_BATCH_CASE(m)                                                      \
-  case m:                                                                      \
-    return px ? batch_launch_t<m, true>(c, b, smem, grid)                      \
-              : batch_launch_t<m, false>(c, b, smem, grid);
-  switch (M) {
-    G4B_BATCH_CASE(1)
-    G4B_BATCH_CASE(3)
-    G4B_BATCH_CASE(5)
-    G4B_BATCH_CASE(7)
-    G4B_BATCH_CASE(9)
-    G4B_BATCH_CASE(11)
-    G4B_BATCH_CASE(13)
-    G4B_BATCH_CASE(15)
-    G4B_BATCH_CASE(17)
-    G4B_BATCH_CASE(21)
-    G4B_BATCH_CASE(25)
-    G4B_BATCH_CASE(33)
-  }
+int adi_batch_launch(g4b_ctx* c, int mode, bool px, const AdiBatchArgs& b, size_t smem,
+                     int grid) {
+#define G4B_BATCH_CASE(m, l)                                                   \
+  case (l == 16 ? 100 : 0) + m:                                                \
+    return px ? batch_launch_t<m, true, l>(c, b, smem, grid)                   \
+              : batch_launch_t<m, false, l>(c, b, smem, grid);
+  switch (mode) { G4B_MODES32(G4B_BATCH_CASE) G4B_MODES16(G4B_BATCH_CASE) }
 #undef G4B_BATCH_CASE
   return fail(G4B_ERR_RANGE, "adi: unsupported elements per lane");
 }
@@ -812,56 +816,66 @@ int g4b_adi_init(g4b_adi* a, double delz, double dgrid, double xks, int ngrid) {
     cwet[i] = cd(0.0, -mupp[i - 1]) * cbet[i - 1];
     cbet[i] = cd(1.0, 0.0) / (cd(1.0, -mmid[i]) - c[i] * cwet[i]);
   }
-  // recurrence coefficients on the padded index range [0, 32M)
-  const int P = 32 * M;
-  std::vector<cd> cb(P, 0.0), q(P, 0.0), sv(P, 0.0), G(P), H(P);
-  for (int k = 0; k < n; ++k) cb[k] = cbet[k];
-  for (int k = 1; k < n; ++k) q[k] = -c[k] * cbet[k];         // y_k += q_k y_{k-1}
-  for (int k = 0; k + 1 < n; ++k) sv[k] = -cwet[k + 1];       // u_k += s_k u_{k+1}
-  std::vector<cd> A(32), B(32);
-  for (int L = 0; L < 32; ++L) {
-    const int k0 = L * M, k1 = k0 + M - 1;
-    cd g = 1.0;
-    for (int k = k0; k <= k1; ++k) {
-      g *= q[k];
-      G[k] = g;
+  // Tables of one row layout: L lanes of M elements, recurrence
+  // coefficients on the padded index range [0, L M).
+  auto tables = [&](const int M, const int L) {
+    const int P = L * M;
+    std::vector<cd> cb(P, 0.0), q(P, 0.0), sv(P, 0.0), G(P), H(P);
+    for (int k = 0; k < n; ++k) cb[k] = cbet[k];
+    for (int k = 1; k < n; ++k) q[k] = -c[k] * cbet[k];         // y_k += q_k y_{k-1}
+    for (int k = 0; k + 1 < n; ++k) sv[k] = -cwet[k + 1];       // u_k += s_k u_{k+1}
+    std::vector<cd> A(L), B(L);
+    for (int lane = 0; lane < L; ++lane) {
+      const int k0 = lane * M, k1 = k0 + M - 1;
+      cd g = 1.0;
+      for (int k = k0; k <= k1; ++k) {
+        g *= q[k];
+        G[k] = g;
+      }
+      cd h = 1.0;
+      for (int k = k1; k >= k0; --k) {
+        h *= sv[k];
+        H[k] = h;
+      }
+      A[lane] = G[k1];
+      B[lane] = H[k0];
     }
-    cd h = 1.0;
-    for (int k = k1; k >= k0; --k) {
-      h *= sv[k];
-      H[k] = h;
+    std::vector<cd> t(tab_total(M, L), 0.0);
+    for (int j = 0; j < M; ++j)
+      for (int lane = 0; lane < L; ++lane) {
+        const int k = lane * M + j;
+        t[tab_cbet(M, L) + j * L + lane] = cb[k];
+        t[tab_G(M, L) + j * L + lane] = G[k];
+        t[tab_H(M, L) + j * L + lane] = H[k];
+        t[tab_S(M, L) + j * L + lane] = sv[k];
+      }
+    std::vector<cd> af = A, ab = B;
+    for (int st = 0; (1 << st) < L; ++st) {
+      const int d = 1 << st;
+      for (int lane = 0; lane < L; ++lane) {
+        t[tab_scanF(M, L) + st * L + lane] = af[lane];
+        t[tab_scanB(M, L) + st * L + lane] = ab[lane];
+      }
+      std::vector<cd> nf = af, nb = ab;
+      for (int lane = 0; lane < L; ++lane) {
+        if (lane >= d) nf[lane] = af[lane] * af[lane - d];
+        if (lane + d < L) nb[lane] = ab[lane] * ab[lane + d];
+      }
+      af.swap(nf);
+      ab.swap(nb);
     }
-    A[L] = G[k1];
-    B[L] = H[k0];
-  }
-  const size_t tot = tab_total(M);
-  std::vector<double2> t64(tot);
-  auto put = [&](size_t i, cd v) { t64[i] = make_double2(v.real(), v.imag()); };
-  for (int j = 0; j < M; ++j)
-    for (int L = 0; L < 32; ++L) {
-      const int k = L * M + j;
-      put(tab_cbet(M) + j * 32 + L, cb[k]);
-      put(tab_G(M) + j * 32 + L, G[k]);
-      put(tab_H(M) + j * 32 + L, H[k]);
-      put(tab_S(M) + j * 32 + L, sv[k]);
-    }
-  std::vector<cd> af = A, ab = B;
-  for (int t = 0; t < 5; ++t) {
-    const int d = 1 << t;
-    for (int L = 0; L < 32; ++L) {
-      put(tab_scanF(M) + t * 32 + L, af[L]);
-      put(tab_scanB(M) + t * 32 + L, ab[L]);
-    }
-    std::vector<cd> nf = af, nb = ab;
-    for (int L = 0; L < 32; ++L) {
-      if (L >= d) nf[L] = af[L] * af[L - d];
-      if (L + d < 32) nb[L] = ab[L] * ab[L + d];
-    }
-    af.swap(nf);
-    ab.swap(nb);
-  }
-  std::vector<float2> t32(tot);
-  for (size_t i = 0; i < tot; ++i) t32[i] = make_float2((float)t64[i].x, (float)t64[i].y);
+    return t;
+  };
+  // FP64 fields solve rows with 32 lanes; FP32 fields with the layout of
+  // their mode (16-lane rows where those fit the row more closely)
+  const int mode32 = pick_mode(n, G4B_MIXED);
+  const std::vector<cd> c64 = tables(M, 32);
+  const std::vector<cd> c32 = tables(mode_M(mode32), mode_L(mode32));
+  std::vector<double2> t64(c64.size());
+  for (size_t k = 0; k < c64.size(); ++k) t64[k] = make_double2(c64[k].real(), c64[k].imag());
+  std::vector<float2> t32(c32.size());
+  for (size_t k = 0; k < c32.size(); ++k)
+    t32[k] = make_float2((float)c32[k].real(), (float)c32[k].imag());
   g4b_ctx* ctx = a->ctx;
   G4B_CUDA_TRY(cudaSetDevice(ctx->device));
   if (a->d_tab64) {
@@ -871,11 +885,11 @@ int g4b_adi_init(g4b_adi* a, double delz, double dgrid, double xks, int ngrid) {
     a->d_tab64 = nullptr;
     a->d_tab32 = nullptr;
   }
-  G4B_CUDA_TRY(dev_alloc(a->ctx, (void**)&a->d_tab64, tot * sizeof(double2)));
-  G4B_CUDA_TRY(dev_alloc(a->ctx, (void**)&a->d_tab32, tot * sizeof(float2)));
-  G4B_CUDA_TRY(cudaMemcpyAsync(a->d_tab64, t64.data(), tot * sizeof(double2),
+  G4B_CUDA_TRY(dev_alloc(a->ctx, (void**)&a->d_tab64, t64.size() * sizeof(double2)));
+  G4B_CUDA_TRY(dev_alloc(a->ctx, (void**)&a->d_tab32, t32.size() * sizeof(float2)));
+  G4B_CUDA_TRY(cudaMemcpyAsync(a->d_tab64, t64.data(), t64.size() * sizeof(double2),
                                cudaMemcpyHostToDevice, ctx->stream));
-  G4B_CUDA_TRY(cudaMemcpyAsync(a->d_tab32, t32.data(), tot * sizeof(float2),
+  G4B_CUDA_TRY(cudaMemcpyAsync(a->d_tab32, t32.data(), t32.size() * sizeof(float2),
                                cudaMemcpyHostToDevice, ctx->stream));
   G4B_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
   a->ngrid = ngrid;
@@ -884,6 +898,7 @@ int g4b_adi_init(g4b_adi* a, double delz, double dgrid, double xks, int ngrid) {
   a->xks = xks;
   a->r = r;
   a->M = M;
+  a->mode32 = mode32;
   a->ready = true;
   return G4B_OK;
 }

@@ -153,6 +153,15 @@ int pick_M(int n) {
   return 0;
 }
 
+int pick_mode(int n, int precision) {
+  const int m32 = pick_M(n);
+  if (precision == G4B_FP64 || m32 == 0) return m32;
+  static const int kM16[] = {5, 7, 9, 11, 13, 15, 17, 21, 25, 33};
+  for (int m : kM16)
+    if (16 * m >= n) return 16 * m < 32 * m32 ? 100 + m : m32;
+  return m32;
+}
+
 static int encode_store_map(g4b_ctx* ctx, CUtensorMap* map, void* base, int n,
                             int ld, int nslice, size_t cell_bytes, int band,
                             int box_rows) {
@@ -394,7 +403,8 @@ int g4b_field_create(g4b_ctx* c, int nslice, int ngrid, double gridmax,
   f->xks = 4.0 * std::asin(1.0) / xlambda;          // Field::init, Field.cpp:78
   f->cell_bytes = precision == G4B_FP64 ? 16 : 8;
   f->ld = precision == G4B_FP64 ? ngrid : ngrid + (ngrid & 1);
-  f->band_rows = precision == G4B_FP64 ? 9 : 10;
+  f->mode = pick_mode(ngrid, precision);
+  f->band_rows = precision == G4B_FP64 ? 9 : (mode_L(f->mode) == 16 ? 20 : 10);
   // TMA store boxes of <= 256 rows; a multiple of 8 rows keeps every box's
   // shared-memory source 128-byte aligned (W * cell * 8 is a multiple of 128).
   f->store_nbox = (ngrid + 255) / 256;

@@ -91,7 +91,8 @@ struct g4b_field {
   CUtensorMap tm_store_a;   // pass Y writes a
   int store_box_rows = 0;   // rows per TMA store box
   int store_nbox = 0;       // boxes per band
-  int band_rows = 0;        // W: rows (warps) per CTA
+  int band_rows = 0;        // W: rows per CTA (one or two per warp)
+  int mode = 0;             // ADI row layout (pick_mode)
   uint64_t bytes = 0;
 };
 
@@ -119,7 +120,8 @@ struct g4b_adi {
   g4b_ctx* ctx = nullptr;
   int ngrid = 0;
   double delz = 0, dgrid = 0, xks = 0, r = 0;
-  int M = 0;                 // elements per lane (odd)
+  int M = 0;                 // elements per lane (odd), 32-lane rows (FP64 fields)
+  int mode32 = 0;            // row layout of FP32 fields (pick_mode)
   // Tables in lane-minor order, complex (double2) and their FP32 copies.
   double2* d_tab64 = nullptr;   // [3][M][32]: cbet, G, H ; then [2][5][32] scans
   float2* d_tab32 = nullptr;
@@ -167,7 +169,7 @@ struct AdiPassArgs {
   size_t src_cap;      // cells reserved per slice in `src`
   const void* tab;     // lane-minor tables of this precision
   int n, ld, nband;
-  int out_off;         // byte offset of the output staging tile
+  int out_off;         // byte offset of the output staging tile (pass X: 0, over the input)
   int box_rows, nbox;  // TMA store boxes per band
   double r;
   int* err;
@@ -216,16 +218,24 @@ int adi_batch_launch(g4b_ctx* c, int M, bool px, const AdiBatchArgs& b, size_t s
 // before any stream capture).
 int adi_configure(g4b_field* f);
 
-// Lane-minor table offsets (in complex elements).
-inline size_t tab_cbet(int M) { (void)M; return 0; }
-inline size_t tab_G(int M) { return (size_t)M * 32; }
-inline size_t tab_H(int M) { return (size_t)2 * M * 32; }
-inline size_t tab_scanF(int M) { return (size_t)3 * M * 32; }
-inline size_t tab_scanB(int M) { return (size_t)3 * M * 32 + 5 * 32; }
-inline size_t tab_S(int M) { return (size_t)3 * M * 32 + 10 * 32; }
-inline size_t tab_total(int M) { return (size_t)4 * M * 32 + 10 * 32; }
+// Lane-minor table offsets (in complex elements) for rows of L lanes with M
+// elements each.
+inline size_t tab_cbet(int M, int L) { (void)M; (void)L; return 0; }
+inline size_t tab_G(int M, int L) { return (size_t)M * L; }
+inline size_t tab_H(int M, int L) { return (size_t)2 * M * L; }
+inline size_t tab_scanF(int M, int L) { return (size_t)3 * M * L; }
+inline size_t tab_scanB(int M, int L) { return (size_t)3 * M * L + 5 * L; }
+inline size_t tab_S(int M, int L) { return (size_t)3 * M * L + 10 * L; }
+inline size_t tab_total(int M, int L) { return (size_t)4 * M * L + 10 * L; }
 
+// Elements per lane for 32-lane rows (0 if n > 1056).
 int pick_M(int n);
+// Row layout ("mode") of the ADI kernels for a grid of n: M for 32-lane rows,
+// 100 + M for 16-lane rows (FP32 fields whose rows fit 16 M slots more
+// closely than 32 M).
+int pick_mode(int n, int precision);
+inline int mode_M(int mode) { return mode % 100; }
+inline int mode_L(int mode) { return mode >= 100 ? 16 : 32; }
 
 }  // namespace g4b
 

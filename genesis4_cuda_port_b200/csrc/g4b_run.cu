@@ -1803,8 +1803,10 @@ int g4b_run_device_bytes(g4b_run* r, uint64_t* bytes) {
 
 namespace {
 
-constexpr int kNumM = 12;
-const int kMList[kNumM] = {1, 3, 5, 7, 9, 11, 13, 15, 17, 21, 25, 33};
+// ADI kernel modes (pick_mode): 32-lane rows, then 16-lane rows
+constexpr int kNumM = 22;
+const int kMList[kNumM] = {1,   3,   5,   7,   9,   11,  13,  15,  17,  21,  25,
+                           33,  105, 107, 109, 111, 113, 115, 117, 121, 125, 133};
 int m_index(int M) {
   for (int i = 0; i < kNumM; ++i)
     if (kMList[i] == M) return i;
@@ -1923,7 +1925,7 @@ int batch_rebuild(g4b_batch* b) {
     for (int sl = 0; sl < r->nslice; ++sl) b->dep_items.push_back(make_int2(s, sl));
     for (int f = 0; f < r->nfield; ++f) {
       g4b_field* F = r->fs[f].f;
-      const int mi = m_index(r->fs[f].adis.empty() ? pick_M(F->ngrid) : r->fs[f].adis[0]->M);
+      const int mi = m_index(F->mode);
       if (mi < 0) return fail(G4B_ERR_RANGE, "g4b_batch: unsupported grid");
       const int nband = (F->ngrid + F->band_rows - 1) / F->band_rows;
       for (int sl = 0; sl < r->nslice; ++sl)
@@ -1934,7 +1936,8 @@ int batch_rebuild(g4b_batch* b) {
       const size_t cb = F->cell_bytes;
       const size_t out_bytes = (size_t)F->store_nbox * F->store_box_rows * W * cb;
       const size_t tx = (size_t)((W + 2) * ld + W * ld) * cb, ty = (size_t)(W * ld) * cb;
-      b->smem_x[mi] = std::max(b->smem_x[mi], (tx + 127) / 128 * 128 + out_bytes);
+      // pass X: the output staging tile overlays the input tile
+      b->smem_x[mi] = std::max(b->smem_x[mi], std::max(tx, out_bytes));
       b->smem_y[mi] = std::max(b->smem_y[mi], (ty + 127) / 128 * 128 + out_bytes);
     }
   }
