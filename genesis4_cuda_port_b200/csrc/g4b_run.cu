@@ -703,8 +703,7 @@ __device__ __forceinline__ void deposit_slice(const DepArgs& a, const int bs, un
       // with `count` the counts per base cell (ext row iy - ylo + 1) and the
       // largest charge weight (qloc), with `add` the contributions at scale
       // Sf of charge weights capped at qc; a quad of lanes holding one
-      // quiet-start beamlet in one cell adds its count with one atomic and its
-      // contributions as integers summed in registers (exact)
+      // quiet-start beamlet in one cell adds its count with one atomic
       float qloc = 0.f;
       auto pass = [&](const bool count, const bool add, const float Sf, const float qc) {
         for (int pb = tid & ~31; pb < np; pb += kDepAccU * kDepThreads) {
@@ -761,17 +760,9 @@ __device__ __forceinline__ void deposit_slice(const DepArgs& a, const int bs, un
             const int c2 = __shfl_xor_sync(0xffffffffu, cidx, 2);
             const int c3 = __shfl_xor_sync(0xffffffffu, cidx, 3);
             const bool quad = cidx >= 0 && c1 == cidx && c2 == cidx && c3 == cidx;
-            if (add && __any_sync(0xffffffffu, quad)) {
-#pragma unroll
-              for (int k = 0; k < 8; ++k) {
-                int t = c[k];
-                t += __shfl_xor_sync(0xffffffffu, t, 1);
-                t += __shfl_xor_sync(0xffffffffu, t, 2);
-                if (quad) c[k] = t;
-              }
-            }
-            if (cidx >= 0 && (!quad || (l & 3) == 0)) {
+            if (cidx >= 0 && (!quad || (l & 3) == 0))
               if (count) atomicAdd(&hist[cidx], quad ? 4 : 1);
+            if (cidx >= 0) {
               if (add) {
                 if (ey >= 0) {
                   const int o = ey * bw + ex;
