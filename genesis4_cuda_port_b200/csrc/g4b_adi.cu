@@ -75,9 +75,19 @@ __device__ __forceinline__ C shfl_down_c(C v, int d) {
 }
 
 
-template <typename T> struct BandW;
-template <> struct BandW<double> { static constexpr int value = 9; static constexpr int blocks = 2; };
-template <> struct BandW<float> { static constexpr int value = 10; static constexpr int blocks = 4; };
+// Warps per CTA and CTAs per SM (launch bounds) of the ADI kernels: FP64 9
+// warps of 32-lane rows; FP32 10 warps of 32-lane rows or 5 warps of two
+// 16-lane rows each (10 rows per band either way; smaller CTAs of 16-lane
+// rows keep six on an SM so that one CTA's loads and stores overlap the
+// others' solves).
+template <typename T, int L> struct BandW {
+  static constexpr int value = sizeof(T) == 8 ? 9 : (L == 16 ? 5 : 10);
+};
+template <typename T, int M, int L> struct AdiBlocks {
+  static constexpr int value =
+      sizeof(T) == 8 ? (M <= 9 ? 2 : 2)
+                     : (L == 16 ? (M <= 9 ? 8 : (M <= 17 ? 6 : 4)) : (M <= 9 ? 4 : 2));
+};
 
 // One band of W rows (pass X) or W transposed columns (pass Y) of slice s.
 // A row is solved by L lanes holding M elements each: L = 32, one row per
@@ -90,7 +100,7 @@ __device__ __forceinline__ void adi_band(const AdiPassArgs& a, const CUtensorMap
                                          uint32_t parity) {
   using C = typename CT<T>::type;
   constexpr int R = 32 / L;                     // rows per warp
-  constexpr int W = BandW<T>::value * R;        // rows per band
+  constexpr int W = BandW<T, L>::value * R;     // rows per band
   constexpr int kScan = L == 32 ? 5 : 4;        // log2 L
   const int n = a.n, ld = a.ld;
   const int r0 = band * W;
@@ -346,14 +356,8 @@ __device__ __forceinline__ void adi_band(const AdiPassArgs& a, const CUtensorMap
   }
 }
 
-template <int M, int L> struct AdiBlocks {
-  static constexpr int value = M <= 9 ? 4 : (L == 16 && M <= 17 ? 3 : 2);
-};
-
 template <typename T, int M, bool PX, int L>
-__global__ void __launch_bounds__(BandW<T>::value * 32,
-                                  (sizeof(T) == 8 ? (M <= 9 ? BandW<T>::blocks : 2)
-                                                  : AdiBlocks<M, L>::value))
+__global__ void __launch_bounds__(BandW<T, L>::value * 32, AdiBlocks<T, M, L>::value)
     adi_pass_kernel(const __grid_constant__ AdiPassArgs a,
                     const __grid_constant__ CUtensorMap tm_out) {
   extern __shared__ __align__(128) unsigned char smem[];
@@ -369,7 +373,7 @@ __global__ void __launch_bounds__(BandW<T>::value * 32,
 // Persistent form over a work list of (run, slice, band) items of many runs
 // (one mbarrier, one phase per item; tensor maps read from global memory).
 template <typename T, int M, bool PX, int L>
-__global__ void __launch_bounds__(BandW<T>::value * 32, AdiBlocks<M, L>::value)
+__global__ void __launch_bounds__(BandW<T, L>::value * 32, AdiBlocks<T, M, L>::value)
     adi_batch_kernel(const __grid_constant__ AdiBatchArgs b) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ uint64_t bar;
@@ -593,7 +597,7 @@ static int configure_pass_t(int device) {
 template <typename T, int M, bool PX, int L>
 static int launch_pass_t(g4b_field* f, const AdiPassArgs& args, const CUtensorMap& tm,
                          size_t smem) {
-  constexpr int W = BandW<T>::value;  // warps per CTA
+  constexpr int W = BandW<T, L>::value;  // warps per CTA
   auto kern = adi_pass_kernel<T, M, PX, L>;
   if (int rc = configure_pass_t<T, M, PX, L>(f->ctx->device)) return rc;
   const unsigned grid = (unsigned)(f->nslice * args.nband);
@@ -739,7 +743,7 @@ static int batch_launch_t(g4b_ctx* c, const AdiBatchArgs& b, size_t smem, int gr
   }
   {
     LaunchScope ls(c, PX ? "batch_adi_x" : "batch_adi_y");
-    kern<<<grid, BandW<float>::value * 32, smem, c->stream>>>(b);
+    kern<<<grid, BandW<float, L>::value * 32, smem, c->stream>>>(b);
   }
   return check_launch(c, "adi_batch_kernel");
 }

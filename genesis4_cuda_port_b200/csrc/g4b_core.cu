@@ -404,7 +404,7 @@ int g4b_field_create(g4b_ctx* c, int nslice, int ngrid, double gridmax,
   f->cell_bytes = precision == G4B_FP64 ? 16 : 8;
   f->ld = precision == G4B_FP64 ? ngrid : ngrid + (ngrid & 1);
   f->mode = pick_mode(ngrid, precision);
-  f->band_rows = precision == G4B_FP64 ? 9 : (mode_L(f->mode) == 16 ? 20 : 10);
+  f->band_rows = precision == G4B_FP64 ? 9 : 10;  // rows per ADI band (both row layouts)
   // TMA store boxes of <= 256 rows; a multiple of 8 rows keeps every box's
   // shared-memory source 128-byte aligned (W * cell * 8 is a multiple of 128).
   f->store_nbox = (ngrid + 255) / 256;
