@@ -432,7 +432,9 @@ constexpr int kDepParts = 1;          // beam-diagnostic records per slice
 constexpr int kDiagThreads = 256;
 constexpr int kDepDiagU = 8;          // particles in flight per thread
 
-template <int NB>
+// U: particles in flight per thread (each thread adds its particles in the
+// same order for every U, so the sums do not depend on it)
+template <int NB, int U = kDepDiagU>
 __device__ __forceinline__ void diag_slice(const BeamDiagArgs& a, const int bs, const int part) {
   __shared__ double dpart[kDiagThreads / 32][kBeamRec + 2 * kMaxBunch];
   const int tid = threadIdx.x, w = tid >> 5, l = tid & 31;
@@ -455,12 +457,12 @@ __device__ __forceinline__ void diag_slice(const BeamDiagArgs& a, const int bs, 
   double bre[NB], bim[NB];
 #pragma unroll
   for (int h = 0; h < NB; ++h) bre[h] = bim[h] = 0.0;
-  for (int pb = tid; pb < np; pb += kDepDiagU * kDiagThreads) {
-    float2 lxy[kDepDiagU], lpp[kDepDiagU];
-    float ldg[kDepDiagU];
-    double lth[kDepDiagU];
+  for (int pb = tid; pb < np; pb += U * kDiagThreads) {
+    float2 lxy[U], lpp[U];
+    float ldg[U];
+    double lth[U];
 #pragma unroll
-    for (int u = 0; u < kDepDiagU; ++u) {
+    for (int u = 0; u < U; ++u) {
       const int p = pb + u * kDiagThreads;
       if (p < np) {
         lxy[u] = xyp[p];
@@ -470,7 +472,7 @@ __device__ __forceinline__ void diag_slice(const BeamDiagArgs& a, const int bs, 
       }
     }
 #pragma unroll
-    for (int u = 0; u < kDepDiagU; ++u) {
+    for (int u = 0; u < U; ++u) {
       if (pb + u * kDiagThreads >= np) break;
       const double x = lxy[u].x, y = lxy[u].y, px = lpp[u].x, py = lpp[u].y;
       const double d = ldg[u];
@@ -569,24 +571,6 @@ template <int NB>
 __global__ void __launch_bounds__(kDiagThreads, 2)
     beam_diag_kernel(const __grid_constant__ BeamDiagArgs a) {
   diag_slice<NB>(a, blockIdx.x / kDepParts, blockIdx.x % kDepParts);
-}
-
-// Batched form: items[i] = (run, slice of that run).
-struct DiagBatchArgs {
-  const BeamDiagArgs* args;
-  const int2* items;
-  const int* nitems;
-};
-
-template <int NB>
-__global__ void __launch_bounds__(kDiagThreads, 2)
-    beam_diag_batch_kernel(const __grid_constant__ DiagBatchArgs b) {
-  const int nitems = *b.nitems * kDepParts;
-  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
-    const int2 w = b.items[it / kDepParts];
-    diag_slice<NB>(b.args[w.x], w.y, it % kDepParts);
-    __syncthreads();
-  }
 }
 
 // Deposition (adi_deposit_source_atomic, FieldSolverADICUDA.cpp:98-174),
@@ -865,7 +849,25 @@ __global__ void __launch_bounds__(kDepThreads, 2) deposit_kernel(const __grid_co
   deposit_slice(a, blockIdx.x, smem);
 }
 
-// Batched form: items[i] = (run, slice of that run).
+// The beam diagnostics and the deposition of a slice by one CTA, one after
+// the other: the form for runs too small to fill the GPU with the
+// diagnostics on a branch of their own (the same device functions, so the
+// same results).
+struct DepDiagLaunch {
+  DepArgs d;
+  BeamDiagArgs b;
+};
+
+template <int NB>
+__global__ void __launch_bounds__(kDepThreads, 2)
+    deposit_diag_kernel(const __grid_constant__ DepDiagLaunch a) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  diag_slice<NB>(a.b, blockIdx.x, 0);
+  __syncthreads();
+  deposit_slice(a.d, blockIdx.x, smem);
+}
+
+// Batched forms: items[i] = (run, slice of that run).
 struct DepBatchArgs {
   const DepArgs* args;
   const int2* items;
@@ -883,10 +885,21 @@ __global__ void __launch_bounds__(kDepThreads, 2)
   }
 }
 
-// Resets the per-slice boxes after the deposition has read them.
-__global__ void bbox_reset_kernel(int4* bbox, int n) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) bbox[i] = make_int4(1 << 30, 1 << 30, -1, -1);
+struct DiagBatchArgs {
+  const BeamDiagArgs* args;
+  const int2* items;
+  const int* nitems;
+};
+
+template <int NB>
+__global__ void __launch_bounds__(kDiagThreads, 2)
+    beam_diag_batch_kernel(const __grid_constant__ DiagBatchArgs b) {
+  const int nitems = *b.nitems;
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const int2 w = b.items[it];
+    diag_slice<NB>(b.args[w.x], w.y, 0);
+    __syncthreads();
+  }
 }
 
 // ---------------------------------------------------------- diag finalize --
@@ -1294,11 +1307,11 @@ int launch_single(g4b_run* r, const StepArgs& L) {
       beam_step_kernel<0><<<r->nchunk, kRunChunk, 0, c->stream>>>(L.bs);
   }
   if (int rc = check_launch(c, "beam_step_kernel")) return rc;
-  // The beam diagnostics depend only on K1; in a captured graph of a run
-  // with slices enough to fill the GPU twice they form a branch of their own
-  // beside the deposition and the ADI passes (filling the SMs those leave
-  // idle), joined before the finalize.  Smaller runs keep one chain: their
-  // kernels are short and a smaller graph instantiates faster.
+  // The beam diagnostics depend only on K1.  A run with slices enough to
+  // fill the GPU twice launches them as a kernel of their own: in a captured
+  // graph a branch beside the deposition and the ADI passes (filling the SMs
+  // those leave idle), joined before the finalize.  A smaller run computes
+  // them in the deposition's CTAs, before each slice's deposition.
   auto diag = [&](cudaStream_t st) {
     LaunchScope ls(c, "run_beam_diag");
     if (r->desc.nbunch == 1)
@@ -1307,20 +1320,31 @@ int launch_single(g4b_run* r, const StepArgs& L) {
       beam_diag_kernel<kMaxBunch><<<r->nslice * kDepParts, kDiagThreads, 0, st>>>(L.bd);
     return check_launch(c, "beam_diag_kernel");
   };
-  const bool branch = r->capturing && r->nslice >= 2 * c->sm_count;
+  const bool own = r->nslice >= 2 * c->sm_count;
+  const bool branch = own && r->capturing;
   if (branch) {
     G4B_CUDA_TRY(cudaEventRecord(r->ev_fork, c->stream));
     G4B_CUDA_TRY(cudaStreamWaitEvent(r->aux, r->ev_fork, 0));
     if (int rc = diag(r->aux)) return rc;
     G4B_CUDA_TRY(cudaEventRecord(r->ev_join, r->aux));
   }
-  {
-    LaunchScope ls(c, "run_deposit");
-    deposit_kernel<<<r->nslice, kDepThreads, kDepSmem, c->stream>>>(L.dd);
+  if (own) {
+    {
+      LaunchScope ls(c, "run_deposit");
+      deposit_kernel<<<r->nslice, kDepThreads, kDepSmem, c->stream>>>(L.dd);
+    }
+    if (int rc = check_launch(c, "deposit_kernel")) return rc;
+    if (!branch)
+      if (int rc = diag(c->stream)) return rc;
+  } else {
+    LaunchScope ls(c, "run_deposit_diag");
+    const DepDiagLaunch dl{L.dd, L.bd};
+    if (r->desc.nbunch == 1)
+      deposit_diag_kernel<1><<<r->nslice, kDepThreads, kDepSmem, c->stream>>>(dl);
+    else
+      deposit_diag_kernel<kMaxBunch><<<r->nslice, kDepThreads, kDepSmem, c->stream>>>(dl);
   }
-  if (int rc = check_launch(c, "deposit_kernel")) return rc;
-  if (!branch)
-    if (int rc = diag(c->stream)) return rc;
+  if (int rc = check_launch(c, "deposit_diag_kernel")) return rc;
   for (int f = 0; f < r->nfield; ++f)
     if (int rc = adi_launch(r->fs[f].f, L.adi[f])) return rc;
   if (branch) G4B_CUDA_TRY(cudaStreamWaitEvent(c->stream, r->ev_join, 0));
@@ -1453,6 +1477,10 @@ int g4b_run_create(g4b_ctx* c, const g4b_run_desc* d, const int64_t* off, g4b_ru
   r->step_doubles = (size_t)d->nslice * (r->rec_beam + 9 * d->nfield);
   cudaFuncSetAttribute(deposit_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)kDepSmem);
+  cudaFuncSetAttribute(deposit_diag_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)kDepSmem);
+  cudaFuncSetAttribute(deposit_diag_kernel<kMaxBunch>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDepSmem);
   *out = r;
   return G4B_OK;
 }
@@ -2058,9 +2086,9 @@ int batch_launch(g4b_batch* b, bool timed) {
                     reinterpret_cast<const int2*>(b->d_items + b->off_dep), counts + 1};
     LaunchScope ls(c, "batch_beam_diag");
     if (b->nb_kind == 1)
-      beam_diag_batch_kernel<1><<<3 * c->sm_count, kDiagThreads, 0, c->stream>>>(a);
+      beam_diag_batch_kernel<1><<<2 * c->sm_count, kDiagThreads, 0, c->stream>>>(a);
     else
-      beam_diag_batch_kernel<kMaxBunch><<<3 * c->sm_count, kDiagThreads, 0, c->stream>>>(a);
+      beam_diag_batch_kernel<kMaxBunch><<<2 * c->sm_count, kDiagThreads, 0, c->stream>>>(a);
   }
   if (int rc = check_launch(c, "beam_diag_batch_kernel")) return rc;
   ev(2);
