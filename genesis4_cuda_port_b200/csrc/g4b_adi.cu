@@ -729,7 +729,8 @@ int adi_run(g4b_adi* adi, g4b_field* f, const void* src, const int4* desc,
 }
 
 template <int M, bool PX, int L>
-static int batch_launch_t(g4b_ctx* c, const AdiBatchArgs& b, size_t smem, int grid) {
+static int batch_launch_t(g4b_ctx* c, cudaStream_t st, const AdiBatchArgs& b, size_t smem,
+                          int grid) {
   static std::atomic<uint64_t> configured{0};
   auto kern = adi_batch_kernel<float, M, PX, L>;
   if (c->device >= 64 || !((configured.load() >> c->device) & 1)) {
@@ -743,17 +744,17 @@ static int batch_launch_t(g4b_ctx* c, const AdiBatchArgs& b, size_t smem, int gr
   }
   {
     LaunchScope ls(c, PX ? "batch_adi_x" : "batch_adi_y");
-    kern<<<grid, BandW<float, L>::value * 32, smem, c->stream>>>(b);
+    kern<<<grid, BandW<float, L>::value * 32, smem, st>>>(b);
   }
   return check_launch(c, "adi_batch_kernel");
 }
 
-int adi_batch_launch(g4b_ctx* c, int mode, bool px, const AdiBatchArgs& b, size_t smem,
-                     int grid) {
+int adi_batch_launch(g4b_ctx* c, cudaStream_t st, int mode, bool px, const AdiBatchArgs& b,
+                     size_t smem, int grid) {
 #define G4B_BATCH_CASE(m, l)                                                   \
   case (l == 16 ? 100 : 0) + m:                                                \
-    return px ? batch_launch_t<m, true, l>(c, b, smem, grid)                   \
-              : batch_launch_t<m, false, l>(c, b, smem, grid);
+    return px ? batch_launch_t<m, true, l>(c, st, b, smem, grid)               \
+              : batch_launch_t<m, false, l>(c, st, b, smem, grid);
   switch (mode) { G4B_MODES32(G4B_BATCH_CASE) G4B_MODES16(G4B_BATCH_CASE) }
 #undef G4B_BATCH_CASE
   return fail(G4B_ERR_RANGE, "adi: unsupported elements per lane");

@@ -212,7 +212,7 @@ struct AdiBatchArgs {
   const int4* items;
   const int* nitems;
 };
-int adi_batch_launch(g4b_ctx* c, int M, bool px, const AdiBatchArgs& b, size_t smem,
+int adi_batch_launch(g4b_ctx* c, cudaStream_t st, int M, bool px, const AdiBatchArgs& b, size_t smem,
                      int grid);
 // Sets the launch attributes of the ADI kernels for this field's grid (done
 // before any stream capture).

@@ -1879,6 +1879,12 @@ struct g4b_batch {
   int tune_left = 0, tune_idx = 0;
   std::vector<float> tune_ms[4];
   cudaEvent_t ev[5] = {};
+  // concurrent branches of a step: the beam diagnostics beside the
+  // deposition and ADI passes; the ADI kernels of different row layouts
+  // beside one another
+  static constexpr int kAux = 4;
+  cudaStream_t aux[kAux] = {};
+  cudaEvent_t ev_fork[2] = {}, ev_diag = nullptr, ev_adi[kNumM] = {};
   // graph of one step for the current composition and shapes
   cudaGraphExec_t gexec = nullptr;
   bool graph_valid = false;
@@ -1919,6 +1925,10 @@ int batch_layout(g4b_batch* b) {
   }
   G4B_CUDA_TRY(cudaMalloc(&b->d_args, o));
   for (auto& e : b->ev) G4B_CUDA_TRY(cudaEventCreate(&e));
+  for (auto& e : b->ev_fork) G4B_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  for (auto& e : b->ev_adi) G4B_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  G4B_CUDA_TRY(cudaEventCreateWithFlags(&b->ev_diag, cudaEventDisableTiming));
+  for (auto& s : b->aux) G4B_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
   return G4B_OK;
 }
 
@@ -2081,18 +2091,33 @@ int batch_launch(g4b_batch* b, bool timed) {
     deposit_batch_kernel<<<b->grid[1], kDepThreads, kDepSmem, c->stream>>>(a);
   }
   if (int rc = check_launch(c, "deposit_batch_kernel")) return rc;
-  {
+  // branches (not while the tuner or the profiler times single kernels)
+  const bool fork = !timed && !c->prof.on;
+  auto diag = [&](cudaStream_t st) {
     DiagBatchArgs a{reinterpret_cast<const BeamDiagArgs*>(b->d_args + b->off_bd),
                     reinterpret_cast<const int2*>(b->d_items + b->off_dep), counts + 1};
     LaunchScope ls(c, "batch_beam_diag");
     if (b->nb_kind == 1)
-      beam_diag_batch_kernel<1><<<2 * c->sm_count, kDiagThreads, 0, c->stream>>>(a);
+      beam_diag_batch_kernel<1><<<2 * c->sm_count, kDiagThreads, 0, st>>>(a);
     else
-      beam_diag_batch_kernel<kMaxBunch><<<2 * c->sm_count, kDiagThreads, 0, c->stream>>>(a);
+      beam_diag_batch_kernel<kMaxBunch><<<2 * c->sm_count, kDiagThreads, 0, st>>>(a);
+    return check_launch(c, "beam_diag_batch_kernel");
+  };
+  if (fork) {
+    G4B_CUDA_TRY(cudaEventRecord(b->ev_fork[0], c->stream));
+    G4B_CUDA_TRY(cudaStreamWaitEvent(b->aux[0], b->ev_fork[0], 0));
+    if (int rc = diag(b->aux[0])) return rc;
+    G4B_CUDA_TRY(cudaEventRecord(b->ev_diag, b->aux[0]));
+  } else if (int rc = diag(c->stream)) {
+    return rc;
   }
-  if (int rc = check_launch(c, "beam_diag_batch_kernel")) return rc;
   ev(2);
   for (int pass = 0; pass < 2; ++pass) {
+    int ngroups = 0;
+    for (int m = 0; m < kNumM; ++m) ngroups += b->counts.adi[m] > 0;
+    const bool par = fork && ngroups > 1;
+    if (par) G4B_CUDA_TRY(cudaEventRecord(b->ev_fork[1], c->stream));
+    int gi = 0;
     for (int m = 0; m < kNumM; ++m) {
       if (b->counts.adi[m] == 0) continue;
       AdiBatchArgs a;
@@ -2101,12 +2126,25 @@ int batch_launch(g4b_batch* b, bool timed) {
       a.items = reinterpret_cast<const int4*>(b->d_items + b->off_adi[m]);
       a.nitems = reinterpret_cast<const int*>(b->d_args) + 4 + m;
       const int g = std::min(b->grid[2], b->counts.adi[m]);
-      if (int rc = adi_batch_launch(c, kMList[m], pass == 0, a, pass ? b->smem_y[m] : b->smem_x[m],
-                                    g))
+      // groups round-robin over the main stream and the branch streams
+      // 1..kAux-1 (stream 0 of the branches carries the diagnostics)
+      cudaStream_t st = c->stream;
+      if (par && gi % g4b_batch::kAux != 0) {
+        st = b->aux[gi % g4b_batch::kAux];
+        G4B_CUDA_TRY(cudaStreamWaitEvent(st, b->ev_fork[1], 0));
+      }
+      if (int rc = adi_batch_launch(c, st, kMList[m], pass == 0, a,
+                                    pass ? b->smem_y[m] : b->smem_x[m], g))
         return rc;
+      if (st != c->stream) G4B_CUDA_TRY(cudaEventRecord(b->ev_adi[gi], st));
+      ++gi;
     }
+    if (par)
+      for (int k = 0; k < gi; ++k)
+        if (k % g4b_batch::kAux != 0) G4B_CUDA_TRY(cudaStreamWaitEvent(c->stream, b->ev_adi[k], 0));
     ev(3 + pass);
   }
+  if (fork) G4B_CUDA_TRY(cudaStreamWaitEvent(c->stream, b->ev_diag, 0));
   {
     LaunchScope ls(c, "batch_diag_finalize");
     finalize_batch_kernel<<<b->grid[3], 256, 0, c->stream>>>(
@@ -2160,6 +2198,13 @@ int g4b_batch_destroy(g4b_batch* b) {
   }
   for (auto e : b->ev)
     if (e) cudaEventDestroy(e);
+  for (auto e : b->ev_fork)
+    if (e) cudaEventDestroy(e);
+  for (auto e : b->ev_adi)
+    if (e) cudaEventDestroy(e);
+  if (b->ev_diag) cudaEventDestroy(b->ev_diag);
+  for (auto s : b->aux)
+    if (s) cudaStreamDestroy(s);
   if (b->d_args) cudaFree(b->d_args);
   dev_free(b->ctx, b->d_items);
   for (int k = 0; k < 2; ++k) {
