@@ -390,7 +390,7 @@ struct DepField {
   float2* src;        // compact tiles, cap cells per slice
   int4* desc;
   int4* bbox;
-  int* mpred;         // [nslice] M of the slice's previous deposition (0: none)
+  int* mpred;         // [nslice][kDepSplit] M of the slice's previous deposition (0: none)
   size_t cap;
   int first, n, ld, nslice, harm, do_source;
   float gridmax, dgrid, inv_dgrid;
@@ -403,7 +403,7 @@ struct DepArgs {
   const double* th;
   const int64_t* off;
   const double* current;
-  float* qpred;       // [nslice] largest charge weight of the previous deposition (0: none)
+  float* qpred;       // [nslice][kDepSplit] largest charge weight of the previous deposition (0: none)
   DepField f[kRunFields];
   int nfield;
   float ax, ay, kx, ky, gradx, grady, gref_f;
@@ -598,6 +598,10 @@ __global__ void __launch_bounds__(kDiagThreads, 2)
 // the slice's bounding box of touched cells (from K1); tiles larger than
 // kDepMaxCells are processed in row bands.
 constexpr int kDepThreads = 256;
+// CTAs per slice: CTA `part` takes the tile's row bands part, part +
+// kDepSplit, ... (a tile of one band leaves the second CTA idle; one of two
+// bands is done by two CTAs side by side instead of one after the other)
+constexpr int kDepSplit = 2;
 constexpr int kDepAccU = 4;           // particles in flight per thread
 constexpr int kDepMaxCells = 8192;    // output cells per band (a multiple of 4)
 constexpr int kDepMaxWidth = 896;     // tile width bound: mixed ngrid <= 880
@@ -614,7 +618,8 @@ __device__ __forceinline__ float dep_charge(const DepArgs& a, const float2 xy, c
   return __fdividef(sqrtf(faw2), a.gref_f + dg);
 }
 
-__device__ __forceinline__ void deposit_slice(const DepArgs& a, const int bs, unsigned char* smem) {
+__device__ __forceinline__ void deposit_slice(const DepArgs& a, const int bs, const int part,
+                                              unsigned char* smem) {
   __shared__ int4 sbox[kRunFields];
   __shared__ int wsum[kDepThreads / 32];
   __shared__ float wmax[kDepThreads / 32];
@@ -625,7 +630,7 @@ __device__ __forceinline__ void deposit_slice(const DepArgs& a, const int bs, un
   const float* dgp = a.dg + p0;
   const double* thp = a.th + p0;
   if (tid < a.nfield) sbox[tid] = a.f[tid].bbox[bs];
-  const float qprev = a.qpred[bs];
+  const float qprev = a.qpred[bs * kDepSplit + part];
   const float q_use = qprev * 1.015625f;  // 0 without a previous deposition
   float q_seen = 0.f;
   bool deposited = false;
@@ -648,7 +653,7 @@ __device__ __forceinline__ void deposit_slice(const DepArgs& a, const int bs, un
       scl /= 4.0 * 510998.95 * npd * F.dgrid_d * F.dgrid_d;
     }
     if (bb.z < 0 || scl == 0.0) {
-      if (tid == 0) F.desc[target] = make_int4(0, 0, 0, 0);
+      if (tid == 0 && part == 0) F.desc[target] = make_int4(0, 0, 0, 0);
       continue;
     }
     int bx0 = bb.x, bw = bb.z - bb.x + 2;
@@ -658,13 +663,13 @@ __device__ __forceinline__ void deposit_slice(const DepArgs& a, const int bs, un
       if (bx0 + bw > F.ld) --bx0;
     }
     if (bw > kDepMaxWidth) {  // excluded by g4b_run_create's ngrid limit
-      if (tid == 0) {
+      if (tid == 0 && part == 0) {
         atomicOr(a.err, kErrBadSlice);
         F.desc[target] = make_int4(0, 0, 0, 0);
       }
       continue;
     }
-    if (tid == 0) F.desc[target] = make_int4(bx0, by0, bw, bh);
+    if (tid == 0 && part == 0) F.desc[target] = make_int4(bx0, by0, bw, bh);
     const int hband = max(1, kDepMaxCells / bw);  // bw <= ngrid + 1 < kDepMaxCells
     const float fh = (float)F.harm;
     // row of output cell o: (o + 1/2) / bw in FP32 is never within
@@ -677,10 +682,10 @@ __device__ __forceinline__ void deposit_slice(const DepArgs& a, const int bs, un
     mf.n = F.n;
     // M of this slice's previous deposition of this field (0: none yet)
     // bounds the contributions of the single-pass form below
-    const int mprev = F.mpred[bs];
+    const int mprev = F.mpred[bs * kDepSplit + part];
     const int m_use = mprev > 0 ? mprev + (mprev >> 2) + 4 : 0;
     int m_seen = 0;
-    for (int yb = 0; yb < bh; yb += hband) {
+    for (int yb = part * hband; yb < bh; yb += kDepSplit * hband) {
       const int hb = min(hband, bh - yb);
       const int ylo = by0 + yb;  // first grid row of this band
       const int nout = hb * bw, nbase = (hb + 1) * bw;
@@ -839,14 +844,14 @@ __device__ __forceinline__ void deposit_slice(const DepArgs& a, const int bs, un
       for (int i = tid; i < nout; i += kDepThreads)
         out[i] = make_float2((float)((double)are[i] * unscale), (float)((double)aim[i] * unscale));
     }
-    if (tid == 0) F.mpred[bs] = m_seen;
+    if (tid == 0 && part * hband < bh) F.mpred[bs * kDepSplit + part] = m_seen;
   }
-  if (tid == 0 && deposited) a.qpred[bs] = q_seen;
+  if (tid == 0 && deposited) a.qpred[bs * kDepSplit + part] = q_seen;
 }
 
 __global__ void __launch_bounds__(kDepThreads, 2) deposit_kernel(const __grid_constant__ DepArgs a) {
   extern __shared__ __align__(128) unsigned char smem[];
-  deposit_slice(a, blockIdx.x, smem);
+  deposit_slice(a, blockIdx.x / kDepSplit, blockIdx.x % kDepSplit, smem);
 }
 
 // The beam diagnostics and the deposition of a slice by one CTA, one after
@@ -862,9 +867,12 @@ template <int NB>
 __global__ void __launch_bounds__(kDepThreads, 2)
     deposit_diag_kernel(const __grid_constant__ DepDiagLaunch a) {
   extern __shared__ __align__(128) unsigned char smem[];
-  diag_slice<NB>(a.b, blockIdx.x, 0);
-  __syncthreads();
-  deposit_slice(a.d, blockIdx.x, smem);
+  const int bs = blockIdx.x / kDepSplit, part = blockIdx.x % kDepSplit;
+  if (part == 0) {
+    diag_slice<NB>(a.b, bs, 0);
+    __syncthreads();
+  }
+  deposit_slice(a.d, bs, part, smem);
 }
 
 // Batched forms: items[i] = (run, slice of that run).
@@ -877,10 +885,10 @@ struct DepBatchArgs {
 __global__ void __launch_bounds__(kDepThreads, 2)
     deposit_batch_kernel(const __grid_constant__ DepBatchArgs b) {
   extern __shared__ __align__(128) unsigned char smem[];
-  const int nitems = *b.nitems;
+  const int nitems = *b.nitems * kDepSplit;
   for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
-    const int2 w = b.items[it];
-    deposit_slice(b.args[w.x], w.y, smem);
+    const int2 w = b.items[it / kDepSplit];
+    deposit_slice(b.args[w.x], w.y, it % kDepSplit, smem);
     __syncthreads();
   }
 }
@@ -1331,7 +1339,7 @@ int launch_single(g4b_run* r, const StepArgs& L) {
   if (own) {
     {
       LaunchScope ls(c, "run_deposit");
-      deposit_kernel<<<r->nslice, kDepThreads, kDepSmem, c->stream>>>(L.dd);
+      deposit_kernel<<<r->nslice * kDepSplit, kDepThreads, kDepSmem, c->stream>>>(L.dd);
     }
     if (int rc = check_launch(c, "deposit_kernel")) return rc;
     if (!branch)
@@ -1340,9 +1348,10 @@ int launch_single(g4b_run* r, const StepArgs& L) {
     LaunchScope ls(c, "run_deposit_diag");
     const DepDiagLaunch dl{L.dd, L.bd};
     if (r->desc.nbunch == 1)
-      deposit_diag_kernel<1><<<r->nslice, kDepThreads, kDepSmem, c->stream>>>(dl);
+      deposit_diag_kernel<1><<<r->nslice * kDepSplit, kDepThreads, kDepSmem, c->stream>>>(dl);
     else
-      deposit_diag_kernel<kMaxBunch><<<r->nslice, kDepThreads, kDepSmem, c->stream>>>(dl);
+      deposit_diag_kernel<kMaxBunch><<<r->nslice * kDepSplit, kDepThreads, kDepSmem,
+                                       c->stream>>>(dl);
   }
   if (int rc = check_launch(c, "deposit_diag_kernel")) return rc;
   for (int f = 0; f < r->nfield; ++f)
@@ -1449,7 +1458,7 @@ int g4b_run_create(g4b_ctx* c, const g4b_run_desc* d, const int64_t* off, g4b_ru
     r->bytes += F.f->bytes;
     F.nband = (F.f->ngrid + F.f->band_rows - 1) / F.f->band_rows;
     A((void**)&F.d_bbox, d->nslice * sizeof(int4));
-    A((void**)&F.d_mpred, d->nslice * sizeof(int));
+    A((void**)&F.d_mpred, d->nslice * kDepSplit * sizeof(int));
     A((void**)&F.d_part, (size_t)d->nslice * F.nband * 9 * 8);
     if (e != cudaSuccess) {
       g4b_run_destroy(r);
@@ -1458,7 +1467,8 @@ int g4b_run_create(g4b_ctx* c, const g4b_run_desc* d, const int64_t* off, g4b_ru
     std::vector<int4> init(d->nslice, make_int4(1 << 30, 1 << 30, -1, -1));
     e = cudaMemcpyAsync(F.d_bbox, init.data(), init.size() * sizeof(int4),
                         cudaMemcpyHostToDevice, c->stream);
-    if (e == cudaSuccess) e = cudaMemsetAsync(F.d_mpred, 0, d->nslice * sizeof(int), c->stream);
+    if (e == cudaSuccess)
+      e = cudaMemsetAsync(F.d_mpred, 0, d->nslice * kDepSplit * sizeof(int), c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) {
       g4b_run_destroy(r);
@@ -1467,8 +1477,9 @@ int g4b_run_create(g4b_ctx* c, const g4b_run_desc* d, const int64_t* off, g4b_ru
   }
   r->rec_beam = kBeamRec + 2 * d->nbunch;
   A((void**)&r->d_beam_part, (size_t)d->nslice * kDepParts * r->rec_beam * 8);
-  A((void**)&r->d_qpred, d->nslice * sizeof(float));
-  if (e == cudaSuccess) e = cudaMemsetAsync(r->d_qpred, 0, d->nslice * sizeof(float), c->stream);
+  A((void**)&r->d_qpred, d->nslice * kDepSplit * sizeof(float));
+  if (e == cudaSuccess)
+    e = cudaMemsetAsync(r->d_qpred, 0, d->nslice * kDepSplit * sizeof(float), c->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) {
     g4b_run_destroy(r);
@@ -1538,8 +1549,9 @@ int g4b_run_upload_beam(g4b_run* r, const double* x, const double* y, const doub
   dev_free(r->ctx, stage);
   // a new beam: the next deposition counts before it accumulates
   for (int f = 0; f < r->nfield && e == cudaSuccess; ++f)
-    e = cudaMemsetAsync(r->fs[f].d_mpred, 0, r->nslice * sizeof(int), s);
-  if (e == cudaSuccess) e = cudaMemsetAsync(r->d_qpred, 0, r->nslice * sizeof(float), s);
+    e = cudaMemsetAsync(r->fs[f].d_mpred, 0, r->nslice * kDepSplit * sizeof(int), s);
+  if (e == cudaSuccess)
+    e = cudaMemsetAsync(r->d_qpred, 0, r->nslice * kDepSplit * sizeof(float), s);
   const cudaError_t es = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return cuda_fail(e, "g4b_run_upload_beam");
   if (es != cudaSuccess) return cuda_fail(es, "g4b_run_upload_beam");
