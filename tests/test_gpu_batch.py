@@ -23,6 +23,9 @@ CONFIGS = [
     dict(nslice=1, npart=2048, ngrid=71, taper=0.0, dgam=3e-4, time_run=False, nsteps=8),
     dict(nslice=3, npart=512, ngrid=33, taper=0.01, dgam=-2e-4, time_run=True, nsteps=6),
     dict(nslice=2, npart=768, ngrid=101, taper=0.0, dgam=0.0, time_run=True, nsteps=7),
+    # 32-lane ADI rows (the grids above use 16-lane rows): a batch of mixed
+    # row layouts runs their ADI kernels on concurrent streams
+    dict(nslice=2, npart=512, ngrid=151, taper=0.005, dgam=1e-4, time_run=True, nsteps=6),
 ]
 
 
@@ -99,7 +102,7 @@ def test_run_joins_a_batch_in_progress(ctx):
     """A run attached while others are mid-way (continuous batching) ends
     with the results it has alone."""
     alone = _alone(ctx)
-    batch = dev.Batch(ctx, 4)
+    batch = dev.Batch(ctx, len(CONFIGS))
     runs = [_make(ctx, k, cfg) for k, cfg in enumerate(CONFIGS)]
     batch.attach(runs[0], 0, CONFIGS[0]["nsteps"])
     batch.attach(runs[1], 0, CONFIGS[1]["nsteps"])
@@ -107,6 +110,7 @@ def test_run_joins_a_batch_in_progress(ctx):
     batch.attach(runs[2], 0, CONFIGS[2]["nsteps"])
     batch.step(2, graph=True)
     batch.attach(runs[3], 0, CONFIGS[3]["nsteps"])
+    batch.attach(runs[4], 0, CONFIGS[4]["nsteps"])
     batch.step(12, graph=True)
     ctx.synchronize()
     for r, cfg, ref in zip(runs, CONFIGS, alone):
