@@ -33,6 +33,9 @@
 namespace g4b {
 
 constexpr int kRunFields = 8;
+constexpr int kStepThreads = 128;  // beam step: two particles per thread
+constexpr int kStepBlocks = 8;     // resident beam-step CTAs per SM (<= 64 registers)
+constexpr int kStepWarps = kStepThreads / 32;
 constexpr int kMaxBunch = 8;
 constexpr int kBeamRec = 23;  // reference stats order (DiagnosticCUDA.cpp:102-125)
 
@@ -70,54 +73,6 @@ struct BeamStepArgs {
   int* err;
 };
 
-// Thick-lens map of one plane over `half` (advance_focusing_plane,
-// src/Core/TrackBeamCUDA.cpp:27-59) for strength s with k = s/gz and
-// w2 = k half^2: a1 = cos w, a2 = sin(w)/sqrt(k), a3 = -k a2 (cosh/sinh for
-// k < 0, drift for k = 0).  For |w2| < 1e-2 (every undulator and quadrupole
-// step of practical lattices) the functions are their Taylor series in w2
-// (truncation < w2^4/40320 < 3e-13); larger phases use the closed forms.
-__device__ __forceinline__ void plane_f(const PlaneMapF m, float half, float& c, float& p,
-                                        float gz, float inv_gz) {
-  if (m.mode == 0) {
-    c += p * half * inv_gz;
-    return;
-  }
-  const float k = m.strength * inv_gz;
-  const float w2 = k * half * half;
-  float a1, a2;
-  if (fabsf(w2) < 1e-2f) {
-    a1 = 1.0f + w2 * (-0.5f + w2 * (1.0f / 24.0f + w2 * (-1.0f / 720.0f)));
-    a2 = half * (1.0f + w2 * (-1.0f / 6.0f + w2 * (1.0f / 120.0f + w2 * (-1.0f / 5040.0f))));
-  } else if (k > 0.f) {
-    const float foc = sqrtf(k);
-    float sn, cs;
-    sincosf(foc * half, &sn, &cs);
-    a1 = cs;
-    a2 = sn / foc;
-  } else {
-    const float foc = sqrtf(-k);
-    a1 = coshf(foc * half);
-    a2 = sinhf(foc * half) / foc;
-  }
-  const float a3 = -a2 * k;
-  const float xt = c - m.offset;
-  c = a1 * xt + a2 * p * inv_gz + m.offset;
-  p = a3 * xt * gz + a1 * p;
-}
-
-// sin and cos of a small angle (|a| < 0.1: Taylor series to a^5 and a^4,
-// truncation below a^7/5040 < 2e-11 and a^6/720 < 1.4e-9, under the FP32
-// rounding of the results); larger angles use sincosf.
-__device__ __forceinline__ void sincos_small(float a, float& s, float& c) {
-  if (fabsf(a) < 0.1f) {
-    const float a2 = a * a;
-    s = a * (1.0f + a2 * (-1.0f / 6.0f + a2 * (1.0f / 120.0f)));
-    c = 1.0f + a2 * (-0.5f + a2 * (1.0f / 24.0f));
-  } else {
-    sincosf(a, &s, &c);
-  }
-}
-
 // Reduce an FP64 angle to [-pi, pi) before FP32 trigonometry (the
 // hardware sine / cosine, __sincosf, has an absolute error below 2^-21.4 on
 // that interval).
@@ -142,16 +97,128 @@ __device__ __forceinline__ bool cell_f(const MixField& f, float x, float y, int&
   return true;
 }
 
+// ---------------------------------------------------- packed FP32 pairs --
+// The beam step advances two particles per thread, one in each lane of a
+// packed FP32 pair: sm_100 executes add, subtract, multiply and fused
+// multiply-add on f32x2 register pairs as one instruction, so every FP32
+// operation of the push serves both particles.  Each lane rounds like the
+// scalar IEEE round-to-nearest operation, so a particle's result does not
+// depend on its partner.
+struct P2 {
+  float2 v;
+};
+__device__ __forceinline__ P2 pr(float a, float b) { return {make_float2(a, b)}; }
+__device__ __forceinline__ P2 bc(float a) { return {make_float2(a, a)}; }
+__device__ __forceinline__ float& ln(P2& p, int l) { return l ? p.v.y : p.v.x; }
+__device__ __forceinline__ float ln(const P2& p, int l) { return l ? p.v.y : p.v.x; }
+__device__ __forceinline__ P2 operator+(P2 a, P2 b) { return {__fadd2_rn(a.v, b.v)}; }
+__device__ __forceinline__ P2 operator*(P2 a, P2 b) { return {__fmul2_rn(a.v, b.v)}; }
+__device__ __forceinline__ P2 fma2(P2 a, P2 b, P2 c) { return {__ffma2_rn(a.v, b.v, c.v)}; }
+__device__ __forceinline__ P2 operator-(P2 a, P2 b) {
+  P2 r;
+  asm("{\n\t.reg .b64 pa, pb, pc;\n\t"
+      "mov.b64 pa, {%2, %3};\n\t"
+      "mov.b64 pb, {%4, %5};\n\t"
+      "sub.rn.f32x2 pc, pa, pb;\n\t"
+      "mov.b64 {%0, %1}, pc;\n\t}"
+      : "=f"(r.v.x), "=f"(r.v.y)
+      : "f"(a.v.x), "f"(a.v.y), "f"(b.v.x), "f"(b.v.y));
+  return r;
+}
+
+// Thick-lens map of one plane over `half` (advance_focusing_plane,
+// src/Core/TrackBeamCUDA.cpp:27-59) for strength s with k = s/gz and
+// w2 = k half^2: a1 = cos w, a2 = sin(w)/sqrt(k), a3 = -k a2 (cosh/sinh for
+// k < 0, drift for k = 0).  For |w2| < 1e-2 (every undulator and quadrupole
+// step of practical lattices) the functions are their Taylor series in w2,
+// a1 = 1 - w2/2 + w2^2/24 - w2^3/720 and a2/half = 1 - w2/6 + w2^2/120 -
+// w2^3/5040 (truncation < w2^4/40320 < 3e-13); larger phases use the closed
+// forms.  lens_coef is one lane of plane2, rounding for rounding.
+__device__ __forceinline__ void lens_coef(float k, float w2, float half, float& a1, float& a2) {
+  if (fabsf(w2) < 1e-2f) {
+    a1 = __fmaf_rn(w2, __fmaf_rn(w2, __fmaf_rn(w2, -1.0f / 720.0f, 1.0f / 24.0f), -0.5f), 1.0f);
+    a2 = __fmul_rn(half, __fmaf_rn(w2, __fmaf_rn(w2, __fmaf_rn(w2, -1.0f / 5040.0f,
+                                                                 1.0f / 120.0f),
+                                                 -1.0f / 6.0f),
+                                   1.0f));
+  } else if (k > 0.f) {
+    const float foc = sqrtf(k);
+    float sn, cs;
+    sincosf(foc * half, &sn, &cs);
+    a1 = cs;
+    a2 = sn / foc;
+  } else {
+    const float foc = sqrtf(-k);
+    a1 = coshf(foc * half);
+    a2 = sinhf(foc * half) / foc;
+  }
+}
+
+// c' = a1 (c - o) + a2 p / gz + o,  p' = a1 p + a3 gz (c - o) with
+// a3 gz = -a2 k gz = -a2 s (o: the element's offset).
+__device__ __forceinline__ void plane2(const PlaneMapF m, float half, P2& c, P2& p, P2 inv_gz) {
+  if (m.mode == 0) {
+    c = fma2(p, bc(half) * inv_gz, c);
+    return;
+  }
+  const P2 k = bc(m.strength) * inv_gz;
+  const P2 w2 = k * bc(half * half);
+  P2 a1, a2;
+  if (fmaxf(fabsf(w2.v.x), fabsf(w2.v.y)) < 1e-2f) {
+    a1 = fma2(w2, fma2(w2, fma2(w2, bc(-1.0f / 720.0f), bc(1.0f / 24.0f)), bc(-0.5f)), bc(1.0f));
+    a2 = bc(half) *
+         fma2(w2, fma2(w2, fma2(w2, bc(-1.0f / 5040.0f), bc(1.0f / 120.0f)), bc(-1.0f / 6.0f)),
+              bc(1.0f));
+  } else {
+    lens_coef(k.v.x, w2.v.x, half, a1.v.x, a2.v.x);
+    lens_coef(k.v.y, w2.v.y, half, a1.v.y, a2.v.y);
+  }
+  const P2 o = bc(m.offset);
+  const P2 xt = c - o;
+  c = fma2(a1, xt, fma2(a2 * inv_gz, p, o));
+  p = fma2(a2 * bc(-m.strength), xt, a1 * p);
+}
+
+// sin and cos of a small angle (|a| < 0.1: Taylor series to a^5 and a^4,
+// truncation below a^7/5040 < 2e-11 and a^6/720 < 1.4e-9, under the FP32
+// rounding of the results); larger angles use sincosf.  sincos_small is one
+// lane of sincos_small2, rounding for rounding.
+__device__ __forceinline__ void sincos_small(float a, float& s, float& c) {
+  if (fabsf(a) < 0.1f) {
+    const float a2 = __fmul_rn(a, a);
+    s = __fmul_rn(a, __fmaf_rn(a2, __fmaf_rn(a2, 1.0f / 120.0f, -1.0f / 6.0f), 1.0f));
+    c = __fmaf_rn(a2, __fmaf_rn(a2, 1.0f / 24.0f, -0.5f), 1.0f);
+  } else {
+    sincosf(a, &s, &c);
+  }
+}
+
+__device__ __forceinline__ void sincos_small2(P2 a, P2& s, P2& c) {
+  if (fmaxf(fabsf(a.v.x), fabsf(a.v.y)) < 0.1f) {
+    const P2 a2 = a * a;
+    s = a * fma2(a2, fma2(a2, bc(1.0f / 120.0f), bc(-1.0f / 6.0f)), bc(1.0f));
+    c = fma2(a2, fma2(a2, bc(1.0f / 24.0f), bc(-0.5f)), bc(1.0f));
+  } else {
+    sincos_small(a.v.x, s.v.x, c.v.x);
+    sincos_small(a.v.y, s.v.y, c.v.y);
+  }
+}
+
 // NF: number of fields when known at compile time (1, 2), 0 = up to 8.
+// One CTA of kStepThreads threads advances a chunk of up to 2 kStepThreads
+// particles of one slice: thread t holds particles t (lane x) and
+// t + kStepThreads (lane y) of the chunk; a dead y lane repeats x and is
+// not stored.
 template <int NF>
 __device__ __forceinline__ void beam_chunk(const BeamStepArgs& a, const int4 ch) {
   constexpr int kF = NF > 0 ? NF : kRunFields;
   const int nfield = NF > 0 ? NF : a.nfield;
-  __shared__ int sbb[kRunFields][4][8];
+  __shared__ int sbb[kRunFields][4][kStepWarps];
   const int slice = ch.x;
   const int tid = threadIdx.x;
-  const bool live = tid < ch.z;
-  const int64_t ip = (((int64_t)ch.w) << 31) + (int64_t)(unsigned)ch.y + tid;
+  const bool live = tid < ch.z, live_y = tid + kStepThreads < ch.z;
+  const int64_t ipx = (((int64_t)ch.w) << 31) + (int64_t)(unsigned)ch.y + tid;
+  const int64_t ipy = live_y ? ipx + kStepThreads : ipx;
   int bb[kF][4];
 #pragma unroll
   for (int f = 0; f < kF; ++f) {
@@ -159,60 +226,72 @@ __device__ __forceinline__ void beam_chunk(const BeamStepArgs& a, const int4 ch)
     bb[f][2] = bb[f][3] = -1;
   }
   if (live) {
-    float2 xy = a.xy[ip], pp = a.pxy[ip];
-    float x = xy.x, y = xy.y, px = pp.x, py = pp.y;
-    float d = a.dg[ip];
-    double t = a.th[ip];
+    const float2 xy0 = a.xy[ipx], xy1 = a.xy[ipy], pp0 = a.pxy[ipx], pp1 = a.pxy[ipy];
+    P2 x = pr(xy0.x, xy1.x), y = pr(xy0.y, xy1.y), px = pr(pp0.x, pp1.x), py = pr(pp0.y, pp1.y);
+    P2 d = pr(a.dg[ipx], a.dg[ipy]);
+    double t[2] = {a.th[ipx], a.th[ipy]};
     // TrackBeamCUDA::track, first half (src/Core/TrackBeamCUDA.cpp:156-204)
     {
-      const float g = a.gref_f + d;
       if (a.pre) {
-        const float gz = sqrtf(g * g - 1.0f - px * px - py * py);
-        float tmp = x;
-        x = a.m00 * tmp + a.m01 * px / gz;
-        px = a.m10 * tmp * gz + a.m11 * px;
-        tmp = y;
-        y = a.m22 * tmp + a.m23 * py / gz;
-        py = a.m32 * tmp * gz + a.m33 * py;
+#pragma unroll
+        for (int l = 0; l < 2; ++l) {
+          float &xl = ln(x, l), &pxl = ln(px, l), &yl = ln(y, l), &pyl = ln(py, l);
+          const float g = a.gref_f + ln(d, l);
+          const float gz = sqrtf(g * g - 1.0f - pxl * pxl - pyl * pyl);
+          float tmp = xl;
+          xl = a.m00 * tmp + a.m01 * pxl / gz;
+          pxl = a.m10 * tmp * gz + a.m11 * pxl;
+          tmp = yl;
+          yl = a.m22 * tmp + a.m23 * pyl / gz;
+          pyl = a.m32 * tmp * gz + a.m33 * pyl;
+        }
       }
-      const float gz2 = g * g - 1.0f - a.aw2 - px * px - py * py;
-      const float inv_gz = rsqrtf(gz2), gz = gz2 * inv_gz;
-      plane_f(a.xm, a.half, x, px, gz, inv_gz);
-      plane_f(a.ym, a.half, y, py, gz, inv_gz);
+      const P2 g = bc(a.gref_f) + d;
+      const P2 gz2 = fma2(g, g, bc(-1.0f - a.aw2)) - fma2(px, px, py * py);
+      const P2 inv_gz = pr(rsqrtf(gz2.v.x), rsqrtf(gz2.v.y));
+      plane2(a.xm, a.half, x, px, inv_gz);
+      plane2(a.ym, a.half, y, py, inv_gz);
     }
     // BeamSolverCUDA::advance push (src/Core/BeamSolverCUDA.cpp:226-409)
-    t += a.autophase;
-    const float dxu = x - a.ax, dyu = y - a.ay;
-    const float awloc = 1.0f + 0.5f * (a.kx * dxu * dxu + a.ky * dyu * dyu) + a.gradx * dxu +
-                        a.grady * dyu;
-    const float btpar = 1.0f + px * px + py * py + a.aw2 * awloc * awloc;
+    t[0] += a.autophase;
+    t[1] += a.autophase;
+    const P2 dxu = x - bc(a.ax), dyu = y - bc(a.ay);
+    const P2 awloc =
+        fma2(bc(a.gradx), dxu,
+             fma2(bc(a.grady), dyu,
+                  fma2(bc(0.5f), fma2(bc(a.kx) * dxu, dxu, bc(a.ky) * dyu * dyu), bc(1.0f))));
+    const P2 btpar = fma2(bc(a.aw2), awloc * awloc, fma2(py, py, fma2(px, px, bc(1.0f))));
     const float ez = (float)a.eloss[slice];
-    float rr[kF], ri[kF], c0[kF], s0[kF];
-    const double t0 = t;
+    // Field sample of each field rotated to the start phase,
+    // w = sc (re - i im) e^{-i h theta0} with sc = rtmp awloc: the field term
+    // of a stage at phase offset dth is then w e^{-i h dth}.
+    P2 wr[kF], wi[kF];
 #pragma unroll
     for (int f = 0; f < kF; ++f) {
-      rr[f] = ri[f] = 0.f;
-      c0[f] = 1.f;
-      s0[f] = 0.f;
+      wr[f] = wi[f] = bc(0.f);
       if (f >= nfield) continue;
       const MixField& F = a.f[f];
-      int ix, iy;
-      float wx, wy;
-      if (cell_f(F, x, y, ix, iy, wx, wy)) {
-        int islice = slice + F.first;  // both in [0, nslice)
-        if (islice >= F.nslice) islice -= F.nslice;
-        const float2* c = F.cells + (size_t)islice * F.n * F.ld + (size_t)iy * F.ld + ix;
-        const float2 c00 = __ldg(c), c10 = __ldg(c + 1), c01 = __ldg(c + F.ld),
-                     c11 = __ldg(c + F.ld + 1);
-        const float w00 = wx * wy, w10 = (1.f - wx) * wy, w01 = wx * (1.f - wy),
-                    w11 = (1.f - wx) * (1.f - wy);
-        const float cre = c00.x * w00 + c10.x * w10 + c01.x * w01 + c11.x * w11;
-        const float cim = c00.y * w00 + c10.y * w10 + c01.y * w01 + c11.y * w11;
-        const float sc = F.rtmp * awloc;
-        rr[f] = sc * cre;
-        ri[f] = -sc * cim;
+      int islice = slice + F.first;  // both in [0, nslice)
+      if (islice >= F.nslice) islice -= F.nslice;
+      const float2* base = F.cells + (size_t)islice * F.n * F.ld;
+      P2 cre = bc(0.f), cim = bc(0.f), cs0, sn0;
+#pragma unroll
+      for (int l = 0; l < 2; ++l) {
+        int ix, iy;
+        float wx, wy;
+        if (cell_f(F, ln(x, l), ln(y, l), ix, iy, wx, wy)) {
+          const float2* c = base + (size_t)iy * F.ld + ix;
+          const float2 c00 = __ldg(c), c10 = __ldg(c + 1), c01 = __ldg(c + F.ld),
+                       c11 = __ldg(c + F.ld + 1);
+          const float w00 = wx * wy, w10 = (1.f - wx) * wy, w01 = wx * (1.f - wy),
+                      w11 = (1.f - wx) * (1.f - wy);
+          ln(cre, l) = c00.x * w00 + c10.x * w10 + c01.x * w01 + c11.x * w11;
+          ln(cim, l) = c00.y * w00 + c10.y * w10 + c01.y * w01 + c11.y * w11;
+        }
+        __sincosf(reduce_angle((double)F.harm * t[l]), &ln(sn0, l), &ln(cs0, l));
       }
-      __sincosf(reduce_angle((double)F.harm * t0), &s0[f], &c0[f]);
+      wr[f] = (bc(F.rtmp) * awloc) * (cre * cs0 - cim * sn0);
+      wi[f] = (bc(-F.rtmp) * awloc) * fma2(cre, sn0, cim * cs0);
     }
     // theta' = ks (1 - 1/b0) + ku with b0 = sqrt(1 - eps), eps = btper0 /
     // gamma^2 ~ 1e-8: the two ~ku terms cancel to the detuning, so the
@@ -224,113 +303,121 @@ __device__ __forceinline__ void beam_chunk(const BeamStepArgs& a, const int4 ch)
     // with B0 = ks eps0 fe(eps0), so theta' = A0 - B0 r to a relative
     // 1e-8 of the field term, and r is formed in FP32 without cancellation.
     // The energy derivative Im(c) / (b0 gs) - ez drops b0 = 1 + O(1e-8).
-    const double d0 = (double)d;
-    const double g0 = a.gref + d0;
-    // 1/g0: one Newton step from the FP32 reciprocal (relative error ~2^-44,
-    // far below what the FP32 results keep)
-    double inv_g0 = (double)__fdividef(1.0f, (float)g0);
-    inv_g0 = fma(inv_g0, fma(-g0, inv_g0, 1.0), inv_g0);
-    const double eps0 = (double)btpar * inv_g0 * inv_g0;
-    const double fe0 = 0.5 + eps0 * (0.375 + eps0 * 0.3125);
-    const double B0d = a.xks * eps0 * fe0;
-    const float A0 = (float)(a.xku - B0d);
-    const float B0 = (float)B0d;
-    const float zt = __fdividef(a.zt0, btpar);  // delta / btpar per unit Re(c)
-    const float ig0 = (float)inv_g0;
-    // stage derivatives at energy offset ds (from g0) and phase offset dth
-    auto ode = [&](float ds, float dth, float& kg, float& kp) {
-      float ctr = 0.f, cti = 0.f;
+    P2 A0, nB0, ig0;
+#pragma unroll
+    for (int l = 0; l < 2; ++l) {
+      const double g0 = a.gref + (double)ln(d, l);
+      // 1/g0: one Newton step from the FP32 reciprocal (relative error
+      // ~2^-44, far below what the FP32 results keep)
+      double inv_g0 = (double)__fdividef(1.0f, (float)g0);
+      inv_g0 = fma(inv_g0, fma(-g0, inv_g0, 1.0), inv_g0);
+      const double eps0 = (double)ln(btpar, l) * inv_g0 * inv_g0;
+      const double fe0 = 0.5 + eps0 * (0.375 + eps0 * 0.3125);
+      const double B0d = a.xks * eps0 * fe0;
+      ln(A0, l) = (float)(a.xku - B0d);
+      ln(nB0, l) = -(float)B0d;
+      ln(ig0, l) = (float)inv_g0;
+    }
+    // delta / btpar per unit Re(c)
+    const P2 zt = bc(a.zt0) * pr(__fdividef(1.0f, btpar.v.x), __fdividef(1.0f, btpar.v.y));
+    const P2 nez = bc(-ez);
+    // stage derivatives (energy kg, phase kp) at energy offset ds (from g0)
+    // and phase offset dth
+    auto ode = [&](P2 ds, P2 dth, P2& kg, P2& kp) {
+      P2 ctr = bc(0.f), cti = bc(0.f);
 #pragma unroll
       for (int f = 0; f < kF; ++f) {
         if (f >= nfield) break;
-        float sd, cd;
-        sincos_small((float)a.f[f].harm * dth, sd, cd);
-        const float c = c0[f] * cd - s0[f] * sd;
-        const float s = s0[f] * cd + c0[f] * sd;
-        ctr += rr[f] * c + ri[f] * s;
-        cti += ri[f] * c - rr[f] * s;
+        P2 sd, cd;
+        sincos_small2(bc((float)a.f[f].harm) * dth, sd, cd);
+        if (f == 0) {
+          ctr = fma2(wr[0], cd, wi[0] * sd);
+          cti = wi[0] * cd - wr[0] * sd;
+        } else {
+          ctr = fma2(wr[f], cd, fma2(wi[f], sd, ctr));
+          cti = fma2(wi[f], cd, cti) - wr[f] * sd;
+        }
       }
-      const float e = ds * ig0;                 // (gs - g0) / g0, |e| <~ 1e-3
-      const float bq = e * (e - 1.0f);          // g0 / gs - 1, error O(e^3)
-      const float ar = zt * ctr;                // delta / btpar
-      const float r = ar + bq * (2.0f + bq) * (1.0f + ar);
-      kp += A0 - B0 * r;
-      kg += cti * (ig0 * (1.0f + bq)) - ez;
+      const P2 e = ds * ig0;               // (gs - g0) / g0, |e| <~ 1e-3
+      const P2 bq = e * (e - bc(1.0f));    // g0 / gs - 1, error O(e^3)
+      const P2 ar = zt * ctr;              // delta / btpar
+      const P2 r = fma2(bq * (bq + bc(2.0f)), ar + bc(1.0f), ar);
+      kp = fma2(nB0, r, A0);
+      kg = fma2(cti, fma2(ig0, bq, ig0), nez);
     };
-    // Genesis RK4 accumulator form (src/Core/BeamSolverCUDA.cpp:258-299) on
-    // the step's energy increment dd and phase increment dt (both small, so
-    // FP32 keeps their relative precision); theta and the stored energy
-    // offset are updated once at the end
-    float dd = 0.f, dt = 0.f;
-    float k2g = 0.f, k3g, k2p = 0.f, k3p;
+    // Fourth-order Runge-Kutta on the step's energy increment dd and phase
+    // increment dt (both small, so FP32 keeps their relative precision; the
+    // classical combination that src/Core/BeamSolverCUDA.cpp:258-299 forms
+    // in accumulator form); theta and the stored energy offset are updated
+    // once at the end
+    P2 k1g, k1p;
     {
       // first stage at the start point: no phase rotation, gs = g0
-      float ctr = 0.f, cti = 0.f;
+      P2 ctr = wr[0], cti = wi[0];
 #pragma unroll
-      for (int f = 0; f < kF; ++f) {
+      for (int f = 1; f < kF; ++f) {
         if (f >= nfield) break;
-        ctr += rr[f] * c0[f] + ri[f] * s0[f];
-        cti += ri[f] * c0[f] - rr[f] * s0[f];
+        ctr = ctr + wr[f];
+        cti = cti + wi[f];
       }
-      k2p = A0 - B0 * (zt * ctr);
-      k2g = cti * ig0 - ez;
+      k1p = fma2(nB0, zt * ctr, A0);
+      k1g = fma2(cti, ig0, nez);
     }
-    float stf = (float)(0.5 * a.delz);
-    dd += stf * k2g;
-    dt += stf * k2p;
-    k3g = k2g;
-    k3p = k2p;
-    k2g = 0.f;
-    k2p = 0.f;
-    ode(dd, dt, k2g, k2p);
-    dd += stf * (k2g - k3g);
-    dt += stf * (k2p - k3p);
-    constexpr float kSixth = 1.0f / 6.0f;
-    k3g *= kSixth;
-    k3p *= kSixth;
-    k2g *= -0.5f;
-    k2p *= -0.5f;
-    ode(dd, dt, k2g, k2p);
-    stf = (float)a.delz;
-    dd += stf * k2g;
-    dt += stf * k2p;
-    k3g -= k2g;
-    k3p -= k2p;
-    k2g *= 2.0f;
-    k2p *= 2.0f;
-    ode(dd, dt, k2g, k2p);
-    dd += stf * (k3g + k2g * kSixth);
-    dt += stf * (k3p + k2p * kSixth);
-    t = t0 + (double)dt;
-    d = (float)(d0 + (double)dd);
-    // applyR56 (src/Core/TrackBeamCUDA.cpp:257-278): theta += R56 (gamma - gamma0)
-    if (a.has_r56) t += a.r56 * ((double)d + a.r56_off);
+    const P2 hh = bc((float)(0.5 * a.delz)), h = bc((float)a.delz);
+    // ug, up: the latest stage's derivatives; sg, sp: k1 + 2 k2 + 2 k3 + k4
+    P2 ug, up;
+    ode(hh * k1g, hh * k1p, ug, up);
+    P2 sg = fma2(bc(2.0f), ug, k1g), sp = fma2(bc(2.0f), up, k1p);
+    ode(hh * ug, hh * up, ug, up);
+    sg = fma2(bc(2.0f), ug, sg);
+    sp = fma2(bc(2.0f), up, sp);
+    ode(h * ug, h * up, ug, up);
+    const P2 h6 = bc((float)(a.delz / 6.0));
+    const P2 dd = h6 * (sg + ug);
+    const P2 dt = h6 * (sp + up);
+#pragma unroll
+    for (int l = 0; l < 2; ++l) {
+      t[l] += (double)ln(dt, l);
+      ln(d, l) = (float)((double)ln(d, l) + (double)ln(dd, l));
+      // applyR56 (src/Core/TrackBeamCUDA.cpp:257-278): theta += R56 (gamma - gamma0)
+      if (a.has_r56) t[l] += a.r56 * ((double)ln(d, l) + a.r56_off);
+    }
     // second half (+corrector on the last half step)
     {
       if (a.post) {
-        px += a.cx;
-        py += a.cy;
+        px = px + bc(a.cx);
+        py = py + bc(a.cy);
       }
-      const float g = a.gref_f + d;
-      const float gz2 = g * g - 1.0f - a.aw2 - px * px - py * py;
-      const float inv_gz = rsqrtf(gz2), gz = gz2 * inv_gz;
-      plane_f(a.xm, a.half, x, px, gz, inv_gz);
-      plane_f(a.ym, a.half, y, py, gz, inv_gz);
+      const P2 g = bc(a.gref_f) + d;
+      const P2 gz2 = fma2(g, g, bc(-1.0f - a.aw2)) - fma2(px, px, py * py);
+      const P2 inv_gz = pr(rsqrtf(gz2.v.x), rsqrtf(gz2.v.y));
+      plane2(a.xm, a.half, x, px, inv_gz);
+      plane2(a.ym, a.half, y, py, inv_gz);
     }
-    a.xy[ip] = make_float2(x, y);
-    a.pxy[ip] = make_float2(px, py);
-    a.dg[ip] = d;
-    a.th[ip] = t;
+    a.xy[ipx] = make_float2(x.v.x, y.v.x);
+    a.pxy[ipx] = make_float2(px.v.x, py.v.x);
+    a.dg[ipx] = d.v.x;
+    a.th[ipx] = t[0];
+    if (live_y) {
+      a.xy[ipy] = make_float2(x.v.y, y.v.y);
+      a.pxy[ipy] = make_float2(px.v.y, py.v.y);
+      a.dg[ipy] = d.v.y;
+      a.th[ipy] = t[1];
+    }
 #pragma unroll
     for (int f = 0; f < kF; ++f) {
       if (f >= nfield) break;
-      int ix, iy;
-      float wx, wy;
-      if (a.f[f].do_source && cell_f(a.f[f], x, y, ix, iy, wx, wy)) {
-        bb[f][0] = min(bb[f][0], ix);
-        bb[f][1] = min(bb[f][1], iy);
-        bb[f][2] = max(bb[f][2], ix);
-        bb[f][3] = max(bb[f][3], iy);
+      if (!a.f[f].do_source) continue;
+#pragma unroll
+      for (int l = 0; l < 2; ++l) {
+        int ix, iy;
+        float wx, wy;
+        if ((l == 0 || live_y) && cell_f(a.f[f], ln(x, l), ln(y, l), ix, iy, wx, wy)) {
+          bb[f][0] = min(bb[f][0], ix);
+          bb[f][1] = min(bb[f][1], iy);
+          bb[f][2] = max(bb[f][2], ix);
+          bb[f][3] = max(bb[f][3], iy);
+        }
       }
     }
   }
@@ -350,7 +437,7 @@ __device__ __forceinline__ void beam_chunk(const BeamStepArgs& a, const int4 ch)
   if (tid < 4 * nfield) {
     const int f = tid >> 2, q = tid & 3;
     int v = sbb[f][q][0];
-    for (int i = 1; i < 8; ++i) v = q < 2 ? min(v, sbb[f][q][i]) : max(v, sbb[f][q][i]);
+    for (int i = 1; i < kStepWarps; ++i) v = q < 2 ? min(v, sbb[f][q][i]) : max(v, sbb[f][q][i]);
     if (a.f[f].do_source) {
       int* b = reinterpret_cast<int*>(&a.f[f].bbox[slice]) + q;
       if (q < 2) {
@@ -363,7 +450,7 @@ __device__ __forceinline__ void beam_chunk(const BeamStepArgs& a, const int4 ch)
 }
 
 template <int NF>
-__global__ void __launch_bounds__(256) beam_step_kernel(const __grid_constant__ BeamStepArgs a) {
+__global__ void __launch_bounds__(kStepThreads, kStepBlocks) beam_step_kernel(const __grid_constant__ BeamStepArgs a) {
   beam_chunk<NF>(a, a.chunks[blockIdx.x]);
 }
 
@@ -375,7 +462,7 @@ struct BeamBatchArgs {
 };
 
 template <int NF>
-__global__ void __launch_bounds__(256) beam_batch_kernel(const __grid_constant__ BeamBatchArgs b) {
+__global__ void __launch_bounds__(kStepThreads, kStepBlocks) beam_batch_kernel(const __grid_constant__ BeamBatchArgs b) {
   const int nitems = *b.nitems;
   for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
     const int2 w = b.items[it];
@@ -1068,7 +1155,7 @@ void g4b_chicane_matrix(double angle, double lb, double ld, double lt, double* m
 
 namespace {
 
-constexpr int kRunChunk = 256;
+constexpr int kRunChunk = 2 * kStepThreads;  // particles per beam-step CTA
 
 // Every argument of one lattice step of one run.
 struct StepArgs {
@@ -1308,11 +1395,11 @@ int launch_single(g4b_run* r, const StepArgs& L) {
   if (L.has_beam) {
     LaunchScope ls(c, "run_beam_step");
     if (r->nfield == 1)
-      beam_step_kernel<1><<<r->nchunk, kRunChunk, 0, c->stream>>>(L.bs);
+      beam_step_kernel<1><<<r->nchunk, kStepThreads, 0, c->stream>>>(L.bs);
     else if (r->nfield == 2)
-      beam_step_kernel<2><<<r->nchunk, kRunChunk, 0, c->stream>>>(L.bs);
+      beam_step_kernel<2><<<r->nchunk, kStepThreads, 0, c->stream>>>(L.bs);
     else
-      beam_step_kernel<0><<<r->nchunk, kRunChunk, 0, c->stream>>>(L.bs);
+      beam_step_kernel<0><<<r->nchunk, kStepThreads, 0, c->stream>>>(L.bs);
   }
   if (int rc = check_launch(c, "beam_step_kernel")) return rc;
   // The beam diagnostics depend only on K1.  A run with slices enough to
@@ -1906,7 +1993,7 @@ struct g4b_batch {
 namespace {
 
 // The tuner's candidates per kernel, in units of SMs.
-const int kTuneBeam[4] = {2, 4, 8, 16};
+const int kTuneBeam[4] = {4, 8, 16, 32};
 const int kTuneDep[4] = {2, 4, 6, 8};
 const int kTuneAdi[4] = {2, 4, 6, 8};
 
@@ -2088,11 +2175,11 @@ int batch_launch(g4b_batch* b, bool timed) {
                     reinterpret_cast<const int2*>(b->d_items + b->off_beam), counts + 0};
     LaunchScope ls(c, "batch_beam_step");
     if (b->nf_kind == 1)
-      beam_batch_kernel<1><<<b->grid[0], kRunChunk, 0, c->stream>>>(a);
+      beam_batch_kernel<1><<<b->grid[0], kStepThreads, 0, c->stream>>>(a);
     else if (b->nf_kind == 2)
-      beam_batch_kernel<2><<<b->grid[0], kRunChunk, 0, c->stream>>>(a);
+      beam_batch_kernel<2><<<b->grid[0], kStepThreads, 0, c->stream>>>(a);
     else
-      beam_batch_kernel<0><<<b->grid[0], kRunChunk, 0, c->stream>>>(a);
+      beam_batch_kernel<0><<<b->grid[0], kStepThreads, 0, c->stream>>>(a);
   }
   if (int rc = check_launch(c, "beam_batch_kernel")) return rc;
   ev(1);
@@ -2167,7 +2254,7 @@ int batch_launch(g4b_batch* b, bool timed) {
 
 void batch_default_grids(g4b_batch* b) {
   const int sm = b->ctx->sm_count;
-  b->grid[0] = 8 * sm;
+  b->grid[0] = 2 * kStepBlocks * sm;
   b->grid[1] = 2 * sm;
   b->grid[2] = 4 * sm;
   b->grid[3] = sm;
