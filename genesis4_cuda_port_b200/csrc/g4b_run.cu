@@ -10,12 +10,14 @@
 //                  bilinear field sample, R56, transverse half step
 //                  (+corrector), and each slice's bounding box of touched
 //                  cells (integer atomics, order independent);
-//   K2 deposit_diag : per slice, the beam diagnostics (FP64 sums) and the
-//                  deterministic exact-integer deposition of every field's
-//                  source into a compact tile;
+//   K2 deposit : per slice, the deterministic exact-integer deposition of
+//                  every field's source into a compact tile; beside it (a
+//                  branch of the captured graph) the beam diagnostics (FP64
+//                  sums);
 //   K3/K4 ADI passes per field (pass Y also zeroes the planes this step's
 //                  slippage zeroes and writes field-diagnostic partials);
-//   K5 diag_finalize : per-slice field diagnostics into the history buffer.
+//   K5 diag_finalize : per-slice beam and field diagnostics into the history
+//                  buffer.
 // The theta derivative ks(1-1/b) + ku is evaluated cancellation-free in FP64
 // as ku - ks*eps/(b(1+b)), eps = btper0/gamma^2 (the two ~ku terms cancel to
 // the detuning).  Slippage is the host's integer index model: `first` and the
@@ -509,12 +511,11 @@ struct BeamDiagArgs {
 };
 
 // Beam diagnostics (DiagnosticCUDA.cpp:102-125), kDepParts CTAs per slice,
-// each over a quarter of the slice's particles: one pass with FP64 sums (the
-// minima and maxima in FP32, exact for FP32 state) into a record of the
-// final layout; the finalize combines a slice's records in a fixed order
-// (sums, minima and maxima of records are the record of the union).
-// Independent of the deposition, so it can run beside it and the ADI
-// passes.
+// each over an equal share of the slice's particles: one pass with FP64
+// sums (the minima and maxima in FP32, exact for FP32 state) into a record
+// of the final layout; the finalize combines a slice's records in a fixed
+// order (sums, minima and maxima of records are the record of the union).
+// Independent of the deposition, so it runs beside it and the ADI passes.
 constexpr int kDepParts = 1;          // beam-diagnostic records per slice
 constexpr int kDiagThreads = 256;
 constexpr int kDepDiagU = 8;          // particles in flight per thread
@@ -941,27 +942,6 @@ __global__ void __launch_bounds__(kDepThreads, 2) deposit_kernel(const __grid_co
   deposit_slice(a, blockIdx.x / kDepSplit, blockIdx.x % kDepSplit, smem);
 }
 
-// The beam diagnostics and the deposition of a slice by one CTA, one after
-// the other: the form for runs too small to fill the GPU with the
-// diagnostics on a branch of their own (the same device functions, so the
-// same results).
-struct DepDiagLaunch {
-  DepArgs d;
-  BeamDiagArgs b;
-};
-
-template <int NB>
-__global__ void __launch_bounds__(kDepThreads, 2)
-    deposit_diag_kernel(const __grid_constant__ DepDiagLaunch a) {
-  extern __shared__ __align__(128) unsigned char smem[];
-  const int bs = blockIdx.x / kDepSplit, part = blockIdx.x % kDepSplit;
-  if (part == 0) {
-    diag_slice<NB>(a.b, bs, 0);
-    __syncthreads();
-  }
-  deposit_slice(a.d, bs, part, smem);
-}
-
 // Batched forms: items[i] = (run, slice of that run).
 struct DepBatchArgs {
   const DepArgs* args;
@@ -989,10 +969,10 @@ struct DiagBatchArgs {
 template <int NB>
 __global__ void __launch_bounds__(kDiagThreads, 2)
     beam_diag_batch_kernel(const __grid_constant__ DiagBatchArgs b) {
-  const int nitems = *b.nitems;
+  const int nitems = *b.nitems * kDepParts;  // (run, slice) items, kDepParts parts each
   for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
-    const int2 w = b.items[it];
-    diag_slice<NB>(b.args[w.x], w.y, 0);
+    const int2 w = b.items[it / kDepParts];
+    diag_slice<NB>(b.args[w.x], w.y, it % kDepParts);
     __syncthreads();
   }
 }
@@ -1024,8 +1004,17 @@ __device__ __forceinline__ void finalize_range(const FinalizeArgs& a, int i0, in
       const int j = i / 9, q = i - 9 * j;
       const int f = j / a.nslice, s = j - f * a.nslice;
       const double* p = a.part[f] + (size_t)s * a.nband[f] * 9 + q;
+      const int nbf = a.nband[f];
       double v = 0.0;
-      for (int b = 0; b < a.nband[f]; ++b) v += p[b * 9];
+      int b = 0;
+      for (; b + 8 <= nbf; b += 8) {  // eight loads in flight, added in band order
+        double t[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) t[k] = p[(b + k) * 9];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) v += t[k];
+      }
+      for (; b < nbf; ++b) v += p[b * 9];
       const int is = (a.nslice + s - a.first_after[f]) % a.nslice;
       a.field_hist[((size_t)f * a.nslice + is) * 9 + q] = v;
     } else if (i < 9 * nf + nb) {
@@ -1402,11 +1391,10 @@ int launch_single(g4b_run* r, const StepArgs& L) {
       beam_step_kernel<0><<<r->nchunk, kStepThreads, 0, c->stream>>>(L.bs);
   }
   if (int rc = check_launch(c, "beam_step_kernel")) return rc;
-  // The beam diagnostics depend only on K1.  A run with slices enough to
-  // fill the GPU twice launches them as a kernel of their own: in a captured
-  // graph a branch beside the deposition and the ADI passes (filling the SMs
-  // those leave idle), joined before the finalize.  A smaller run computes
-  // them in the deposition's CTAs, before each slice's deposition.
+  // The beam diagnostics depend only on K1: in a captured graph they are a
+  // branch beside the deposition and the ADI passes (on SMs those leave
+  // idle), joined before the finalize; direct launches run them after the
+  // deposition.
   auto diag = [&](cudaStream_t st) {
     LaunchScope ls(c, "run_beam_diag");
     if (r->desc.nbunch == 1)
@@ -1415,32 +1403,20 @@ int launch_single(g4b_run* r, const StepArgs& L) {
       beam_diag_kernel<kMaxBunch><<<r->nslice * kDepParts, kDiagThreads, 0, st>>>(L.bd);
     return check_launch(c, "beam_diag_kernel");
   };
-  const bool own = r->nslice >= 2 * c->sm_count;
-  const bool branch = own && r->capturing;
+  const bool branch = r->capturing;
   if (branch) {
     G4B_CUDA_TRY(cudaEventRecord(r->ev_fork, c->stream));
     G4B_CUDA_TRY(cudaStreamWaitEvent(r->aux, r->ev_fork, 0));
     if (int rc = diag(r->aux)) return rc;
     G4B_CUDA_TRY(cudaEventRecord(r->ev_join, r->aux));
   }
-  if (own) {
-    {
-      LaunchScope ls(c, "run_deposit");
-      deposit_kernel<<<r->nslice * kDepSplit, kDepThreads, kDepSmem, c->stream>>>(L.dd);
-    }
-    if (int rc = check_launch(c, "deposit_kernel")) return rc;
-    if (!branch)
-      if (int rc = diag(c->stream)) return rc;
-  } else {
-    LaunchScope ls(c, "run_deposit_diag");
-    const DepDiagLaunch dl{L.dd, L.bd};
-    if (r->desc.nbunch == 1)
-      deposit_diag_kernel<1><<<r->nslice * kDepSplit, kDepThreads, kDepSmem, c->stream>>>(dl);
-    else
-      deposit_diag_kernel<kMaxBunch><<<r->nslice * kDepSplit, kDepThreads, kDepSmem,
-                                       c->stream>>>(dl);
+  {
+    LaunchScope ls(c, "run_deposit");
+    deposit_kernel<<<r->nslice * kDepSplit, kDepThreads, kDepSmem, c->stream>>>(L.dd);
   }
-  if (int rc = check_launch(c, "deposit_diag_kernel")) return rc;
+  if (int rc = check_launch(c, "deposit_kernel")) return rc;
+  if (!branch)
+    if (int rc = diag(c->stream)) return rc;
   for (int f = 0; f < r->nfield; ++f)
     if (int rc = adi_launch(r->fs[f].f, L.adi[f])) return rc;
   if (branch) G4B_CUDA_TRY(cudaStreamWaitEvent(c->stream, r->ev_join, 0));
@@ -1575,10 +1551,6 @@ int g4b_run_create(g4b_ctx* c, const g4b_run_desc* d, const int64_t* off, g4b_ru
   r->step_doubles = (size_t)d->nslice * (r->rec_beam + 9 * d->nfield);
   cudaFuncSetAttribute(deposit_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)kDepSmem);
-  cudaFuncSetAttribute(deposit_diag_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)kDepSmem);
-  cudaFuncSetAttribute(deposit_diag_kernel<kMaxBunch>,
-                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDepSmem);
   *out = r;
   return G4B_OK;
 }
