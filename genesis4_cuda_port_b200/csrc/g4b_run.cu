@@ -691,6 +691,7 @@ constexpr int kDepThreads = 256;
 // bands is done by two CTAs side by side instead of one after the other)
 constexpr int kDepSplit = 2;
 constexpr int kDepAccU = 4;           // particles in flight per thread
+constexpr int kDepWideThreads = 512;  // the deposition CTA of runs of few slices
 constexpr int kDepMaxCells = 8192;    // output cells per band (a multiple of 4)
 constexpr int kDepMaxWidth = 896;     // tile width bound: mixed ngrid <= 880
 // re and im planes, then the counts per base cell ((hb + 1) bw <= cells + width)
@@ -706,11 +707,14 @@ __device__ __forceinline__ float dep_charge(const DepArgs& a, const float2 xy, c
   return __fdividef(sqrtf(faw2), a.gref_f + dg);
 }
 
+// T threads per CTA, U particles in flight per thread: the integer sums and
+// the maxima do not depend on either, so every instance gives the same bits.
+template <int T = kDepThreads, int U = kDepAccU>
 __device__ __forceinline__ void deposit_slice(const DepArgs& a, const int bs, const int part,
                                               unsigned char* smem) {
   __shared__ int4 sbox[kRunFields];
-  __shared__ int wsum[kDepThreads / 32];
-  __shared__ float wmax[kDepThreads / 32];
+  __shared__ int wsum[T / 32];
+  __shared__ float wmax[T / 32];
   const int tid = threadIdx.x, w = tid >> 5, l = tid & 31;
   const int64_t p0 = a.off[bs];
   const int np = (int)(a.off[bs + 1] - p0);  // at most 65536 particles per slice
@@ -783,13 +787,13 @@ __device__ __forceinline__ void deposit_slice(const DepArgs& a, const int bs, co
       // quiet-start beamlet in one cell adds its count with one atomic
       float qloc = 0.f;
       auto pass = [&](const bool count, const bool add, const float Sf, const float qc) {
-        for (int pb = tid & ~31; pb < np; pb += kDepAccU * kDepThreads) {
-          float2 lxy[kDepAccU];
-          float ldg[kDepAccU];
-          double lth[kDepAccU];
+        for (int pb = tid & ~31; pb < np; pb += U * T) {
+          float2 lxy[U];
+          float ldg[U];
+          double lth[U];
 #pragma unroll
-          for (int u = 0; u < kDepAccU; ++u) {
-            const int p = pb + u * kDepThreads + l;
+          for (int u = 0; u < U; ++u) {
+            const int p = pb + u * T + l;
             if (p < np) {
               lxy[u] = xyp[p];
               ldg[u] = dgp[p];
@@ -797,8 +801,8 @@ __device__ __forceinline__ void deposit_slice(const DepArgs& a, const int bs, co
             }
           }
 #pragma unroll
-          for (int u = 0; u < kDepAccU; ++u) {
-            const int p = pb + u * kDepThreads + l;
+          for (int u = 0; u < U; ++u) {
+            const int p = pb + u * T + l;
             int cidx = -1, ey = 0, ex = 0;
             int c[8] = {0, 0, 0, 0, 0, 0, 0, 0};
             if (p < np) {
@@ -863,7 +867,7 @@ __device__ __forceinline__ void deposit_slice(const DepArgs& a, const int bs, co
       auto zero_acc = [&]() {
         int4* r4 = reinterpret_cast<int4*>(are);
         int4* i4 = reinterpret_cast<int4*>(aim);
-        for (int i = tid; i < (nout + 3) >> 2; i += kDepThreads) {
+        for (int i = tid; i < (nout + 3) >> 2; i += T) {
           r4[i] = make_int4(0, 0, 0, 0);
           i4[i] = make_int4(0, 0, 0, 0);
         }
@@ -871,7 +875,7 @@ __device__ __forceinline__ void deposit_slice(const DepArgs& a, const int bs, co
       __syncthreads();
       {
         int4* h4 = reinterpret_cast<int4*>(hist);
-        for (int i = tid; i < (nbase + 3) >> 2; i += kDepThreads) h4[i] = make_int4(0, 0, 0, 0);
+        for (int i = tid; i < (nbase + 3) >> 2; i += T) h4[i] = make_int4(0, 0, 0, 0);
       }
       const bool single = m_use > 0 && q_use > 0.f && q_use < 3.0e38f;
       double S = 0.0;
@@ -891,7 +895,7 @@ __device__ __forceinline__ void deposit_slice(const DepArgs& a, const int bs, co
       __syncthreads();
       // the largest number M of contributions any output cell receives
       int mloc = 0;
-      for (int o = tid; o < nout; o += kDepThreads) {
+      for (int o = tid; o < nout; o += T) {
         const int r = (int)(((float)o + 0.5f) * inv_bw), x = o - r * bw;
         int m = hist[(r + 1) * bw + x] + hist[r * bw + x];
         if (x > 0) m += hist[(r + 1) * bw + x - 1] + hist[r * bw + x - 1];
@@ -908,7 +912,7 @@ __device__ __forceinline__ void deposit_slice(const DepArgs& a, const int bs, co
       __syncthreads();
       int M = wsum[0];
       float qm = wmax[0];
-      for (int i = 1; i < kDepThreads / 32; ++i) {
+      for (int i = 1; i < T / 32; ++i) {
         M = max(M, wsum[i]);
         qm = fmaxf(qm, wmax[i]);
       }
@@ -916,7 +920,7 @@ __device__ __forceinline__ void deposit_slice(const DepArgs& a, const int bs, co
       float2* out = F.src + (size_t)target * F.cap + (size_t)yb * bw;
       if (M == 0 || !(qm > 0.f) || !(qm < 3.0e38f)) {
         if (M > 0) atomicOr(a.err, kErrFixedRange);  // non-finite charge
-        for (int i = tid; i < nout; i += kDepThreads) out[i] = make_float2(0.f, 0.f);
+        for (int i = tid; i < nout; i += T) out[i] = make_float2(0.f, 0.f);
         continue;
       }
       q_seen = fmaxf(q_seen, qm);
@@ -929,7 +933,7 @@ __device__ __forceinline__ void deposit_slice(const DepArgs& a, const int bs, co
       }
       __syncthreads();
       const double unscale = scl / S;
-      for (int i = tid; i < nout; i += kDepThreads)
+      for (int i = tid; i < nout; i += T)
         out[i] = make_float2((float)((double)are[i] * unscale), (float)((double)aim[i] * unscale));
     }
     if (tid == 0 && part * hband < bh) F.mpred[bs * kDepSplit + part] = m_seen;
@@ -940,6 +944,15 @@ __device__ __forceinline__ void deposit_slice(const DepArgs& a, const int bs, co
 __global__ void __launch_bounds__(kDepThreads, 2) deposit_kernel(const __grid_constant__ DepArgs a) {
   extern __shared__ __align__(128) unsigned char smem[];
   deposit_slice(a, blockIdx.x / kDepSplit, blockIdx.x % kDepSplit, smem);
+}
+
+// Runs of few slices (less than one CTA per SM): a slice's particles spread
+// over kDepWideThreads threads of one CTA per SM, twice the particles in
+// flight of a 256-thread CTA (same results).
+__global__ void __launch_bounds__(kDepWideThreads, 1)
+    deposit_wide_kernel(const __grid_constant__ DepArgs a) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  deposit_slice<kDepWideThreads, kDepAccU>(a, blockIdx.x / kDepSplit, blockIdx.x % kDepSplit, smem);
 }
 
 // Batched forms: items[i] = (run, slice of that run).
@@ -1412,7 +1425,10 @@ int launch_single(g4b_run* r, const StepArgs& L) {
   }
   {
     LaunchScope ls(c, "run_deposit");
-    deposit_kernel<<<r->nslice * kDepSplit, kDepThreads, kDepSmem, c->stream>>>(L.dd);
+    if (r->nslice * kDepSplit < c->sm_count)
+      deposit_wide_kernel<<<r->nslice * kDepSplit, kDepWideThreads, kDepSmem, c->stream>>>(L.dd);
+    else
+      deposit_kernel<<<r->nslice * kDepSplit, kDepThreads, kDepSmem, c->stream>>>(L.dd);
   }
   if (int rc = check_launch(c, "deposit_kernel")) return rc;
   if (!branch)
@@ -1550,6 +1566,8 @@ int g4b_run_create(g4b_ctx* c, const g4b_run_desc* d, const int64_t* off, g4b_ru
   }
   r->step_doubles = (size_t)d->nslice * (r->rec_beam + 9 * d->nfield);
   cudaFuncSetAttribute(deposit_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)kDepSmem);
+  cudaFuncSetAttribute(deposit_wide_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)kDepSmem);
   *out = r;
   return G4B_OK;
