@@ -1019,15 +1019,15 @@ __device__ __forceinline__ void finalize_range(const FinalizeArgs& a, int i0, in
       const double* p = a.part[f] + (size_t)s * a.nband[f] * 9 + q;
       const int nbf = a.nband[f];
       double v = 0.0;
-      int b = 0;
-      for (; b + 8 <= nbf; b += 8) {  // eight loads in flight, added in band order
-        double t[8];
+      for (int b0 = 0; b0 < nbf; b0 += 32) {  // up to 32 loads in flight, added in band order
+        const int m = min(32, nbf - b0);
+        double t[32];
 #pragma unroll
-        for (int k = 0; k < 8; ++k) t[k] = p[(b + k) * 9];
+        for (int k = 0; k < 32; ++k) t[k] = k < m ? p[(b0 + k) * 9] : 0.0;
 #pragma unroll
-        for (int k = 0; k < 8; ++k) v += t[k];
+        for (int k = 0; k < 32; ++k)
+          if (k < m) v += t[k];
       }
-      for (; b < nbf; ++b) v += p[b * 9];
       const int is = (a.nslice + s - a.first_after[f]) % a.nslice;
       a.field_hist[((size_t)f * a.nslice + is) * 9 + q] = v;
     } else if (i < 9 * nf + nb) {
