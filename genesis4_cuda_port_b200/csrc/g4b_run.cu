@@ -11,9 +11,10 @@
 //                  (+corrector), and each slice's bounding box of touched
 //                  cells (integer atomics, order independent);
 //   K2 deposit : per slice, the deterministic exact-integer deposition of
-//                  every field's source into a compact tile; beside it (a
-//                  branch of the captured graph) the beam diagnostics (FP64
-//                  sums);
+//                  every field's source into a compact tile, and the beam
+//                  diagnostics (FP64 sums): a branch of the captured graph
+//                  beside the deposition in runs that fill the GPU, in the
+//                  deposition's CTAs (first) in smaller runs;
 //   K3/K4 ADI passes per field (pass Y also zeroes the planes this step's
 //                  slippage zeroes and writes field-diagnostic partials);
 //   K5 diag_finalize : per-slice beam and field diagnostics into the history
@@ -545,7 +546,8 @@ __device__ __forceinline__ void diag_slice(const BeamDiagArgs& a, const int bs, 
   double bre[NB], bim[NB];
 #pragma unroll
   for (int h = 0; h < NB; ++h) bre[h] = bim[h] = 0.0;
-  for (int pb = tid; pb < np; pb += U * kDiagThreads) {
+  // in a wider CTA only the first kDiagThreads threads sum (the same layout)
+  for (int pb = tid < kDiagThreads ? tid : np; pb < np; pb += U * kDiagThreads) {
     float2 lxy[U], lpp[U];
     float ldg[U];
     double lth[U];
@@ -600,7 +602,7 @@ __device__ __forceinline__ void diag_slice(const BeamDiagArgs& a, const int bs, 
   for (int k = 0; k < 12; ++k) {
     double t = sm[k];
     for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
-    if (l == 0) dpart[w][k < 10 ? k + 2 : k - 10] = t;
+    if (l == 0 && w < kDiagThreads / 32) dpart[w][k < 10 ? k + 2 : k - 10] = t;
   }
 #pragma unroll
   for (int i = 0; i < 5; ++i) {
@@ -609,7 +611,7 @@ __device__ __forceinline__ void diag_slice(const BeamDiagArgs& a, const int bs, 
       lo = fminf(lo, __shfl_xor_sync(0xffffffffu, lo, o));
       hi = fmaxf(hi, __shfl_xor_sync(0xffffffffu, hi, o));
     }
-    if (l == 0) {
+    if (l == 0 && w < kDiagThreads / 32) {
       dpart[w][13 + 2 * i] = lo;
       dpart[w][14 + 2 * i] = hi;
     }
@@ -622,7 +624,7 @@ __device__ __forceinline__ void diag_slice(const BeamDiagArgs& a, const int bs, 
       tr += __shfl_xor_sync(0xffffffffu, tr, o);
       ti += __shfl_xor_sync(0xffffffffu, ti, o);
     }
-    if (l == 0) {
+    if (l == 0 && w < kDiagThreads / 32) {
       dpart[w][kBeamRec + 2 * h] = tr;
       dpart[w][kBeamRec + 2 * h + 1] = ti;
     }
@@ -946,13 +948,27 @@ __global__ void __launch_bounds__(kDepThreads, 2) deposit_kernel(const __grid_co
   deposit_slice(a, blockIdx.x / kDepSplit, blockIdx.x % kDepSplit, smem);
 }
 
-// Runs of few slices (less than one CTA per SM): a slice's particles spread
-// over kDepWideThreads threads of one CTA per SM, twice the particles in
-// flight of a 256-thread CTA (same results).
-__global__ void __launch_bounds__(kDepWideThreads, 1)
-    deposit_wide_kernel(const __grid_constant__ DepArgs a) {
+// The beam diagnostics and the deposition of a slice by one CTA, one after
+// the other: the form of runs too small to fill the GPU (a graph branch for
+// their diagnostics would cost more to instantiate than it saves).  Runs of
+// fewer slices than SMs take T = 512 threads, twice the particles in flight
+// of a 256-thread CTA for the deposition; the diagnostics use the first
+// kDiagThreads threads, so every form gives the same bits.
+struct DepDiagLaunch {
+  DepArgs d;
+  BeamDiagArgs b;
+};
+
+template <int NB, int T>
+__global__ void __launch_bounds__(T, 512 / T)
+    deposit_diag_kernel(const __grid_constant__ DepDiagLaunch a) {
   extern __shared__ __align__(128) unsigned char smem[];
-  deposit_slice<kDepWideThreads, kDepAccU>(a, blockIdx.x / kDepSplit, blockIdx.x % kDepSplit, smem);
+  const int bs = blockIdx.x / kDepSplit, part = blockIdx.x % kDepSplit;
+  if (part == 0) {
+    diag_slice<NB>(a.b, bs, 0);
+    __syncthreads();
+  }
+  deposit_slice<T, kDepAccU>(a.d, bs, part, smem);
 }
 
 // Batched forms: items[i] = (run, slice of that run).
@@ -1404,10 +1420,11 @@ int launch_single(g4b_run* r, const StepArgs& L) {
       beam_step_kernel<0><<<r->nchunk, kStepThreads, 0, c->stream>>>(L.bs);
   }
   if (int rc = check_launch(c, "beam_step_kernel")) return rc;
-  // The beam diagnostics depend only on K1: in a captured graph they are a
-  // branch beside the deposition and the ADI passes (on SMs those leave
-  // idle), joined before the finalize; direct launches run them after the
-  // deposition.
+  // The beam diagnostics depend only on K1.  A run with slices enough to
+  // fill the GPU twice launches them as a kernel of their own: in a captured
+  // graph a branch beside the deposition and the ADI passes (on SMs those
+  // leave idle), joined before the finalize.  A smaller run computes them in
+  // the deposition's CTAs, before each slice's deposition.
   auto diag = [&](cudaStream_t st) {
     LaunchScope ls(c, "run_beam_diag");
     if (r->desc.nbunch == 1)
@@ -1416,23 +1433,41 @@ int launch_single(g4b_run* r, const StepArgs& L) {
       beam_diag_kernel<kMaxBunch><<<r->nslice * kDepParts, kDiagThreads, 0, st>>>(L.bd);
     return check_launch(c, "beam_diag_kernel");
   };
-  const bool branch = r->capturing;
+  const bool own = r->nslice >= 2 * c->sm_count;
+  const bool branch = own && r->capturing;
   if (branch) {
     G4B_CUDA_TRY(cudaEventRecord(r->ev_fork, c->stream));
     G4B_CUDA_TRY(cudaStreamWaitEvent(r->aux, r->ev_fork, 0));
     if (int rc = diag(r->aux)) return rc;
     G4B_CUDA_TRY(cudaEventRecord(r->ev_join, r->aux));
   }
-  {
-    LaunchScope ls(c, "run_deposit");
-    if (r->nslice * kDepSplit < c->sm_count)
-      deposit_wide_kernel<<<r->nslice * kDepSplit, kDepWideThreads, kDepSmem, c->stream>>>(L.dd);
-    else
+  if (own) {
+    {
+      LaunchScope ls(c, "run_deposit");
       deposit_kernel<<<r->nslice * kDepSplit, kDepThreads, kDepSmem, c->stream>>>(L.dd);
+    }
+    if (int rc = check_launch(c, "deposit_kernel")) return rc;
+    if (!branch)
+      if (int rc = diag(c->stream)) return rc;
+  } else {
+    LaunchScope ls(c, "run_deposit_diag");
+    const DepDiagLaunch dl{L.dd, L.bd};
+    const unsigned grid = (unsigned)(r->nslice * kDepSplit);
+    const bool wide = r->nslice * kDepSplit < c->sm_count;
+    if (r->desc.nbunch == 1) {
+      if (wide)
+        deposit_diag_kernel<1, kDepWideThreads><<<grid, kDepWideThreads, kDepSmem, c->stream>>>(dl);
+      else
+        deposit_diag_kernel<1, kDepThreads><<<grid, kDepThreads, kDepSmem, c->stream>>>(dl);
+    } else {
+      if (wide)
+        deposit_diag_kernel<kMaxBunch, kDepWideThreads>
+            <<<grid, kDepWideThreads, kDepSmem, c->stream>>>(dl);
+      else
+        deposit_diag_kernel<kMaxBunch, kDepThreads><<<grid, kDepThreads, kDepSmem, c->stream>>>(dl);
+    }
+    if (int rc = check_launch(c, "deposit_diag_kernel")) return rc;
   }
-  if (int rc = check_launch(c, "deposit_kernel")) return rc;
-  if (!branch)
-    if (int rc = diag(c->stream)) return rc;
   for (int f = 0; f < r->nfield; ++f)
     if (int rc = adi_launch(r->fs[f].f, L.adi[f])) return rc;
   if (branch) G4B_CUDA_TRY(cudaStreamWaitEvent(c->stream, r->ev_join, 0));
@@ -1567,8 +1602,14 @@ int g4b_run_create(g4b_ctx* c, const g4b_run_desc* d, const int64_t* off, g4b_ru
   r->step_doubles = (size_t)d->nslice * (r->rec_beam + 9 * d->nfield);
   cudaFuncSetAttribute(deposit_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)kDepSmem);
-  cudaFuncSetAttribute(deposit_wide_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)kDepSmem);
+  cudaFuncSetAttribute(deposit_diag_kernel<1, kDepThreads>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDepSmem);
+  cudaFuncSetAttribute(deposit_diag_kernel<kMaxBunch, kDepThreads>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDepSmem);
+  cudaFuncSetAttribute(deposit_diag_kernel<1, kDepWideThreads>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDepSmem);
+  cudaFuncSetAttribute(deposit_diag_kernel<kMaxBunch, kDepWideThreads>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDepSmem);
   *out = r;
   return G4B_OK;
 }
