@@ -72,6 +72,7 @@ _SIGS = {
     "g4b_ctx_synchronize": (C.c_int, [C.c_void_p]),
     "g4b_ctx_launch_count": (C.c_int, [C.c_void_p, c_uint64_p]),
     "g4b_ctx_sm_count": (C.c_int, [C.c_void_p, c_int_p]),
+    "g4b_ctx_selftest_wait": (C.c_int, [C.c_void_p, C.c_uint, c_int_p]),
     "g4b_ctx_profile": (C.c_int, [C.c_void_p, C.c_int]),
     "g4b_ctx_profile_read": (C.c_int, [C.c_void_p, C.c_int, C.c_char_p, c_uint64_p,
                                        c_double_p, c_int_p]),

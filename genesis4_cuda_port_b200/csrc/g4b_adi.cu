@@ -93,9 +93,11 @@ template <typename T, int M, int L> struct AdiBlocks {
 // A row is solved by L lanes holding M elements each: L = 32, one row per
 // warp; L = 16, two rows per warp (one per half), for rows that fit 16 M
 // slots more closely than 32 M.  bar is an initialised mbarrier; parity the
-// phase this band waits on.
+// phase this band waits on.  Returns false, with nothing solved or stored, if
+// the band's rows did not arrive within the bounded wait (the device error
+// flag then says so); the result is the same in every thread of the CTA.
 template <typename T, int M, bool PX, int L>
-__device__ __forceinline__ void adi_band(const AdiPassArgs& a, const CUtensorMap* tm_out, int s,
+__device__ __forceinline__ bool adi_band(const AdiPassArgs& a, const CUtensorMap* tm_out, int s,
                                          int band, unsigned char* smem, uint64_t* bar,
                                          uint32_t parity) {
   using C = typename CT<T>::type;
@@ -147,8 +149,8 @@ __device__ __forceinline__ void adi_band(const AdiPassArgs& a, const CUtensorMap
         for (int k = tid; k < ld; k += blockDim.x) tile[t * ld + k] = C{0, 0};
     }
   }
-  ptx::mbar_wait_bounded(bar, parity, a.err);
-  __syncthreads();
+  const bool arrived = ptx::mbar_wait_bounded(bar, parity, a.err);
+  if (!__syncthreads_and(arrived)) return false;
 
   const T r = (T)a.r;
   const C* tab = reinterpret_cast<const C*>(a.tab);
@@ -354,6 +356,7 @@ __device__ __forceinline__ void adi_band(const AdiPassArgs& a, const CUtensorMap
     ptx::bulk_commit();
     ptx::bulk_wait_read0();
   }
+  return true;
 }
 
 template <typename T, int M, bool PX, int L>
@@ -388,7 +391,9 @@ __global__ void __launch_bounds__(BandW<T, L>::value * 32, AdiBlocks<T, M, L>::v
     const int4 w = b.items[it];
     const CUtensorMap* tm = b.maps + w.x;
     if (threadIdx.x == 0) ptx::fence_tensormap_acquire(tm);
-    adi_band<T, M, PX, L>(b.args[w.x], tm, w.y, w.z, smem, &bar, parity);
+    // a band whose rows never arrived leaves the barrier's phase open: stop
+    // (the error flag reports it) rather than wait on it again
+    if (!adi_band<T, M, PX, L>(b.args[w.x], tm, w.y, w.z, smem, &bar, parity)) return;
     parity ^= 1u;
     __syncthreads();
   }

@@ -374,6 +374,51 @@ int g4b_ctx_sm_count(g4b_ctx* c, int* count) {
   return G4B_OK;
 }
 
+}  // extern "C"
+
+namespace {
+// One CTA arrives on an mbarrier announcing 16 bytes that no copy will ever
+// deliver (no asynchronous operation targets this barrier), so the phase
+// cannot complete: the bounded wait gives up after `limit` polls, sets the
+// error word and returns.
+__global__ void wait_selftest_kernel(int* err, uint32_t limit, int* arrived) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x == 0) {
+    g4b::ptx::mbar_init(&bar, 1);
+    g4b::ptx::fence_mbar_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) g4b::ptx::mbar_expect_tx(&bar, 16u);
+  const bool ok = g4b::ptx::mbar_wait_bounded(&bar, 0u, err, limit);
+  if (threadIdx.x == 0) *arrived = ok ? 1 : 0;
+}
+}  // namespace
+
+extern "C" {
+
+int g4b_ctx_selftest_wait(g4b_ctx* c, unsigned spin_limit, int* timed_out) {
+  if (!c || !timed_out) return fail(G4B_ERR_ARG, "g4b_ctx_selftest_wait: null arg");
+  if (spin_limit == 0 || spin_limit > (1u << 20))
+    return fail(G4B_ERR_RANGE, "g4b_ctx_selftest_wait: spin_limit must be in [1, 2^20]");
+  G4B_CUDA_TRY(cudaSetDevice(c->device));
+  int* d = nullptr;  // the kernel's "arrived" answer
+  G4B_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void**>(&d), sizeof(int), c->stream));
+  G4B_CUDA_TRY(cudaMemsetAsync(d, 0xff, sizeof(int), c->stream));
+  wait_selftest_kernel<<<1, 32, 0, c->stream>>>(c->d_error, spin_limit, d);
+  count_launch(c);
+  const cudaError_t le = cudaGetLastError();
+  int arrived = -1;
+  cudaError_t e = le;
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(&arrived, d, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
+  cudaFreeAsync(d, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "g4b_ctx_selftest_wait");
+  *timed_out = arrived == 0 ? 1 : 0;
+  // the kernel's timeout is reported (and cleared) like any device error
+  return read_device_error(c, "g4b_ctx_selftest_wait");
+}
+
 // ------------------------------------------------------------------ field ---
 
 int g4b_field_create(g4b_ctx* c, int nslice, int ngrid, double gridmax,

@@ -217,7 +217,18 @@ struct DiagScratch {
   double* d = nullptr;
   size_t cap = 0;
 };
-// scratch keyed by the owning object; freed with the process (small)
+// Grow-on-demand scratch of the diagnostics entry points, one buffer per
+// calling host thread and device: a thread may drive contexts on several
+// devices, and a buffer is only ever used (and freed) with its own device
+// current.  Freed with the process (small).
+constexpr int kDiagScratchDevices = 64;
+int diag_scratch(int device, DiagScratch** out) {
+  static thread_local DiagScratch per_device[kDiagScratchDevices];
+  if (device < 0 || device >= kDiagScratchDevices)
+    return fail(G4B_ERR_RANGE, "diagnostics: device index above 63");
+  *out = &per_device[device];
+  return G4B_OK;
+}
 int ensure(DiagScratch& s, size_t n) {
   if (s.cap >= n) return G4B_OK;
   if (s.d) cudaFree(s.d);
@@ -276,11 +287,12 @@ int g4b_diag_beam(g4b_beam* b, int nharm, int need_aux, double* stats, double* b
   if (b->precision != G4B_FP64) return fail(G4B_ERR_ARG, "g4b_diag_beam: FP64 beam expected");
   g4b_ctx* c = b->ctx;
   G4B_CUDA_TRY(cudaSetDevice(c->device));
-  static thread_local DiagScratch scratch;
+  DiagScratch* scratch = nullptr;
+  if (int rc = diag_scratch(c->device, &scratch)) return rc;
   const size_t ns = b->nslice;
   const size_t need = ns * 23 + 2 * ns * nharm;
-  if (int rc = ensure(scratch, need)) return rc;
-  double* d_stats = scratch.d;
+  if (int rc = ensure(*scratch, need)) return rc;
+  double* d_stats = scratch->d;
   double* d_bre = d_stats + ns * 23;
   double* d_bim = d_bre + ns * nharm;
   {
@@ -304,10 +316,11 @@ int g4b_diag_field(g4b_field* f, double* stats, double* center) {
   if (!f || !stats || !center) return fail(G4B_ERR_ARG, "g4b_diag_field: null arg");
   g4b_ctx* c = f->ctx;
   G4B_CUDA_TRY(cudaSetDevice(c->device));
-  static thread_local DiagScratch scratch;
+  DiagScratch* scratch = nullptr;
+  if (int rc = diag_scratch(c->device, &scratch)) return rc;
   const size_t ns = f->nslice;
-  if (int rc = ensure(scratch, ns * 9)) return rc;
-  double* d_stats = scratch.d;
+  if (int rc = ensure(*scratch, ns * 9)) return rc;
+  double* d_stats = scratch->d;
   double* d_center = d_stats + ns * 7;
   {
     LaunchScope ls(c, "diag_field");

@@ -283,10 +283,11 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 }
 
 // Bounded wait: returns false (and sets the device error flag) if the phase
-// did not complete within kWaitSpinLimit polls.
+// did not complete within `limit` polls.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity,
-                                                  int* err_flag) {
-  for (uint32_t i = 0; i < kWaitSpinLimit; ++i) {
+                                                  int* err_flag,
+                                                  uint32_t limit = kWaitSpinLimit) {
+  for (uint32_t i = 0; i < limit; ++i) {
     if (mbar_try_wait(bar, parity)) return true;
   }
   atomicOr(err_flag, kErrWaitTimeout);

@@ -527,7 +527,7 @@ template <int NB, int U = kDepDiagU>
 __device__ __forceinline__ void diag_slice(const BeamDiagArgs& a, const int bs, const int part) {
   __shared__ double dpart[kDiagThreads / 32][kBeamRec + 2 * kMaxBunch];
   const int tid = threadIdx.x, w = tid >> 5, l = tid & 31;
-  const int nall = (int)(a.off[bs + 1] - a.off[bs]);  // at most 65536 per slice
+  const int nall = (int)(a.off[bs + 1] - a.off[bs]);  // at most kRunMaxNp per slice
   const int per = (nall + kDepParts - 1) / kDepParts;
   const int first = min(part * per, nall);
   const int64_t p0 = a.off[bs] + first;
@@ -719,7 +719,7 @@ __device__ __forceinline__ void deposit_slice(const DepArgs& a, const int bs, co
   __shared__ float wmax[T / 32];
   const int tid = threadIdx.x, w = tid >> 5, l = tid & 31;
   const int64_t p0 = a.off[bs];
-  const int np = (int)(a.off[bs + 1] - p0);  // at most 65536 particles per slice
+  const int np = (int)(a.off[bs + 1] - p0);  // at most kRunMaxNp per slice
   const float2* xyp = a.xy + p0;
   const float* dgp = a.dg + p0;
   const double* thp = a.th + p0;
@@ -1174,6 +1174,7 @@ void g4b_chicane_matrix(double angle, double lb, double ld, double lt, double* m
 namespace {
 
 constexpr int kRunChunk = 2 * kStepThreads;  // particles per beam-step CTA
+constexpr int kRunMaxNp = 65536;              // particles per slice (deposition scale)
 
 // Every argument of one lattice step of one run.
 struct StepArgs {
@@ -1502,8 +1503,20 @@ std::vector<int> state_key(g4b_run* r) {
 extern "C" {
 
 int g4b_run_create(g4b_ctx* c, const g4b_run_desc* d, const int64_t* off, g4b_run** out) {
-  if (!c || !d || !off || !out) return fail(G4B_ERR_ARG, "g4b_run_create: null arg");
+  if (!d || !off || !out) return fail(G4B_ERR_ARG, "g4b_run_create: null arg");
   *out = nullptr;
+  // The exact-integer deposition scales a slice's contributions so that the
+  // fullest cell of its tile sums to at most 2^30; with at most kRunMaxNp
+  // particles per slice every contribution keeps at least 2^30 / kRunMaxNp =
+  // 2^14 quanta.  Checked before anything touches the device.
+  if (d->nslice > 0)
+    for (int s = 0; s < d->nslice; ++s)
+      if (off[s + 1] - off[s] > kRunMaxNp)
+        return fail(G4B_ERR_RANGE, "g4b_run_create: slice " + std::to_string(s) + " holds " +
+                                       std::to_string(off[s + 1] - off[s]) +
+                                       " particles; the mixed form takes at most " +
+                                       std::to_string(kRunMaxNp) + " per slice");
+  if (!c) return fail(G4B_ERR_ARG, "g4b_run_create: null ctx");
   if (d->nslice <= 0 || d->nfield < 1 || d->nfield > kRunFields || d->nbunch < 1 ||
       d->nbunch > kMaxBunch || !(d->gamma_ref > 1) || !(d->lambda0 > 0) || !(d->sample > 0))
     return fail(G4B_ERR_ARG, "g4b_run_create: bad descriptor");

@@ -92,6 +92,13 @@ int g4b_ctx_synchronize(g4b_ctx* ctx);
 int g4b_ctx_launch_count(g4b_ctx* ctx, uint64_t* count);
 /* SM count of the context's device. */
 int g4b_ctx_sm_count(g4b_ctx* ctx, int* count);
+/* Self-test of the bounded waits every kernel uses on its mbarriers (no
+ * counterpart in the reference, whose kernels have no waits): a one-CTA
+ * kernel waits on an mbarrier phase that nothing completes, gives up after
+ * spin_limit polls (1 .. 2^20), sets the context's device error word and
+ * returns.  *timed_out = 1 when the wait gave up; the call then returns
+ * G4B_ERR_DEVICE ("wait timeout") and leaves the context usable. */
+int g4b_ctx_selftest_wait(g4b_ctx* ctx, unsigned spin_limit, int* timed_out);
 /* Per-kernel CUDA-event timing on the context's stream (the reference only
  * has wall-clock phase timers, src/Core/Gencore.cpp:163-270).  Enabling
  * clears the totals; reading synchronises the stream.  names receives
@@ -230,6 +237,8 @@ typedef struct g4b_run_desc {
   int precision;        /* G4B_MIXED                                        */
 } g4b_run_desc;
 
+/* At most 65536 particles per slice (G4B_ERR_RANGE otherwise): the
+ * exact-integer deposition keeps at least 2^14 quanta per contribution. */
 int g4b_run_create(g4b_ctx* ctx, const g4b_run_desc* desc,
                    const int64_t* slice_offsets, g4b_run** out);
 int g4b_run_destroy(g4b_run* run);

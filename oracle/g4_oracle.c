@@ -12,6 +12,9 @@
 #include "g4_oracle.h"
 
 #include <math.h>
+#ifndef M_PI
+#define M_PI 3.14159265358979323846
+#endif
 #include <stdlib.h>
 #include <string.h>
 #ifdef _OPENMP
@@ -721,4 +724,131 @@ void g4o_step(int nslice, const int64_t* off, const double* current,
     g4o_slippage(nslice, f->ngrid, slippage, sample, time_run, periodic,
                  &f->accuslip, &f->first, f->cells);
   }
+}
+
+/* ---- beam loading: Hammersley quiet start + shot noise ------------------
+ * The loader of upstream GENESIS 1.3 v4 is absent from the reference tree.
+ * This restates, operation for operation, the loader the drop-in host layer
+ * uses (beamlets of nbins particles at Hammersley points with radical
+ * inverses in bases 2, 3, 5, 7, 11 mapped through the inverse normal CDF,
+ * phase base 13; Fawley shot noise from a SplitMix64 stream per slice), so
+ * the CPU baseline starts from the same bits without loading the product. */
+static double g4o_radical_inverse(uint64_t i, unsigned base) {
+  double inv = 1.0 / base, f = inv, r = 0.0;
+  while (i) {
+    r += f * (double)(i % base);
+    i /= base;
+    f *= inv;
+  }
+  return r;
+}
+
+/* Inverse normal CDF: P. J. Acklam's rational approximation (2003) refined by
+ * one Halley step against erfc. */
+static double g4o_inv_normal(double p) {
+  static const double a[] = {-3.969683028665376e+01, 2.209460984245205e+02,
+                             -2.759285104469687e+02, 1.383577518672690e+02,
+                             -3.066479806614716e+01, 2.506628277459239e+00};
+  static const double b[] = {-5.447609879822406e+01, 1.615858368580409e+02,
+                             -1.556989798598866e+02, 6.680131188771972e+01,
+                             -1.328068155288572e+01};
+  static const double c[] = {-7.784894002430293e-03, -3.223964580411365e-01,
+                             -2.400758277161838e+00, -2.549732539343734e+00,
+                             4.374664141464968e+00, 2.938163982698783e+00};
+  static const double d[] = {7.784695709041462e-03, 3.224671290700398e-01,
+                             2.445134137142996e+00, 3.754408661907416e+00};
+  if (p <= 0.0) return -40.0;
+  if (p >= 1.0) return 40.0;
+  double x;
+  const double plow = 0.02425, phigh = 1 - plow;
+  if (p < plow) {
+    const double q = sqrt(-2 * log(p));
+    x = (((((c[0] * q + c[1]) * q + c[2]) * q + c[3]) * q + c[4]) * q + c[5]) /
+        ((((d[0] * q + d[1]) * q + d[2]) * q + d[3]) * q + 1);
+  } else if (p <= phigh) {
+    const double q = p - 0.5, r = q * q;
+    x = (((((a[0] * r + a[1]) * r + a[2]) * r + a[3]) * r + a[4]) * r + a[5]) * q /
+        (((((b[0] * r + b[1]) * r + b[2]) * r + b[3]) * r + b[4]) * r + 1);
+  } else {
+    const double q = sqrt(-2 * log(1 - p));
+    x = -(((((c[0] * q + c[1]) * q + c[2]) * q + c[3]) * q + c[4]) * q + c[5]) /
+        ((((d[0] * q + d[1]) * q + d[2]) * q + d[3]) * q + 1);
+  }
+  const double e = 0.5 * erfc(-x / sqrt(2.0)) - p;
+  const double u = e * sqrt(2 * M_PI) * exp(x * x / 2);
+  return x - u / (1 + x * u / 2);
+}
+
+static double g4o_uniform(uint64_t* s) {
+  *s += 0x9e3779b97f4a7c15ull;
+  uint64_t z = *s;
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+  z ^= z >> 31;
+  return ((double)(z >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+}
+
+static double g4o_normal(uint64_t* s) {
+  const double u1 = g4o_uniform(s), u2 = g4o_uniform(s);
+  return sqrt(-2 * log(u1)) * cos(2 * M_PI * u2);
+}
+
+int g4o_load_beam(const g4o_beam_spec* sp, const double* current, double* x,
+                  double* y, double* px, double* py, double* gamma,
+                  double* theta, int64_t* off) {
+  if (sp->nslice <= 0 || sp->npart < 0 || sp->nbins <= 0 || sp->npart % sp->nbins)
+    return 1;
+  const int nbl = sp->npart / sp->nbins;
+  const double gref = sp->gamma0;
+  const double epx = sp->ex / gref, epy = sp->ey / gref;
+  const double sx = sqrt(epx * sp->betax), sy = sqrt(epy * sp->betay);
+  const double spx = sqrt(epx / sp->betax), spy = sqrt(epy / sp->betay);
+  const double twopi = 2 * M_PI;
+  const double ce = 1.602176634e-19, c0 = 299792458.0;
+  off[0] = 0;
+  for (int s = 0; s < sp->nslice; ++s) off[s + 1] = (int64_t)(s + 1) * sp->npart;
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int s = 0; s < sp->nslice; ++s) {
+    uint64_t rng = sp->seed * 0x100000001b3ull + (uint64_t)s * 0x9e3779b97f4a7c15ull + 1;
+    const int64_t base = (int64_t)s * sp->npart;
+    const int nbl1 = nbl > 1 ? nbl : 1;
+    const double ne = current[s] * sp->slicelength / (ce * c0) / nbl1;
+    for (int j = 0; j < nbl; ++j) {
+      const uint64_t idx = (uint64_t)s * nbl + j + 1;
+      const double g1 = g4o_inv_normal(g4o_radical_inverse(idx, 2));
+      const double g2 = g4o_inv_normal(g4o_radical_inverse(idx, 3));
+      const double g3 = g4o_inv_normal(g4o_radical_inverse(idx, 5));
+      const double g4 = g4o_inv_normal(g4o_radical_inverse(idx, 7));
+      const double g5 = g4o_inv_normal(g4o_radical_inverse(idx, 11));
+      const double th0 = twopi / sp->nbins * g4o_radical_inverse(idx, 13);
+      const double xv = sx * g1 + sp->xcenter;
+      const double yv = sy * g3 + sp->ycenter;
+      const double xp = spx * (g2 - sp->alphax * g1);
+      const double yp = spy * (g4 - sp->alphay * g3);
+      const double gv = gref + sp->delgam * g5;
+      const double pxv = gv * xp + sp->pxcenter;
+      const double pyv = gv * yp + sp->pycenter;
+      double an[64], bn[64];
+      const int nh = sp->nbins / 2;
+      for (int h = 1; h <= nh && h <= 64; ++h) {
+        const double sig = (sp->shotnoise && ne > 0) ? sqrt(2.0 / ne) / h : 0.0;
+        an[h - 1] = sig * g4o_normal(&rng);
+        bn[h - 1] = sig * g4o_normal(&rng);
+      }
+      for (int k = 0; k < sp->nbins; ++k) {
+        const int64_t p = base + (int64_t)j * sp->nbins + k;
+        const double th = th0 + twopi * k / sp->nbins;
+        double dth = 0.0;
+        for (int h = 1; h <= nh && h <= 64; ++h)
+          dth += an[h - 1] * cos(h * th) + bn[h - 1] * sin(h * th);
+        x[p] = xv;
+        y[p] = yv;
+        px[p] = pxv;
+        py[p] = pyv;
+        gamma[p] = gv;
+        theta[p] = th + dth;
+      }
+    }
+  }
+  return 0;
 }

@@ -118,6 +118,20 @@ void g4o_step(int nslice, const int64_t* off, const double* current,
               double* px, double* py, double* gamma, double* theta,
               double* work);
 
+/* Beam loading: Hammersley quiet start + shot noise, the same operations as
+ * the drop-in host layer's loader (the upstream GENESIS loader is absent from
+ * the reference tree).  Fields match g4h_beam_spec. */
+typedef struct g4o_beam_spec {
+  int nslice, npart, nbins, shotnoise;
+  uint64_t seed;
+  double gamma0, delgam, ex, ey, betax, betay, alphax, alphay;
+  double xcenter, ycenter, pxcenter, pycenter, reflength, slicelength;
+} g4o_beam_spec;
+
+int g4o_load_beam(const g4o_beam_spec* spec, const double* current, double* x,
+                  double* y, double* px, double* py, double* gamma,
+                  double* theta, int64_t* slice_offsets);
+
 /* Threads the OpenMP runtime uses (for reporting). */
 int g4o_num_threads(void);
 void g4o_set_num_threads(int n);

@@ -1,0 +1,186 @@
+"""The CUDA path and the oracle against the reference's own CUDA classes, live.
+
+oracle/_ref/libg4ref.so is the reference's FieldSolverADICUDA, BeamSolverCUDA,
+TrackBeamCUDA, ControlCUDA and DiagnosticCUDA (src/Core/*.cpp), compiled
+unmodified from the reference tree (oracle/ref/Makefile).  These tests run it
+beside the FP64 drop-in kernels and the oracle at the configurations' grid
+sizes (ngrid 151, 201, and 513, where the reference switches from PCR to
+its Thomas fallback), and compare the drop-in deck's step-0 diagnostic
+records with DiagnosticCUDA::calc on the same loaded beam and field.
+Tolerance 1e-12 of the largest magnitude (summation order differs: the
+reference adds the source with FP64 atomics and solves by PCR).
+"""
+import math
+
+import numpy as np
+import pytest
+
+from genesis4_cuda_port_b200 import device as dev
+from genesis4_cuda_port_b200 import host
+from oracle import pyoracle as orc
+from oracle import refpy
+from tests import synth
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not refpy.available(),
+                                 reason="oracle/_ref/libg4ref.so not built (needs the "
+                                        "reference tree at build time)")]
+
+
+def _rel(a, b):
+    return float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = dev.Context(0)
+    yield c
+    c.synchronize()
+
+
+@pytest.mark.parametrize("nslice,ngrid,gridmax", [(2, 151, 2e-4), (3, 201, 2e-4),
+                                                  (1, 513, 3e-4)])
+def test_field_step_three_ways(ctx, nslice, ngrid, gridmax):
+    off, p = synth.beam(nslice, 1500, seed=ngrid, ragged=nslice > 2)
+    cur = np.linspace(3000.0, 1500.0, nslice)
+    cells = synth.field(nslice, ngrid, gridmax, seed=ngrid + 1, amplitude=1e12)
+    ku2 = synth.KU ** 2
+    st = synth.und_step(ax=1e-6, kx=0.5 * ku2, ky=0.5 * ku2, gradx=10.0)
+    fc = synth.coupling()
+    first = nslice - 1
+    ref = refpy.field_advance(cells, gridmax=gridmax, xlambda=synth.LAMBDA0, first=first,
+                              delz=st.delz, fc=fc, step=st, off=off, current=cur, parts=p)
+    assert _rel(ref, cells) > 1e-3
+    ora = cells.copy()
+    orc.adi_advance(ora, harm=1, gridmax=gridmax, xks=2 * np.pi / synth.LAMBDA0,
+                    delz=st.delz, fc=fc, enabled=True, step=st, off=off, current=cur,
+                    parts=p, first=first)
+    assert _rel(ora, ref) < 1e-12
+    beam = dev.BeamState(ctx, off, synth.GAMMA0)
+    beam.upload(p)
+    beam.set_current(cur)
+    fld = dev.FieldState(ctx, nslice, ngrid, gridmax, synth.LAMBDA0)
+    fld.upload(cells)
+    fld.first = first
+    adi = dev.FieldSolverADICUDA(ctx)
+    adi.init(st.delz, fld.dgrid, fld.xks, ngrid)
+    adi.advance(fld, beam, st, fc=fc)
+    assert _rel(fld.download(), ref) < 1e-12
+    for o in (adi, fld, beam):
+        o.close()
+
+
+def test_push_two_harmonics_three_ways(ctx):
+    nslice = 3
+    off, p = synth.beam(nslice, 2000, seed=41)
+    ku2 = synth.KU ** 2
+    st = synth.und_step(ax=1e-6, kx=0.4 * ku2, ky=0.6 * ku2, grady=8.0, autophase=0.2)
+    spec = [(1, 201, 2e-4, 1), (3, 101, 1.5e-4, 2)]
+    fields, states = [], []
+    for i, (h, n, gm, f0) in enumerate(spec):
+        c = synth.field(nslice, n, gm, seed=50 + i, amplitude=5e10 / h)
+        fields.append(dict(cells=c, first=f0, harm=h, gridmax=gm,
+                           xlambda=synth.LAMBDA0 / h, fc=synth.coupling(harm=h)))
+        fs = dev.FieldState(ctx, nslice, n, gm, synth.LAMBDA0 / h, harm=h)
+        fs.upload(c)
+        fs.first = f0
+        states.append(fs)
+    long_esc = np.array([1e3, -2e3, 5e2])
+    ref = synth.copy_parts(p)
+    refpy.beam_advance(off, st, fields, ref, long_esc=long_esc)
+    ora = synth.copy_parts(p)
+    orc.push(off, st, fields, ora, slice_eloss=-long_esc / 511000.0)
+    beam = dev.BeamState(ctx, off, synth.GAMMA0)
+    beam.upload(p)
+    beam.set_eloss(-long_esc / 511000.0)
+    beam.advance(states, [f["fc"] for f in fields], st)
+    got = beam.download()
+    dg = ref["gamma"] - p["gamma"]
+    for name, q in (("oracle", ora), ("cuda", got)):
+        assert np.max(np.abs((q["gamma"] - p["gamma"]) - dg)) < 1e-12 * np.max(np.abs(dg)), name
+        np.testing.assert_allclose(q["theta"], ref["theta"], rtol=1e-13, atol=0, err_msg=name)
+    for o in states + [beam]:
+        o.close()
+
+
+LAT = """
+D1: DRIFT = { l = 0.2 };
+QF: QUADRUPOLE = { l = 0.1, k1 = 2.0 };
+UND: UNDULATOR = { lambdau = 0.02, nwig = 20, aw = 1.8, helical = False };
+CELL: LINE = { UND, D1, QF, D1 };
+"""
+
+DECK = """
+&setup
+rootname = g
+lattice = g.lat
+beamline = CELL
+lambda0 = 1.0e-10
+gamma0 = 20000
+delz = 0.1
+npart = 512
+nbins = 4
+seed = 7
+&end
+&time
+slen = 1.2e-9
+sample = 4
+&end
+&field
+power = 1e5
+dgrid = 1.5e-4
+ngrid = 65
+waist_size = 30e-6
+&end
+&beam
+current = 2500
+delgam = 1.0
+ex = 0.5e-6
+ey = 0.5e-6
+betax = 12.0
+betay = 9.0
+alphax = 0.3
+alphay = -0.2
+&end
+&track
+bunchharm = 3
+&end
+"""
+
+
+def test_deck_step0_records_match_reference_diagnostics():
+    deck = host.Deck(DECK, LAT)
+    res = deck.run()
+    s = deck.info()
+    lam, ns = s["lambda0"], s["nslice"]
+    spec = host.BeamSpec(nslice=ns, npart=s["npart"], nbins=4, shotnoise=1, seed=7,
+                         gamma0=s["gamma0"], delgam=1.0, ex=0.5e-6, ey=0.5e-6,
+                         betax=s["betax"], betay=s["betay"], alphax=s["alphax"],
+                         alphay=s["alphay"], xcenter=0.0, ycenter=0.0, pxcenter=0.0,
+                         pycenter=0.0, reflength=lam, slicelength=lam * s["sample"])
+    cur = np.full(ns, s["current"])
+    off, p = host.load_beam(spec, cur)
+    plane = host.gaussian_field(65, 1.5e-4, lam, 1e5, 30e-6)
+    cells = np.broadcast_to(plane, (ns, 65, 65)).copy()
+    beam, flds = refpy.diag(off, p, nharm=3, current=cur,
+                            fields=[dict(cells=cells, gridmax=1.5e-4, xlambda=lam)],
+                            slicelength=lam * s["sample"])
+    compared = 0
+    for k, ref in beam.items():
+        if k not in res.beam:
+            continue
+        got = res.beam[k][0]
+        np.testing.assert_allclose(got, ref, rtol=1e-11, atol=1e-13 * np.max(np.abs(ref)),
+                                   err_msg=k)
+        compared += 1
+    assert compared >= 30, compared
+    compared = 0
+    for k, ref in flds[0].items():
+        if k not in res.field[0]:
+            continue
+        got = res.field[0][k][0] if res.field[0][k].ndim > 1 else res.field[0][k][:1]
+        np.testing.assert_allclose(got, ref, rtol=1e-11, atol=1e-13 * np.max(np.abs(ref)),
+                                   err_msg=k)
+        compared += 1
+    assert compared >= 12, compared
+    assert math.isfinite(float(res.field[0]["power"][-1].sum()))
