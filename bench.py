@@ -327,43 +327,110 @@ def _stats(prof, alg, steps):
     return per
 
 
-def accuracy():
-    """P(z) and |b1|(z) of the mixed form against the FP64 oracle on the
-    steady-state FEL (1 slice, 8192 particles, ngrid 151, 1 kW seed, whole
-    lattice): max relative power error and max absolute bunching error."""
-    from genesis4_cuda_port_b200 import device as dev, workloads
-    from oracle import pyoracle as orc
-    wl = workloads.steady_state()
-    off, parts = wl.make_beam()
-    cells = wl.make_field()
-    lat = wl.make_lattice()
-    n = lat.nstep
-    p = {k: v.copy() for k, v in parts.items()}
-    f = dict(cells=cells.copy(), gridmax=wl.gridmax, xlambda=wl.lambda0, fc=0.0, first=0,
-             accuslip=0.0)
-    cur = np.full(1, wl.current)
-    pz, bz = [], []
-    for i in range(n):
-        f["fc"] = lat.fc(i, 1)
-        orc.step(off, cur, lat.steps[i], wl.lambda0, lat.slip[i], 1.0, False, False, [f], p)
-        pz.append(orc.diag_field(f["cells"], 0)[0][0, 0])
-        s_, bre, bim = orc.diag_beam(off, p, 1)
-        bz.append(abs(bre[0, 0] + 1j * bim[0, 0]) / s_[0, 12])
-    ctx = dev.Context(int(os.environ.get("LOCAL_RANK", "0")))
+def fp64_history(ctx, wl, off, parts, cells, lat, nstep):
+    """The FP64 drop-in over nstep lattice steps (per-phase calls through the C
+    ABI): summed power and per-slice |b1| after every step, the final
+    per-slice centre-cell field (beam-slice order) and the final beam sums."""
+    from genesis4_cuda_port_b200 import device as dev
+    beam = dev.BeamState(ctx, off, wl.gamma0)
+    beam.upload(parts)
+    beam.set_current(np.full(wl.nslice, wl.current))
+    fld = dev.FieldState(ctx, wl.nslice, wl.ngrid, wl.gridmax, wl.lambda0)
+    fld.upload(cells)
+    adi = dev.FieldSolverADICUDA(ctx)
+    pz, b1 = [], []
+    for i in range(nstep):
+        st = lat.steps[i]
+        fc = lat.fc(i, 1)
+        beam.track(st, st.delz * 0.5, False)
+        beam.advance([fld], [fc], st)
+        beam.apply_r56(st, wl.lambda0)
+        beam.track(st, st.delz * 0.5, True)
+        adi.init(st.delz, fld.dgrid, fld.xks, wl.ngrid)
+        adi.advance(fld, beam, st, fc)
+        fld.apply_slippage(lat.slip[i], wl.sample, time_run=wl.nslice > 1,
+                           periodic=wl.periodic)
+        fs, cen = fld.diagnostics()
+        bs, bre, bim = beam.diagnostics(1)
+        pz.append(fs[:, 0].sum())
+        b1.append(np.hypot(bre[:, 0], bim[:, 0]) / np.maximum(bs[:, 12], 1))
+    out = {"pz": np.array(pz), "b1": np.array(b1), "center": cen[:, 0] + 1j * cen[:, 1],
+           "gsum": bs[:, 0].sum(), "g2sum": bs[:, 1].sum(), "count": bs[:, 12].sum()}
+    for o in (adi, fld, beam):
+        o.close()
+    return out
+
+
+def mixed_history(ctx, wl, off, parts, cells, lat, nstep):
+    """The fused mixed-precision run over nstep steps (graph replay), with the
+    same quantities as fp64_history read from its device-side history."""
+    from genesis4_cuda_port_b200 import device as dev
     run = dev.Run(ctx, off, fields=[(1, wl.ngrid, wl.gridmax)], lambda0=wl.lambda0,
-                  gamma_ref=wl.gamma0, sample=1.0, time_run=False, nbunch=1)
+                  gamma_ref=wl.gamma0, sample=wl.sample, time_run=wl.nslice > 1,
+                  periodic=wl.periodic, nbunch=1)
     run.upload_beam(parts)
     run.upload_field(0, cells, 0)
-    run.set_current(cur)
-    run.set_lattice(lat.steps, [[lat.fc(i, 1)] for i in range(n)], lat.slip)
-    run.advance(0, n, graph=True)
-    hb, hf = run.history_range(0, n)
-    pm = hf[:, 0, 0, 0]
-    bm = np.abs(hb[:, 0, 23] + 1j * hb[:, 0, 24]) / hb[:, 0, 12]
-    pz, bz = np.array(pz), np.array(bz)
-    return {"workload": wl.name, "pz_rel_err_max": float(np.max(np.abs(pm - pz) / pz)),
-            "b1_abs_err_max": float(np.max(np.abs(bm - bz))),
-            "power_gain": float(pz[-1] / pz[0]), "gates": {"pz_rel": 1e-3, "b1_abs": 1e-3}}
+    run.set_current(np.full(wl.nslice, wl.current))
+    run.set_lattice(lat.steps[:nstep], [[lat.fc(i, 1)] for i in range(nstep)],
+                    lat.slip[:nstep], hist_steps=nstep)
+    run.advance(0, nstep, graph=True)
+    hb, hf = run.history_range(0, nstep)
+    run.close()
+    last_b, last_f = hb[-1], hf[-1, 0]
+    return {"pz": hf[:, 0, :, 0].sum(axis=1),
+            "b1": np.hypot(hb[:, :, 23], hb[:, :, 24]) / np.maximum(hb[:, :, 12], 1),
+            "center": last_f[:, 7] + 1j * last_f[:, 8],
+            "gsum": last_b[:, 0].sum(), "g2sum": last_b[:, 1].sum(),
+            "count": last_b[:, 12].sum()}
+
+
+def accuracy_metrics(test, ref):
+    """Errors of one history against a reference history (dicts as returned by
+    fp64_history / mixed_history): P(z) relative before saturation (up to the
+    reference's power maximum), per-slice |b1|(z) absolute, the on-axis
+    spectrum at the end (|FFT over slices of the centre-cell field|^2,
+    relative to its peak) and the final energy spread (relative)."""
+    pz_t, pz_r = test["pz"], ref["pz"]
+    k = int(np.argmax(pz_r)) + 1
+    spec = lambda h: np.abs(np.fft.fft(h["center"])) ** 2  # noqa: E731
+    sig = lambda h: np.sqrt(max(h["g2sum"] / h["count"] - (h["gsum"] / h["count"]) ** 2, 0.0))  # noqa: E731
+    s_t, s_r = spec(test), spec(ref)
+    return {"pz_rel_err_max": float(np.max(np.abs(pz_t[:k] - pz_r[:k]) / pz_r[:k])),
+            "b1_abs_err_max": float(np.max(np.abs(test["b1"] - ref["b1"]))),
+            "spectrum_rel_err": float(np.max(np.abs(s_t - s_r)) / np.max(s_r)),
+            "energy_spread_rel_err": float(abs(sig(test) - sig(ref)) / sig(ref)),
+            "power_gain": float(pz_r[-1] / pz_r[0]), "b1_final_max": float(ref["b1"][-1].max()),
+            "presaturation_steps": k}
+
+
+ACCURACY_GATES = {"pz_rel": 1e-3, "b1_abs": 1e-3}
+
+
+def accuracy():
+    """The mixed form against the FP64 drop-in (itself held to the FP64
+    oracle within 1e-9 by the GPU tests) on the two exponential-gain
+    workloads: steady state (1 slice, 1 kW seed) and periodic time-dependent
+    SASE (64 slices x 8192 from shot noise, ngrid 201), both over 1032 steps.
+    Reports P(z), |b1|(z), on-axis spectrum and final energy-spread errors
+    beside the power gain."""
+    from genesis4_cuda_port_b200 import device as dev, workloads
+    ctx = dev.Context(int(os.environ.get("LOCAL_RANK", "0")))
+    out = []
+    for wl in (workloads.steady_state_high_gain(), workloads.sase_periodic_high_gain()):
+        off, parts = wl.make_beam()
+        cells = wl.make_field()
+        lat = wl.make_lattice()
+        ref = fp64_history(ctx, wl, off, parts, cells, lat, lat.nstep)
+        mix = mixed_history(ctx, wl, off, parts, cells, lat, lat.nstep)
+        m = accuracy_metrics(mix, ref)
+        m["workload"] = wl.name
+        m["reference"] = "FP64 drop-in"
+        m["gates"] = ACCURACY_GATES
+        m["within_gates"] = (m["pz_rel_err_max"] <= ACCURACY_GATES["pz_rel"] and
+                             m["b1_abs_err_max"] <= ACCURACY_GATES["b1_abs"])
+        out.append(m)
+    ctx.close()
+    return out
 
 
 def _engine_clocks():

@@ -765,11 +765,62 @@ int adi_batch_launch(g4b_ctx* c, cudaStream_t st, int mode, bool px, const AdiBa
   return fail(G4B_ERR_RANGE, "adi: unsupported elements per lane");
 }
 
+// adi_compute_slice_scl + the deterministic deposition
+// (src/Core/FieldSolverADICUDA.cpp:75-174) of an FP64 beam into the field's
+// compact source tiles; shared by the ADI and FFT solvers.
+int fp64_deposit(g4b_field* f, g4b_beam* b, const g4b_step* st, double fc) {
+  g4b_ctx* c = f->ctx;
+  const int harm = f->harm;
+  {
+    LaunchScope ls(c, "slice_scl");
+    slice_scl_kernel<<<(b->nslice + 127) / 128, 128, 0, c->stream>>>(
+        b->nslice, b->d_off, b->d_current, fc, f->xks, f->dgrid, st->delz, kVacimp,
+        kEev, b->d_scl);
+  }
+  if (int rc = check_launch(c, "slice_scl_kernel")) return rc;
+  DepositArgs da{};
+  da.x = b->x;
+  da.y = b->y;
+  da.gamma = b->gamma;
+  da.theta = b->theta;
+  da.off = b->d_off;
+  da.scl = b->d_scl;
+  da.src = static_cast<double2*>(f->src);
+  da.desc = f->desc;
+  da.src_cap = (size_t)f->ngrid * f->ld;
+  da.nslice = f->nslice;
+  da.n = f->ngrid;
+  da.ld = f->ld;
+  da.first = f->first;
+  da.harm = harm;
+  da.gridmax = f->gridmax;
+  da.dgrid = f->dgrid;
+  da.ax = st->ax;
+  da.ay = st->ay;
+  da.kx = st->kx;
+  da.ky = st->ky;
+  da.gradx = st->gradx;
+  da.grady = st->grady;
+  da.err = c->d_error;
+  const size_t acc_bytes = 96 * 1024;
+  da.acc_cells = (int)(acc_bytes / 16);
+  G4B_CUDA_TRY(cudaFuncSetAttribute(deposit_slice_kernel,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)acc_bytes));  // per device, cheap
+  {
+    LaunchScope ls(c, "deposit");
+    deposit_slice_kernel<<<f->nslice, 512, acc_bytes, c->stream>>>(da);
+  }
+  if (int rc = check_launch(c, "deposit_slice_kernel")) return rc;
+  return G4B_OK;
+}
+
 }  // namespace g4b
 
 using namespace g4b;
 
 extern "C" {
+
 
 int g4b_adi_create(g4b_ctx* c, g4b_adi** out) {
   if (!c || !out) return fail(G4B_ERR_ARG, "g4b_adi_create: null arg");
@@ -931,47 +982,7 @@ int g4b_adi_advance(g4b_adi* adi, g4b_field* f, g4b_beam* b, const g4b_step* st,
   const bool use_source = do_source && b->npart > 0;
   const void* src = nullptr;
   if (use_source) {
-    {
-      LaunchScope ls(c, "slice_scl");
-      slice_scl_kernel<<<(b->nslice + 127) / 128, 128, 0, c->stream>>>(
-          b->nslice, b->d_off, b->d_current, fc, f->xks, f->dgrid, st->delz, kVacimp,
-          kEev, b->d_scl);
-    }
-    if (int rc = check_launch(c, "slice_scl_kernel")) return rc;
-    DepositArgs da{};
-    da.x = b->x;
-    da.y = b->y;
-    da.gamma = b->gamma;
-    da.theta = b->theta;
-    da.off = b->d_off;
-    da.scl = b->d_scl;
-    da.src = static_cast<double2*>(f->src);
-    da.desc = f->desc;
-    da.src_cap = (size_t)f->ngrid * f->ld;
-    da.nslice = f->nslice;
-    da.n = f->ngrid;
-    da.ld = f->ld;
-    da.first = f->first;
-    da.harm = harm;
-    da.gridmax = f->gridmax;
-    da.dgrid = f->dgrid;
-    da.ax = st->ax;
-    da.ay = st->ay;
-    da.kx = st->kx;
-    da.ky = st->ky;
-    da.gradx = st->gradx;
-    da.grady = st->grady;
-    da.err = c->d_error;
-    const size_t acc_bytes = 96 * 1024;
-    da.acc_cells = (int)(acc_bytes / 16);
-    G4B_CUDA_TRY(cudaFuncSetAttribute(deposit_slice_kernel,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)acc_bytes));  // per device, cheap
-    {
-      LaunchScope ls(c, "deposit");
-      deposit_slice_kernel<<<f->nslice, 512, acc_bytes, c->stream>>>(da);
-    }
-    if (int rc = check_launch(c, "deposit_slice_kernel")) return rc;
+    if (int rc = fp64_deposit(f, b, st, fc)) return rc;
     src = f->src;
   }
   return adi_run(adi, f, src, f->desc, nullptr);

@@ -157,6 +157,8 @@ struct LaunchScope {
 // streams' work (cudaFree would synchronise the whole device); released
 // blocks stay in the pool for reuse.
 cudaError_t dev_alloc(g4b_ctx* ctx, void** p, size_t bytes);
+// slice scale + deterministic FP64 deposition into f's compact source tiles
+int fp64_deposit(g4b_field* f, g4b_beam* b, const g4b_step* st, double fc);
 void dev_free(g4b_ctx* ctx, void* p);
 
 int check_launch(g4b_ctx* ctx, const char* what);

@@ -49,6 +49,38 @@ void FieldSolverADICUDA::advance(double, Field* field, Beam* beam, Undulator* un
         "FieldSolverADICUDA::advance");
 }
 
+// ------------------------------------------------------- FieldSolverFFTCUDA --
+FieldSolverFFTCUDA::FieldSolverFFTCUDA() {
+  check(g4b_fft_create(cuda_context(), &fft_), "FieldSolverFFTCUDA");
+}
+
+FieldSolverFFTCUDA::~FieldSolverFFTCUDA() { g4b_fft_destroy(fft_); }
+
+// FieldSolverFFTCUDA::initSourceFilter (src/Core/FieldSolverFFTCUDA.cpp:214-222)
+void FieldSolverFFTCUDA::initSourceFilter(double xc, double yc, double sig, bool filter) {
+  check(g4b_fft_init_filter(fft_, xc, yc, sig, filter ? 1 : 0),
+        "FieldSolverFFTCUDA::initSourceFilter");
+}
+
+// FieldSolverFFTCUDA::init (src/Core/FieldSolverFFTCUDA.cpp:246-293)
+void FieldSolverFFTCUDA::init(double delz, double dgrid, double xks, unsigned int ngrid) {
+  check(g4b_fft_init(fft_, delz, dgrid, xks, (int)ngrid), "FieldSolverFFTCUDA::init");
+}
+
+// FieldSolverFFTCUDA::advance (src/Core/FieldSolverFFTCUDA.cpp:295-483)
+void FieldSolverFFTCUDA::advance(double, Field* field, Beam* beam, Undulator* und) {
+  if (!field || !beam || !und)
+    throw std::runtime_error(
+        "FieldSolverFFTCUDA::advance_gpu received a null field/beam/undulator pointer");
+  if (!field->fieldSoA) field->pack_field_to_soa();
+  if (!beam->beamSoA) beam->pack_beam_to_soa();
+  check(g4b_field_set_first(field->fieldSoA, field->first), "FieldSolverFFTCUDA::advance");
+  const int harm = field->getHarm();
+  check(g4b_fft_advance(fft_, field->fieldSoA, beam->beamSoA, &und->current(), und->fc(harm),
+                        field->isEnabled() ? 1 : 0),
+        "FieldSolverFFTCUDA::advance");
+}
+
 // -------------------------------------------------------------------- Field --
 Field::Field() = default;
 
@@ -74,17 +106,22 @@ void Field::init(int nsize, int ngrid_in, double dgrid_in, double xlambda0, doub
   accuslip = 0;
 }
 
-// Field::initSolver (src/Core/Field.cpp:87-110): CUDA ADI solver; the FFT
-// solver and the upstream CPU solvers are not part of this build.
-void Field::initSolver(bool isFFT, bool, double, double, double, bool use_cuda,
-                       bool low_memory_adisolver) {
+// Field::initSolver (src/Core/Field.cpp:87-110): the CUDA FFT solver (with
+// its source filter) or the CUDA ADI solver; the upstream CPU solvers are not
+// part of this build.
+void Field::initSolver(bool isFFT, bool filter, double xc, double yc, double sig,
+                       bool use_cuda, bool low_memory_adisolver) {
   if (!use_cuda)
     throw std::runtime_error(
         "Field::initSolver: use_cuda=false selects the upstream CPU solvers, which this "
         "build does not contain");
-  if (isFFT) throw std::runtime_error("Field::initSolver: fft_fieldsolver is not supported");
   low_memory_ = low_memory_adisolver;
-  solver.reset(new FieldSolverADICUDA(low_memory_adisolver));
+  if (isFFT) {
+    solver.reset(new FieldSolverFFTCUDA());
+    solver->initSourceFilter(xc, yc, sig, filter);
+  } else {
+    solver.reset(new FieldSolverADICUDA(low_memory_adisolver));
+  }
 }
 
 void Field::disable(double conv) {  // include/Field.h:117-125

@@ -61,6 +61,19 @@ class FieldSolverADICUDA : public FieldSolver {
   bool atomic_source_;
 };
 
+// FieldSolverFFTCUDA (include/FieldSolverFFTCUDA.h:15-20)
+class FieldSolverFFTCUDA : public FieldSolver {
+ public:
+  FieldSolverFFTCUDA();
+  ~FieldSolverFFTCUDA() override;
+  void init(double delz, double dgrid, double xks, unsigned int ngrid) override;
+  void advance(double delz, Field* field, Beam* beam, Undulator* und) override;
+  void initSourceFilter(double xc, double yc, double sig, bool filter) override;
+
+ private:
+  g4b_fft* fft_ = nullptr;
+};
+
 // Field (include/Field.h:32-99)
 class Field {
  public:

@@ -207,6 +207,8 @@ struct Deck {
   double current = 1000;
   // &track
   bool use_cuda = true, low_memory = false, periodic = false;
+  bool fft = false, src_filter = false;          // &track fft_fieldsolver, source_filter
+  double xcut = 1, ycut = 1, sigmoid = 1;        // &track xcut, ycut, sigmoid
   int precision = G4B_FP64, output_step = 1, beam_dump = 0, field_dump = 0;
   double zstop = 1e9;
   Undulator und;
@@ -336,9 +338,11 @@ bool parse_deck(const std::string& text, const std::string* lat_text, const std:
       d.periodic = r.flag("periodic", false);
       d.use_cuda = r.flag("use_cuda", true);
       d.low_memory = r.flag("low_memory_adisolver", false);
-      const bool fft = r.flag("fft_fieldsolver", false);
-      const bool src_filter = r.flag("source_filter", false);
-      r.num("xcut", 1), r.num("ycut", 1), r.num("sigmoid", 1);
+      d.fft = r.flag("fft_fieldsolver", false);
+      d.src_filter = r.flag("source_filter", false);
+      d.xcut = r.num("xcut", 1);
+      d.ycut = r.num("ycut", 1);
+      d.sigmoid = r.num("sigmoid", 1);
       if (r.has("s0")) d.s0 = r.num("s0", 0.0);
       if (r.has("slen")) d.slen = r.num("slen", 0.0);
       const std::string prec = lower(r.str("precision", "fp64"));
@@ -351,8 +355,8 @@ bool parse_deck(const std::string& text, const std::string* lat_text, const std:
         set_error("deck: &track precision must be fp64 or mixed");
         return false;
       }
-      if (fft || src_filter) {
-        set_error("deck: fft_fieldsolver and source_filter are not supported");
+      if (d.fft && d.precision == G4B_MIXED) {
+        set_error("deck: fft_fieldsolver runs the FP64 drop-in form (precision = fp64)");
         return false;
       }
       if (sort_step != 0) {
@@ -535,7 +539,7 @@ int g4h_deck_run(g4h_deck* dk, g4h_result** out) {
       for (int s = 0; s < ns; ++s)
         for (size_t k = 0; k < plane.size() / 2; ++k)
           f->field[s][k] = std::complex<double>(plane[2 * k], plane[2 * k + 1]) * ph;
-      f->initSolver(false, false, 1, 1, 1, true, d.low_memory);
+      f->initSolver(d.fft, d.src_filter, d.xcut, d.ycut, d.sigmoid, true, d.low_memory);
       fl.push_back(f.get());
       fields.push_back(std::move(f));
     }

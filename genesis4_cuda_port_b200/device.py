@@ -254,6 +254,39 @@ class FieldSolverADICUDA:
             pass
 
 
+class FieldSolverFFTCUDA:
+    """The reference's FieldSolverFFTCUDA: spectral propagator with the
+    optional sigmoid source filter (initSourceFilter), init, advance."""
+
+    def __init__(self, ctx: Context):
+        self.ctx, self.lib = ctx, ctx.lib
+        h = C.c_void_p()
+        check(self.lib.g4b_fft_create(ctx.h, C.byref(h)))
+        self.h = h
+
+    def init_source_filter(self, xc: float, yc: float, sig: float, filt: bool) -> None:
+        check(self.lib.g4b_fft_init_filter(self.h, xc, yc, sig, int(filt)))
+
+    def init(self, delz: float, dgrid: float, xks: float, ngrid: int) -> None:
+        check(self.lib.g4b_fft_init(self.h, delz, dgrid, xks, ngrid))
+
+    def advance(self, field: FieldState, beam: BeamState, step: Step, fc: float,
+                enabled: bool = True) -> None:
+        check(self.lib.g4b_fft_advance(self.h, field.h, beam.h, C.byref(step), fc,
+                                       int(enabled)))
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.g4b_fft_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class Run:
     """The fused mixed-precision form: a whole FEL run resident on the device
     (beam + up to 8 fields sharing the slicing), advanced per lattice step by

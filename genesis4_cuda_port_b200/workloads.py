@@ -17,6 +17,10 @@ QD: QUADRUPOLE = { l = 0.1, k1 = -1.5 };
 FEL: LINE = { UND, QF, UND, QD, UND };
 """
 
+# the same cell three times over (1032 steps): long enough for the configs'
+# beam at 0.1 um normalised emittance to reach the exponential regime
+HIGH_GAIN_LAT = SASE_LAT + "FEL3: LINE = { 3*FEL };\n"
+
 
 @dataclass
 class Workload:
@@ -39,6 +43,7 @@ class Workload:
     seed: int = 1
     sample: float = 1.0
     harmonics: tuple = (1,)
+    periodic: bool = False
     lattice: str = SASE_LAT
     beamline: str = "FEL"
     extra: dict = field(default_factory=dict)
@@ -113,6 +118,25 @@ def large_sase_h3(nslice=8192, npart=16384, ngrid=255):
     """Large SASE with fundamental and 3rd-harmonic fields."""
     return Workload(f"SASE {nslice} x {npart}, ngrid {ngrid}, h=1 and h=3", nslice,
                     npart, ngrid, harmonics=(1, 3))
+
+
+def steady_state_high_gain(npart=8192, ngrid=151, seed_power=1e3):
+    """Steady-state FEL in the exponential regime: the steady-state beam at
+    0.1 um normalised emittance over the cell three times (1032 steps); the
+    1 kW seed grows by about 1e5 with the bunching still rising at the end."""
+    return Workload(f"steady-state high gain 1 slice x {npart}, ngrid {ngrid}, eps_n 0.1 um, "
+                    "3 x 344 steps", 1, npart, ngrid, shotnoise=False, seed_power=seed_power,
+                    emit_n=0.1e-6, lattice=HIGH_GAIN_LAT, beamline="FEL3")
+
+
+def sase_periodic_high_gain(nslice=64, npart=8192, ngrid=201):
+    """Time-dependent SASE from shot noise in the exponential regime: the SASE
+    beam at 0.1 um normalised emittance, slippage every step with periodic
+    slices (radiation leaving the window re-enters at its tail, as inside a
+    long flat-top bunch), 1032 steps; the power grows by about 5e4."""
+    return Workload(f"periodic SASE high gain {nslice} slices x {npart}, ngrid {ngrid}, "
+                    "eps_n 0.1 um, 3 x 344 steps", nslice, npart, ngrid, emit_n=0.1e-6,
+                    periodic=True, lattice=HIGH_GAIN_LAT, beamline="FEL3")
 
 
 WORKLOADS = {"steady": steady_state, "sase": sase, "sase_h3": large_sase_h3}

@@ -209,6 +209,30 @@ int g4b_diag_field(g4b_field* f, double* stats, double* center);
  * caller.  Synchronises the context's stream, like g4b_diag_field. */
 int g4b_diag_field_static(g4b_field* f, double* stats, double* center);
 
+/* ---- FFT field solver ------------------------------------------------------
+ * Replaces FieldSolverFFTCUDA (include/FieldSolverFFTCUDA.h:15-20,
+ * src/Core/FieldSolverFFTCUDA.cpp:157-483): the spectral propagator
+ *   u' = IFFT2( FFT2(u) exp(i k2 dz) + 2 filter FFT2(S) ) / n^2,
+ *   k2 = -(kx^2 + ky^2) / (2 ks),
+ * with the ADI solver's deterministic source S and the sigmoid source filter.
+ * The batched 2-D transforms are this library's own kernels (no cuFFT).
+ * FP64 fields, ngrid <= 256. */
+typedef struct g4b_fft g4b_fft;
+int g4b_fft_create(g4b_ctx* ctx, g4b_fft** out);
+int g4b_fft_destroy(g4b_fft* solver);
+/* FieldSolverFFTCUDA::initSourceFilter (src/Core/FieldSolverFFTCUDA.cpp:214-222):
+ * the filter 1 / (1 + exp((sqrt((dx/(n xc))^2 + (dy/(n yc))^2) - 1) / sig))
+ * is applied only when filter != 0 and xc, yc, sig > 0; it takes effect at
+ * the next g4b_fft_init. */
+int g4b_fft_init_filter(g4b_fft* solver, double xc, double yc, double sig, int filter);
+/* FieldSolverFFTCUDA::init (src/Core/FieldSolverFFTCUDA.cpp:246-293): the
+ * tables are rebuilt when ngrid, dgrid or xks change (the reference keys
+ * them on ngrid alone); delz is the step the next advance propagates. */
+int g4b_fft_init(g4b_fft* solver, double delz, double dgrid, double xks, int ngrid);
+/* FieldSolverFFTCUDA::advance (src/Core/FieldSolverFFTCUDA.cpp:295-483). */
+int g4b_fft_advance(g4b_fft* solver, g4b_field* f, g4b_beam* b, const g4b_step* step,
+                    double fc, int enabled);
+
 /* ---- fused mixed-precision run -------------------------------------------
  * A whole FEL run resident on the device: FP32 particles and complex64
  * fields with the phase theta in FP64, advanced per lattice step by a fused

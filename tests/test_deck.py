@@ -93,11 +93,19 @@ def test_steady_state_without_time_group():
     ("use_cuda = 1\nfoo = 2", "unknown"),
     ("use_cuda = 0", "use_cuda"),
     ("precision = fp16", "precision"),
-    ("fft_fieldsolver = true", "fft_fieldsolver"),
+    ("fft_fieldsolver = true\nprecision = mixed", "fft_fieldsolver"),
 ])
 def test_track_errors(bad, msg):
     with pytest.raises(G4BError, match=msg):
         host.Deck(deck(track=bad), LAT)
+
+
+def test_fft_solver_keys_are_accepted():
+    """&track fft_fieldsolver / source_filter / xcut / ycut / sigmoid select the
+    FFT field solver with its source filter (Track.cpp:95-105)."""
+    d = host.Deck(deck(track="fft_fieldsolver = true\nsource_filter = true\nxcut = 0.3\n"
+                             "ycut = 0.3\nsigmoid = 0.05"), LAT)
+    assert d.info()["precision"] == 0
 
 
 def test_structure_errors():
