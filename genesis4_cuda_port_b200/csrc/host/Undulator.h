@@ -29,6 +29,8 @@ class Undulator {
 
   // iteration (Gencore main loop: `while (und->advance(rank))`)
   void reset() { istep_ = -1; }
+  // position the iteration at step i (the next advance() goes to i + 1)
+  void seek(int i) { istep_ = i; }
   bool advance(int /*rank*/ = 0) { return ++istep_ < (int)steps.size(); }
   int getStep() const { return istep_; }
   int nstep() const { return (int)steps.size(); }

@@ -1,8 +1,11 @@
 // classes.cpp -- Field, Beam, solvers and slippage over the g4b C ABI.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <mutex>
 
+#include "g4file.h"
+#include "g4h_internal.h"
 #include "genesis4.h"
 
 namespace g4h {
@@ -303,14 +306,163 @@ bool ControlCUDA::applySlippage(double slippage, Field* field) {
 }
 
 // ControlCUDA::applyMarker (src/Core/ControlCUDA.cpp:131-146): bring the
-// state to the host before a dump; the dump files themselves (upstream HDF5
-// writers) are not part of this build.  Sorting is not requested.
-bool ControlCUDA::applyMarker(Beam* beam, std::vector<Field*>* field, Undulator* und, bool&) {
+// state to the host before a dump, then the host-side marker actions.
+bool ControlCUDA::applyMarker(Control* control, Beam* beam, std::vector<Field*>* field,
+                              Undulator* und, bool& error_IO) {
   const int marker = und->getMarker();
   if (marker & 1) beam->unpack_soa_to_beam();
   if (marker & 2)
     for (Field* f : *field) f->unpack_soa_to_field();
+  return control->applyMarker(beam, field, und, error_IO);
+}
+
+// ---------------------------------------------------------------- Control --
+void Control::init(int, int, const std::string& fnbase, Beam*, std::vector<Field*>*,
+                   Undulator*, bool, bool, bool) {
+  fnbase_ = fnbase;
+  written_.clear();
+}
+
+// Marker actions on the host state: beam (bit 0) and field (bit 1) dumps.
+// Sorting (bit 2) is not part of this build; the stop bit is the loop's.
+bool Control::applyMarker(Beam* beam, std::vector<Field*>* field, Undulator* und,
+                          bool& error_IO) {
+  const int marker = und->getMarker();
+  if (fnbase_.empty() || !(marker & 3)) return false;
+  const int step = std::max(0, std::min(und->getStep(), und->nstep()));
+  const std::string tag = fnbase_ + "." + std::to_string(step);
+  if (marker & 1) {
+    const std::string path = tag + ".par.g4";
+    if (!write_beam_dump(path, *beam)) {
+      error_IO = true;
+      return false;
+    }
+    written_.push_back(path);
+  }
+  if (marker & 2)
+    for (Field* f : *field) {
+      const int h = f->getHarm();
+      const std::string path = h == 1 ? tag + ".fld.g4" : tag + ".h" + std::to_string(h) + ".fld.g4";
+      if (!write_field_dump(path, *f)) {
+        error_IO = true;
+        return false;
+      }
+      written_.push_back(path);
+    }
   return false;
+}
+
+// ------------------------------------------------------------------ dumps --
+// Particle dump (upstream .par.h5 names): per slice "sliceNNNNNN/{gamma,
+// theta, x, y, px, py, current}", and "beamletsize", "one4one",
+// "refposition", "slicecount", "slicelength" (the reference length),
+// "slicespacing" (the slice length).
+bool write_beam_dump(const std::string& path, const Beam& beam) {
+  DataFile f;
+  const int ns = (int)beam.beam.size();
+  for (int s = 0; s < ns; ++s) {
+    const auto& sl = beam.beam[s];
+    const uint64_t n = sl.size();
+    std::vector<double> v[6];
+    for (auto& a : v) a.resize(n);
+    for (uint64_t k = 0; k < n; ++k) {
+      const Particle& p = sl[k];
+      v[0][k] = p.gamma, v[1][k] = p.theta, v[2][k] = p.x, v[3][k] = p.y, v[4][k] = p.px,
+      v[5][k] = p.py;
+    }
+    const std::string g = slice_group(s) + "/";
+    const char* names[6] = {"gamma", "theta", "x", "y", "px", "py"};
+    for (int c = 0; c < 6; ++c) f.add(g + names[c], {n}, v[c]);
+    f.add_scalar(g + "current", s < (int)beam.current.size() ? beam.current[s] : 0.0);
+  }
+  f.add_scalar("beamletsize", beam.nbins);
+  f.add_scalar("one4one", beam.one4one ? 1.0 : 0.0);
+  f.add_scalar("refposition", beam.s0);
+  f.add_scalar("slicecount", ns);
+  f.add_scalar("slicelength", beam.reflength);
+  f.add_scalar("slicespacing", beam.slicelength);
+  return f.write(path);
+}
+
+// Field dump (upstream .fld.h5 names): per slice "sliceNNNNNN/field-real"
+// and "field-imag" (ngrid x ngrid, rows along y), and "gridpoints",
+// "gridsize", "refposition", "slicecount", "slicespacing", "wavelength"; plus
+// "accuslip", the slippage not yet applied, so that a run resumed from the
+// dump shifts its slices on the same steps.
+bool write_field_dump(const std::string& path, const Field& fld) {
+  DataFile f;
+  const int ns = (int)fld.field.size();
+  const uint64_t n = (uint64_t)fld.ngrid;
+  for (int s = 0; s < ns; ++s) {
+    const auto& pl = fld.field[(s + fld.first) % ns];  // beam slice s
+    std::vector<double> re(n * n), im(n * n);
+    for (uint64_t k = 0; k < n * n; ++k) re[k] = pl[k].real(), im[k] = pl[k].imag();
+    f.add(slice_group(s) + "/field-real", {n, n}, re);
+    f.add(slice_group(s) + "/field-imag", {n, n}, im);
+  }
+  f.add_scalar("gridpoints", (double)n);
+  f.add_scalar("gridsize", fld.dgrid);
+  f.add_scalar("refposition", fld.s0);
+  f.add_scalar("slicecount", ns);
+  f.add_scalar("slicespacing", fld.slicelength);
+  f.add_scalar("wavelength", fld.xlambda);
+  f.add_scalar("accuslip", fld.accuslip);
+  return f.write(path);
+}
+
+bool read_beam_dump(const std::string& path, Beam& beam) {
+  DataFile f;
+  if (!f.read(path)) return false;
+  const Dataset* cnt = f.find("slicecount");
+  if (!cnt || cnt->data.empty() || (int)cnt->data[0] != (int)beam.beam.size()) {
+    set_error(path + ": the dump's slice count differs from the deck's");
+    return false;
+  }
+  for (int s = 0; s < (int)beam.beam.size(); ++s) {
+    const std::string g = slice_group(s) + "/";
+    const Dataset* v[6] = {f.find(g + "gamma"), f.find(g + "theta"), f.find(g + "x"),
+                           f.find(g + "y"), f.find(g + "px"), f.find(g + "py")};
+    for (auto* d : v)
+      if (!d || d->data.size() != v[0]->data.size()) {
+        set_error(path + ": slice " + std::to_string(s + 1) + " is incomplete");
+        return false;
+      }
+    auto& sl = beam.beam[s];
+    sl.resize(v[0]->data.size());
+    for (size_t k = 0; k < sl.size(); ++k)
+      sl[k] = Particle{v[0]->data[k], v[1]->data[k], v[2]->data[k],
+                       v[3]->data[k], v[4]->data[k], v[5]->data[k]};
+    if (const Dataset* c = f.find(g + "current"))
+      if (s < (int)beam.current.size() && !c->data.empty()) beam.current[s] = c->data[0];
+  }
+  return true;
+}
+
+bool read_field_dump(const std::string& path, Field& fld) {
+  DataFile f;
+  if (!f.read(path)) return false;
+  const Dataset* cnt = f.find("slicecount");
+  const Dataset* gp = f.find("gridpoints");
+  const int ns = (int)fld.field.size();
+  if (!cnt || cnt->data.empty() || (int)cnt->data[0] != ns || !gp || gp->data.empty() ||
+      (int)gp->data[0] != fld.ngrid) {
+    set_error(path + ": the dump's slice count or grid differs from the deck's");
+    return false;
+  }
+  const size_t nn = (size_t)fld.ngrid * fld.ngrid;
+  for (int s = 0; s < ns; ++s) {
+    const Dataset* re = f.find(slice_group(s) + "/field-real");
+    const Dataset* im = f.find(slice_group(s) + "/field-imag");
+    if (!re || !im || re->data.size() != nn || im->data.size() != nn) {
+      set_error(path + ": slice " + std::to_string(s + 1) + " is incomplete");
+      return false;
+    }
+    for (size_t k = 0; k < nn; ++k) fld.field[s][k] = {re->data[k], im->data[k]};
+  }
+  fld.first = 0;
+  const Dataset* acc = f.find("accuslip");
+  fld.accuslip = acc && !acc->data.empty() ? acc->data[0] : 0.0;
+  return true;
 }
 
 }  // namespace g4h

@@ -6,6 +6,8 @@
 #include <cstdio>
 #include <cstring>
 
+#include "g4file.h"
+#include "g4h_internal.h"
 #include "genesis4.h"
 
 namespace g4h {
@@ -298,15 +300,20 @@ bool DiagnosticCUDA::calcField(Field* field, std::map<std::string, std::vector<d
 // Step order per lattice step: marker -> Beam::track -> Field::track (every
 // field) -> slippage -> diagnostics on output steps.  A marker placed after
 // lattice step k acts at the start of step k+1 (the last one after the loop).
-bool Gencore::run(Beam* beam, std::vector<Field*>* field, Undulator* und, bool isTime, bool,
-                  bool periodic, bool use_cuda, FilterDiagnostics& filter, Diagnostic& diag,
-                  GencoreTimers* timers) {
+bool Gencore::run(Beam* beam, std::vector<Field*>* field, Setup* setup, Undulator* und,
+                  bool isTime, bool isScan, bool periodic, bool use_cuda,
+                  FilterDiagnostics& filter, Diagnostic& diag, GencoreTimers* timers) {
   if (!use_cuda)
     throw std::runtime_error("Gencore::run: use_cuda=false needs the upstream CPU solvers");
   g4b_ctx* ctx = cuda_context();
   beam->setUseCuda(true);
   beam->pack_beam_to_soa();
   for (Field* f : *field) f->pack_field_to_soa();
+  std::string rn, fnbase;
+  setup->getRootName(&rn);
+  setup->RootName_to_FileName(&fnbase, &rn);
+  Control host_control;
+  host_control.init(0, 1, fnbase, beam, field, und, isTime, isScan, periodic);
   ControlCUDA control;
   control.init(0, 1, isTime, periodic, beam->slicelength / beam->reflength);
   DiagnosticCUDA dcuda;
@@ -326,8 +333,8 @@ bool Gencore::run(Beam* beam, std::vector<Field*>* field, Undulator* und, bool i
   };
   while (und->advance(0)) {
     bool error_IO = false;
-    control.applyMarker(beam, field, und, error_IO);
-    if (error_IO) return false;
+    control.applyMarker(&host_control, beam, field, und, error_IO);
+    if (error_IO) throw std::runtime_error("Gencore::run: marker dump: " + std::string(last_error()));
     const double delz = und->steplength();
     phase(t.beam, [&] { beam->track(delz, field, und); });
     phase(t.field, [&] {
@@ -347,17 +354,75 @@ bool Gencore::run(Beam* beam, std::vector<Field*>* field, Undulator* und, bool i
     for (Field* f : *field) f->unpack_soa_to_field();
   });
   bool error_IO = false;  // last marker action (src/Core/Gencore.cpp:276-279)
-  control.applyMarker(beam, field, und, error_IO);
+  und->seek(t.steps);      // the marker after the last step taken
+  control.applyMarker(&host_control, beam, field, und, error_IO);
+  if (error_IO) throw std::runtime_error("Gencore::run: marker dump: " + std::string(last_error()));
   check(g4b_ctx_synchronize(ctx), "Gencore::run");
   if (timers) *timers = t;
+  // write out diagnostic arrays (src/Core/Gencore.cpp:297)
+  if (!diag.writeToOutputFile(beam, field, setup, und))
+    throw std::runtime_error("Gencore::run: output file: " + std::string(last_error()));
+  return true;
+}
+
+// The records as <fnbase>.out.g4: "Beam/<record>" [nz][nslice] (global
+// records [nz]), "Field/<record>" for the first field and "Field<h>/..." for
+// a field of harmonic h, "Lattice/zplot" (output positions) and the per-step
+// lattice tables "Lattice/{z, dz, aw, ku, kx, ky, qf, cx, cy, chic_angle,
+// slippage}", "Meta/{nslice, nfield, steps}".
+bool Diagnostic::writeToOutputFile(Beam* beam, std::vector<Field*>* field, Setup* setup,
+                                   Undulator* und) {
+  std::string rn, fnbase;
+  setup->getRootName(&rn);
+  setup->RootName_to_FileName(&fnbase, &rn);
+  output_file.clear();
+  if (fnbase.empty()) return true;
+  DataFile f;
+  const uint64_t nz = zout.size(), ns = beam->beam.size();
+  auto put_group = [&](const std::string& g, const std::map<std::string, std::vector<double>>& m) {
+    for (auto& [k, v] : m) {
+      if (v.size() == nz * ns && ns > 0)
+        f.add(g + "/" + k, {nz, ns}, v);
+      else
+        f.add(g + "/" + k, {(uint64_t)v.size()}, v);
+    }
+  };
+  if (val.size() > 2) put_group("Beam", val[2]);
+  std::map<int, int> seen;
+  for (size_t i = 0; i < field->size() && 3 + i < val.size(); ++i) {
+    const int h = (*field)[i]->getHarm();
+    std::string g = h == 1 ? "Field" : "Field" + std::to_string(h);
+    if (seen[h]++) g += "_" + std::to_string(seen[h]);
+    put_group(g, val[3 + i]);
+  }
+  f.add("Lattice/zplot", {nz}, zout);
+  const uint64_t nst = und->nstep();
+  std::vector<double> z(nst), dz(nst), aw(nst), ku(nst), kx(nst), ky(nst), qf(nst), cx(nst),
+      cy(nst), ang(nst), slip(nst);
+  for (uint64_t i = 0; i < nst; ++i) {
+    const LatticeStep& s = und->steps[i];
+    z[i] = s.z, dz[i] = s.st.delz, aw[i] = s.st.aw, ku[i] = s.st.ku, kx[i] = s.st.kx,
+    ky[i] = s.st.ky, qf[i] = s.st.qf, cx[i] = s.st.cx, cy[i] = s.st.cy,
+    ang[i] = s.st.chic_angle, slip[i] = s.slip;
+  }
+  const std::pair<const char*, std::vector<double>*> lat[] = {
+      {"z", &z}, {"dz", &dz}, {"aw", &aw}, {"ku", &ku}, {"kx", &kx}, {"ky", &ky},
+      {"qf", &qf}, {"cx", &cx}, {"cy", &cy}, {"chic_angle", &ang}, {"slippage", &slip}};
+  for (auto& [k, v] : lat) f.add(std::string("Lattice/") + k, {nst}, *v);
+  f.add_scalar("Meta/nslice", (double)ns);
+  f.add_scalar("Meta/nfield", (double)field->size());
+  f.add_scalar("Meta/steps", (double)nst);
+  const std::string path = fnbase + ".out.g4";
+  if (!f.write(path)) return false;
+  output_file = path;
   return true;
 }
 
 // The same loop as one resident mixed-precision run (g4b_run): the lattice is
 // uploaded once, the steps are replayed from a CUDA graph and the per-step
 // diagnostic sums are read back from the run's history after the loop.
-bool run_mixed(Beam* beam, std::vector<Field*>* field, Undulator* und, bool isTime,
-               bool periodic, FilterDiagnostics& filter, Diagnostic& diag,
+bool run_mixed(Beam* beam, std::vector<Field*>* field, Setup* setup, Undulator* und,
+               bool isTime, bool periodic, FilterDiagnostics& filter, Diagnostic& diag,
                GencoreTimers* timers) {
   const int nslice = (int)beam->beam.size();
   const int nfield = (int)field->size();
@@ -475,12 +540,59 @@ bool run_mixed(Beam* beam, std::vector<Field*>* field, Undulator* und, bool isTi
     }
   }
 
+  // final state (or the state at a dump marker) back into the host objects
+  auto pull_state = [&]() {
+    std::vector<double> x(np), y(np), px(np), py(np), g(np), th(np);
+    check(g4b_run_download_beam(run, x.data(), y.data(), px.data(), py.data(), g.data(),
+                                th.data()),
+          "run_mixed");
+    size_t k = 0;
+    for (auto& s : beam->beam)
+      for (auto& p : s) {
+        p.x = x[k], p.y = y[k], p.px = px[k], p.py = py[k], p.gamma = g[k], p.theta = th[k];
+        ++k;
+      }
+    for (int i = 0; i < nfield; ++i) {
+      Field* f = (*field)[i];
+      const size_t plane = (size_t)f->ngrid * f->ngrid;
+      std::vector<double> cells(2 * plane * nslice);
+      check(g4b_run_download_field(run, i, cells.data(), &f->first), "run_mixed");
+      for (int s = 0; s < nslice; ++s)
+        std::memcpy(f->field[s].data(), cells.data() + 2 * plane * s, 16 * plane);
+    }
+  };
+  std::string rn, fnbase;
+  setup->getRootName(&rn);
+  setup->RootName_to_FileName(&fnbase, &rn);
+  Control host_control;
+  host_control.init(0, 1, fnbase, beam, field, und, isTime, false, periodic);
+  auto marker = [&](int steps_taken) {
+    und->seek(steps_taken);
+    bool error_IO = false;
+    host_control.applyMarker(beam, field, und, error_IO);
+    if (error_IO) throw std::runtime_error("run_mixed: marker dump: " + std::string(last_error()));
+  };
+  // the loop stops where a dump marker acts, to bring the state to the host
+  std::vector<int> cuts;
+  if (!fnbase.empty())
+    for (int i = 0; i + 1 < nrun; ++i)
+      if (und->steps[i].marker & 3) cuts.push_back(i + 1);
+  cuts.push_back(nrun);
   g4b_ctx* ctx = cuda_context();
-  check(g4b_ctx_synchronize(ctx), "run_mixed");
-  const double t0 = now_s();
-  check(g4b_run_advance(run, 0, nrun, 1), "run_mixed");
-  check(g4b_ctx_synchronize(ctx), "run_mixed");
-  const double t1 = now_s();
+  double loop_s = 0.0;
+  int done = 0;
+  for (int c : cuts) {
+    check(g4b_ctx_synchronize(ctx), "run_mixed");
+    const double t0 = now_s();
+    if (c > done) check(g4b_run_advance(run, done, c - done, 1), "run_mixed");
+    check(g4b_ctx_synchronize(ctx), "run_mixed");
+    loop_s += now_s() - t0;
+    done = c;
+    if (c < nrun) {
+      pull_state();
+      marker(c);
+    }
+  }
 
   const size_t rec = 23 + 2 * (size_t)nharm;
   std::vector<double> hb((size_t)nslice * rec), hf((size_t)nfield * nslice * 9);
@@ -507,32 +619,15 @@ bool run_mixed(Beam* beam, std::vector<Field*>* field, Undulator* und, bool isTi
     }
     ++iz;
   }
-  // final state back into the host objects
-  {
-    std::vector<double> x(np), y(np), px(np), py(np), g(np), th(np);
-    check(g4b_run_download_beam(run, x.data(), y.data(), px.data(), py.data(), g.data(),
-                                th.data()),
-          "run_mixed");
-    size_t k = 0;
-    for (auto& s : beam->beam)
-      for (auto& p : s) {
-        p.x = x[k], p.y = y[k], p.px = px[k], p.py = py[k], p.gamma = g[k], p.theta = th[k];
-        ++k;
-      }
-  }
-  for (int i = 0; i < nfield; ++i) {
-    Field* f = (*field)[i];
-    const size_t plane = (size_t)f->ngrid * f->ngrid;
-    std::vector<double> cells(2 * plane * nslice);
-    check(g4b_run_download_field(run, i, cells.data(), &f->first), "run_mixed");
-    for (int s = 0; s < nslice; ++s)
-      std::memcpy(f->field[s].data(), cells.data() + 2 * plane * s, 16 * plane);
-  }
+  pull_state();
+  marker(nrun);  // the last marker action (src/Core/Gencore.cpp:276-279)
   if (timers) {
     *timers = GencoreTimers{};
-    timers->beam = t1 - t0;  // whole fused loop
+    timers->beam = loop_s;  // the fused loop (without the dump stops)
     timers->steps = nrun;
   }
+  if (!diag.writeToOutputFile(beam, field, setup, und))
+    throw std::runtime_error("run_mixed: output file: " + std::string(last_error()));
   return true;
 }
 

@@ -156,12 +156,49 @@ class Beam {
   int bharm = 1;
 };
 
+// upstream Setup subset: the output file base (Setup::getRootName,
+// Setup::RootName_to_FileName).  With outputdir empty no file is written.
+class Setup {
+ public:
+  std::string rootname = "genesis", outputdir;
+  void getRootName(std::string* rn) const { *rn = rootname; }
+  void RootName_to_FileName(std::string* fn, const std::string* rn) const {
+    *fn = outputdir.empty() ? std::string() : outputdir + "/" + *rn;
+  }
+};
+
+// upstream Control subset: the marker actions on the host state, which
+// ControlCUDA::applyMarker forwards to (src/Core/ControlCUDA.cpp:131-146):
+// beam dumps (marker bit 0) as <fnbase>.<steps taken>.par.g4 and field dumps
+// (bit 1) as <fnbase>.<steps taken>.fld.g4 (harmonic h > 1: .h<h>.fld.g4),
+// in the G4DS format of g4file.cpp.  Slices are written in beam order.
+class Control {
+ public:
+  void init(int rank, int size, const std::string& fnbase, Beam* beam,
+            std::vector<Field*>* field, Undulator* und, bool isTime, bool isScan,
+            bool periodic);
+  bool applyMarker(Beam* beam, std::vector<Field*>* field, Undulator* und, bool& error_IO);
+  const std::vector<std::string>& written() const { return written_; }
+
+ private:
+  std::string fnbase_;
+  std::vector<std::string> written_;
+};
+
+// Dump files of one beam / one field (G4DS, the upstream .par.h5 / .fld.h5
+// dataset names) and their readers for &importbeam / &importfield.
+bool write_beam_dump(const std::string& path, const Beam& beam);
+bool write_field_dump(const std::string& path, const Field& field);
+bool read_beam_dump(const std::string& path, Beam& beam);
+bool read_field_dump(const std::string& path, Field& field);
+
 // slippage / markers (include/ControlCUDA.h:15-23)
 class ControlCUDA {
  public:
   void init(int rank, int size, bool isTime, bool periodic, double sample);
   bool applySlippage(double slippage, Field* field);
-  bool applyMarker(Beam* beam, std::vector<Field*>* field, Undulator* und, bool& error_IO);
+  bool applyMarker(Control* control, Beam* beam, std::vector<Field*>* field, Undulator* und,
+                   bool& error_IO);
 
  private:
   bool timerun_ = false, periodic_ = false;
@@ -187,7 +224,11 @@ struct FilterDiagnostics {
 struct Diagnostic {
   std::vector<double> zout;
   std::vector<std::map<std::string, std::vector<double>>> val;
+  std::string output_file;  // written by writeToOutputFile (empty: none)
   void init(int nz, int nslice, int nfield, const FilterDiagnostics& filter);
+  // Diagnostic::writeToOutputFile (called at src/Core/Gencore.cpp:297): the
+  // records, output positions and lattice tables as <fnbase>.out.g4 (G4DS).
+  bool writeToOutputFile(Beam* beam, std::vector<Field*>* field, Setup* setup, Undulator* und);
 };
 
 class DiagnosticCUDA {  // include/DiagnosticCUDA.h:17-31
@@ -214,15 +255,19 @@ struct GencoreTimers {
 
 class Gencore {  // include/Gencore.h:20-23
  public:
-  bool run(Beam* beam, std::vector<Field*>* field, Undulator* und, bool isTime, bool isScan,
-           bool periodic, bool use_cuda, FilterDiagnostics& filter, Diagnostic& diag,
-           GencoreTimers* timers = nullptr);
+  // The reference's arguments, then the records (the reference keeps its
+  // Diagnostic inside run and writes it to file; here the caller gets it too)
+  // and optional phase timers.
+  bool run(Beam* beam, std::vector<Field*>* field, Setup* setup, Undulator* und, bool isTime,
+           bool isScan, bool periodic, bool use_cuda, FilterDiagnostics& filter,
+           Diagnostic& diag, GencoreTimers* timers = nullptr);
 };
 
 // Fused mixed-precision run of the same loop (g4b_run): beam and fields stay
-// on the device in FP32 (+FP64 theta); the diagnostics are read back at the end.
-bool run_mixed(Beam* beam, std::vector<Field*>* field, Undulator* und, bool isTime,
-               bool periodic, FilterDiagnostics& filter, Diagnostic& diag,
+// on the device in FP32 (+FP64 theta); the diagnostics are read back at the
+// end; the loop stops at dump markers to bring the state to the host.
+bool run_mixed(Beam* beam, std::vector<Field*>* field, Setup* setup, Undulator* und,
+               bool isTime, bool periodic, FilterDiagnostics& filter, Diagnostic& diag,
                GencoreTimers* timers = nullptr);
 
 // Derived diagnostics from raw per-slice sums (the host part of

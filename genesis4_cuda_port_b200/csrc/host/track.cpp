@@ -212,7 +212,20 @@ struct Deck {
   int precision = G4B_FP64, output_step = 1, beam_dump = 0, field_dump = 0;
   double zstop = 1e9;
   Undulator und;
+  // files: the deck's directory, &setup outputdir, &importbeam / &importfield
+  std::string base, outputdir, import_beam;
+  struct ImportField {
+    std::string file;
+    int harm = 1;
+  };
+  std::vector<ImportField> import_fields;
 };
+
+// a deck's file name, relative to the deck's directory unless absolute
+std::string deck_path(const std::string& base, const std::string& f) {
+  if (f.empty() || f[0] == '/' || base.empty()) return f;
+  return base + "/" + f;
+}
 
 bool parse_deck(const std::string& text, const std::string* lat_text, const std::string& base,
                 Deck& d) {
@@ -226,6 +239,7 @@ bool parse_deck(const std::string& text, const std::string* lat_text, const std:
     if (name == "setup") {
       have_setup = true;
       d.rootname = r.str("rootname", d.rootname);
+      d.outputdir = r.str("outputdir", "");
       d.latfile = r.str("lattice", "");
       d.beamline = r.str("beamline", "");
       d.gamma0 = r.num("gamma0", d.gamma0);
@@ -300,6 +314,25 @@ bool parse_deck(const std::string& text, const std::string* lat_text, const std:
         return false;
       }
       d.fields.push_back(f);
+    } else if (name == "importbeam") {  // upstream &importbeam: a particle dump
+      d.import_beam = deck_path(base, r.str("file", ""));
+      r.flag("time", true);
+      if (!r.done()) return false;
+      if (d.import_beam.empty()) {
+        set_error("deck: &importbeam needs file");
+        return false;
+      }
+    } else if (name == "importfield") {  // upstream &importfield: a field dump
+      Deck::ImportField fi;
+      fi.file = deck_path(base, r.str("file", ""));
+      fi.harm = (int)r.num("harmonic", 1);
+      r.flag("time", true);
+      if (!r.done()) return false;
+      if (fi.file.empty()) {
+        set_error("deck: &importfield needs file");
+        return false;
+      }
+      d.import_fields.push_back(fi);
     } else if (name == "beam") {
       have_beam = true;
       g4h_beam_spec& b = d.beam;
@@ -411,6 +444,16 @@ bool parse_deck(const std::string& text, const std::string* lat_text, const std:
   d.beam.seed = d.seed;
   d.beam.reflength = d.lambda0;
   d.beam.slicelength = d.lambda0 * d.sample;
+  d.base = base;
+  for (auto& fi : d.import_fields) {
+    bool found = false;
+    for (auto& f : d.fields) found |= f.harm == fi.harm;
+    if (!found) {
+      set_error("deck: &importfield harmonic " + std::to_string(fi.harm) +
+                " has no &field of that harmonic");
+      return false;
+    }
+  }
   return true;
 }
 
@@ -424,6 +467,7 @@ struct g4h_deck {
 
 struct g4h_result {
   Diagnostic diag;
+  std::string output_file;
   int nslice = 0, nfield = 0, nsteps = 0;
   double seconds = 0;
   std::vector<std::vector<double>> field_out;  // final cells per field
@@ -513,7 +557,9 @@ int g4h_deck_run(g4h_deck* dk, g4h_result** out) {
     beam.init(ns, d.nbins, d.lambda0, d.lambda0 * d.sample, d.s0, false);
     beam.gamma_ref = d.gamma0;
     std::fill(beam.current.begin(), beam.current.end(), d.current);
-    {
+    if (!d.import_beam.empty()) {
+      if (!read_beam_dump(d.import_beam, beam)) return G4B_ERR_ARG;
+    } else {
       const size_t n = (size_t)ns * d.npart;
       std::vector<double> x(n), y(n), px(n), py(n), g(n), th(n);
       std::vector<int64_t> off(ns + 1);
@@ -539,6 +585,8 @@ int g4h_deck_run(g4h_deck* dk, g4h_result** out) {
       for (int s = 0; s < ns; ++s)
         for (size_t k = 0; k < plane.size() / 2; ++k)
           f->field[s][k] = std::complex<double>(plane[2 * k], plane[2 * k + 1]) * ph;
+      for (auto& imp : d.import_fields)
+        if (imp.harm == fi.harm && !read_field_dump(imp.file, *f)) return G4B_ERR_ARG;
       f->initSolver(d.fft, d.src_filter, d.xcut, d.ycut, d.sigmoid, true, d.low_memory);
       fl.push_back(f.get());
       fields.push_back(std::move(f));
@@ -546,14 +594,21 @@ int g4h_deck_run(g4h_deck* dk, g4h_result** out) {
     auto res = std::make_unique<g4h_result>();
     GencoreTimers t;
     const bool isTime = d.time && ns > 1;
+    // files go to &setup outputdir (relative to the deck's directory), else
+    // to the deck's directory; a deck given as text without either writes none
+    Setup setup;
+    setup.rootname = d.rootname;
+    setup.outputdir = !d.outputdir.empty() ? deck_path(d.base, d.outputdir) : d.base;
     if (d.precision == G4B_MIXED) {
-      run_mixed(&beam, &fl, &d.und, isTime, d.periodic, d.filter, res->diag, &t);
+      run_mixed(&beam, &fl, &setup, &d.und, isTime, d.periodic, d.filter, res->diag, &t);
       res->seconds = t.beam;
     } else {
       Gencore core;
-      core.run(&beam, &fl, &d.und, isTime, false, d.periodic, true, d.filter, res->diag, &t);
+      core.run(&beam, &fl, &setup, &d.und, isTime, false, d.periodic, true, d.filter,
+               res->diag, &t);
       res->seconds = t.beam + t.field + t.slip + t.diag;
     }
+    res->output_file = res->diag.output_file;
     res->nslice = ns;
     res->nfield = (int)fl.size();
     res->nsteps = t.steps;
@@ -571,6 +626,20 @@ int g4h_deck_run(g4h_deck* dk, g4h_result** out) {
     set_error(e.what());
     return G4B_ERR_CUDA;
   }
+}
+
+int g4h_result_output_file(g4h_result* r, char* buf, int buflen, int* needed) {
+  if (!r) {
+    set_error("g4h_result_output_file: null result");
+    return G4B_ERR_ARG;
+  }
+  if (needed) *needed = (int)r->output_file.size() + 1;
+  if (buf && buflen > 0) {
+    const size_t n = std::min((size_t)buflen - 1, r->output_file.size());
+    std::memcpy(buf, r->output_file.data(), n);
+    buf[n] = 0;
+  }
+  return G4B_OK;
 }
 
 int g4h_result_destroy(g4h_result* r) {

@@ -82,6 +82,10 @@ def load():
     h.g4h_result_get.argtypes = [C.c_void_p, C.c_int, C.c_char_p, _lib.c_double_p,
                                  C.c_int64, _lib.c_int64_p]
     h.g4h_result_field.argtypes = [C.c_void_p, C.c_int, _lib.c_double_p, _lib.c_int_p]
+    h.g4h_result_output_file.argtypes = [C.c_void_p, C.c_char_p, C.c_int, _lib.c_int_p]
+    h.g4h_file_list.argtypes = [C.c_char_p, C.c_char_p, C.c_int, _lib.c_int_p]
+    h.g4h_file_read.argtypes = [C.c_char_p, C.c_char_p, _lib.c_double_p, C.c_int64,
+                                _lib.c_int64_p, _lib.c_int_p, _lib.c_int64_p]
     _h = h
     return h
 
@@ -225,6 +229,15 @@ class Result:
         _check(load().g4h_result_keys(self.h, g, buf, need.value, None))
         return {k: self._get(g, k) for k in buf.value.decode().split("\n") if k}
 
+    @property
+    def output_file(self) -> str:
+        """Path of the run's G4DS output file ("" when none was written)."""
+        need = C.c_int()
+        _check(load().g4h_result_output_file(self.h, None, 0, C.byref(need)))
+        buf = C.create_string_buffer(need.value)
+        _check(load().g4h_result_output_file(self.h, buf, need.value, None))
+        return buf.value.decode()
+
     def final_field(self, i: int = 0):
         ngrid = int(self.field[i]["ngrid"][0])
         out = np.empty((self.nslice, ngrid, ngrid), np.complex128)
@@ -332,3 +345,43 @@ def serve(cfg: EngineConfig, jobs, arrival, records: bool = False):
     _check(h.g4h_serve(C.byref(cfg), arr, dptr(arrival), len(jobs), dptr(lat), dptr(power),
                        dptr(rec) if rec is not None else None, C.byref(st)))
     return st, lat, power, rec
+
+
+# ---- G4DS files (output records and dumps) ------------------------------------
+
+def read_g4ds(path) -> dict:
+    """Every dataset of a G4DS file (the format written by the host layer for
+    its output records and marker dumps; described in include/g4h.h) as
+    {name: float64 array shaped by its dimensions}.  Pure Python."""
+    import struct
+    data = Path(path).read_bytes()
+    if data[:8] != b"G4DS\x00\x00\x00\x01":
+        raise ValueError(f"{path} is not a G4DS file")
+    (count,) = struct.unpack_from("<Q", data, 8)
+    pos, out = 16, {}
+    for _ in range(count):
+        (nl,) = struct.unpack_from("<I", data, pos)
+        name = data[pos + 4:pos + 4 + nl].decode()
+        pos += 4 + nl
+        typ, rank = struct.unpack_from("<II", data, pos)
+        pos += 8
+        dims = struct.unpack_from(f"<{rank}Q", data, pos)
+        pos += 8 * rank
+        n = int(np.prod(dims)) if rank else 1
+        arr = np.frombuffer(data, dtype="<f8" if typ == 0 else "<i8", count=n, offset=pos)
+        out[name] = arr.reshape(dims).copy()
+        pos += 8 * n
+    return out
+
+
+def file_dataset(path, name) -> np.ndarray:
+    """One dataset through the host library's reader (g4h_file_read)."""
+    n = C.c_int64()
+    rank = C.c_int()
+    dims = (C.c_int64 * 8)()
+    _check(load().g4h_file_read(str(path).encode(), name.encode(), None, 0, C.byref(n),
+                                C.byref(rank), dims))
+    out = np.empty(n.value)
+    _check(load().g4h_file_read(str(path).encode(), name.encode(), dptr(out), n.value, None,
+                                None, None))
+    return out.reshape([dims[i] for i in range(rank.value)])

@@ -115,8 +115,27 @@ int g4h_result_keys(g4h_result* res, int group, char* buf, int buflen, int* need
  * for per-slice records, nz for Global/ records. */
 int g4h_result_get(g4h_result* res, int group, const char* key, double* out,
                    int64_t capacity, int64_t* length);
+/* Path of the run's output file (<outputdir>/<rootname>.out.g4, written when
+ * the deck names &setup outputdir or was parsed with a base_dir; "" if none).
+ * Diagnostic::writeToOutputFile, called at src/Core/Gencore.cpp:297. */
+int g4h_result_output_file(g4h_result* res, char* buf, int buflen, int* needed);
 /* Final cells of field i (2*nslice*ngrid^2 doubles) and its `first`. */
 int g4h_result_field(g4h_result* res, int ifield, double* cells, int* first);
+
+/* ---- output and dump files ------------------------------------------------
+ * The upstream HDF5 files (.out.h5 records, .par.h5 particle dumps, .fld.h5
+ * field dumps; written by Diagnostic::writeToOutputFile and by the marker
+ * actions ControlCUDA::applyMarker forwards to, src/Core/ControlCUDA.cpp:131-146)
+ * are written here with the same dataset path names into G4DS files:
+ *   "G4DS" 0 0 0 1 | u64 count | per dataset: u32 name length, name,
+ *   u32 type (0 = float64, 1 = int64), u32 rank, rank x u64 dims,
+ *   product(dims) x 8 bytes, all little-endian.
+ * Dumps are read back by the deck groups &importbeam / &importfield. */
+/* '\n'-separated dataset names of a file. */
+int g4h_file_list(const char* path, char* buf, int buflen, int* needed);
+/* One dataset: up to capacity values, its length, rank and dims (<= 8). */
+int g4h_file_read(const char* path, const char* name, double* out, int64_t capacity,
+                  int64_t* length, int* rank, int64_t* dims);
 
 /* ---- many runs on one GPU: batched scan and served stream ----------------
  * A job is one mixed-precision FEL run on the shared lattice of the engine
