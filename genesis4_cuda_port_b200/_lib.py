@@ -99,6 +99,10 @@ _SIGS = {
                                C.c_double, C.c_int]),
     "g4b_adi_advance": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p,
                                   C.POINTER(Step), C.c_double, C.c_int]),
+    "g4b_field_plane_bytes": (C.c_int, [C.c_void_p, C.POINTER(C.c_size_t)]),
+    "g4b_field_plane_out": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "g4b_field_plane_in": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "g4b_field_zero_plane": (C.c_int, [C.c_void_p, C.c_int]),
     "g4b_fft_create": (C.c_int, [C.c_void_p, c_void_pp]),
     "g4b_fft_destroy": (C.c_int, [C.c_void_p]),
     "g4b_fft_init_filter": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_double,

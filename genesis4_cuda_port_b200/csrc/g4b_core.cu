@@ -757,4 +757,42 @@ int g4b_slippage(g4b_field* f, double shift, double sample, int time_run,
   return G4B_OK;
 }
 
+// One storage plane (ngrid rows of ld cells, the state's precision) to / from
+// device memory, on the context's stream: the pack / unpack of the slippage
+// plane exchange between ranks (src/Core/ControlCUDA.cpp:27-66, :195-235).
+int g4b_field_plane_bytes(g4b_field* f, size_t* bytes) {
+  if (!f || !bytes) return fail(G4B_ERR_ARG, "g4b_field_plane_bytes: null arg");
+  *bytes = (size_t)f->ngrid * f->ld * f->cell_bytes;
+  return G4B_OK;
+}
+
+int g4b_field_plane_out(g4b_field* f, int slice, void* dst_device) {
+  if (!f || !dst_device) return fail(G4B_ERR_ARG, "g4b_field_plane_out: null arg");
+  if (slice < 0 || slice >= f->nslice) return fail(G4B_ERR_RANGE, "g4b_field_plane_out: slice");
+  G4B_CUDA_TRY(cudaSetDevice(f->ctx->device));
+  const size_t pb = (size_t)f->ngrid * f->ld * f->cell_bytes;
+  G4B_CUDA_TRY(cudaMemcpyAsync(dst_device, static_cast<const char*>(f->a) + pb * slice, pb,
+                               cudaMemcpyDeviceToDevice, f->ctx->stream));
+  return G4B_OK;
+}
+
+int g4b_field_plane_in(g4b_field* f, int slice, const void* src_device) {
+  if (!f || !src_device) return fail(G4B_ERR_ARG, "g4b_field_plane_in: null arg");
+  if (slice < 0 || slice >= f->nslice) return fail(G4B_ERR_RANGE, "g4b_field_plane_in: slice");
+  G4B_CUDA_TRY(cudaSetDevice(f->ctx->device));
+  const size_t pb = (size_t)f->ngrid * f->ld * f->cell_bytes;
+  G4B_CUDA_TRY(cudaMemcpyAsync(static_cast<char*>(f->a) + pb * slice, src_device, pb,
+                               cudaMemcpyDeviceToDevice, f->ctx->stream));
+  return G4B_OK;
+}
+
+int g4b_field_zero_plane(g4b_field* f, int slice) {
+  if (!f) return fail(G4B_ERR_ARG, "g4b_field_zero_plane: null arg");
+  if (slice < 0 || slice >= f->nslice) return fail(G4B_ERR_RANGE, "g4b_field_zero_plane: slice");
+  G4B_CUDA_TRY(cudaSetDevice(f->ctx->device));
+  const size_t pb = (size_t)f->ngrid * f->ld * f->cell_bytes;
+  G4B_CUDA_TRY(cudaMemsetAsync(static_cast<char*>(f->a) + pb * slice, 0, pb, f->ctx->stream));
+  return G4B_OK;
+}
+
 }  // extern "C"

@@ -124,6 +124,16 @@ int g4b_field_download(g4b_field* f, double* host_cells);
  * (include/Field.h:68). */
 int g4b_field_set_first(g4b_field* f, int first);
 int g4b_field_get_first(g4b_field* f, int* first);
+/* Slice decomposition over ranks (the multi-rank branch of
+ * ControlCUDA::applySlippage, src/Core/ControlCUDA.cpp:195-244, with its
+ * plane pack/unpack kernels :27-66): one storage plane of the field state
+ * (ngrid rows of the padded row pitch, in the state's precision; plane_bytes
+ * gives its size) copied to or from device memory such as a communication
+ * buffer, and a plane zeroed, asynchronously on the context's stream. */
+int g4b_field_plane_bytes(g4b_field* f, size_t* bytes);
+int g4b_field_plane_out(g4b_field* f, int slice, void* dst_device);
+int g4b_field_plane_in(g4b_field* f, int slice, const void* src_device);
+int g4b_field_zero_plane(g4b_field* f, int slice);
 /* Bytes of device memory the field holds (state + solver scratch). */
 int g4b_field_device_bytes(g4b_field* f, uint64_t* bytes);
 
