@@ -276,8 +276,10 @@ __device__ __forceinline__ bool adi_band(const AdiPassArgs& a, const CUtensorMap
     // ix = r0 + row, rows iy = gl*M + j of the solved plane
     __shared__ double dpart[W][9];
     // each lane sums its M cells in the state precision T (exact cell
-    // offsets; FP32 partials of <= 33 terms) and the lanes, warps and bands
-    // are then added in FP64
+    // offsets; partials of <= 33 terms, rounding at the level of the state's
+    // own); the lanes of a column add in FP64 (<= 32 terms); the power and
+    // the other sums of the band's warps and (in the finalize) of the bands
+    // are added with compensation (csum_*), as are the slices on the host
     const T shift = (T)(-0.5 * (double)(n - 1));
     const double dx = (double)iy + (double)shift;  // iy is the column index in pass Y
     T tp = 0, ty1 = 0, ty2 = 0, tre = 0, tim = 0;
@@ -336,9 +338,9 @@ __device__ __forceinline__ bool adi_band(const AdiPassArgs& a, const CUtensorMap
     }
     __syncthreads();
     if (tid < 9) {
-      double t = dpart[0][tid];
-      for (int w = 1; w < W; ++w) t += dpart[w][tid];
-      a.diag[((size_t)s * a.nband + band) * 9 + tid] = t;
+      double t = dpart[0][tid], tc = 0.0;
+      for (int w = 1; w < W; ++w) ptx::csum_add(t, tc, dpart[w][tid]);
+      a.diag[((size_t)s * a.nband + band) * 9 + tid] = t + tc;
     }
   }
   if (PX) __syncthreads();  // out overlays the input tile

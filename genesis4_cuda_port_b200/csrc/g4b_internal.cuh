@@ -284,6 +284,29 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
+// Compensated FP64 accumulation (Neumaier's variant of Kahan summation): s
+// holds the running sum, c the rounding errors of its additions (TwoSum), so
+// that s + c carries the sum to about twice FP64 precision independently of
+// the number of terms.
+__device__ __forceinline__ void csum_add(double& s, double& c, double x) {
+  const double t = s + x;
+  c += fabs(s) >= fabs(x) ? (s - t) + x : (x - t) + s;
+  s = t;
+}
+// Combine another compensated partial (s2, c2) into (s, c).
+__device__ __forceinline__ void csum_merge(double& s, double& c, double s2, double c2) {
+  csum_add(s, c, s2);
+  c += c2;
+}
+// Butterfly reduction of compensated partials over the lanes of width-w groups.
+__device__ __forceinline__ void csum_warp(double& s, double& c, int width) {
+  for (int o = width / 2; o > 0; o >>= 1) {
+    const double s2 = __shfl_xor_sync(0xffffffffu, s, o);
+    const double c2 = __shfl_xor_sync(0xffffffffu, c, o);
+    csum_merge(s, c, s2, c2);
+  }
+}
+
 // Bounded wait: returns false (and sets the device error flag) if the phase
 // did not complete within `limit` polls.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity,

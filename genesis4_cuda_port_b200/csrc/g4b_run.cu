@@ -526,6 +526,7 @@ constexpr int kDepDiagU = 8;          // particles in flight per thread
 template <int NB, int U = kDepDiagU>
 __device__ __forceinline__ void diag_slice(const BeamDiagArgs& a, const int bs, const int part) {
   __shared__ double dpart[kDiagThreads / 32][kBeamRec + 2 * kMaxBunch];
+  __shared__ double bcomp[kDiagThreads / 32][2 * kMaxBunch];  // bunching compensations
   const int tid = threadIdx.x, w = tid >> 5, l = tid & 31;
   const int nall = (int)(a.off[bs + 1] - a.off[bs]);  // at most kRunMaxNp per slice
   const int per = (nall + kDepParts - 1) / kDepParts;
@@ -543,9 +544,11 @@ __device__ __forceinline__ void diag_slice(const BeamDiagArgs& a, const int bs, 
   // minima / maxima of x, px, y, py (reference start values -+1e5) and dg
   float mn[5] = {1.0e5f, 1.0e5f, 1.0e5f, 1.0e5f, INFINITY};
   float mx[5] = {-1.0e5f, -1.0e5f, -1.0e5f, -1.0e5f, -INFINITY};
-  double bre[NB], bim[NB];
+  // bunching sums: compensated FP64 (csum_*) per thread, over the warp and
+  // over the CTA's warps
+  double bre[NB], bim[NB], brc[NB], bic[NB];
 #pragma unroll
-  for (int h = 0; h < NB; ++h) bre[h] = bim[h] = 0.0;
+  for (int h = 0; h < NB; ++h) bre[h] = bim[h] = brc[h] = bic[h] = 0.0;
   // in a wider CTA only the first kDiagThreads threads sum (the same layout)
   for (int pb = tid < kDiagThreads ? tid : np; pb < np; pb += U * kDiagThreads) {
     float2 lxy[U], lpp[U];
@@ -586,8 +589,8 @@ __device__ __forceinline__ void diag_slice(const BeamDiagArgs& a, const int bs, 
 #pragma unroll
       for (int h = 0; h < NB; ++h) {
         if (h >= a.nbunch) break;
-        bre[h] += ch;
-        bim[h] += sh;
+        ptx::csum_add(bre[h], brc[h], (double)ch);
+        ptx::csum_add(bim[h], bic[h], (double)sh);
         const float nc = __fmaf_rn(ch, c1, -__fmul_rn(sh, s1));
         const float ns = __fmaf_rn(sh, c1, __fmul_rn(ch, s1));
         ch = nc;
@@ -619,14 +622,14 @@ __device__ __forceinline__ void diag_slice(const BeamDiagArgs& a, const int bs, 
 #pragma unroll
   for (int h = 0; h < NB; ++h) {
     if (h >= a.nbunch) break;
-    double tr = bre[h], ti = bim[h];
-    for (int o = 16; o > 0; o >>= 1) {
-      tr += __shfl_xor_sync(0xffffffffu, tr, o);
-      ti += __shfl_xor_sync(0xffffffffu, ti, o);
-    }
+    double tr = bre[h], trc = brc[h], ti = bim[h], tic = bic[h];
+    ptx::csum_warp(tr, trc, 32);
+    ptx::csum_warp(ti, tic, 32);
     if (l == 0 && w < kDiagThreads / 32) {
       dpart[w][kBeamRec + 2 * h] = tr;
       dpart[w][kBeamRec + 2 * h + 1] = ti;
+      bcomp[w][2 * h] = trc;
+      bcomp[w][2 * h + 1] = tic;
     }
   }
   __syncthreads();
@@ -637,7 +640,13 @@ __device__ __forceinline__ void diag_slice(const BeamDiagArgs& a, const int bs, 
     const double N = (double)np;
     const int op = tid < 13 ? 0 : (tid < kBeamRec ? ((tid - 13) % 2 == 0 ? 1 : 2) : 0);
     double t = N;
-    if (tid != 12) {
+    if (tid >= kBeamRec) {  // bunching: the warps' compensated partials
+      const int q = tid - kBeamRec;
+      double tc = bcomp[0][q];
+      t = dpart[0][tid];
+      for (int i = 1; i < kDiagThreads / 32; ++i) ptx::csum_merge(t, tc, dpart[i][tid], bcomp[i][q]);
+      t += tc;
+    } else if (tid != 12) {
       t = dpart[0][tid];
       for (int i = 1; i < kDiagThreads / 32; ++i) {
         const double u = dpart[i][tid];
@@ -1034,16 +1043,17 @@ __device__ __forceinline__ void finalize_range(const FinalizeArgs& a, int i0, in
       const int f = j / a.nslice, s = j - f * a.nslice;
       const double* p = a.part[f] + (size_t)s * a.nband[f] * 9 + q;
       const int nbf = a.nband[f];
-      double v = 0.0;
-      for (int b0 = 0; b0 < nbf; b0 += 32) {  // up to 32 loads in flight, added in band order
+      double v = 0.0, vc = 0.0;  // compensated sum of the bands, in band order
+      for (int b0 = 0; b0 < nbf; b0 += 32) {  // up to 32 loads in flight
         const int m = min(32, nbf - b0);
         double t[32];
 #pragma unroll
         for (int k = 0; k < 32; ++k) t[k] = k < m ? p[(b0 + k) * 9] : 0.0;
 #pragma unroll
         for (int k = 0; k < 32; ++k)
-          if (k < m) v += t[k];
+          if (k < m) ptx::csum_add(v, vc, t[k]);
       }
+      v += vc;
       const int is = (a.nslice + s - a.first_after[f]) % a.nslice;
       a.field_hist[((size_t)f * a.nslice + is) * 9 + q] = v;
     } else if (i < 9 * nf + nb) {
