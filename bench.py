@@ -134,21 +134,23 @@ def replica_throughput(world, nslice, steps, ms):
 
 
 def profile_traffic(kernel, wl):
-    """DRAM bytes per launch of a mixed kernel from the committed ncu summary
-    (captured on 1024 slices x 8192 particles, ngrid 201), scaled by the
-    particles or cells of this workload; None if not profiled."""
-    path = ROOT / "profiles" / "mixed_step_sase1024x8192_n201.md"
+    """DRAM bytes per launch of a mixed kernel from the committed ncu counters
+    (profiles/mixed_step_sase1024x8192_n201.traffic.json, captured on 1024
+    slices x 8192 particles, ngrid 201), scaled by the particles or cells of
+    this workload; None if not profiled."""
+    path = ROOT / "profiles" / "mixed_step_sase1024x8192_n201.traffic.json"
     if not path.exists():
         return None
-    for line in path.read_text().splitlines():
-        f = line.split()
-        if len(f) == 3 and f[0] == "traffic" and f[1] == kernel:
-            if kernel.startswith("adi"):
-                scale = wl.nslice * wl.ngrid ** 2 / (1024 * 201 ** 2)
-            else:
-                scale = wl.nslice * wl.npart / (1024 * 8192)
-            return int(float(f[2]) * scale)
-    return None
+    d = json.loads(path.read_text())
+    b = d["bytes_per_launch"].get(kernel)
+    if b is None:
+        return None
+    w = d["workload"]
+    if kernel.startswith("adi"):
+        scale = wl.nslice * wl.ngrid ** 2 / (w["nslice"] * w["ngrid"] ** 2)
+    else:
+        scale = wl.nslice * wl.npart / (w["nslice"] * w["npart"])
+    return int(b * scale)
 
 
 def measured_peak():
@@ -693,7 +695,7 @@ def run_ours(args, wl, rank, world):
             "peak_source": peak_kind, "unit": "GB/s", "frac": d["gbs"] / peak,
             "traffic": profile_traffic(dom, wl), "alg_bytes_per_launch": d["alg_bytes"],
             "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch, "
-                              "profiles/mixed_step_sase1024x8192_n201.md",
+                              "profiles/mixed_step_sase1024x8192_n201.traffic.json",
             "timing": "CUDA events around each launch on the launching stream, "
                       f"{kp} direct-launch steps following the graph-timed region"}
 
