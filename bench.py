@@ -53,10 +53,11 @@ def parse_args(argv=None):
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-accuracy", action="store_true")
-    p.add_argument("--workload", choices=["sase", "scan", "serve", "sase_h3", "steady"],
+    p.add_argument("--workload", choices=["sase", "scan", "serve", "sase_h3", "steady", "fft"],
                    default="sase",
                    help="sase: the headline line; the others measure the batched scan, "
-                        "the served stream, the large SASE with h=1 and h=3, steady state")
+                        "the served stream, the large SASE with h=1 and h=3, steady state, "
+                        "the FFT field solver")
     p.add_argument("--runs", type=int, default=256, help="scan: runs in the batch")
     p.add_argument("--requests", type=int, default=400, help="serve: requests in the stream")
     p.add_argument("--rate", type=float, default=200.0, help="serve: arrivals per second")
@@ -586,6 +587,65 @@ def run_steady(args):
     print(json.dumps(line), flush=True)
 
 
+def run_fft(args):
+    """The FFT field solver (FieldSolverFFTCUDA form, FP64) on the headline
+    field: 1024 slices, ngrid 201, the SASE beam's source every step; device
+    time per field step and per kernel (CUDA events on the library's
+    stream), beside the ADI solver on the same state."""
+    import torch
+    from genesis4_cuda_port_b200 import device as dev, workloads
+    wl = workloads.sase(args.nslice, args.npart, args.ngrid)
+    ctx = dev.Context(int(os.environ.get("LOCAL_RANK", "0")))
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    off, parts = wl.make_beam()
+    lat = wl.make_lattice()
+    beam = dev.BeamState(ctx, off, wl.gamma0)
+    beam.upload(parts)
+    beam.set_current(np.full(wl.nslice, wl.current))
+    fld = dev.FieldState(ctx, wl.nslice, wl.ngrid, wl.gridmax, wl.lambda0)
+    rng = np.random.default_rng(3)
+    cells = (rng.normal(size=(wl.nslice, wl.ngrid, wl.ngrid)) +
+             1j * rng.normal(size=(wl.nslice, wl.ngrid, wl.ngrid))) * 1e9
+    fld.upload(cells)
+    st, fc = lat.steps[0], lat.fc(0, 1)
+    out = {}
+    for name, solver in (("fft", dev.FieldSolverFFTCUDA(ctx)), ("adi", dev.FieldSolverADICUDA(ctx))):
+        solver.init(st.delz, fld.dgrid, fld.xks, wl.ngrid)
+        for _ in range(args.warmup):
+            solver.advance(fld, beam, st, fc)
+        ctx.synchronize()
+        ctx.profile(True)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            solver.advance(fld, beam, st, fc)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        prof = ctx.profile_read()
+        ctx.profile(False)
+        out[name] = {"ms_per_step": e0.elapsed_time(e1) / args.steps,
+                     "kernels": {k: {"launches": c, "avg_ms": t / max(c, 1)}
+                                 for k, (c, t) in prof.items()}}
+        solver.close()
+    C = wl.nslice * wl.ngrid ** 2
+    alg = {"fft_rows_fwd": 32 * C, "fft_cols": 32 * C, "fft_rows_inv": 32 * C}
+    peak, kind = measured_peak()
+    k = out["fft"]["kernels"]
+    dom = max((n for n in k if n in alg), key=lambda n: k[n]["avg_ms"])
+    gbs = alg[dom] / (k[dom]["avg_ms"] / 1e3) / 1e9
+    line = {"metric": "slice-steps/s of the FFT field step (FP64)",
+            "value": wl.nslice / (out["fft"]["ms_per_step"] / 1e3), "unit": "slice-steps/s",
+            "higher_is_better": True, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": out["fft"]["ms_per_step"], "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"FFT field step {wl.nslice} slices, ngrid {wl.ngrid}, "
+                                   f"source of {wl.npart} particles per slice"},
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": gbs, "peak": peak,
+                         "peak_source": kind, "unit": "GB/s", "frac": gbs / peak,
+                         "alg_bytes_per_launch": alg[dom], "traffic": None},
+            "fft": out["fft"], "adi_same_state": out["adi"]}
+    print(json.dumps(line), flush=True)
+
+
 def run_ours(args, wl, rank, world):
     import torch
 
@@ -745,7 +805,7 @@ def main(argv=None):
     if args.workload != "sase":
         if rank == 0:
             {"scan": run_scan, "serve": run_serve, "sase_h3": run_h3,
-             "steady": run_steady}[args.workload](args)
+             "steady": run_steady, "fft": run_fft}[args.workload](args)
         return
     run_ours(args, wl, rank, world)
 
