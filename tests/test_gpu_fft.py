@@ -174,7 +174,9 @@ def test_fft_deck_matches_the_oracle():
                         sig=0.05)
         acc, first, _ = orc.slippage(cells, lat.slip[i], s["sample"], True, False, acc, first)
         power.append(orc.diag_field(cells, first)[0][:, 0])
-    power = np.array(power)
+    dgrid = 2 * gm / (n - 1)
+    scl = dgrid * 510998.95 / xks  # raw sum of |u|^2 -> W (DiagnosticCUDA.cpp:686, :735)
+    power = np.array(power) * scl * scl / 376.73031346177
     got = res.field[0]["power"]
     assert got.shape == power.shape
     assert abs(power[-1].sum() - power[0].sum()) > 1e-3 * power[0].sum()

@@ -27,6 +27,14 @@ pytestmark = [pytest.mark.gpu,
                                         "reference tree at build time)")]
 
 
+def _rtol(record):
+    """1e-11, except for the energy spread sqrt(<g^2> - <g>^2): at gamma ~ 1e4
+    and a spread ~ 1 it amplifies the rounding of the FP64 sums (taken in a
+    different order by the reference's block reduction) by <g^2>/spread^2 ~ 1e8,
+    so 1e-6 there."""
+    return 1e-6 if record.endswith("energyspread") else 1e-11
+
+
 def _rel(a, b):
     return float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
 
@@ -170,7 +178,7 @@ def test_deck_step0_records_match_reference_diagnostics():
         if k not in res.beam:
             continue
         got = res.beam[k][0]
-        np.testing.assert_allclose(got, ref, rtol=1e-11, atol=1e-13 * np.max(np.abs(ref)),
+        np.testing.assert_allclose(got, ref, rtol=_rtol(k), atol=1e-13 * np.max(np.abs(ref)),
                                    err_msg=k)
         compared += 1
     assert compared >= 30, compared
@@ -179,7 +187,7 @@ def test_deck_step0_records_match_reference_diagnostics():
         if k not in res.field[0]:
             continue
         got = res.field[0][k][0] if res.field[0][k].ndim > 1 else res.field[0][k][:1]
-        np.testing.assert_allclose(got, ref, rtol=1e-11, atol=1e-13 * np.max(np.abs(ref)),
+        np.testing.assert_allclose(got, ref, rtol=_rtol(k), atol=1e-13 * np.max(np.abs(ref)),
                                    err_msg=k)
         compared += 1
     assert compared >= 12, compared
