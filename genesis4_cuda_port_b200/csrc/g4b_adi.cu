@@ -464,7 +464,9 @@ __device__ __forceinline__ V block_reduce(V v, V* sh, bool is_max) {
   return r;
 }
 
-__global__ void __launch_bounds__(512) deposit_slice_kernel(const DepositArgs a) {
+constexpr int kDepFp64U = 2;  // particles in flight per thread (FP64 deposition)
+
+__global__ void __launch_bounds__(512, 2) deposit_slice_kernel(const DepositArgs a) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ double shd[16];
   __shared__ int shi[16];
@@ -478,20 +480,36 @@ __global__ void __launch_bounds__(512) deposit_slice_kernel(const DepositArgs a)
 
   double qmax = 0.0;
   int ixmin = 1 << 30, iymin = 1 << 30, ixmax = -1, iymax = -1, cnt = 0;
+  const int nt = blockDim.x;
   if (scl != 0.0) {
-    for (int64_t p = p0 + tid; p < p1; p += blockDim.x) {
-      int ix, iy;
-      double wx, wy;
-      const double xp = a.x[p], yp = a.y[p];
-      if (!dep_cell(a, xp, yp, ix, iy, wx, wy)) continue;
-      const double q = fabs(dep_weight(a, xp, yp, a.gamma[p]));
-      qmax = q > qmax ? q : qmax;
-      if (!(q <= 1e300)) qmax = INFINITY;  // NaN or inf
-      ixmin = min(ixmin, ix);
-      ixmax = max(ixmax, ix);
-      iymin = min(iymin, iy);
-      iymax = max(iymax, iy);
-      ++cnt;
+    // kDepFp64U particles in flight per thread: their loads are issued
+    // before any of them is processed
+    for (int64_t pb = p0 + tid; pb < p1; pb += (int64_t)kDepFp64U * nt) {
+      double lx[kDepFp64U], ly[kDepFp64U], lg[kDepFp64U];
+#pragma unroll
+      for (int u = 0; u < kDepFp64U; ++u) {
+        const int64_t p = pb + (int64_t)u * nt;
+        if (p < p1) {
+          lx[u] = a.x[p];
+          ly[u] = a.y[p];
+          lg[u] = a.gamma[p];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < kDepFp64U; ++u) {
+        if (pb + (int64_t)u * nt >= p1) break;
+        int ix, iy;
+        double wx, wy;
+        if (!dep_cell(a, lx[u], ly[u], ix, iy, wx, wy)) continue;
+        const double q = fabs(dep_weight(a, lx[u], ly[u], lg[u]));
+        qmax = q > qmax ? q : qmax;
+        if (!(q <= 1e300)) qmax = INFINITY;  // NaN or inf
+        ixmin = min(ixmin, ix);
+        ixmax = max(ixmax, ix);
+        iymin = min(iymin, iy);
+        iymax = max(iymax, iy);
+        ++cnt;
+      }
     }
   }
   qmax = block_reduce<double>(qmax, shd, true);
@@ -531,15 +549,29 @@ __global__ void __launch_bounds__(512) deposit_slice_kernel(const DepositArgs a)
     const int hb = min(band_h, by0 + bh - yb);
     for (int i = tid; i < 2 * hb * bw; i += blockDim.x) acc[i] = 0ull;
     __syncthreads();
-    for (int64_t p = p0 + tid; p < p1; p += blockDim.x) {
+    for (int64_t pb = p0 + tid; pb < p1; pb += (int64_t)kDepFp64U * nt) {
+      double lx[kDepFp64U], ly[kDepFp64U], lg[kDepFp64U], lt[kDepFp64U];
+#pragma unroll
+      for (int u = 0; u < kDepFp64U; ++u) {
+        const int64_t p = pb + (int64_t)u * nt;
+        if (p < p1) {
+          lx[u] = a.x[p];
+          ly[u] = a.y[p];
+          lg[u] = a.gamma[p];
+          lt[u] = a.theta[p];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < kDepFp64U; ++u) {
+      if (pb + (int64_t)u * nt >= p1) break;
       int ix, iy;
       double wx, wy;
-      const double xp = a.x[p], yp = a.y[p];
+      const double xp = lx[u], yp = ly[u];
       if (!dep_cell(a, xp, yp, ix, iy, wx, wy)) continue;
       if (iy + 1 < yb || iy >= yb + hb) continue;
-      const double q = dep_weight(a, xp, yp, a.gamma[p]);
+      const double q = dep_weight(a, xp, yp, lg[u]);
       double sn, cs;
-      sincos(hphase * a.theta[p], &sn, &cs);
+      sincos(hphase * lt[u], &sn, &cs);
       const double vre = sn * q * scale, vim = cs * q * scale;
       const double w[4] = {wx * wy, (1.0 - wx) * wy, wx * (1.0 - wy),
                            (1.0 - wx) * (1.0 - wy)};
@@ -552,6 +584,7 @@ __global__ void __launch_bounds__(512) deposit_slice_kernel(const DepositArgs a)
         const int cell = ry * bw + (cx[c] - bx0);
         atomicAdd(&acc[2 * cell], (unsigned long long)__double2ll_rn(vre * w[c]));
         atomicAdd(&acc[2 * cell + 1], (unsigned long long)__double2ll_rn(vim * w[c]));
+      }
       }
     }
     __syncthreads();

@@ -187,8 +187,10 @@ def test_deck_step0_records_match_reference_diagnostics():
         if k not in res.field[0]:
             continue
         got = res.field[0][k][0] if res.field[0][k].ndim > 1 else res.field[0][k][:1]
-        np.testing.assert_allclose(got, ref, rtol=_rtol(k), atol=1e-13 * np.max(np.abs(ref)),
-                                   err_msg=k)
+        # centroids of the centred symmetric seed are rounding noise (~1e-22 m):
+        # an absolute floor far below any grid spacing
+        atol = max(1e-13 * np.max(np.abs(ref)), 1e-15 if "position" in k else 0.0)
+        np.testing.assert_allclose(got, ref, rtol=_rtol(k), atol=atol, err_msg=k)
         compared += 1
     assert compared >= 12, compared
     assert math.isfinite(float(res.field[0]["power"][-1].sum()))
