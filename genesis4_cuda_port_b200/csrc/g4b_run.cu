@@ -544,11 +544,12 @@ __device__ __forceinline__ void diag_slice(const BeamDiagArgs& a, const int bs, 
   // minima / maxima of x, px, y, py (reference start values -+1e5) and dg
   float mn[5] = {1.0e5f, 1.0e5f, 1.0e5f, 1.0e5f, INFINITY};
   float mx[5] = {-1.0e5f, -1.0e5f, -1.0e5f, -1.0e5f, -INFINITY};
-  // bunching sums: compensated FP64 (csum_*) per thread, over the warp and
-  // over the CTA's warps
-  double bre[NB], bim[NB], brc[NB], bic[NB];
+  // bunching sums: each thread adds its FP32 terms (at most 256: 65536
+  // particles over 256 threads) in FP64, within 2^-45 of their magnitude;
+  // the warp and the CTA's warps add with compensation (csum_*)
+  double bre[NB], bim[NB];
 #pragma unroll
-  for (int h = 0; h < NB; ++h) bre[h] = bim[h] = brc[h] = bic[h] = 0.0;
+  for (int h = 0; h < NB; ++h) bre[h] = bim[h] = 0.0;
   // in a wider CTA only the first kDiagThreads threads sum (the same layout)
   for (int pb = tid < kDiagThreads ? tid : np; pb < np; pb += U * kDiagThreads) {
     float2 lxy[U], lpp[U];
@@ -589,8 +590,8 @@ __device__ __forceinline__ void diag_slice(const BeamDiagArgs& a, const int bs, 
 #pragma unroll
       for (int h = 0; h < NB; ++h) {
         if (h >= a.nbunch) break;
-        ptx::csum_add(bre[h], brc[h], (double)ch);
-        ptx::csum_add(bim[h], bic[h], (double)sh);
+        bre[h] += ch;
+        bim[h] += sh;
         const float nc = __fmaf_rn(ch, c1, -__fmul_rn(sh, s1));
         const float ns = __fmaf_rn(sh, c1, __fmul_rn(ch, s1));
         ch = nc;
@@ -622,7 +623,7 @@ __device__ __forceinline__ void diag_slice(const BeamDiagArgs& a, const int bs, 
 #pragma unroll
   for (int h = 0; h < NB; ++h) {
     if (h >= a.nbunch) break;
-    double tr = bre[h], trc = brc[h], ti = bim[h], tic = bic[h];
+    double tr = bre[h], trc = 0.0, ti = bim[h], tic = 0.0;
     ptx::csum_warp(tr, trc, 32);
     ptx::csum_warp(ti, tic, 32);
     if (l == 0 && w < kDiagThreads / 32) {
