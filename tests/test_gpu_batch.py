@@ -116,3 +116,26 @@ def test_run_joins_a_batch_in_progress(ctx):
     for r, cfg, ref in zip(runs, CONFIGS, alone):
         _same(_result(r, cfg["nsteps"]), ref)
     batch.close()
+
+
+def test_one_launch_adi_equals_the_two_pass_form(ctx):
+    """A run of at least 68 slices solves both ADI passes in one persistent
+    launch with R' in an L2-resident ring; the same run advanced by the batch
+    engine (two passes through DRAM) gives the same bits, with slippage every
+    step and the diagnostics of every step."""
+    cfg = dict(nslice=150, npart=256, ngrid=65, taper=0.0, dgam=0.0, time_run=True, nsteps=5)
+    alone = _make(ctx, 9, cfg)
+    alone.advance(0, cfg["nsteps"], graph=False)
+    ref = _result(alone, cfg["nsteps"])
+    alone.close()
+    graphed = _make(ctx, 9, cfg)
+    graphed.advance(0, cfg["nsteps"], graph=True)
+    _same(_result(graphed, cfg["nsteps"]), ref)
+    graphed.close()
+    batch = dev.Batch(ctx, 2)
+    run = _make(ctx, 9, cfg)
+    batch.attach(run, 0, cfg["nsteps"])
+    batch.step(cfg["nsteps"], graph=False)
+    ctx.synchronize()
+    _same(_result(run, cfg["nsteps"]), ref)
+    batch.close()
