@@ -92,7 +92,14 @@ _SIGS = {
     "g4b_beam_download": (C.c_int, [C.c_void_p] + [c_double_p] * 6),
     "g4b_beam_set_current": (C.c_int, [C.c_void_p, c_double_p]),
     "g4b_beam_set_eloss": (C.c_int, [C.c_void_p, c_double_p]),
+    "g4b_beam_set_particle_ez": (C.c_int, [C.c_void_p, c_double_p]),
+    "g4b_beam_get_particle_ez": (C.c_int, [C.c_void_p, c_double_p]),
     "g4b_beam_device_bytes": (C.c_int, [C.c_void_p, c_uint64_p]),
+    "g4b_efield_create": (C.c_int, [C.c_void_p, C.c_double, C.c_int, C.c_int, C.c_int,
+                                    C.c_double, c_void_pp]),
+    "g4b_efield_destroy": (C.c_int, [C.c_void_p]),
+    "g4b_efield_has_short_range": (C.c_int, [C.c_void_p]),
+    "g4b_efield_short_range": (C.c_int, [C.c_void_p, C.c_void_p, C.c_double]),
     "g4b_adi_create": (C.c_int, [C.c_void_p, c_void_pp]),
     "g4b_adi_destroy": (C.c_int, [C.c_void_p]),
     "g4b_adi_init": (C.c_int, [C.c_void_p, C.c_double, C.c_double,

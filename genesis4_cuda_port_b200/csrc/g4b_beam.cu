@@ -165,6 +165,7 @@ struct PushArgs {
   const double *x, *y, *px, *py;
   const int4* chunks;
   const double* eloss;
+  const double* pez;  // per-particle loss, or null: the slice's eloss
   PushField f[kMaxFields];
   int nfield;
   double xks, xku, aw, autophase, delz, ax, ay, kx, ky, gradx, grady;
@@ -241,7 +242,8 @@ __global__ void __launch_bounds__(256) push_kernel(const PushArgs a) {
   const double dx = xp - a.ax, dy = yp - a.ay;
   const double awloc = 1.0 + 0.5 * (a.kx * dx * dx + a.ky * dy * dy) + a.gradx * dx + a.grady * dy;
   const double btpar = 1.0 + pxp * pxp + pyp * pyp + a.aw * a.aw * awloc * awloc;
-  const double ez = a.eloss[slice];
+  // load_longitudinal_ez (src/Core/BeamSolverCUDA.cpp:184-195)
+  const double ez = a.pez ? a.pez[ip] : a.eloss[slice];
   double rr[NF > 0 ? NF : kMaxFields], ri[NF > 0 ? NF : kMaxFields];
 #pragma unroll
   for (int i = 0; i < (NF > 0 ? NF : kMaxFields); ++i) {
@@ -389,6 +391,7 @@ int g4b_beam_advance(g4b_beam* b, g4b_field* const* fields, const double* fc, in
   a.py = b->py;
   a.chunks = b->d_chunks;
   a.eloss = b->d_eloss;
+  a.pez = b->use_pez ? b->d_pez : nullptr;
   a.nfield = nfield;
   double xks_local = 1.0;
   for (int i = 0; i < nfield; ++i) {

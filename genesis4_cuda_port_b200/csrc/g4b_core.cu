@@ -660,7 +660,7 @@ int g4b_beam_destroy(g4b_beam* b) {
   if (!b) return G4B_OK;
   ctx_quiesce(b->ctx);
   void* ptrs[] = {b->x, b->y, b->px, b->py, b->gamma, b->theta, b->d_off,
-                  b->d_current, b->d_eloss, b->d_scl, b->d_chunks};
+                  b->d_current, b->d_eloss, b->d_scl, b->d_chunks, b->d_pez};
   for (void* p : ptrs) dev_free(b->ctx, p);
   ctx_release(b->ctx);
   delete b;

@@ -113,6 +113,10 @@ struct g4b_beam {
   double* d_current = nullptr;
   double* d_eloss = nullptr;
   double* d_scl = nullptr;           // per-slice source scale
+  // per-particle loss (space charge + slice loss); the push reads it in
+  // place of d_eloss while use_pez is set
+  double* d_pez = nullptr;
+  int use_pez = 0;
   // CTA work chunks: (slice, begin, end) over the particle index space.
   int nchunk = 0;
   int4* d_chunks = nullptr;          // x = slice, y = begin lo, z = end lo, w = hi bits

@@ -265,6 +265,18 @@ void TrackBeamCUDA::applyR56(Beam* beam, Undulator* und, double lambda0) {
   check(g4b_beam_r56(beam->beamSoA, &und->current(), lambda0), "TrackBeamCUDA::applyR56");
 }
 
+BeamSolverCUDA::~BeamSolverCUDA() { g4b_efield_destroy(efield); }
+
+void BeamSolverCUDA::initEField(double rmax, int ngrid, int nz, int nphi, double lambda,
+                                bool longr) {
+  if (longr)
+    throw std::runtime_error("BeamSolverCUDA::initEField: long-range space charge is not built");
+  g4b_efield_destroy(efield);
+  efield = nullptr;
+  check(g4b_efield_create(cuda_context(), rmax, ngrid, nz, nphi, lambda, &efield),
+        "BeamSolverCUDA::initEField");
+}
+
 // BeamSolverCUDA::advance (src/Core/BeamSolverCUDA.cpp:449-683)
 void BeamSolverCUDA::advance(double, Beam* beam, std::vector<Field*>* field, Undulator* und) {
   if (!beam || !field || !und)
@@ -280,6 +292,13 @@ void BeamSolverCUDA::advance(double, Beam* beam, std::vector<Field*>* field, Und
     fc.push_back(und->fc(f->getHarm()));
   }
   if (fl.size() > 8) throw std::runtime_error("BeamSolverCUDA::advance exceeds kMaxBeamSolverFields");
+  // short-range space charge: per-particle loss before the push
+  // (src/Core/BeamSolverCUDA.cpp:519-547)
+  if (g4b_efield_has_short_range(efield)) {
+    const g4b_step& st = und->current();
+    const double gammaz2 = st.gamma_ref * st.gamma_ref / (1.0 + st.aw * st.aw);
+    check(g4b_efield_short_range(efield, beam->beamSoA, gammaz2), "BeamSolverCUDA::advance");
+  }
   check(g4b_beam_advance(beam->beamSoA, fl.data(), fc.data(), (int)fl.size(), &und->current()),
         "BeamSolverCUDA::advance");
 }

@@ -115,6 +115,13 @@ class TrackBeamCUDA {  // include/TrackBeamCUDA.h:7-15
 
 class BeamSolverCUDA {  // include/BeamSolverCUDA.h:17-37
  public:
+  BeamSolverCUDA() = default;
+  BeamSolverCUDA(const BeamSolverCUDA&) = delete;
+  BeamSolverCUDA& operator=(const BeamSolverCUDA&) = delete;
+  ~BeamSolverCUDA();
+  // include/BeamSolverCUDA.h:41-43: short-range space charge on the device
+  // (g4b_efield); longrange (upstream's long-range model) is not built
+  void initEField(double rmax, int ngrid, int nz, int nphi, double lambda, bool longr);
   void advance(double delz, Beam* beam, std::vector<Field*>* field, Undulator* und);
   void track(double delz, Beam* beam, Undulator* und, bool last) {
     tracker.track(delz, beam, und, last);
@@ -126,6 +133,7 @@ class BeamSolverCUDA {  // include/BeamSolverCUDA.h:17-37
  private:
   bool onlyFundamental = false;
   TrackBeamCUDA tracker;
+  g4b_efield* efield = nullptr;
 };
 
 // Beam (include/Beam.h:24-105)
@@ -134,6 +142,10 @@ class Beam {
   Beam();
   virtual ~Beam();
   void init(int nsize, int nbins, double reflen, double slicelen, double s0, bool one4one);
+  // include/Beam.h:128-133
+  void initEField(double rmax, int ngrid, int nz, int nphi, double lambda, bool longr) {
+    cuda_solver.initEField(rmax, ngrid, nz, nphi, lambda, longr);
+  }
   void track(double delz, std::vector<Field*>* field, Undulator* und);
   void setUseCuda(bool in) { useCudaSolver_ = in; }
   void init_beamSoA();

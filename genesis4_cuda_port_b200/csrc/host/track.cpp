@@ -2,7 +2,7 @@
 //
 // A deck is a sequence of `&group key=value ... &end` blocks, read in order
 // as upstream GENESIS 1.3 v4 does: &setup, &lattice, &time, &field (one per
-// harmonic), &beam, &track.  The keys follow the upstream manual; &track
+// harmonic), &beam, &efield, &track.  The keys follow the upstream manual; &track
 // keeps the reference's keys (src/Main/Track.cpp:8-96, incl. use_cuda and
 // low_memory_adisolver) and adds `precision = fp64 | mixed`, which selects
 // between the drop-in FP64 classes and the fused mixed-precision run.
@@ -211,6 +211,9 @@ struct Deck {
   double xcut = 1, ycut = 1, sigmoid = 1;        // &track xcut, ycut, sigmoid
   int precision = G4B_FP64, output_step = 1, beam_dump = 0, field_dump = 0;
   double zstop = 1e9;
+  // &efield: short-range space charge (upstream manual keys)
+  double sc_rmax = 0;
+  int sc_ngrid = 100, sc_nz = 0, sc_nphi = 0;
   Undulator und;
   // files: the deck's directory, &setup outputdir, &importbeam / &importfield
   std::string base, outputdir, import_beam;
@@ -359,6 +362,21 @@ bool parse_deck(const std::string& text, const std::string* lat_text, const std:
       r.num("bunchphase", 0.0);
       r.num("emodphase", 0.0);
       if (!r.done()) return false;
+    } else if (name == "efield") {
+      d.sc_rmax = r.num("rmax", 0.0);
+      d.sc_ngrid = (int)r.num("ngrid", 100);
+      d.sc_nz = (int)r.num("nz", 0);
+      d.sc_nphi = (int)r.num("nphi", 0);
+      const bool longrange = r.flag("longrange", false);
+      if (!r.done()) return false;
+      if (longrange) {
+        set_error("deck: &efield longrange (upstream's long-range model) is not supported");
+        return false;
+      }
+      if (d.sc_rmax < 0 || d.sc_ngrid < 0 || d.sc_nz < 0 || d.sc_nphi < 0) {
+        set_error("deck: &efield needs rmax, ngrid, nz, nphi >= 0");
+        return false;
+      }
     } else if (name == "track") {
       have_track = true;
       d.zstop = r.num("zstop", 1e9);
@@ -390,6 +408,10 @@ bool parse_deck(const std::string& text, const std::string* lat_text, const std:
       }
       if (d.fft && d.precision == G4B_MIXED) {
         set_error("deck: fft_fieldsolver runs the FP64 drop-in form (precision = fp64)");
+        return false;
+      }
+      if (d.sc_nz > 0 && d.sc_rmax > 0 && d.precision == G4B_MIXED) {
+        set_error("deck: &efield space charge runs the FP64 drop-in form (precision = fp64)");
         return false;
       }
       if (sort_step != 0) {
@@ -591,6 +613,8 @@ int g4h_deck_run(g4h_deck* dk, g4h_result** out) {
       fl.push_back(f.get());
       fields.push_back(std::move(f));
     }
+    if (d.sc_nz > 0 && d.sc_rmax > 0)  // Beam::initEField (include/Beam.h:128-133)
+      beam.initEField(d.sc_rmax, d.sc_ngrid, d.sc_nz, d.sc_nphi, d.lambda0, false);
     auto res = std::make_unique<g4h_result>();
     GencoreTimers t;
     const bool isTime = d.time && ns > 1;

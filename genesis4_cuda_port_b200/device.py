@@ -190,6 +190,19 @@ class BeamState:
         a = None if eloss is None else np.ascontiguousarray(eloss, dtype=np.float64)
         check(self.lib.g4b_beam_set_eloss(self.h, dptr(a)))
 
+    def set_particle_ez(self, ez=None) -> None:
+        """Per-particle loss the push reads in place of the slice loss (None:
+        back to the slice loss)."""
+        a = None if ez is None else np.ascontiguousarray(ez, dtype=np.float64)
+        if a is not None:
+            assert a.size == self.npart
+        check(self.lib.g4b_beam_set_particle_ez(self.h, dptr(a)))
+
+    def particle_ez(self) -> np.ndarray:
+        out = np.empty(self.npart)
+        check(self.lib.g4b_beam_get_particle_ez(self.h, dptr(out)))
+        return out
+
     # TrackBeamCUDA::track / applyR56 and BeamSolverCUDA::advance
     def track(self, step: Step, delz: float, last: bool) -> None:
         check(self.lib.g4b_beam_track(self.h, C.byref(step), delz, int(last)))
@@ -278,6 +291,36 @@ class FieldSolverFFTCUDA:
     def close(self) -> None:
         if getattr(self, "h", None):
             self.lib.g4b_fft_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class EFieldSolver:
+    """Short-range space charge on the device: BeamSolverCUDA::initEField
+    (rmax, ngrid, nz, nphi, lambda) and EFieldSolver::shortRange over every
+    slice, writing the beam's per-particle loss."""
+
+    def __init__(self, ctx: Context, rmax: float, ngrid: int, nz: int, nphi: int,
+                 lambda0: float):
+        self.ctx, self.lib = ctx, ctx.lib
+        h = C.c_void_p()
+        check(self.lib.g4b_efield_create(ctx.h, rmax, ngrid, nz, nphi, lambda0, C.byref(h)))
+        self.h = h
+
+    def has_short_range(self) -> bool:
+        return bool(self.lib.g4b_efield_has_short_range(self.h))
+
+    def short_range(self, beam: BeamState, gammaz2: float) -> None:
+        check(self.lib.g4b_efield_short_range(self.h, beam.h, gammaz2))
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.g4b_efield_destroy(self.h)
             self.h = None
 
     def __del__(self):

@@ -156,7 +156,36 @@ int g4b_beam_set_current(g4b_beam* b, const double* current);
 /* Per-slice longitudinal field loss -longESC/511000 that the push subtracts
  * (src/Core/BeamSolverCUDA.cpp:549-560).  NULL clears it to zero. */
 int g4b_beam_set_eloss(g4b_beam* b, const double* slice_eloss);
+/* Per-particle longitudinal loss, npart values in particle order, that the
+ * push reads in place of the slice loss: the reference's h_particle_ez
+ * (getEField(ip) - longESC/511000, src/Core/BeamSolverCUDA.cpp:525-547) and
+ * its UseParticleEz kernels (:184-195).  NULL returns to the slice loss. */
+int g4b_beam_set_particle_ez(g4b_beam* b, const double* ez);
+/* Copies the per-particle loss out (G4B_ERR_STATE when none is set). */
+int g4b_beam_get_particle_ez(g4b_beam* b, double* ez);
 int g4b_beam_device_bytes(g4b_beam* b, uint64_t* bytes);
+
+/* ---- short-range space charge ------------------------------------------------
+ * The solver behind BeamSolverCUDA::initEField (include/BeamSolverCUDA.h:41-43)
+ * and EFieldSolver::shortRange, which the reference runs on the host for
+ * every slice (src/Core/BeamSolverCUDA.cpp:523-547); here on the device.
+ * Per slice: the density modes e^{-i(l theta + m phi)}, l = 1..nz,
+ * m = -nphi..nphi, on ngrid radial cells out to rmax x the largest particle
+ * radius about the slice centroid; one radial tridiagonal solve per mode of
+ * (1/r d/dr r d/dr - m^2/r^2 - (l k_s)^2/gammaz2) u = -S; the particle's
+ * loss = -2 Z0 k_s I/(eev gammaz2) sum_l l Im[u_l e^{i l theta}] + slice loss,
+ * written to the beam's per-particle buffer (g4b_beam_set_particle_ez).
+ * Limits: nz*(2*nphi+1)*ngrid <= 5120, at most 2^22 particles per slice. */
+typedef struct g4b_efield g4b_efield;
+int g4b_efield_create(g4b_ctx* ctx, double rmax, int ngrid, int nz, int nphi, double lambda,
+                      g4b_efield** out);
+int g4b_efield_destroy(g4b_efield* e);
+/* EFieldSolver::hasShortRange: nz > 0, ngrid > 0 and rmax > 0. */
+int g4b_efield_has_short_range(const g4b_efield* e);
+/* EFieldSolver::shortRange over every slice of an FP64 beam, with
+ * gammaz2 = gamma_ref^2/(1 + aw^2) (src/Core/BeamSolverCUDA.cpp:521); uses the
+ * beam's current and slice loss.  A no-op when short range is off. */
+int g4b_efield_short_range(g4b_efield* e, g4b_beam* b, double gammaz2);
 
 /* ---- ADI field solver --------------------------------------------------------
  * FieldSolverADICUDA (include/FieldSolverADICUDA.h:20-25). */

@@ -487,7 +487,16 @@ void g4o_push(int nslice, const int64_t* off, const g4b_step* st,
               const g4o_field_view* fields, int nfield,
               const double* slice_eloss, const double* x, const double* y,
               const double* px, const double* py, double* gamma,
-              double* theta) { /* :449-683 and :226-409 */
+              double* theta) {
+  g4o_push_ez(nslice, off, st, fields, nfield, slice_eloss, NULL, x, y, px, py, gamma, theta);
+}
+
+void g4o_push_ez(int nslice, const int64_t* off, const g4b_step* st,
+                 const g4o_field_view* fields, int nfield,
+                 const double* slice_eloss, const double* particle_ez,
+                 const double* x, const double* y, const double* px,
+                 const double* py, double* gamma,
+                 double* theta) { /* :449-683 and :226-409 */
   if (nfield <= 0 || nfield > G4O_MAX_FIELDS) return;
   double rtmp[G4O_MAX_FIELDS], rharm[G4O_MAX_FIELDS];
   double xks_local = 1.0;
@@ -502,8 +511,10 @@ void g4o_push(int nslice, const int64_t* off, const g4b_step* st,
   const double delz = st->delz;
 #pragma omp parallel for schedule(dynamic, 1)
   for (int is = 0; is < nslice; is++) {
-    const double ez = slice_eloss ? slice_eloss[is] : 0.0;
+    const double ez_slice = slice_eloss ? slice_eloss[is] : 0.0;
     for (int64_t ip = off[is]; ip < off[is + 1]; ip++) {
+      /* load_longitudinal_ez (src/Core/BeamSolverCUDA.cpp:184-195) */
+      const double ez = particle_ez ? particle_ez[ip] : ez_slice;
       double g = gamma[ip];
       double th = theta[ip] + st->autophase;
       const double xp = x[ip], yp = y[ip];

@@ -81,6 +81,13 @@ void g4o_push(int nslice, const int64_t* off, const g4b_step* st,
               const double* slice_eloss, const double* x, const double* y,
               const double* px, const double* py, double* gamma,
               double* theta);
+/* The same with a per-particle loss (NULL: the slice loss), the reference's
+ * UseParticleEz kernels (src/Core/BeamSolverCUDA.cpp:184-195, 633-680). */
+void g4o_push_ez(int nslice, const int64_t* off, const g4b_step* st,
+                 const g4o_field_view* fields, int nfield,
+                 const double* slice_eloss, const double* particle_ez,
+                 const double* x, const double* y, const double* px,
+                 const double* py, double* gamma, double* theta);
 
 /* ControlCUDA::applySlippage, one rank (src/Core/ControlCUDA.cpp:148-252). */
 int g4o_slippage(int nslice, int ngrid, double shift, double sample,

@@ -72,6 +72,8 @@ def load():
     lib.g4o_r56.argtypes = [C.c_int64, sp, C.c_double, dp, dp]
     lib.g4o_push.argtypes = [C.c_int, i64p, sp, C.POINTER(FieldView), C.c_int,
                              dp, dp, dp, dp, dp, dp, dp]
+    lib.g4o_push_ez.argtypes = [C.c_int, i64p, sp, C.POINTER(FieldView), C.c_int,
+                                dp, dp, dp, dp, dp, dp, dp, dp]
     lib.g4o_slippage.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double,
                                  C.c_int, C.c_int, dp, ip, dp]
     lib.g4o_slippage.restype = C.c_int
@@ -162,8 +164,9 @@ def r56(parts, step, lambda0):
                    _d(parts["theta"]))
 
 
-def push(off, step, fields, parts, slice_eloss=None):
-    """fields: list of dicts(cells complex128 [S,n,n], first, harm, gridmax, xlambda, fc)."""
+def push(off, step, fields, parts, slice_eloss=None, particle_ez=None):
+    """fields: list of dicts(cells complex128 [S,n,n], first, harm, gridmax, xlambda, fc);
+    particle_ez: per-particle loss read in place of slice_eloss."""
     off, offp = _off(off)
     nf = len(fields)
     views = (FieldView * nf)()
@@ -182,9 +185,10 @@ def push(off, step, fields, parts, slice_eloss=None):
         views[i].fc = f["fc"]
         views[i].cells = cells.reshape(-1).view(np.float64).ctypes.data_as(dp)
     el = None if slice_eloss is None else np.ascontiguousarray(slice_eloss, np.float64)
-    load().g4o_push(len(off) - 1, offp, C.byref(step), views, nf, _d(el),
-                    _d(parts["x"]), _d(parts["y"]), _d(parts["px"]), _d(parts["py"]),
-                    _d(parts["gamma"]), _d(parts["theta"]))
+    pe = None if particle_ez is None else np.ascontiguousarray(particle_ez, np.float64)
+    load().g4o_push_ez(len(off) - 1, offp, C.byref(step), views, nf, _d(el), _d(pe),
+                       _d(parts["x"]), _d(parts["y"]), _d(parts["px"]), _d(parts["py"]),
+                       _d(parts["gamma"]), _d(parts["theta"]))
 
 
 def slippage(field, shift, sample, time_run, periodic, accuslip, first):
@@ -551,3 +555,93 @@ def gaussian_field(ngrid, gridmax, xlambda, power, w0):
     unit = dgrid * EEV / ks
     amp = np.sqrt(power * VACIMP / (unit * unit * s)) if (power > 0 and s > 0) else 0.0
     return (g * amp).astype(np.complex128)
+
+
+# ---------------------------------------------------------------------------
+# Short-range space charge.  The reference hands this to upstream GENESIS
+# 1.3 v4's EFieldSolver::shortRange on the host (src/Core/BeamSolverCUDA.cpp:
+# 523-547), which is absent from the reference tree: this restates the
+# device model of g4b_efield_short_range (radial finite-volume solve of
+# (1/r d/dr r d/dr - m^2/r^2 - (l k_s)^2/gamma_z^2) u = -S per density mode),
+# and tests pin it to the closed-form solution of the continuous problem.
+# PARITY UNPINNED against upstream.
+
+SC_FIX = 2.0 ** 40
+
+
+def sc_solve(acc, npart, m, kdr2):
+    """Radial Thomas solve of one mode in cell units: acc = the mode's
+    fixed-point cell sums (complex, already divided by 2^40), npart = slice
+    particle count, kdr2 = (l k_s dr)^2 / gamma_z^2.  Returns u per cell."""
+    n = acc.size
+    rhs = -acc / (2.0 * np.pi * npart)
+    cp = np.zeros(n)
+    d = np.zeros(n, complex)
+    pc, pd = 0.0, 0.0
+    for j in range(n):
+        rc, lo, up = j + 0.5, float(j), float(j + 1)
+        diag = -lo - (2.0 * up if j == n - 1 else up) - (m * m / (rc * rc) + kdr2) * rc
+        den = diag - lo * pc
+        pc = up / den if j < n - 1 else 0.0
+        pd = (rhs[j] - lo * pd) / den
+        cp[j], d[j] = pc, pd
+    u = d.copy()
+    for j in range(n - 2, -1, -1):
+        u[j] = d[j] - cp[j] * u[j + 1]
+    return u
+
+
+def short_range(off, parts, current, gammaz2, *, rmax, ngrid, nz, nphi, lambda0,
+                slice_eloss=None, return_modes=False):
+    """Per-particle loss (space charge + slice loss) of every particle."""
+    off = np.asarray(off, np.int64)
+    ns = off.size - 1
+    el = np.zeros(ns) if slice_eloss is None else np.asarray(slice_eloss, np.float64)
+    ks = 2.0 * np.pi / lambda0
+    coef = -2.0 * VACIMP * ks / (EEV * gammaz2)
+    out = np.zeros(int(off[-1]))
+    modes = []
+    for s in range(ns):
+        b, e = int(off[s]), int(off[s + 1])
+        npart = e - b
+        if npart == 0:
+            modes.append(None)
+            continue
+        x, y, th = parts["x"][b:e], parts["y"][b:e], parts["theta"][b:e]
+        xc, yc = x.sum() / npart, y.sum() / npart
+        dx, dy = x - xc, y - yc
+        r = np.sqrt(dx * dx + dy * dy)
+        R = rmax * np.sqrt(np.max(dx * dx + dy * dy))
+        if not R > 0 or current[s] == 0:
+            out[b:e] = el[s]
+            modes.append(None)
+            continue
+        dr = R / ngrid
+        j = np.minimum((r / dr).astype(np.int64), ngrid - 1)
+        safe = np.where(r > 0, r, 1.0)
+        cph, sph = np.where(r > 0, dx / safe, 1.0), np.where(r > 0, dy / safe, 0.0)
+        total = np.zeros(npart)
+        us = {}
+        for l in range(1, nz + 1):
+            cl, sl = np.cos(l * th), np.sin(l * th)
+            ph = {0: cl - 1j * sl}
+            pr, pi_, qr, qi = cl, -sl, cl, -sl
+            for m in range(1, nphi + 1):
+                pr, pi_ = pr * cph + pi_ * sph, pi_ * cph - pr * sph
+                qr, qi = qr * cph - qi * sph, qi * cph + qr * sph
+                ph[m], ph[-m] = pr + 1j * pi_, qr + 1j * qi
+            kdr2 = (l * ks * dr) ** 2 / gammaz2
+            acc_l = 0.0
+            for m in range(-nphi, nphi + 1):
+                qre = np.zeros(ngrid, np.int64)
+                qim = np.zeros(ngrid, np.int64)
+                np.add.at(qre, j, np.rint(ph[m].real * SC_FIX).astype(np.int64))
+                np.add.at(qim, j, np.rint(ph[m].imag * SC_FIX).astype(np.int64))
+                u = sc_solve((qre + 1j * qim) / SC_FIX, npart, m, kdr2)
+                us[(l, m)] = u
+                # Im[u e^{i(l theta + m phi)}] = Im[u conj(phase)]
+                acc_l = acc_l + np.imag(u[j] * np.conj(ph[m]))
+            total += l * acc_l
+        out[b:e] = el[s] + coef * current[s] * total
+        modes.append(dict(dr=dr, xc=xc, yc=yc, u=us))
+    return (out, modes) if return_modes else out

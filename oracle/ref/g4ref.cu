@@ -228,6 +228,7 @@ int g4ref_beam_advance(int nslice, const int* off, const g4b_step* st, int nfiel
     Beam beam;
     load_beam(beam, nslice, off, x, y, px, py, gamma, theta, nullptr);
     if (longESC) beam.longESC.assign(longESC, longESC + nslice);
+    g4ref_sc::off = off;
     BeamSolverCUDA solver;
     solver.advance(st->delz, &beam, &fields, &und);
     check(cudaGetLastError(), "beam advance");
@@ -239,6 +240,8 @@ int g4ref_beam_advance(int nslice, const int* off, const g4b_step* st, int nfiel
     return fail(e);
   }
 }
+
+void g4ref_set_particle_ez(const double* ez) { g4ref_sc::field = ez; }
 
 int g4ref_track(int npart, const g4b_step* st, double delz, int last_step, double* x,
                 double* y, double* px, double* py, const double* gamma) {

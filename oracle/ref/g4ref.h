@@ -58,6 +58,12 @@ int g4ref_beam_advance(int nslice, const int* slice_offsets,
                        const double* y, const double* px, const double* py,
                        double* gamma, double* theta);
 
+/* Per-particle field for the next g4ref_beam_advance calls (slice-contiguous,
+ * NULL = space charge off): the stand-in EFieldSolver then reports short
+ * range on and returns these values from getEField, so BeamSolverCUDA takes
+ * its per-particle branch (src/Core/BeamSolverCUDA.cpp:525-547). */
+void g4ref_set_particle_ez(const double* ez);
+
 /* TrackBeamCUDA::track (src/Core/TrackBeamCUDA.cpp:156-204), including its
  * corrector / chicane calls. */
 int g4ref_track(int npart, const g4b_step* st, double delz, int last_step,

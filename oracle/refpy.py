@@ -59,6 +59,8 @@ def load():
                                         C.c_double, C.c_double, C.c_double]
     lib.g4ref_beam_advance.argtypes = [C.c_int, ip, sp, C.c_int, ip, ip, ip, dp, dp, dp, dpp,
                                        dp, dp, dp, dp, dp, dp, dp]
+    lib.g4ref_set_particle_ez.argtypes = [dp]
+    lib.g4ref_set_particle_ez.restype = None
     lib.g4ref_track.argtypes = [C.c_int, sp, C.c_double, C.c_int, dp, dp, dp, dp, dp]
     lib.g4ref_r56.argtypes = [C.c_int, sp, C.c_double, dp, dp]
     lib.g4ref_slippage.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_int,
@@ -115,9 +117,10 @@ def field_advance(cells, *, solver=0, gridmax, xlambda, harm=1, first=0, enabled
     return out
 
 
-def beam_advance(off, step, fields, parts, long_esc=None):
+def beam_advance(off, step, fields, parts, long_esc=None, particle_field=None):
     """BeamSolverCUDA::advance; fields: dicts(cells, first, harm, gridmax,
-    xlambda, fc).  Updates parts['gamma'], parts['theta'] in place."""
+    xlambda, fc).  Updates parts['gamma'], parts['theta'] in place.
+    particle_field: per-particle getEField values (short range on)."""
     offa, offp = _i32(off)
     nf = len(fields)
     keep = [np.ascontiguousarray(f["cells"], dtype=np.complex128) for f in fields]
@@ -129,6 +132,16 @@ def beam_advance(off, step, fields, parts, long_esc=None):
     fc = np.array([f["fc"] for f in fields])
     ptrs = (dp * nf)(*[c.reshape(-1).view(np.float64).ctypes.data_as(dp) for c in keep])
     le = None if long_esc is None else np.ascontiguousarray(long_esc, np.float64)
+    pf = None if particle_field is None else np.ascontiguousarray(particle_field, np.float64)
+    load().g4ref_set_particle_ez(_d(pf))
+    try:
+        _beam_advance_call(offa, offp, step, nf, first, ngrid, harm, gm, xl, fc, ptrs, le,
+                           parts)
+    finally:
+        load().g4ref_set_particle_ez(None)
+
+
+def _beam_advance_call(offa, offp, step, nf, first, ngrid, harm, gm, xl, fc, ptrs, le, parts):
     _chk(load().g4ref_beam_advance(len(offa) - 1, offp, C.byref(step), nf,
                                    first.ctypes.data_as(ip), ngrid.ctypes.data_as(ip),
                                    harm.ctypes.data_as(ip), _d(gm), _d(xl), _d(fc), ptrs,

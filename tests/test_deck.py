@@ -108,6 +108,28 @@ def test_fft_solver_keys_are_accepted():
     assert d.info()["precision"] == 0
 
 
+def _with_efield(text, efield):
+    return text.replace("&track", f"&efield\n{efield}\n&end\n\n&track", 1)
+
+
+def test_efield_group_is_accepted_for_the_fp64_form():
+    """&efield rmax / ngrid / nz / nphi (upstream's short-range space charge)
+    selects the device solver behind BeamSolverCUDA::initEField."""
+    d = host.Deck(_with_efield(deck(), "rmax = 2.0\nngrid = 50\nnz = 2\nnphi = 1"), LAT)
+    assert d.info()["precision"] == 0
+
+
+@pytest.mark.parametrize("efield,track,msg", [
+    ("rmax = 2\nnz = 1\nlongrange = true", "use_cuda = 1", "longrange"),
+    ("rmax = 2\nnz = 1", "precision = mixed", "space charge"),
+    ("rmax = 2\nnz = -1", "use_cuda = 1", "efield"),
+    ("rmax = 2\nnz = 1\nfoo = 1", "use_cuda = 1", "unknown"),
+])
+def test_efield_errors(efield, track, msg):
+    with pytest.raises(G4BError, match=msg):
+        host.Deck(_with_efield(deck(track=track), efield), LAT)
+
+
 def test_structure_errors():
     with pytest.raises(G4BError, match="not closed"):
         host.Deck("&setup\nlattice = a\n&beam\n&end\n", LAT)
