@@ -99,7 +99,7 @@ template <typename T, int M, int L> struct AdiBlocks {
 template <typename T, int M, bool PX, int L>
 __device__ __forceinline__ bool adi_band(const AdiPassArgs& a, const CUtensorMap* tm_out, int s,
                                          int band, unsigned char* smem, uint64_t* bar,
-                                         uint32_t parity, int slot) {
+                                         uint32_t parity) {
   using C = typename CT<T>::type;
   constexpr int R = 32 / L;                     // rows per warp
   constexpr int W = BandW<T, L>::value * R;     // rows per band
@@ -128,9 +128,7 @@ __device__ __forceinline__ bool adi_band(const AdiPassArgs& a, const CUtensorMap
   const int srow_hi = min(min(r0 + W, n), sd.y + sd.w);
   const bool band_src = has_src && sbw > 0 && srow_lo < srow_hi;
   if (tid == 0) {
-    // pass Y reads R' of slice s from plane `slot` of its input (s itself, or
-    // the slice's place in the ring of the one-launch form)
-    const C* in = reinterpret_cast<const C*>(a.in) + (size_t)(PX ? s : slot) * plane;
+    const C* in = reinterpret_cast<const C*>(a.in) + (size_t)s * plane;
     const uint32_t bytes_in = (uint32_t)((hi - lo + 1) * ld * sizeof(C));
     const uint32_t bytes_s =
         band_src ? (uint32_t)((srow_hi - srow_lo) * sbw * sizeof(C)) : 0u;
@@ -354,10 +352,9 @@ __device__ __forceinline__ bool adi_band(const AdiPassArgs& a, const CUtensorMap
   ptx::fence_proxy_async();
   __syncthreads();
   if (tid == 0) {
-    // pass X writes R' to plane `slot` of its output (s, or the ring place)
     for (int i = 0; i < a.nbox; ++i)
       ptx::tma_store_3d(tm_out, out + (size_t)i * a.box_rows * W, 2 * r0,
-                        i * a.box_rows, PX ? slot : s);
+                        i * a.box_rows, s);
     ptx::bulk_commit();
     ptx::bulk_wait_read0();
   }
@@ -375,8 +372,7 @@ __global__ void __launch_bounds__(BandW<T, L>::value * 32, AdiBlocks<T, M, L>::v
     ptx::fence_mbar_init();
   }
   __syncthreads();
-  const int s = blockIdx.x / a.nband;
-  adi_band<T, M, PX, L>(a, &tm_out, s, blockIdx.x % a.nband, smem, &bar, 0u, s);
+  adi_band<T, M, PX, L>(a, &tm_out, blockIdx.x / a.nband, blockIdx.x % a.nband, smem, &bar, 0u);
 }
 
 // Persistent form over a work list of (run, slice, band) items of many runs
@@ -399,103 +395,8 @@ __global__ void __launch_bounds__(BandW<T, L>::value * 32, AdiBlocks<T, M, L>::v
     if (threadIdx.x == 0) ptx::fence_tensormap_acquire(tm);
     // a band whose rows never arrived leaves the barrier's phase open: stop
     // (the error flag reports it) rather than wait on it again
-    if (!adi_band<T, M, PX, L>(b.args[w.x], tm, w.y, w.z, smem, &bar, parity, w.y)) return;
+    if (!adi_band<T, M, PX, L>(b.args[w.x], tm, w.y, w.z, smem, &bar, parity)) return;
     parity ^= 1u;
-    __syncthreads();
-  }
-}
-
-// ---- both passes in one persistent launch, R' in an L2-resident ring ----
-// The two-launch form writes R' of every slice to DRAM and reads it back.
-// Here CTAs take work items by ticket in the order X(0), X(1), ...,
-// interleaved with Y(s - lag) once s >= lag: pass X of slice s stores R' in
-// ring plane s % ring (the first `ring` planes of the field's R' buffer),
-// pass Y of slice s reads it there lag slices later, while it is still in
-// L2; the ring is small (ring planes) and rewritten in place, so its dirty
-// lines rarely leave L2.  A pass-Y item waits until all pass-X bands of its
-// slice have stored (xdone), a pass-X item until the pass-Y bands of the
-// slice that last used its ring plane have read it (ydone).  Every wait is
-// for an item with an earlier ticket, which a running CTA holds, so the
-// waits end; each is bounded all the same: a wait that gives up sets the
-// error word and the abort flag, and every CTA then stops.  The arithmetic
-// per band is adi_band's, so the results are those of the two-launch form.
-struct AdiRingArgs {
-  AdiPassArgs x, y;     // pass X (in: the field) and pass Y (in: the R' ring)
-  const int4* items;    // (0 = X / 1 = Y, slice, band, 0) in ticket order
-  int nitems, ring;
-  int* sync;            // [0] ticket, [1] abort, [2, 2+nslice) xdone, then ydone
-  int nslice;
-};
-
-constexpr uint32_t kRingSpinLimit = 1u << 24;  // polls of ~64 ns: about a second
-
-__device__ __forceinline__ bool ring_wait(const int* cnt, int need, int* abort_flag, int* err) {
-  for (uint32_t i = 0; i < kRingSpinLimit; ++i) {
-    int v;
-    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(cnt) : "memory");
-    if (v >= need) return true;
-    if (*reinterpret_cast<volatile int*>(abort_flag)) return false;
-    __nanosleep(64);
-  }
-  atomicOr(err, kErrWaitTimeout);
-  atomicExch(abort_flag, 1);
-  return false;
-}
-
-template <int M, int L>
-__global__ void __launch_bounds__(BandW<float, L>::value * 32, AdiBlocks<float, M, L>::value)
-    adi_ring_kernel(const __grid_constant__ AdiRingArgs g,
-                    const __grid_constant__ CUtensorMap tm_x,
-                    const __grid_constant__ CUtensorMap tm_y) {
-  extern __shared__ __align__(128) unsigned char smem[];
-  __shared__ uint64_t bar;
-  __shared__ int cur;
-  int* ticket = g.sync;
-  int* abort_flag = g.sync + 1;
-  int* xdone = g.sync + 2;
-  int* ydone = xdone + g.nslice;
-  if (threadIdx.x == 0) {
-    ptx::mbar_init(&bar, 1);
-    ptx::fence_mbar_init();
-  }
-  __syncthreads();
-  uint32_t parity = 0;
-  for (;;) {
-    if (threadIdx.x == 0) {
-      int t = atomicAdd(ticket, 1);
-      if (t < g.nitems) {
-        const int4 w = g.items[t];
-        bool ok = true;
-        if (w.x == 1)
-          ok = ring_wait(xdone + w.y, g.x.nband, abort_flag, g.x.err);
-        else if (w.y >= g.ring)
-          ok = ring_wait(ydone + (w.y - g.ring), g.y.nband, abort_flag, g.x.err);
-        // the bulk copies and tensor stores that follow (async proxy) come
-        // after the acquired counts (generic proxy)
-        asm volatile("fence.proxy.async.global;" ::: "memory");
-        if (!ok) t = g.nitems;
-      }
-      cur = t;
-    }
-    __syncthreads();
-    const int t = cur;
-    if (t >= g.nitems) break;
-    const int4 w = g.items[t];
-    const int slot = w.y % g.ring;
-    const bool ok = w.x == 0
-        ? adi_band<float, M, true, L>(g.x, &tm_x, w.y, w.z, smem, &bar, parity, slot)
-        : adi_band<float, M, false, L>(g.y, &tm_y, w.y, w.z, smem, &bar, parity, slot);
-    parity ^= 1u;
-    if (!ok) {
-      if (threadIdx.x == 0) atomicExch(abort_flag, 1);
-      break;
-    }
-    if (threadIdx.x == 0) {
-      if (w.x == 0) ptx::bulk_wait0();  // this band's R' stores have completed
-      asm volatile("fence.proxy.async.global;" ::: "memory");
-      __threadfence();
-      atomicAdd((w.x == 0 ? xdone : ydone) + w.y, 1);
-    }
     __syncthreads();
   }
 }
@@ -858,88 +759,6 @@ int adi_launch(g4b_field* f, const AdiPlan& P) {
   return P.precision == G4B_FP64
              ? launch_pass_m<double, false>(P.M, f, P.y, *P.tm_y, P.smem_y)
              : launch_pass_m<float, false>(P.M, f, P.y, *P.tm_y, P.smem_y);
-}
-
-template <int M, int L>
-static int ring_launch_t(g4b_field* f, const AdiPlan& P) {
-  auto kern = adi_ring_kernel<M, L>;
-  g4b_ctx* c = f->ctx;
-  const size_t smem = std::max(P.smem_x_max, P.smem_y);
-  constexpr int threads = BandW<float, L>::value * 32;
-  static std::atomic<uint64_t> configured{0};
-  if (c->device >= 64 || !((configured.load() >> c->device) & 1)) {
-    cudaFuncAttributes fa;
-    cudaError_t e = cudaFuncGetAttributes(&fa, kern);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaFuncGetAttributes(adi_ring)");
-    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             227 * 1024 - (int)fa.sharedSizeBytes);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(adi_ring)");
-    if (c->device < 64) configured.fetch_or(1ull << c->device);
-  }
-  if (f->ring_grid == 0) {
-    int per_sm = 0;
-    G4B_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem));
-    f->ring_grid = std::max(1, std::min(f->ring_nitems, per_sm * c->sm_count));
-  }
-  AdiRingArgs g{};
-  g.x = P.x;
-  g.y = P.y;
-  g.items = f->ring_items;
-  g.nitems = f->ring_nitems;
-  g.ring = f->ring_planes;
-  g.sync = f->ring_sync;
-  g.nslice = f->nslice;
-  G4B_CUDA_TRY(cudaMemsetAsync(f->ring_sync, 0, (size_t)(2 + 2 * f->nslice) * sizeof(int),
-                               c->stream));
-  {
-    LaunchScope ls(c, "adi_ring");
-    kern<<<f->ring_grid, threads, smem, c->stream>>>(g, *P.tm_x, *P.tm_y);
-  }
-  return check_launch(c, "adi_ring_kernel");
-}
-
-// Work items and counters of the ring form, built once per field (outside
-// any stream capture: the items are copied from host memory).
-int adi_ring_prepare(g4b_field* f) {
-  if (f->precision != G4B_MIXED || f->nslice < kAdiRingMinSlices || f->ring_items)
-    return G4B_OK;
-  g4b_ctx* c = f->ctx;
-  const int nband = (f->ngrid + f->band_rows - 1) / f->band_rows;
-  // ticket order: round r gives pass X of slice r, then pass Y of slice r - lag
-  std::vector<int4> items;
-  const int S = f->nslice;
-  for (int r = 0; r < S + kAdiRingLag; ++r) {
-    if (r < S)
-      for (int b = 0; b < nband; ++b) items.push_back(make_int4(0, r, b, 0));
-    if (r >= kAdiRingLag)
-      for (int b = 0; b < nband; ++b) items.push_back(make_int4(1, r - kAdiRingLag, b, 0));
-  }
-  G4B_CUDA_TRY(dev_alloc(c, (void**)&f->ring_items, items.size() * sizeof(int4)));
-  G4B_CUDA_TRY(cudaMemcpyAsync(f->ring_items, items.data(), items.size() * sizeof(int4),
-                               cudaMemcpyHostToDevice, c->stream));
-  G4B_CUDA_TRY(dev_alloc(c, (void**)&f->ring_sync, (size_t)(2 + 2 * S) * sizeof(int)));
-  G4B_CUDA_TRY(cudaStreamSynchronize(c->stream));  // the host vector goes out of scope
-  f->ring_nitems = (int)items.size();
-  f->ring_planes = kAdiRingPlanes;
-  return G4B_OK;
-}
-
-int adi_ring_launch(g4b_field* f, const AdiPlan& P, bool* launched) {
-  *launched = false;
-  if (P.precision != G4B_MIXED || !f->ring_items || P.x.nband * f->band_rows < f->ngrid)
-    return G4B_OK;
-#define G4B_RING_CASE(m, l) \
-  case (l == 16 ? 100 : 0) + m: rc = ring_launch_t<m, l>(f, P); break;
-  int rc = G4B_OK;
-  switch (P.M) {
-    G4B_MODES32(G4B_RING_CASE)
-    G4B_MODES16(G4B_RING_CASE)
-    default:
-      return G4B_OK;  // not a ring layout: the caller runs the two launches
-  }
-#undef G4B_RING_CASE
-  if (rc == G4B_OK) *launched = true;
-  return rc;
 }
 
 int adi_run(g4b_adi* adi, g4b_field* f, const void* src, const int4* desc,

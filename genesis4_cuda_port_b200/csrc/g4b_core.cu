@@ -487,8 +487,6 @@ int g4b_field_destroy(g4b_field* f) {
   dev_free(f->ctx, f->b);
   dev_free(f->ctx, f->src);
   dev_free(f->ctx, f->desc);
-  dev_free(f->ctx, f->ring_items);
-  dev_free(f->ctx, f->ring_sync);
   ctx_release(f->ctx);
   delete f;
   return G4B_OK;

@@ -94,10 +94,6 @@ struct g4b_field {
   int band_rows = 0;        // W: rows per CTA (one or two per warp)
   int mode = 0;             // ADI row layout (pick_mode)
   uint64_t bytes = 0;
-  // one-launch ADI with an L2-resident R' ring (FP32 fields; adi_ring_launch)
-  int4* ring_items = nullptr;  // work items in ticket order
-  int* ring_sync = nullptr;    // ticket, abort flag, per-slice X / Y band counts
-  int ring_nitems = 0, ring_planes = 0, ring_grid = 0;
 };
 
 struct g4b_beam {
@@ -214,17 +210,6 @@ struct AdiPlan {
 int adi_plan(g4b_adi* adi, g4b_field* f, const void* src, const int4* desc,
              const AdiYExtras* ex, AdiPlan& plan);
 int adi_launch(g4b_field* f, const AdiPlan& plan);
-// Both passes of a plan in one persistent launch with R' kept in a ring of
-// L2-resident planes (FP32 fields with at least kAdiRingMinSlices slices);
-// returns G4B_OK having launched nothing when the field does not qualify
-// (*launched = false), so the caller falls back to adi_launch.
-constexpr int kAdiRingLag = 32;          // slices between a slice's pass X and pass Y
-constexpr int kAdiRingPlanes = kAdiRingLag + 2;
-constexpr int kAdiRingMinSlices = 2 * kAdiRingPlanes;
-int adi_ring_launch(g4b_field* f, const AdiPlan& plan, bool* launched);
-// Builds the ring form's work items and counters for an eligible field (a
-// no-op otherwise); called where the field is created, outside captures.
-int adi_ring_prepare(g4b_field* f);
 // Batched passes (mixed precision): items[i] = (run, slice, band, 0) of the
 // runs whose ADI uses M elements per lane; args / maps indexed by run.
 struct AdiBatchArgs {

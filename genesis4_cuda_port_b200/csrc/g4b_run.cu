@@ -741,12 +741,9 @@ __device__ __forceinline__ void deposit_slice(const DepArgs& a, const int bs, co
   __syncthreads();  // sbox is read by every thread below
 
   // ---- deposition of every field with a source this step ----
-  // [hb * bw] cell sums, real and imaginary part packed in one 64-bit integer
-  // (im * 2^32 + re): one shared atomic per corner adds both, and since every
-  // kept cell sum stays within 2^30 in magnitude, re is the low word read as
-  // a signed integer and im the rest, exactly
-  unsigned long long* acc = reinterpret_cast<unsigned long long*>(smem);
-  int* hist = reinterpret_cast<int*>(acc + kDepMaxCells);  // [(hb + 1) * bw] counts per base cell
+  int* are = reinterpret_cast<int*>(smem);        // [hb * bw] real parts
+  int* aim = are + kDepMaxCells;                  // [hb * bw] imaginary parts
+  int* hist = aim + kDepMaxCells;                 // [(hb + 1) * bw] counts per base cell
   const double npd = (double)np;
   for (int fi = 0; fi < a.nfield; ++fi) {
     const DepField& F = a.f[fi];
@@ -860,18 +857,19 @@ __device__ __forceinline__ void deposit_slice(const DepArgs& a, const int bs, co
               if (count) atomicAdd(&hist[cidx], quad ? 4 : 1);
             if (cidx >= 0) {
               if (add) {
-                auto pk = [](int re, int im) {
-                  return (unsigned long long)((long long)im * 4294967296LL + (long long)re);
-                };
                 if (ey >= 0) {
                   const int o = ey * bw + ex;
-                  atomicAdd(&acc[o], pk(c[0], c[1]));
-                  atomicAdd(&acc[o + 1], pk(c[2], c[3]));
+                  atomicAdd(&are[o], c[0]);
+                  atomicAdd(&aim[o], c[1]);
+                  atomicAdd(&are[o + 1], c[2]);
+                  atomicAdd(&aim[o + 1], c[3]);
                 }
                 if (ey + 1 < hb) {
                   const int o = (ey + 1) * bw + ex;
-                  atomicAdd(&acc[o], pk(c[4], c[5]));
-                  atomicAdd(&acc[o + 1], pk(c[6], c[7]));
+                  atomicAdd(&are[o], c[4]);
+                  atomicAdd(&aim[o], c[5]);
+                  atomicAdd(&are[o + 1], c[6]);
+                  atomicAdd(&aim[o + 1], c[7]);
                 }
               }
             }
@@ -879,8 +877,12 @@ __device__ __forceinline__ void deposit_slice(const DepArgs& a, const int bs, co
         }
       };
       auto zero_acc = [&]() {
-        int4* a4 = reinterpret_cast<int4*>(acc);
-        for (int i = tid; i < (nout + 1) >> 1; i += T) a4[i] = make_int4(0, 0, 0, 0);
+        int4* r4 = reinterpret_cast<int4*>(are);
+        int4* i4 = reinterpret_cast<int4*>(aim);
+        for (int i = tid; i < (nout + 3) >> 2; i += T) {
+          r4[i] = make_int4(0, 0, 0, 0);
+          i4[i] = make_int4(0, 0, 0, 0);
+        }
       };
       __syncthreads();
       {
@@ -943,12 +945,8 @@ __device__ __forceinline__ void deposit_slice(const DepArgs& a, const int bs, co
       }
       __syncthreads();
       const double unscale = scl / S;
-      for (int i = tid; i < nout; i += T) {
-        const long long t = (long long)acc[i];
-        const int re = (int)(unsigned int)(unsigned long long)t;  // the low word, signed
-        const int im = (int)((t - (long long)re) >> 32);
-        out[i] = make_float2((float)((double)re * unscale), (float)((double)im * unscale));
-      }
+      for (int i = tid; i < nout; i += T)
+        out[i] = make_float2((float)((double)are[i] * unscale), (float)((double)aim[i] * unscale));
     }
     if (tid == 0 && part * hband < bh) F.mpred[bs * kDepSplit + part] = m_seen;
   }

@@ -118,11 +118,10 @@ def test_run_joins_a_batch_in_progress(ctx):
     batch.close()
 
 
-def test_one_launch_adi_equals_the_two_pass_form(ctx):
-    """A run of at least 68 slices solves both ADI passes in one persistent
-    launch with R' in an L2-resident ring; the same run advanced by the batch
-    engine (two passes through DRAM) gives the same bits, with slippage every
-    step and the diagnostics of every step."""
+def test_many_slices_alone_graphed_and_batched_agree(ctx):
+    """A 150-slice time-dependent run with slippage every step: direct
+    launches, graph replay and the batch engine give the same bits, state and
+    the diagnostics of every step."""
     cfg = dict(nslice=150, npart=256, ngrid=65, taper=0.0, dgam=0.0, time_run=True, nsteps=5)
     alone = _make(ctx, 9, cfg)
     alone.advance(0, cfg["nsteps"], graph=False)
