@@ -95,6 +95,9 @@ _SIGS = {
     "g4b_beam_set_particle_ez": (C.c_int, [C.c_void_p, c_double_p]),
     "g4b_beam_get_particle_ez": (C.c_int, [C.c_void_p, c_double_p]),
     "g4b_beam_device_bytes": (C.c_int, [C.c_void_p, c_uint64_p]),
+    "g4b_isr_rates": (C.c_int, [C.c_double, C.c_double, C.c_int, c_double_p, c_double_p]),
+    "g4b_beam_incoherent": (C.c_int, [C.c_void_p, C.c_void_p, C.c_double, C.c_int, C.c_int,
+                                      C.c_int, C.c_uint64, C.c_uint64]),
     "g4b_efield_create": (C.c_int, [C.c_void_p, C.c_double, C.c_int, C.c_int, C.c_int,
                                     C.c_double, c_void_pp]),
     "g4b_efield_destroy": (C.c_int, [C.c_void_p]),

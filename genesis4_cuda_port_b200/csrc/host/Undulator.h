@@ -42,6 +42,7 @@ class Undulator {
   double getku() const { return steps[istep_].st.ku; }
   double getGammaRef() const { return gamma0; }
   double autophase() const { return steps[istep_].st.autophase; }
+  bool isHelical() const { return steps[istep_].helical != 0; }
   double slippage() const { return steps[istep_].slip; }
   double getz() const { return istep_ < 0 ? 0.0 : steps[istep_].z; }
   // markers acting at the start of the current step: those placed after the

@@ -242,8 +242,16 @@ void Beam::unpack_soa_to_beam() {  // src/Core/Beam.cpp:457-525
     }
 }
 
-// Beam::track, CUDA branch (src/Core/Beam.cpp:111-134).  Incoherent
-// synchrotron radiation and collective effects are not part of this build.
+void Incoherent::apply(Beam* beam, Undulator* und, double delz) {
+  if (!spread_ && !loss_) return;
+  check(g4b_beam_incoherent(beam->beamSoA, &und->current(), delz, und->isHelical() ? 1 : 0,
+                            loss_ ? 1 : 0, spread_ ? 1 : 0, seed_, counter_++),
+        "Incoherent::apply");
+}
+
+// Beam::track, CUDA branch (src/Core/Beam.cpp:111-134): incoherent
+// synchrotron radiation on the device state after the push; wakes
+// (col.apply) reach the push as the slice loss.
 void Beam::track(double delz, std::vector<Field*>* field, Undulator* und) {
   for (auto* f : *field) f->setStepsize(delz);
   if (!useCudaSolver_)
@@ -251,6 +259,7 @@ void Beam::track(double delz, std::vector<Field*>* field, Undulator* und) {
   if (!beamSoA) pack_beam_to_soa();
   cuda_solver.track(delz * 0.5, this, und, false);
   cuda_solver.advance(delz, this, field, und);
+  incoherent.apply(this, und, delz);
   cuda_solver.applyR56(this, und, reflength);
   cuda_solver.track(delz * 0.5, this, und, true);
 }

@@ -136,12 +136,35 @@ class BeamSolverCUDA {  // include/BeamSolverCUDA.h:17-37
   g4b_efield* efield = nullptr;
 };
 
+// Upstream Incoherent (absent from the reference tree), on the device state:
+// init(base, rank, spread, loss) as Beam::initIncoherent (include/Beam.h:124-126)
+// calls it; apply(beam, und, delz) as Beam::track does after the push
+// (src/Core/Beam.cpp:126).  The seed is base + rank; each apply draws with a
+// new counter.
+class Incoherent {
+ public:
+  void init(int base, int rank, bool spread, bool loss) {
+    seed_ = (uint64_t)(int64_t)base + (uint64_t)rank;
+    spread_ = spread;
+    loss_ = loss;
+  }
+  void apply(Beam* beam, Undulator* und, double delz);
+
+ private:
+  uint64_t seed_ = 0, counter_ = 0;
+  bool spread_ = false, loss_ = false;
+};
+
 // Beam (include/Beam.h:24-105)
 class Beam {
  public:
   Beam();
   virtual ~Beam();
   void init(int nsize, int nbins, double reflen, double slicelen, double s0, bool one4one);
+  // include/Beam.h:124-126
+  void initIncoherent(int base, int rank, bool spread, bool loss) {
+    incoherent.init(base, rank, spread, loss);
+  }
   // include/Beam.h:128-133
   void initEField(double rmax, int ngrid, int nz, int nphi, double lambda, bool longr) {
     cuda_solver.initEField(rmax, ngrid, nz, nphi, lambda, longr);
@@ -163,6 +186,7 @@ class Beam {
   g4b_beam* beamSoA = nullptr;  // device state (Genesis4BeamSoA)
 
  private:
+  Incoherent incoherent;
   BeamSolverCUDA cuda_solver;
   bool useCudaSolver_ = false;
   int bharm = 1;

@@ -198,6 +198,12 @@ class BeamState:
             assert a.size == self.npart
         check(self.lib.g4b_beam_set_particle_ez(self.h, dptr(a)))
 
+    def incoherent(self, step: Step, delz: float, *, helical: bool = False, loss: bool = True,
+                   spread: bool = True, seed: int = 0, counter: int = 0) -> None:
+        """Incoherent synchrotron radiation of one undulator step (Incoherent::apply)."""
+        check(self.lib.g4b_beam_incoherent(self.h, C.byref(step), delz, int(helical),
+                                           int(loss), int(spread), seed, counter))
+
     def particle_ez(self) -> np.ndarray:
         out = np.empty(self.npart)
         check(self.lib.g4b_beam_get_particle_ez(self.h, dptr(out)))

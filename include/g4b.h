@@ -165,6 +165,21 @@ int g4b_beam_set_particle_ez(g4b_beam* b, const double* ez);
 int g4b_beam_get_particle_ez(g4b_beam* b, double* ez);
 int g4b_beam_device_bytes(g4b_beam* b, uint64_t* bytes);
 
+/* ---- incoherent synchrotron radiation ---------------------------------------
+ * The step the reference leaves to upstream Incoherent::apply(Beam*,
+ * Undulator*, delz) on the host particle copies (src/Core/Beam.cpp:126,
+ * Beam::initIncoherent(base, rank, spread, loss), include/Beam.h:124-126),
+ * here on the device state of an FP64 beam, inside undulators only:
+ * gamma -= loss delz gamma^2 (loss = (2/3) r_e ku^2 aw^2) and
+ * gamma += sqrt(spread delz) gamma^2 z (spread = (14/15) lambdabar_c r_e ku^3
+ * K^2 F(K); planar K = sqrt(2) aw, F = 1.42 K + 1/(1 + 1.5 K + 0.95 K^2);
+ * helical K = aw, F = 1.70 K + 1/(1 + 1.88 K + 0.80 K^2)), z ~ N(0,1) from
+ * Philox4x32-10 keyed by seed with counter (particle index, counter) and the
+ * Box-Muller transform.  Pass a different counter every step. */
+int g4b_isr_rates(double aw, double ku, int helical, double* loss, double* spread);
+int g4b_beam_incoherent(g4b_beam* b, const g4b_step* st, double delz, int helical,
+                        int do_loss, int do_spread, uint64_t seed, uint64_t counter);
+
 /* ---- short-range space charge ------------------------------------------------
  * The solver behind BeamSolverCUDA::initEField (include/BeamSolverCUDA.h:41-43)
  * and EFieldSolver::shortRange, which the reference runs on the host for

@@ -863,3 +863,53 @@ int g4o_load_beam(const g4o_beam_spec* sp, const double* current, double* x,
   }
   return 0;
 }
+
+/* ---- incoherent synchrotron radiation -----------------------------------
+ * Restates the device model of g4b_beam_incoherent (the reference leaves it
+ * to upstream Incoherent::apply on the host, src/Core/Beam.cpp:126; upstream
+ * is absent): gamma += -loss gamma^2 + sigma gamma^2 z, z from Philox4x32-10
+ * (Salmon et al., SC 2011) keyed by the seed with counter (index, counter)
+ * and the Box-Muller transform.  loss and sigma already hold the step
+ * length: loss = rate delz, sigma = sqrt(spread rate delz). */
+static void philox_round(uint32_t c[4], uint32_t k0, uint32_t k1) {
+  const uint64_t p0 = (uint64_t)0xD2511F53u * c[0];
+  const uint64_t p1 = (uint64_t)0xCD9E8D57u * c[2];
+  const uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+  const uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+  const uint32_t n0 = hi1 ^ c[1] ^ k0, n2 = hi0 ^ c[3] ^ k1;
+  c[0] = n0;
+  c[1] = lo1;
+  c[2] = n2;
+  c[3] = lo0;
+}
+
+void g4o_philox4x32_10(uint32_t ctr[4], const uint32_t key[2]) {
+  uint32_t k0 = key[0], k1 = key[1];
+  for (int r = 0; r < 10; r++) {
+    philox_round(ctr, k0, k1);
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+}
+
+static double unit53(uint32_t a, uint32_t b) {
+  return ((double)(a >> 5) * 67108864.0 + (double)(b >> 6) + 0.5) * (1.0 / 9007199254740992.0);
+}
+
+void g4o_incoherent(int64_t n, double* gamma, double loss, double sigma, uint64_t seed,
+                    uint64_t counter) {
+  const uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < n; i++) {
+    const double g = gamma[i], g2 = g * g;
+    double dg = -loss * g2;
+    if (sigma > 0.0) {
+      uint32_t c[4] = {(uint32_t)i, (uint32_t)((uint64_t)i >> 32), (uint32_t)counter,
+                       (uint32_t)(counter >> 32)};
+      g4o_philox4x32_10(c, key);
+      const double u = unit53(c[0], c[1]), v = unit53(c[2], c[3]);
+      dg += sigma * g2 * (sqrt(-2.0 * log(u)) * cos(6.283185307179586 * v));
+    }
+    gamma[i] = g + dg;
+  }
+}

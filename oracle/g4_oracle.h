@@ -143,6 +143,15 @@ int g4o_load_beam(const g4o_beam_spec* spec, const double* current, double* x,
 int g4o_num_threads(void);
 void g4o_set_num_threads(int n);
 
+/* Philox4x32-10 (Salmon et al., SC 2011) on one counter block, in place. */
+void g4o_philox4x32_10(uint32_t ctr[4], const uint32_t key[2]);
+/* Incoherent synchrotron radiation of one step, restating g4b_beam_incoherent:
+ * gamma += -loss gamma^2 + sigma gamma^2 z (loss = rate delz, sigma =
+ * sqrt(spread rate delz)); z ~ N(0,1) from Philox4x32-10 keyed by seed with
+ * counter (index lo, index hi, counter lo, counter hi) and Box-Muller. */
+void g4o_incoherent(int64_t n, double* gamma, double loss, double sigma, uint64_t seed,
+                    uint64_t counter);
+
 #ifdef __cplusplus
 }
 #endif

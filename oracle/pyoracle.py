@@ -72,6 +72,11 @@ def load():
     lib.g4o_r56.argtypes = [C.c_int64, sp, C.c_double, dp, dp]
     lib.g4o_push.argtypes = [C.c_int, i64p, sp, C.POINTER(FieldView), C.c_int,
                              dp, dp, dp, dp, dp, dp, dp]
+    lib.g4o_philox4x32_10.argtypes = [C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
+    lib.g4o_philox4x32_10.restype = None
+    lib.g4o_incoherent.argtypes = [C.c_int64, dp, C.c_double, C.c_double, C.c_uint64,
+                                   C.c_uint64]
+    lib.g4o_incoherent.restype = None
     lib.g4o_push_ez.argtypes = [C.c_int, i64p, sp, C.POINTER(FieldView), C.c_int,
                                 dp, dp, dp, dp, dp, dp, dp, dp]
     lib.g4o_slippage.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double,
@@ -645,3 +650,37 @@ def short_range(off, parts, current, gammaz2, *, rmax, ngrid, nz, nphi, lambda0,
         out[b:e] = el[s] + coef * current[s] * total
         modes.append(dict(dr=dr, xc=xc, yc=yc, u=us))
     return (out, modes) if return_modes else out
+
+
+# ---------------------------------------------------------------------------
+# Incoherent synchrotron radiation (the device model of g4b_beam_incoherent;
+# upstream's Incoherent class, which the reference calls on the host,
+# src/Core/Beam.cpp:126, is absent: PARITY UNPINNED against upstream).
+
+RE = 2.8179403262e-15
+LAMBDA_C = 3.8615926796e-13
+
+
+def philox4x32_10(ctr, key):
+    c = (C.c_uint32 * 4)(*[int(v) & 0xFFFFFFFF for v in ctr])
+    k = (C.c_uint32 * 2)(*[int(v) & 0xFFFFFFFF for v in key])
+    load().g4o_philox4x32_10(c, k)
+    return [int(v) for v in c]
+
+
+def isr_rates(aw, ku, helical=False):
+    """(loss, spread): d gamma/dz = -loss gamma^2, d<dgamma^2>/dz = spread gamma^4."""
+    if not (aw > 0 and ku > 0):
+        return 0.0, 0.0
+    K = aw if helical else np.sqrt(2.0) * aw
+    F = (1.70 * K + 1 / (1 + 1.88 * K + 0.80 * K * K)) if helical else \
+        (1.42 * K + 1 / (1 + 1.5 * K + 0.95 * K * K))
+    return 2.0 / 3.0 * RE * ku * ku * aw * aw, 14.0 / 15.0 * LAMBDA_C * RE * ku ** 3 * K * K * F
+
+
+def incoherent(gamma, *, aw, ku, delz, helical=False, loss=True, spread=True, seed=0,
+               counter=0):
+    """One step in place on a float64 array."""
+    lr, sr = isr_rates(aw, ku, helical)
+    load().g4o_incoherent(gamma.size, _d(gamma), lr * delz if loss else 0.0,
+                          float(np.sqrt(sr * delz)) if spread else 0.0, seed, counter)
