@@ -449,7 +449,7 @@ def run_scan(args):
     clk = _engine_clocks()
     clk.start()
     time.sleep(0.5)
-    rb, _, _ = host.scan(workloads.engine(wl, max_runs=len(jobs), tune=True, mode=0), jobs)
+    rb, _, _ = host.scan(workloads.engine(wl, max_runs=len(jobs), tune=2, mode=0), jobs)
     c = clk.stop()
     rs, _, _ = host.scan(workloads.engine(wl, max_runs=len(jobs), mode=1), jobs)
     line = {"metric": "slice-steps/s, batched steady-state scan", "value": rb.value,
@@ -461,6 +461,8 @@ def run_scan(args):
                        "prng_seed": 1, "params": params},
             "seconds": rb.seconds, "slice_steps": rb.slice_steps,
             "device_bytes": rb.device_bytes, "launch_shapes": list(rb.grids),
+            "row_layouts": {"runs_on_16_lane_rows": rb.layouts_16,
+                            "runs_moved_by_the_tuner": rb.layouts_switched},
             "one_at_a_time": {"value": rs.value, "seconds": rs.seconds},
             "batched_over_one_at_a_time": rb.value / rs.value, "clocks": c}
     print(json.dumps(line), flush=True)

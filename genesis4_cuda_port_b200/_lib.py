@@ -95,6 +95,10 @@ _SIGS = {
     "g4b_beam_set_particle_ez": (C.c_int, [C.c_void_p, c_double_p]),
     "g4b_beam_get_particle_ez": (C.c_int, [C.c_void_p, c_double_p]),
     "g4b_beam_device_bytes": (C.c_int, [C.c_void_p, c_uint64_p]),
+    "g4b_batch_tune_layouts": (C.c_int, [C.c_void_p]),
+    "g4b_run_get_layouts": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
+    "g4b_run_set_layouts": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
+    "g4b_default_layout": (C.c_int, [C.c_int]),
     "g4b_isr_rates": (C.c_int, [C.c_double, C.c_double, C.c_int, c_double_p, c_double_p]),
     "g4b_beam_incoherent": (C.c_int, [C.c_void_p, C.c_void_p, C.c_double, C.c_int, C.c_int,
                                       C.c_int, C.c_uint64, C.c_uint64]),

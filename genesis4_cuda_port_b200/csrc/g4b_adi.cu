@@ -704,7 +704,14 @@ int adi_plan(g4b_adi* adi, g4b_field* f, const void* src, const int4* desc,
   args.err = f->ctx->d_error;
   args.box_rows = f->store_box_rows;
   args.nbox = f->store_nbox;
-  args.tab = f->precision == G4B_FP64 ? (const void*)adi->d_tab64 : (const void*)adi->d_tab32;
+  if (f->precision == G4B_FP64)
+    args.tab = adi->d_tab64;
+  else if (f->mode == adi->mode32)
+    args.tab = adi->d_tab32;
+  else if (f->mode == adi->mode32_alt && adi->d_tab32_alt)
+    args.tab = adi->d_tab32_alt;
+  else
+    return fail(G4B_ERR_STATE, "adi: solver and field row layouts differ");
   const size_t cb = f->cell_bytes;
   const size_t out_bytes = (size_t)f->store_nbox * f->store_box_rows * W * cb;
   auto smem_for = [&](bool px, bool with_src) {
@@ -721,7 +728,7 @@ int adi_plan(g4b_adi* adi, g4b_field* f, const void* src, const int4* desc,
     args.out_off = (int)out_off;
     return out_off + out_bytes;
   };
-  P.M = f->precision == G4B_FP64 ? adi->M : adi->mode32;
+  P.M = f->precision == G4B_FP64 ? adi->M : f->mode;
   if (P.M != f->mode) return fail(G4B_ERR_STATE, "adi: solver and field row layouts differ");
   P.precision = f->precision;
   P.grid = (unsigned)(f->nslice * args.nband);
@@ -872,6 +879,7 @@ int g4b_adi_destroy(g4b_adi* a) {
   ctx_quiesce(a->ctx);
   dev_free(a->ctx, a->d_tab64);
   dev_free(a->ctx, a->d_tab32);
+  dev_free(a->ctx, a->d_tab32_alt);
   ctx_release(a->ctx);
   delete a;
   return G4B_OK;
@@ -964,29 +972,41 @@ int g4b_adi_init(g4b_adi* a, double delz, double dgrid, double xks, int ngrid) {
   };
   // FP64 fields solve rows with 32 lanes; FP32 fields with the layout of
   // their mode (16-lane rows where those fit the row more closely)
-  const int mode32 = pick_mode(n, G4B_MIXED);
+  // (and the tables of the other FP32 layout, which the batch tuner may pick)
+  const int mode32 = pick_mode(n, G4B_MIXED), mode32_alt = alt_mode(n);
   const std::vector<cd> c64 = tables(M, 32);
-  const std::vector<cd> c32 = tables(mode_M(mode32), mode_L(mode32));
+  auto to32 = [&](int mode) {
+    const std::vector<cd> c = tables(mode_M(mode), mode_L(mode));
+    std::vector<float2> t(c.size());
+    for (size_t k = 0; k < c.size(); ++k) t[k] = make_float2((float)c[k].real(), (float)c[k].imag());
+    return t;
+  };
   std::vector<double2> t64(c64.size());
   for (size_t k = 0; k < c64.size(); ++k) t64[k] = make_double2(c64[k].real(), c64[k].imag());
-  std::vector<float2> t32(c32.size());
-  for (size_t k = 0; k < c32.size(); ++k)
-    t32[k] = make_float2((float)c32[k].real(), (float)c32[k].imag());
+  const std::vector<float2> t32 = to32(mode32);
+  const std::vector<float2> t32a = mode32_alt ? to32(mode32_alt) : std::vector<float2>();
   g4b_ctx* ctx = a->ctx;
   G4B_CUDA_TRY(cudaSetDevice(ctx->device));
   if (a->d_tab64) {
     cudaStreamSynchronize(ctx->stream);
     dev_free(a->ctx, a->d_tab64);
     dev_free(a->ctx, a->d_tab32);
+    dev_free(a->ctx, a->d_tab32_alt);
     a->d_tab64 = nullptr;
     a->d_tab32 = nullptr;
+    a->d_tab32_alt = nullptr;
   }
   G4B_CUDA_TRY(dev_alloc(a->ctx, (void**)&a->d_tab64, t64.size() * sizeof(double2)));
   G4B_CUDA_TRY(dev_alloc(a->ctx, (void**)&a->d_tab32, t32.size() * sizeof(float2)));
+  if (!t32a.empty())
+    G4B_CUDA_TRY(dev_alloc(a->ctx, (void**)&a->d_tab32_alt, t32a.size() * sizeof(float2)));
   G4B_CUDA_TRY(cudaMemcpyAsync(a->d_tab64, t64.data(), t64.size() * sizeof(double2),
                                cudaMemcpyHostToDevice, ctx->stream));
   G4B_CUDA_TRY(cudaMemcpyAsync(a->d_tab32, t32.data(), t32.size() * sizeof(float2),
                                cudaMemcpyHostToDevice, ctx->stream));
+  if (!t32a.empty())
+    G4B_CUDA_TRY(cudaMemcpyAsync(a->d_tab32_alt, t32a.data(), t32a.size() * sizeof(float2),
+                                 cudaMemcpyHostToDevice, ctx->stream));
   G4B_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
   a->ngrid = ngrid;
   a->delz = delz;
@@ -995,6 +1015,7 @@ int g4b_adi_init(g4b_adi* a, double delz, double dgrid, double xks, int ngrid) {
   a->r = r;
   a->M = M;
   a->mode32 = mode32;
+  a->mode32_alt = mode32_alt;
   a->ready = true;
   return G4B_OK;
 }

@@ -153,13 +153,39 @@ int pick_M(int n) {
   return 0;
 }
 
+static int pick_M16(int n) {
+  static const int kM16[] = {5, 7, 9, 11, 13, 15, 17, 21, 25, 33};
+  for (int m : kM16)
+    if (16 * m >= n) return m;
+  return 0;
+}
+
 int pick_mode(int n, int precision) {
   const int m32 = pick_M(n);
   if (precision == G4B_FP64 || m32 == 0) return m32;
-  static const int kM16[] = {5, 7, 9, 11, 13, 15, 17, 21, 25, 33};
-  for (int m : kM16)
-    if (16 * m >= n) return 16 * m < 32 * m32 ? 100 + m : m32;
-  return m32;
+  const int m16 = pick_M16(n);
+  return m16 && 16 * m16 < 32 * m32 ? 100 + m16 : m32;
+}
+
+int alt_mode(int n) {
+  const int m32 = pick_M(n), m16 = pick_M16(n);
+  if (!m32 || !m16) return 0;
+  return pick_mode(n, G4B_MIXED) == m32 ? 100 + m16 : m32;
+}
+
+int field_set_layout(g4b_field* f, int mode) {
+  if (!f) return fail(G4B_ERR_ARG, "field layout: null field");
+  if (mode == f->mode) return G4B_OK;
+  if (f->precision != G4B_MIXED ||
+      (mode != pick_mode(f->ngrid, G4B_MIXED) && mode != alt_mode(f->ngrid)))
+    return fail(G4B_ERR_RANGE, "field layout: not a row layout of this grid");
+  const int old = f->mode;
+  f->mode = mode;
+  if (int rc = adi_configure(f)) {
+    f->mode = old;
+    return rc;
+  }
+  return G4B_OK;
 }
 
 static int encode_store_map(g4b_ctx* ctx, CUtensorMap* map, void* base, int n,

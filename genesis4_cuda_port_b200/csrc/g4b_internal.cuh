@@ -126,9 +126,11 @@ struct g4b_adi {
   double delz = 0, dgrid = 0, xks = 0, r = 0;
   int M = 0;                 // elements per lane (odd), 32-lane rows (FP64 fields)
   int mode32 = 0;            // row layout of FP32 fields (pick_mode)
+  int mode32_alt = 0;        // the other FP32 row layout (alt_mode), 0 if none
   // Tables in lane-minor order, complex (double2) and their FP32 copies.
   double2* d_tab64 = nullptr;   // [3][M][32]: cbet, G, H ; then [2][5][32] scans
   float2* d_tab32 = nullptr;
+  float2* d_tab32_alt = nullptr;  // tables of mode32_alt
   bool ready = false;
 };
 
@@ -240,6 +242,11 @@ int pick_M(int n);
 // 100 + M for 16-lane rows (FP32 fields whose rows fit 16 M slots more
 // closely than 32 M).
 int pick_mode(int n, int precision);
+// The other FP32 row layout of an n-point row (32 lanes <-> 16 lanes), 0 if none.
+int alt_mode(int n);
+// Switches an FP32 field between its two row layouts (pick_mode / alt_mode).
+// The solve is the same linear system; its FP32 rounding depends on the layout.
+int field_set_layout(g4b_field* f, int mode);
 inline int mode_M(int mode) { return mode % 100; }
 inline int mode_L(int mode) { return mode >= 100 ? 16 : 32; }
 

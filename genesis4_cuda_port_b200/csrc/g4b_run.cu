@@ -1500,6 +1500,7 @@ std::vector<int> state_key(g4b_run* r) {
   std::vector<int> k;
   for (int f = 0; f < r->nfield; ++f) {
     k.push_back(r->fs[f].first);
+    k.push_back(r->fs[f].f->mode);  // the ADI row layout the graph launches
     double a = r->fs[f].accuslip;
     int v[2];
     std::memcpy(v, &a, 8);
@@ -2032,6 +2033,7 @@ struct g4b_batch {
   int grid[4] = {0, 0, 0, 0};    // beam, deposit, adi, finalize
   int tune_left = 0, tune_idx = 0;
   std::vector<float> tune_ms[4];
+
   cudaEvent_t ev[5] = {};
   // concurrent branches of a step: the beam diagnostics beside the
   // deposition and ADI passes; the ADI kernels of different row layouts
@@ -2422,6 +2424,102 @@ int g4b_batch_tune(g4b_batch* b) {
   b->tune_left = 4;
   b->tune_idx = 0;
   for (auto& v : b->tune_ms) v.assign(4, 0.f);
+  return G4B_OK;
+}
+
+// The ADI row layouts, then the launch shapes as g4b_batch_tune.  For every
+// grid size among the attached runs' fields that has two row layouts (32
+// lanes of M elements, 16 lanes of M' elements), both passes are timed in
+// each layout on a scratch field of that grid (up to 128 slices of zeros,
+// best of three launches after one untimed), before any step: the runs'
+// state never advances in a trial layout, so every step of the batch uses
+// the chosen layouts and equals an alone run given the same layouts.
+int g4b_batch_tune_layouts(g4b_batch* b) {
+  if (!b) return fail(G4B_ERR_ARG, "g4b_batch_tune_layouts: null batch");
+  g4b_ctx* c = b->ctx;
+  G4B_CUDA_TRY(cudaSetDevice(c->device));
+  struct Group {
+    int n = 0, nslice = 0;
+    double gridmax = 0, xlambda = 0, delz = 0;
+    std::vector<g4b_field*> fields;
+  };
+  std::vector<Group> groups;
+  for (int s = 0; s < b->max_runs; ++s) {
+    g4b_run* r = b->runs[s];
+    if (!r || b->next[s] >= b->last[s] || r->steps.empty()) continue;
+    for (int f = 0; f < r->nfield; ++f) {
+      g4b_field* F = r->fs[f].f;
+      if (!alt_mode(F->ngrid)) continue;
+      Group* g = nullptr;
+      for (auto& x : groups)
+        if (x.n == F->ngrid) g = &x;
+      if (!g) {
+        groups.emplace_back();
+        g = &groups.back();
+        g->n = F->ngrid;
+        g->gridmax = F->gridmax;
+        g->xlambda = F->xlambda;
+        g->delz = r->steps[0].delz > 0 ? r->steps[0].delz : 0.015;
+      }
+      g->nslice += F->nslice;
+      g->fields.push_back(F);
+    }
+  }
+  for (Group& g : groups) {
+    g4b_field* f = nullptr;
+    g4b_adi* adi = nullptr;
+    int rc = g4b_field_create(c, std::min(g.nslice, 128), g.n, g.gridmax, g.xlambda, 1,
+                              G4B_MIXED, 0, &f);
+    if (rc == G4B_OK) rc = g4b_adi_create(c, &adi);
+    if (rc == G4B_OK) rc = g4b_adi_init(adi, g.delz, f->dgrid, f->xks, g.n);
+    const int modes[2] = {pick_mode(g.n, G4B_MIXED), alt_mode(g.n)};
+    float best[2] = {1e30f, 1e30f};
+    for (int k = 0; k < 2 && rc == G4B_OK; ++k) {
+      rc = field_set_layout(f, modes[k]);
+      AdiPlan P;
+      if (rc == G4B_OK) rc = adi_plan(adi, f, nullptr, f->desc, nullptr, P);
+      for (int it = 0; it < 4 && rc == G4B_OK; ++it) {
+        cudaEventRecord(b->ev[0], c->stream);
+        rc = adi_launch(f, P);
+        cudaEventRecord(b->ev[1], c->stream);
+        if (rc == G4B_OK) {
+          cudaError_t e = cudaEventSynchronize(b->ev[1]);
+          if (e != cudaSuccess) rc = cuda_fail(e, "g4b_batch_tune_layouts");
+        }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, b->ev[0], b->ev[1]);
+        if (it > 0) best[k] = std::min(best[k], ms);
+      }
+    }
+    if (rc == G4B_OK) rc = read_device_error(c, "g4b_batch_tune_layouts");
+    g4b_adi_destroy(adi);
+    g4b_field_destroy(f);
+    if (rc != G4B_OK) return rc;
+    const int pick = best[1] < best[0] ? modes[1] : modes[0];
+    for (g4b_field* F : g.fields)
+      if (int r2 = field_set_layout(F, pick)) return r2;
+  }
+  b->dirty = true;
+  b->graph_valid = false;
+  return g4b_batch_tune(b);
+}
+int g4b_default_layout(int ngrid) { return pick_mode(ngrid, G4B_MIXED); }
+
+// ADI row layouts of a run's fields: M elements per lane on 32-lane rows, or
+// 100 + M on 16-lane rows (two rows per warp).
+int g4b_run_get_layouts(g4b_run* r, int* modes) {
+  if (!r || !modes) return fail(G4B_ERR_ARG, "g4b_run_get_layouts: null arg");
+  for (int f = 0; f < r->nfield; ++f) modes[f] = r->fs[f].f->mode;
+  return G4B_OK;
+}
+
+// Sets them (each the default or the other layout of the field's grid), e.g.
+// to rerun a batch-tuned run alone with the same FP32 rounding.
+int g4b_run_set_layouts(g4b_run* r, const int* modes) {
+  if (!r || !modes) return fail(G4B_ERR_ARG, "g4b_run_set_layouts: null arg");
+  G4B_CUDA_TRY(cudaSetDevice(r->ctx->device));
+  for (int f = 0; f < r->nfield; ++f)
+    if (int rc = field_set_layout(r->fs[f].f, modes[f])) return rc;
   return G4B_OK;
 }
 

@@ -289,8 +289,12 @@ int g4h_scan(const g4h_engine_config* cfg, const g4h_job* jobs, int njobs,
         g4b_batch_attach(batch, runs[i], 0, (int)ins[i]->steps.size(), &slot);
       }
       // the tuner times its candidate shapes on the first steps of the
-      // real runs: shapes do not change results
-      if (cfg->tune) g4b_batch_tune(batch);
+      // real runs (launch shapes do not change results; with tune = 2 it
+      // also picks the ADI row layouts, which set the FP32 rounding)
+      if (cfg->tune >= 2)
+        g4b_batch_tune_layouts(batch);
+      else if (cfg->tune)
+        g4b_batch_tune(batch);
     }
     check(g4b_ctx_synchronize(ctx), "g4h_scan");
     const double t0 = now_s();
@@ -309,6 +313,13 @@ int g4h_scan(const g4h_engine_config* cfg, const g4h_job* jobs, int njobs,
     res->njobs = njobs;
     res->grids[0] = res->grids[1] = res->grids[2] = res->grids[3] = 0;
     if (batch) g4b_batch_shapes(batch, res->grids);
+    res->layouts_16 = res->layouts_switched = 0;
+    for (int i = 0; i < njobs; ++i) {
+      int modes[8] = {0};
+      g4b_run_get_layouts(runs[i], modes);
+      res->layouts_16 += modes[0] >= 100;
+      res->layouts_switched += modes[0] != g4b_default_layout(jobs[i].ngrid);
+    }
     uint64_t bytes = 0;
     for (auto* r : runs) {
       uint64_t b = 0;

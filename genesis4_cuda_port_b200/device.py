@@ -397,6 +397,15 @@ class Run:
         a = np.ascontiguousarray(np.broadcast_to(current, (self.nslice,)), dtype=np.float64)
         check(self.lib.g4b_run_set_current(self.h, dptr(a)))
 
+    def layouts(self) -> list:
+        out = (C.c_int * 8)()
+        check(self.lib.g4b_run_get_layouts(self.h, out))
+        return list(out[: len(self.fields)])
+
+    def set_layouts(self, layouts) -> None:
+        arr = (C.c_int * 8)(*layouts)
+        check(self.lib.g4b_run_set_layouts(self.h, arr))
+
     def set_eloss(self, eloss=None) -> None:
         a = None if eloss is None else np.ascontiguousarray(eloss, dtype=np.float64)
         check(self.lib.g4b_run_set_eloss(self.h, dptr(a)))
@@ -486,6 +495,10 @@ class Batch:
 
     def tune(self) -> None:
         check(self.lib.g4b_batch_tune(self.h))
+
+    def tune_layouts(self) -> None:
+        """Launch shapes, then the ADI row layouts (g4b_batch_tune_layouts)."""
+        check(self.lib.g4b_batch_tune_layouts(self.h))
 
     def shapes(self):
         g = (C.c_int * 4)()

@@ -279,7 +279,8 @@ class EngineConfig(C.Structure):
 
 class ScanResult(C.Structure):
     _fields_ = [("value", C.c_double), ("seconds", C.c_double), ("slice_steps", C.c_double),
-                ("device_bytes", C.c_double), ("njobs", C.c_int), ("grids", C.c_int * 4)]
+                ("device_bytes", C.c_double), ("njobs", C.c_int), ("grids", C.c_int * 4),
+                ("layouts_16", C.c_int), ("layouts_switched", C.c_int)]
 
 
 class ServeStats(C.Structure):
@@ -299,8 +300,9 @@ def _bind_engine(h):
 
 
 def engine_config(lattice: str, beamline: str, delz: float, gamma_ref: float, lambda0: float,
-                  max_runs: int = 256, graph: bool = True, tune: bool = True, mode: int = 0,
+                  max_runs: int = 256, graph: bool = True, tune: int = 1, mode: int = 0,
                   threads: int = 0, reserve_bytes: float = 4e9) -> EngineConfig:
+    """tune: 0 off, 1 launch shapes, 2 ADI row layouts and launch shapes."""
     c = EngineConfig()
     c._keep = (lattice.encode(), beamline.encode())
     c.lattice, c.beamline = c._keep

@@ -374,8 +374,22 @@ int g4b_batch_step(g4b_batch* batch, int nsteps, int use_graph);
 /* Autotuner: the next 4 steps try candidate launch shapes (CTAs per SM) for
  * each kernel, timed with CUDA events; the fastest shape per kernel stays. */
 int g4b_batch_tune(g4b_batch* batch);
+/* Autotuner with row shapes: the launch shapes as g4b_batch_tune, then, for
+ * every group of fields sharing an ADI row layout that has another one (a row
+ * of n cells as 32 lanes x M elements or as 16 lanes x M' elements, two rows
+ * per warp), one timed step in the current layouts and one with the group
+ * switched; the faster stays.  The layout sets the FP32 rounding of the row
+ * solve (the same linear system), so results of a layout-tuned batch equal an
+ * alone run given the same layouts (g4b_run_set_layouts). */
+int g4b_batch_tune_layouts(g4b_batch* batch);
 /* CTAs of the beam, deposition, ADI and finalize launches in use. */
 int g4b_batch_shapes(g4b_batch* batch, int* grids4);
+/* ADI row layouts of a run's fields: M (32-lane rows of M elements) or
+ * 100 + M (16-lane rows), and setting them (the default layout of the grid,
+ * g4b_default_layout, or its other one). */
+int g4b_run_get_layouts(g4b_run* run, int* layouts);
+int g4b_run_set_layouts(g4b_run* run, const int* layouts);
+int g4b_default_layout(int ngrid);
 /* Stream marks: g4b_ctx_mark records a point in the context's stream and
  * returns its ticket; g4b_ctx_mark_query reports (or with wait, waits for)
  * the completion of everything enqueued before it.  The last 256 tickets

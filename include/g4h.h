@@ -156,7 +156,7 @@ typedef struct g4h_engine_config {
   const char* beamline;
   double delz, gamma_ref, lambda0;
   int max_runs;          /* batch slots                                      */
-  int use_graph, tune;
+  int use_graph, tune;   /* tune: 1 launch shapes, 2 also ADI row layouts  */
   int mode;              /* scan: 0 batched, 1 one run after another         */
   int threads;           /* input-preparation threads (0 = cores - 2)        */
   double reserve_bytes;  /* serve: device memory kept free at admission      */
@@ -167,6 +167,8 @@ typedef struct g4h_scan_result {
   double seconds, slice_steps, device_bytes;
   int njobs;
   int grids[4];          /* launch shapes the batch used                     */
+  int layouts_16;        /* runs whose ADI rows ended on 16-lane layouts     */
+  int layouts_switched;  /* runs the row-layout tuner moved off the default  */
 } g4h_scan_result;
 
 typedef struct g4h_serve_stats {

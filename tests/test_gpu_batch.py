@@ -138,3 +138,51 @@ def test_many_slices_alone_graphed_and_batched_agree(ctx):
     ctx.synchronize()
     _same(_result(run, cfg["nsteps"]), ref)
     batch.close()
+
+
+def test_row_layout_tuner_keeps_batch_equal_to_alone(ctx):
+    """g4b_batch_tune_layouts times both ADI row layouts of every grid on a
+    scratch field before the first step; every step then runs in the chosen
+    layouts, so each run equals an alone run given the same layouts."""
+    lib = ctx.lib
+    batch = dev.Batch(ctx, 8)
+    runs = [_make(ctx, k, cfg) for k, cfg in enumerate(CONFIGS)]
+    for r, cfg in zip(runs, CONFIGS):
+        batch.attach(r, 0, cfg["nsteps"])
+    batch.tune_layouts()
+    longest = max(cfg["nsteps"] for cfg in CONFIGS)
+    batch.step(longest + 2, graph=True)
+    ctx.synchronize()
+    for k, (r, cfg) in enumerate(zip(runs, CONFIGS)):
+        lay = r.layouts()
+        default = lib.g4b_default_layout(cfg["ngrid"])
+        assert lay[0] == default or (lay[0] >= 100) != (default >= 100)
+        alone = _make(ctx, k, cfg)
+        alone.set_layouts(lay)
+        alone.advance(0, cfg["nsteps"], graph=False)
+        _same(_result(r, cfg["nsteps"]), _result(alone, cfg["nsteps"]))
+        alone.close()
+    batch.close()
+
+
+def test_both_row_layouts_solve_the_same_system(ctx):
+    """The other row layout of a grid changes only the FP32 rounding of the
+    row solve; a layout that is not one of the grid's two is refused."""
+    k, cfg = 3, CONFIGS[3]  # ngrid 101: 16 lanes x 7 by default, 32 lanes x 5 the other
+    a = _make(ctx, k, cfg)
+    a.advance(0, cfg["nsteps"], graph=False)
+    ra = _result(a, cfg["nsteps"])
+    b = _make(ctx, k, cfg)
+    lay = b.layouts()
+    other = 5 if lay[0] >= 100 else 107
+    b.set_layouts([other])
+    assert b.layouts() == [other]
+    b.advance(0, cfg["nsteps"], graph=False)
+    rb = _result(b, cfg["nsteps"])
+    assert not np.array_equal(ra[1], rb[1])
+    scale = np.max(np.abs(ra[1]))
+    assert np.max(np.abs(ra[1] - rb[1])) < 1e-4 * scale
+    with pytest.raises(Exception):
+        b.set_layouts([9])
+    a.close()
+    b.close()
