@@ -108,7 +108,8 @@ __global__ void __launch_bounds__(kScThreads) short_range_kernel(const ScArgs a)
     for (int64_t p = p0 + tid; p < p1; p += nt) {
       const double dx = a.x[p] - xc, dy = a.y[p] - yc;
       const double r = sqrt(dx * dx + dy * dy);
-      const int j = min((int)(r / dr), n - 1);
+      const double q = r / dr;  // NaN or beyond the wall: the last cell
+      const int j = q >= 0.0 && q < (double)n ? (int)q : n - 1;
       const double cph = r > 0.0 ? dx / r : 1.0, sph = r > 0.0 ? dy / r : 0.0;
       const double th = a.theta[p];
       for (int l = 1; l <= a.nz; ++l) {
@@ -166,7 +167,8 @@ __global__ void __launch_bounds__(kScThreads) short_range_kernel(const ScArgs a)
     for (int64_t p = p0 + tid; p < p1; p += nt) {
       const double dx = a.x[p] - xc, dy = a.y[p] - yc;
       const double r = sqrt(dx * dx + dy * dy);
-      const int j = min((int)(r / dr), n - 1);
+      const double q = r / dr;  // NaN or beyond the wall: the last cell
+      const int j = q >= 0.0 && q < (double)n ? (int)q : n - 1;
       const double cph = r > 0.0 ? dx / r : 1.0, sph = r > 0.0 ? dy / r : 0.0;
       const double th = a.theta[p];
       double sum = 0.0;

@@ -622,7 +622,9 @@ def short_range(off, parts, current, gammaz2, *, rmax, ngrid, nz, nphi, lambda0,
             modes.append(None)
             continue
         dr = R / ngrid
-        j = np.minimum((r / dr).astype(np.int64), ngrid - 1)
+        q = r / dr
+        ok = (q >= 0) & (q < ngrid)  # NaN or beyond the wall: the last cell
+        j = np.where(ok, np.where(ok, q, 0).astype(np.int64), ngrid - 1)
         safe = np.where(r > 0, r, 1.0)
         cph, sph = np.where(r > 0, dx / safe, 1.0), np.where(r > 0, dy / safe, 0.0)
         total = np.zeros(npart)
