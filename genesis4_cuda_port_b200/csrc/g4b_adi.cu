@@ -547,7 +547,16 @@ __global__ void __launch_bounds__(512, 2) deposit_slice_kernel(const DepositArgs
 
   for (int yb = by0; yb < by0 + bh; yb += band_h) {
     const int hb = min(band_h, by0 + bh - yb);
-    for (int i = tid; i < 2 * hb * bw; i += blockDim.x) acc[i] = 0ull;
+    // four 32-bit planes per band: low and high words of the real and the
+    // imaginary 64-bit sums (a 64-bit shared atomic costs about four 32-bit
+    // ones; the low word's carry goes to the high word, so every sum is the
+    // exact 64-bit integer whatever the order of the adds)
+    const int ncell = hb * bw;
+    unsigned int* lre = reinterpret_cast<unsigned int*>(acc);
+    unsigned int* lim = lre + ncell;
+    int* hre = reinterpret_cast<int*>(lim + ncell);
+    int* him = hre + ncell;
+    for (int i = tid; i < 2 * ncell; i += blockDim.x) acc[i] = 0ull;
     __syncthreads();
     for (int64_t pb = p0 + tid; pb < p1; pb += (int64_t)kDepFp64U * nt) {
       double lx[kDepFp64U], ly[kDepFp64U], lg[kDepFp64U], lt[kDepFp64U];
@@ -582,18 +591,21 @@ __global__ void __launch_bounds__(512, 2) deposit_slice_kernel(const DepositArgs
         const int ry = cy[c] - yb;
         if (ry < 0 || ry >= hb) continue;
         const int cell = ry * bw + (cx[c] - bx0);
-        atomicAdd(&acc[2 * cell], (unsigned long long)__double2ll_rn(vre * w[c]));
-        atomicAdd(&acc[2 * cell + 1], (unsigned long long)__double2ll_rn(vim * w[c]));
+        const long long cr = __double2ll_rn(vre * w[c]), ci = __double2ll_rn(vim * w[c]);
+        const unsigned int rlo = (unsigned int)cr, ilo = (unsigned int)ci;
+        const unsigned int rold = atomicAdd(&lre[cell], rlo);
+        const unsigned int iold = atomicAdd(&lim[cell], ilo);
+        atomicAdd(&hre[cell], (int)(cr >> 32) + (rold + rlo < rold ? 1 : 0));
+        atomicAdd(&him[cell], (int)(ci >> 32) + (iold + ilo < iold ? 1 : 0));
       }
       }
     }
     __syncthreads();
     double2* out = S + (size_t)(yb - by0) * bw;
-    for (int i = tid; i < hb * bw; i += blockDim.x) {
-      double2 val;
-      val.x = (double)(long long)acc[2 * i] * unscale;
-      val.y = (double)(long long)acc[2 * i + 1] * unscale;
-      out[i] = val;
+    for (int i = tid; i < ncell; i += blockDim.x) {
+      const long long sr = (long long)(((unsigned long long)(unsigned int)hre[i] << 32) | lre[i]);
+      const long long si = (long long)(((unsigned long long)(unsigned int)him[i] << 32) | lim[i]);
+      out[i] = make_double2((double)sr * unscale, (double)si * unscale);
     }
     __syncthreads();
   }

@@ -24,12 +24,20 @@
 // algorithm: with w_j = exp(-i pi j^2 / n), DFT_n(x)_k = w_k (a * h)_k, a_j =
 // x_j w_j, h_t = conj(w_t), a circular convolution of length 512 >= 2n - 1
 // done as FFT_512 -> multiply by the precomputed FFT_512(h) -> inverse FFT.
-// The 512-point FFT lives in one warp: lane l holds x[32 j + l] in register
-// j (j < 16); a 16-point DFT in registers, the twiddles W_512^(l k1), and a
-// 32-point DFT across lanes by shuffles (four-step factorisation
-// 512 = 16 x 32).  Its output is in the permuted order
-// k = brev4(r) + 16 brev5(l), which only the pointwise multiply sees; the
-// inverse runs the same butterflies backwards and returns natural order.
+// The 512-point FFT lives in one warp: lane l holds x[32 r + l] in register
+// r (r < 16).  With j = j0 + 8 j1 + 64 j2 and k = k0 + 8 k1 + 64 k2 it is
+// three radix-8 stages (decimation in frequency):
+//   A: per (j0, j1) an 8-point DFT over j2 -> k0, times W_512^((j0 + 8 j1) k0);
+//   B: per (j0, k0) an 8-point DFT over j1 -> k1, times W_64^(j0 k1);
+//   C: per (k1, k0) an 8-point DFT over j0 -> k2.
+// Each lane holds two groups of eight (registers 2 s + b), so every stage
+// runs in registers; between stages the warp regroups its 512 values through
+// a private shared-memory buffer (rows of nine entries: no bank conflicts),
+// two exchanges in place of the five shuffle rounds of a cross-lane radix-2
+// form.  The output is in the permuted order (lane l, register 2 s + b) ->
+// k0 + 8 k1 + 64 k2 with q = l + 32 b, k0 = q / 8, k1 = q % 8, k2 = brev3(s),
+// which only the pointwise multiply sees; the inverse runs the stages back
+// (decimation in time, conjugate twiddles) and returns natural order.
 #include <algorithm>
 #include <cmath>
 #include <complex>
@@ -73,68 +81,202 @@ __device__ __forceinline__ double2 zmul(double2 a, double2 b) {
 __device__ __forceinline__ double2 zmulc(double2 a, double2 b) {
   return make_double2(fma(a.x, b.x, a.y * b.y), fma(a.y, b.x, -a.x * b.y));
 }
-__device__ __forceinline__ double2 shfl_xor2(double2 v, int m) {
-  v.x = __shfl_xor_sync(0xffffffffu, v.x, m);
-  v.y = __shfl_xor_sync(0xffffffffu, v.y, m);
-  return v;
+__host__ __device__ constexpr int brev3(int k) { return ((k & 1) << 2) | (k & 2) | ((k & 4) >> 2); }
+
+constexpr int kXbRow = 9;              // padded row of eight
+constexpr int kXb = 8 * 8 * kXbRow;    // exchange buffer per warp (double2)
+constexpr double kS = 0.70710678118654752440;
+
+__device__ __forceinline__ double2 mul_w1(double2 z) {  // x (1 - i)/sqrt2
+  return make_double2(kS * (z.x + z.y), kS * (z.y - z.x));
 }
-__host__ __device__ constexpr int brev4(int r) {
-  return ((r & 1) << 3) | ((r & 2) << 1) | ((r & 4) >> 1) | ((r & 8) >> 3);
+__device__ __forceinline__ double2 mul_w2(double2 z) { return make_double2(z.y, -z.x); }  // x (-i)
+__device__ __forceinline__ double2 mul_w3(double2 z) {  // x (-1 - i)/sqrt2
+  return make_double2(kS * (z.y - z.x), -kS * (z.x + z.y));
+}
+__device__ __forceinline__ double2 mul_c1(double2 z) {  // x (1 + i)/sqrt2
+  return make_double2(kS * (z.x - z.y), kS * (z.x + z.y));
+}
+__device__ __forceinline__ double2 mul_c2(double2 z) { return make_double2(-z.y, z.x); }  // x i
+__device__ __forceinline__ double2 mul_c3(double2 z) {  // x (-1 + i)/sqrt2
+  return make_double2(-kS * (z.x + z.y), kS * (z.x - z.y));
 }
 
-// Forward 512-point DFT (exp(-2 pi i jk / 512)) of x[32 j + lane] = v[j];
-// afterwards v[r] of lane l holds X[brev4(r) + 16 brev5(l)].
-__device__ __forceinline__ void fft512_fwd(double2 (&v)[16], int lane, const double2* tw) {
-#pragma unroll
-  for (int h = 8; h >= 1; h >>= 1)
-#pragma unroll
-    for (int blk = 0; blk < 16; blk += 2 * h)
-#pragma unroll
-      for (int t = 0; t < h; ++t) {
-        const double2 a = v[blk + t], b = v[blk + t + h];
-        v[blk + t] = zadd(a, b);
-        v[blk + t + h] = t == 0 ? zsub(a, b) : zmul(zsub(a, b), tw[t * (256 / h)]);
-      }
-#pragma unroll
-  for (int r = 1; r < 16; ++r) v[r] = zmul(v[r], tw[(lane * brev4(r)) & (kFftM - 1)]);
-#pragma unroll
-  for (int h = 16; h >= 1; h >>= 1) {
-    const bool upper = (lane & h) != 0;
-    const double2 w = tw[(lane & (h - 1)) * (256 / h)];
-#pragma unroll
-    for (int r = 0; r < 16; ++r) {
-      const double2 p = shfl_xor2(v[r], h);
-      v[r] = upper ? zmul(zsub(p, v[r]), w) : zadd(v[r], p);
-    }
+// 8-point DFT of v[2 s + B], s = 0..7 (radix-2, decimation in frequency):
+// X[k] lands in slot brev3(k).
+template <int B>
+__device__ __forceinline__ void dft8(double2 (&v)[16]) {
+#define G4B_A(s) v[2 * (s) + B]
+  {
+    double2 x = G4B_A(0), y = G4B_A(4);
+    G4B_A(0) = zadd(x, y);
+    G4B_A(4) = zsub(x, y);
+    x = G4B_A(1), y = G4B_A(5);
+    G4B_A(1) = zadd(x, y);
+    G4B_A(5) = mul_w1(zsub(x, y));
+    x = G4B_A(2), y = G4B_A(6);
+    G4B_A(2) = zadd(x, y);
+    G4B_A(6) = mul_w2(zsub(x, y));
+    x = G4B_A(3), y = G4B_A(7);
+    G4B_A(3) = zadd(x, y);
+    G4B_A(7) = mul_w3(zsub(x, y));
   }
+#pragma unroll
+  for (int blk = 0; blk < 8; blk += 4) {
+    double2 x = G4B_A(blk), y = G4B_A(blk + 2);
+    G4B_A(blk) = zadd(x, y);
+    G4B_A(blk + 2) = zsub(x, y);
+    x = G4B_A(blk + 1), y = G4B_A(blk + 3);
+    G4B_A(blk + 1) = zadd(x, y);
+    G4B_A(blk + 3) = mul_w2(zsub(x, y));
+  }
+#pragma unroll
+  for (int blk = 0; blk < 8; blk += 2) {
+    const double2 x = G4B_A(blk), y = G4B_A(blk + 1);
+    G4B_A(blk) = zadd(x, y);
+    G4B_A(blk + 1) = zsub(x, y);
+  }
+}
+
+// Unnormalised inverse of dft8 (decimation in time, conjugate twiddles):
+// input in its output order, x[j] in slot j.
+template <int B>
+__device__ __forceinline__ void idft8(double2 (&v)[16]) {
+#pragma unroll
+  for (int blk = 0; blk < 8; blk += 2) {
+    const double2 x = G4B_A(blk), y = G4B_A(blk + 1);
+    G4B_A(blk) = zadd(x, y);
+    G4B_A(blk + 1) = zsub(x, y);
+  }
+#pragma unroll
+  for (int blk = 0; blk < 8; blk += 4) {
+    double2 x = G4B_A(blk), y = G4B_A(blk + 2);
+    G4B_A(blk) = zadd(x, y);
+    G4B_A(blk + 2) = zsub(x, y);
+    x = G4B_A(blk + 1), y = mul_c2(G4B_A(blk + 3));
+    G4B_A(blk + 1) = zadd(x, y);
+    G4B_A(blk + 3) = zsub(x, y);
+  }
+  {
+    double2 x = G4B_A(0), y = G4B_A(4);
+    G4B_A(0) = zadd(x, y);
+    G4B_A(4) = zsub(x, y);
+    x = G4B_A(1), y = mul_c1(G4B_A(5));
+    G4B_A(1) = zadd(x, y);
+    G4B_A(5) = zsub(x, y);
+    x = G4B_A(2), y = mul_c2(G4B_A(6));
+    G4B_A(2) = zadd(x, y);
+    G4B_A(6) = zsub(x, y);
+    x = G4B_A(3), y = mul_c3(G4B_A(7));
+    G4B_A(3) = zadd(x, y);
+    G4B_A(7) = zsub(x, y);
+  }
+#undef G4B_A
+}
+
+// Multiplies slot s of group B by W^(e k), k = brev3(s), e given by the
+// table entries w1 = W^e, w2 = W^(2e), w4 = W^(4e) (CONJ: by the conjugates).
+template <bool CONJ>
+__device__ __forceinline__ double2 tmul(double2 z, double2 w) { return CONJ ? zmulc(z, w) : zmul(z, w); }
+// slot s holds k = brev3(s): 1 -> 4, 2 -> 2, 3 -> 6, 4 -> 1, 5 -> 5, 6 -> 3, 7 -> 7
+template <int B, bool CONJ>
+__device__ __forceinline__ void twiddle8(double2 (&v)[16], double2 w1, double2 w2, double2 w4) {
+  v[2 * 4 + B] = tmul<CONJ>(v[2 * 4 + B], w1);
+  v[2 * 2 + B] = tmul<CONJ>(v[2 * 2 + B], w2);
+  v[2 * 1 + B] = tmul<CONJ>(v[2 * 1 + B], w4);
+  double2 w = zmul(w2, w1);  // k = 3
+  v[2 * 6 + B] = tmul<CONJ>(v[2 * 6 + B], w);
+  w = zmul(w4, w1);  // k = 5
+  v[2 * 5 + B] = tmul<CONJ>(v[2 * 5 + B], w);
+  w = zmul(w4, w2);  // k = 6
+  v[2 * 3 + B] = tmul<CONJ>(v[2 * 3 + B], w);
+  w = zmul(w, w1);  // k = 7
+  v[2 * 7 + B] = tmul<CONJ>(v[2 * 7 + B], w);
+}
+
+// Forward 512-point DFT (exp(-2 pi i jk / 512)) of x[32 r + lane] = v[r];
+// tw = W_512^j (j < 512), xb = this warp's kXb-entry exchange buffer.
+__device__ __forceinline__ void fft512_fwd(double2 (&v)[16], int lane, const double2* tw,
+                                           double2* xb) {
+  const int lo = lane & 7, hi = lane >> 3;
+  // stage A: group b is (j0, j1) = (lo, 4 b + hi), g = j0 + 8 j1 = lane + 32 b
+  dft8<0>(v);
+  dft8<1>(v);
+  twiddle8<0, false>(v, tw[lane], tw[2 * lane], tw[4 * lane]);
+  twiddle8<1, false>(v, tw[lane + 32], tw[2 * lane + 64], tw[4 * lane + 128]);
+  // regroup by (j0, k0): entry k0 * 72 + j1 * 9 + j0
+#pragma unroll
+  for (int b = 0; b < 2; ++b)
+#pragma unroll
+    for (int s = 0; s < 8; ++s) xb[brev3(s) * 8 * kXbRow + (4 * b + hi) * kXbRow + lo] = v[2 * s + b];
+  __syncwarp();
+#pragma unroll
+  for (int b = 0; b < 2; ++b)
+#pragma unroll
+    for (int j1 = 0; j1 < 8; ++j1) v[2 * j1 + b] = xb[(hi + 4 * b) * 8 * kXbRow + j1 * kXbRow + lo];
+  __syncwarp();
+  // stage B: group b is (j0, k0) = (lo, hi + 4 b); W_64^(j0 k1) = W_512^(8 j0 k1)
+  dft8<0>(v);
+  dft8<1>(v);
+  {
+    const double2 w1 = tw[8 * lo], w2 = tw[16 * lo], w4 = tw[32 * lo];
+    twiddle8<0, false>(v, w1, w2, w4);
+    twiddle8<1, false>(v, w1, w2, w4);
+  }
+  // regroup by (k1, k0): entry k0 * 72 + k1 * 9 + j0
+#pragma unroll
+  for (int b = 0; b < 2; ++b)
+#pragma unroll
+    for (int s = 0; s < 8; ++s) xb[(hi + 4 * b) * 8 * kXbRow + brev3(s) * kXbRow + lo] = v[2 * s + b];
+  __syncwarp();
+#pragma unroll
+  for (int b = 0; b < 2; ++b)
+#pragma unroll
+    for (int j0 = 0; j0 < 8; ++j0) v[2 * j0 + b] = xb[(hi + 4 * b) * 8 * kXbRow + lo * kXbRow + j0];
+  __syncwarp();
+  // stage C: group b is (k1, k0) = (lo, hi + 4 b)
+  dft8<0>(v);
+  dft8<1>(v);
 }
 
 // Unnormalised inverse (exp(+2 pi i jk / 512)) of fft512_fwd: input in its
-// output order, output v[j] of lane l = 512 x[32 j + l].
-__device__ __forceinline__ void fft512_inv(double2 (&v)[16], int lane, const double2* tw) {
+// output order, output v[r] of lane l = 512 x[32 r + l].
+__device__ __forceinline__ void fft512_inv(double2 (&v)[16], int lane, const double2* tw,
+                                           double2* xb) {
+  const int lo = lane & 7, hi = lane >> 3;
+  idft8<0>(v);
+  idft8<1>(v);
 #pragma unroll
-  for (int h = 1; h <= 16; h <<= 1) {
-    const bool upper = (lane & h) != 0;
-    const double2 w = tw[(lane & (h - 1)) * (256 / h)];
+  for (int b = 0; b < 2; ++b)
 #pragma unroll
-    for (int r = 0; r < 16; ++r) {
-      const double2 p = shfl_xor2(v[r], h);
-      v[r] = upper ? zsub(p, zmulc(v[r], w)) : zadd(v[r], zmulc(p, w));
-    }
+    for (int j0 = 0; j0 < 8; ++j0) xb[(hi + 4 * b) * 8 * kXbRow + lo * kXbRow + j0] = v[2 * j0 + b];
+  __syncwarp();
+#pragma unroll
+  for (int b = 0; b < 2; ++b)
+#pragma unroll
+    for (int s = 0; s < 8; ++s) v[2 * s + b] = xb[(hi + 4 * b) * 8 * kXbRow + brev3(s) * kXbRow + lo];
+  __syncwarp();
+  {
+    const double2 w1 = tw[8 * lo], w2 = tw[16 * lo], w4 = tw[32 * lo];
+    twiddle8<0, true>(v, w1, w2, w4);
+    twiddle8<1, true>(v, w1, w2, w4);
   }
+  idft8<0>(v);
+  idft8<1>(v);
 #pragma unroll
-  for (int r = 1; r < 16; ++r) v[r] = zmulc(v[r], tw[(lane * brev4(r)) & (kFftM - 1)]);
+  for (int b = 0; b < 2; ++b)
 #pragma unroll
-  for (int h = 1; h <= 8; h <<= 1)
+    for (int j1 = 0; j1 < 8; ++j1) xb[(hi + 4 * b) * 8 * kXbRow + j1 * kXbRow + lo] = v[2 * j1 + b];
+  __syncwarp();
 #pragma unroll
-    for (int blk = 0; blk < 16; blk += 2 * h)
+  for (int b = 0; b < 2; ++b)
 #pragma unroll
-      for (int t = 0; t < h; ++t) {
-        const double2 a = v[blk + t];
-        const double2 b = t == 0 ? v[blk + t + h] : zmulc(v[blk + t + h], tw[t * (256 / h)]);
-        v[blk + t] = zadd(a, b);
-        v[blk + t + h] = zsub(a, b);
-      }
+    for (int s = 0; s < 8; ++s) v[2 * s + b] = xb[brev3(s) * 8 * kXbRow + (4 * b + hi) * kXbRow + lo];
+  __syncwarp();
+  twiddle8<0, true>(v, tw[lane], tw[2 * lane], tw[4 * lane]);
+  twiddle8<1, true>(v, tw[lane + 32], tw[2 * lane + 64], tw[4 * lane + 128]);
+  idft8<0>(v);
+  idft8<1>(v);
 }
 
 // DFT_n of one line (INV: the unnormalised inverse, exp(+2 pi i jk / n)),
@@ -142,17 +284,17 @@ __device__ __forceinline__ void fft512_inv(double2 (&v)[16], int lane, const dou
 // the same layout (entries at and beyond n are not meaningful).
 template <bool INV>
 __device__ __forceinline__ void line_dft(double2 (&v)[16], int lane, int n, const double2* tw,
-                                         const double2* chirp, const double2* H) {
+                                         const double2* chirp, const double2* H, double2* xb) {
 #pragma unroll
   for (int j = 0; j < 16; ++j) {
     const int i = 32 * j + lane;
     if (i < n) v[j] = INV ? zmulc(v[j], chirp[i]) : zmul(v[j], chirp[i]);
     else v[j] = make_double2(0.0, 0.0);
   }
-  fft512_fwd(v, lane, tw);
+  fft512_fwd(v, lane, tw, xb);
 #pragma unroll
   for (int r = 0; r < 16; ++r) v[r] = zmul(v[r], H[lane * 16 + r]);
-  fft512_inv(v, lane, tw);
+  fft512_inv(v, lane, tw, xb);
 #pragma unroll
   for (int j = 0; j < 16; ++j) {
     const int i = 32 * j + lane;
@@ -188,67 +330,70 @@ __device__ __forceinline__ void load_src_row(double2 (&v)[16], const FftArgs& a,
 }
 
 // pass A: rows forward along x, written transposed.  SRC: the source rows too.
+// The warps' exchange buffers double as the transposition tile once every
+// warp's transform is done.
 template <bool SRC>
-__global__ void __launch_bounds__(kFftWarps * 32) fft_rows_fwd_kernel(const FftArgs a) {
+__global__ void __launch_bounds__(kFftWarps * 32, 2) fft_rows_fwd_kernel(const FftArgs a) {
   extern __shared__ __align__(16) double2 sm[];
   load_tables(sm, a, true, false);
   const double2* tw = sm;
   const double2* ch = sm + kFftM;
   const double2* hf = ch + kFftMaxN;
-  double2* tile = sm + kTabDoubles2 + kFftM;  // [kx][kFftPitch]
-  double2* stile = tile + (size_t)kFftMaxN * kFftPitch;
+  double2* xall = sm + kTabDoubles2 + kFftM;  // kFftWarps exchange buffers
+  double2* tile = xall;                       // [kx][kFftPitch], after the transforms
   const int n = a.n, s = blockIdx.x / a.nband, band = blockIdx.x % a.nband;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double2* xb = xall + warp * kXb;
   const int iy0 = band * kFftWarps, iy = iy0 + warp;
   const int rows = min(kFftWarps, n - iy0);
   __syncthreads();
-  if (warp < rows) {
+  for (int part = 0; part < (SRC ? 2 : 1); ++part) {
     double2 v[16];
-    const double2* row = a.u + ((size_t)s * n + iy) * a.ld;
+    if (warp < rows) {
+      if (part == 0) {
+        const double2* row = a.u + ((size_t)s * n + iy) * a.ld;
 #pragma unroll
-    for (int j = 0; j < 16; ++j) {
-      const int i = 32 * j + lane;
-      v[j] = i < n ? row[i] : make_double2(0.0, 0.0);
+        for (int j = 0; j < 16; ++j) {
+          const int i = 32 * j + lane;
+          v[j] = i < n ? row[i] : make_double2(0.0, 0.0);
+        }
+      } else {
+        load_src_row(v, a, s, iy, lane);
+      }
+      line_dft<false>(v, lane, n, tw, ch, hf, xb);
     }
-    line_dft<false>(v, lane, n, tw, ch, hf);
-#pragma unroll
-    for (int j = 0; j < 16; ++j) {
-      const int k = 32 * j + lane;
-      if (k < n) tile[k * kFftPitch + warp] = v[j];
-    }
-    if (SRC) {
-      load_src_row(v, a, s, iy, lane);
-      line_dft<false>(v, lane, n, tw, ch, hf);
+    __syncthreads();  // every transform done: the buffers become the tile
+    if (warp < rows) {
 #pragma unroll
       for (int j = 0; j < 16; ++j) {
         const int k = 32 * j + lane;
-        if (k < n) stile[k * kFftPitch + warp] = v[j];
+        if (k < n) tile[k * kFftPitch + warp] = v[j];
       }
     }
-  }
-  __syncthreads();
-  for (int idx = threadIdx.x; idx < n * kFftWarps; idx += blockDim.x) {
-    const int k = idx / kFftWarps, r = idx % kFftWarps;
-    if (r < rows) {
-      const size_t o = ((size_t)s * n + k) * a.ld + iy0 + r;
-      a.T[o] = tile[k * kFftPitch + r];
-      if (SRC) a.ST[o] = stile[k * kFftPitch + r];
+    __syncthreads();
+    double2* dst = part == 0 ? a.T : a.ST;
+    for (int idx = threadIdx.x; idx < n * kFftWarps; idx += blockDim.x) {
+      const int k = idx / kFftWarps, r = idx % kFftWarps;
+      if (r < rows) dst[((size_t)s * n + k) * a.ld + iy0 + r] = tile[k * kFftPitch + r];
     }
+    if (SRC && part == 0) __syncthreads();  // the tile is read before the next transforms
   }
 }
 
 // pass B: lines along y, forward, propagator (+ filtered source), inverse.
 template <bool FILTER>
-__global__ void __launch_bounds__(kFftWarps * 32) fft_cols_kernel(const FftArgs a) {
+__global__ void __launch_bounds__(kFftWarps * 32, FILTER ? 1 : 2) fft_cols_kernel(const FftArgs a) {
   extern __shared__ __align__(16) double2 sm[];
   load_tables(sm, a, true, true);
   const double2* tw = sm;
   const double2* ch = sm + kFftM;
   const double2* hf = ch + kFftMaxN;
   const double2* hi = hf + kFftM;
-  double2* stage = sm + kTabDoubles2 + 2 * kFftM;  // [warp][256] filtered source spectrum
+  double2* xall = sm + kTabDoubles2 + 2 * kFftM;  // kFftWarps exchange buffers
+  double2* stage = xall + kFftWarps * kXb;        // [warp][256] filtered source spectrum
   const int n = a.n, s = blockIdx.x / a.nband, band = blockIdx.x % a.nband;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double2* xb = xall + warp * kXb;
   const int kx = band * kFftWarps + warp;
   __syncthreads();
   if (kx >= n) return;
@@ -263,7 +408,7 @@ __global__ void __launch_bounds__(kFftWarps * 32) fft_cols_kernel(const FftArgs 
       const int i = 32 * j + lane;
       v[j] = i < n ? sline[i] : make_double2(0.0, 0.0);
     }
-    line_dft<false>(v, lane, n, tw, ch, hf);
+    line_dft<false>(v, lane, n, tw, ch, hf, xb);
 #pragma unroll
     for (int j = 0; j < 16; ++j) {
       const int k = 32 * j + lane;
@@ -278,7 +423,7 @@ __global__ void __launch_bounds__(kFftWarps * 32) fft_cols_kernel(const FftArgs 
     const int i = 32 * j + lane;
     v[j] = i < n ? line[i] : make_double2(0.0, 0.0);
   }
-  line_dft<false>(v, lane, n, tw, ch, hf);
+  line_dft<false>(v, lane, n, tw, ch, hf, xb);
 #pragma unroll
   for (int j = 0; j < 16; ++j) {
     const int k = 32 * j + lane;
@@ -287,7 +432,7 @@ __global__ void __launch_bounds__(kFftWarps * 32) fft_cols_kernel(const FftArgs 
       if (FILTER) v[j] = zadd(v[j], stage[warp * kFftMaxN + k]);
     }
   }
-  line_dft<true>(v, lane, n, tw, ch, hi);
+  line_dft<true>(v, lane, n, tw, ch, hi, xb);
 #pragma unroll
   for (int j = 0; j < 16; ++j) {
     const int i = 32 * j + lane;
@@ -295,15 +440,18 @@ __global__ void __launch_bounds__(kFftWarps * 32) fft_cols_kernel(const FftArgs 
   }
 }
 
-// pass C: rows back along x from the transposed layout, scaled, + 2 S.
+// pass C: rows back along x from the transposed layout, scaled, + 2 S.  The
+// gather tile becomes the warps' exchange buffers once every warp has read
+// its row from it.
 template <bool ADD_SRC>
-__global__ void __launch_bounds__(kFftWarps * 32) fft_rows_inv_kernel(const FftArgs a) {
+__global__ void __launch_bounds__(kFftWarps * 32, 2) fft_rows_inv_kernel(const FftArgs a) {
   extern __shared__ __align__(16) double2 sm[];
   load_tables(sm, a, false, true);
   const double2* tw = sm;
   const double2* ch = sm + kFftM;
   const double2* hi = ch + kFftMaxN;
-  double2* tile = sm + kTabDoubles2 + kFftM;  // [kx][kFftPitch]
+  double2* xall = sm + kTabDoubles2 + kFftM;  // [kx][kFftPitch], then exchange buffers
+  double2* tile = xall;
   const int n = a.n, s = blockIdx.x / a.nband, band = blockIdx.x % a.nband;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int iy0 = band * kFftWarps, iy = iy0 + warp;
@@ -314,23 +462,29 @@ __global__ void __launch_bounds__(kFftWarps * 32) fft_rows_inv_kernel(const FftA
         r < rows ? a.T[((size_t)s * n + k) * a.ld + iy0 + r] : make_double2(0.0, 0.0);
   }
   __syncthreads();
-  if (warp >= rows) return;
   double2 v[16];
 #pragma unroll
   for (int j = 0; j < 16; ++j) {
     const int k = 32 * j + lane;
     v[j] = k < n ? tile[k * kFftPitch + warp] : make_double2(0.0, 0.0);
   }
-  line_dft<true>(v, lane, n, tw, ch, hi);
-  double2 sv[16];
-  if (ADD_SRC) load_src_row(sv, a, s, iy, lane);
+  __syncthreads();  // every row read: the tile becomes the exchange buffers
+  if (warp >= rows) return;
+  line_dft<true>(v, lane, n, tw, ch, hi, xall + warp * kXb);
+  // the source row of the compact tile (zero outside it), read as it is added
+  const int4 d = ADD_SRC ? a.desc[s] : make_int4(0, 0, 0, 0);
+  const bool in_rows = ADD_SRC && d.z > 0 && iy >= d.y && iy < d.y + d.w;
+  const double2* srow = a.src + (size_t)s * a.src_cap + (size_t)(iy - d.y) * d.z - d.x;
   double2* row = a.out + ((size_t)s * n + iy) * a.ld;
 #pragma unroll
   for (int j = 0; j < 16; ++j) {
     const int x = 32 * j + lane;
     if (x < n) {
       double2 o = make_double2(v[j].x * a.scale, v[j].y * a.scale);
-      if (ADD_SRC) o = make_double2(fma(2.0, sv[j].x, o.x), fma(2.0, sv[j].y, o.y));
+      if (in_rows && x >= d.x && x < d.x + d.z) {
+        const double2 sv = srow[x];
+        o = make_double2(fma(2.0, sv.x, o.x), fma(2.0, sv.y, o.y));
+      }
       row[x] = o;
     }
   }
@@ -372,7 +526,7 @@ namespace {
 using cld = std::complex<long double>;
 
 // FFT_512 of h by the definition, in long double, divided by 512 and stored
-// in the warp FFT's output order (lane * 16 + r <-> brev4(r) + 16 brev5(lane)).
+// in the warp FFT's output order (lane l, register r <-> k0 + 8 k1 + 64 k2).
 std::vector<double2> permuted_spectrum(const std::vector<cld>& h) {
   const long double pi = 3.141592653589793238462643383279502884L;
   std::vector<cld> H(kFftM);
@@ -385,15 +539,11 @@ std::vector<double2> permuted_spectrum(const std::vector<cld>& h) {
     }
     H[k] = acc / (long double)kFftM;
   }
-  auto brev5 = [](int l) {
-    int r = 0;
-    for (int b = 0; b < 5; ++b) r |= ((l >> b) & 1) << (4 - b);
-    return r;
-  };
   std::vector<double2> out(kFftM);
   for (int l = 0; l < 32; ++l)
     for (int r = 0; r < 16; ++r) {
-      const cld v = H[brev4(r) + 16 * brev5(l)];
+      const int q = l + 32 * (r & 1);
+      const cld v = H[(q >> 3) + 8 * (q & 7) + 64 * brev3(r >> 1)];
       out[l * 16 + r] = make_double2((double)v.real(), (double)v.imag());
     }
   return out;
@@ -582,11 +732,15 @@ int g4b_fft_advance(g4b_fft* s, g4b_field* f, g4b_beam* b, const g4b_step* st, d
   a.scale = 1.0 / ((double)n * (double)n);
   const unsigned grid = (unsigned)(f->nslice * a.nband);
   const size_t tab = (size_t)kTabDoubles2 * sizeof(double2);
-  const size_t tile = (size_t)kFftMaxN * kFftPitch * sizeof(double2);
-  const size_t smem_a = tab + kFftM * sizeof(double2) + (filt ? 2 : 1) * tile;
+  // exchange buffers of the warps, which in passes A and C also hold the
+  // transposition tile (kFftMaxN x kFftPitch entries)
+  const size_t xbuf = std::max((size_t)kFftWarps * kXb, (size_t)kFftMaxN * kFftPitch) *
+                      sizeof(double2);
+  const size_t smem_a = tab + kFftM * sizeof(double2) + xbuf;
   const size_t smem_b = tab + 2 * kFftM * sizeof(double2) +
+                        (size_t)kFftWarps * kXb * sizeof(double2) +
                         (filt ? (size_t)kFftWarps * kFftMaxN * sizeof(double2) : 0);
-  const size_t smem_c = tab + kFftM * sizeof(double2) + tile;
+  const size_t smem_c = tab + kFftM * sizeof(double2) + xbuf;
   {
     auto ka = filt ? fft_rows_fwd_kernel<true> : fft_rows_fwd_kernel<false>;
     if (int rc = set_smem((const void*)ka, smem_a)) return rc;
