@@ -2429,11 +2429,14 @@ int g4b_batch_tune(g4b_batch* b) {
 
 // The ADI row layouts, then the launch shapes as g4b_batch_tune.  For every
 // grid size among the attached runs' fields that has two row layouts (32
-// lanes of M elements, 16 lanes of M' elements), both passes are timed in
-// each layout on a scratch field of that grid (up to 128 slices of zeros,
+// lanes of M elements, 16 lanes of M' elements) and at least
+// kTuneRowsMinSlices slices in the batch, both passes are timed in each
+// layout on a scratch field of that grid (its slice count up to 128, zeros,
 // best of three launches after one untimed), before any step: the runs'
 // state never advances in a trial layout, so every step of the batch uses
 // the chosen layouts and equals an alone run given the same layouts.
+constexpr int kTuneRowsMinSlices = 32;
+
 int g4b_batch_tune_layouts(g4b_batch* b) {
   if (!b) return fail(G4B_ERR_ARG, "g4b_batch_tune_layouts: null batch");
   g4b_ctx* c = b->ctx;
@@ -2466,6 +2469,10 @@ int g4b_batch_tune_layouts(g4b_batch* b) {
     }
   }
   for (Group& g : groups) {
+    // a grid with few slices in the batch keeps its default: its passes are
+    // launch-bound, and a switch would add a row-layout group (two more
+    // launches per step) to the batch
+    if (g.nslice < kTuneRowsMinSlices) continue;
     g4b_field* f = nullptr;
     g4b_adi* adi = nullptr;
     int rc = g4b_field_create(c, std::min(g.nslice, 128), g.n, g.gridmax, g.xlambda, 1,

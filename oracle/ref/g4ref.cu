@@ -158,7 +158,10 @@ void load_beam(Beam& b, int nslice, const int* off, const double* x, const doubl
   b.current.resize(nslice, 0.0);
   b.longESC.assign(nslice, 0.0);
   b.eloss.assign(nslice, 0.0);
+  // host slices sized as the device layout (BeamSolverCUDA's short-range
+  // branch counts them, src/Core/BeamSolverCUDA.cpp:529-542); contents unused
   b.beam.resize(nslice);
+  for (int is = 0; is < nslice; ++is) b.beam[is].resize(off[is + 1] - off[is]);
 }
 
 void fetch(CudaDeviceBuffer<double>& d, double* h, size_t n) {

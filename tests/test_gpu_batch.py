@@ -145,15 +145,21 @@ def test_row_layout_tuner_keeps_batch_equal_to_alone(ctx):
     scratch field before the first step; every step then runs in the chosen
     layouts, so each run equals an alone run given the same layouts."""
     lib = ctx.lib
+    # a grid with 40 slices in the batch is timed in both layouts; the
+    # others (fewer than 32 slices of their grid) keep their defaults
+    cfgs = CONFIGS + [dict(nslice=40, npart=256, ngrid=101, taper=0.0, dgam=0.0,
+                           time_run=True, nsteps=6)]
     batch = dev.Batch(ctx, 8)
-    runs = [_make(ctx, k, cfg) for k, cfg in enumerate(CONFIGS)]
-    for r, cfg in zip(runs, CONFIGS):
+    runs = [_make(ctx, k, cfg) for k, cfg in enumerate(cfgs)]
+    for r, cfg in zip(runs, cfgs):
         batch.attach(r, 0, cfg["nsteps"])
     batch.tune_layouts()
-    longest = max(cfg["nsteps"] for cfg in CONFIGS)
+    longest = max(cfg["nsteps"] for cfg in cfgs)
     batch.step(longest + 2, graph=True)
     ctx.synchronize()
-    for k, (r, cfg) in enumerate(zip(runs, CONFIGS)):
+    for k, (r, cfg) in enumerate(zip(runs, cfgs)):
+        if cfg["nslice"] < 32:
+            assert r.layouts()[0] == lib.g4b_default_layout(cfg["ngrid"])
         lay = r.layouts()
         default = lib.g4b_default_layout(cfg["ngrid"])
         assert lay[0] == default or (lay[0] >= 100) != (default >= 100)
