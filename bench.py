@@ -244,7 +244,33 @@ def run_reference(args, wl, rank, budget_s=240.0):
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
+    line["reference_cuda"] = reference_cuda(wl, off, parts, cur, cells, lat, args)
     print(json.dumps(line), flush=True)
+
+
+def reference_cuda(wl, off, parts, cur, cells, lat, args):
+    """The reference's own CUDA classes (src/Core/*.cpp, compiled unmodified
+    into oracle/_ref) stepping the same workload on this GPU from device-
+    resident state, in Gencore::run's order: the reference's GPU speed beside
+    its CPU arm.  None where the library or a GPU is missing."""
+    from oracle import refpy
+    if not refpy.available():
+        return None
+    try:
+        if refpy.load().g4ref_device_count() < 1:
+            return None
+        n = lat.nstep
+        ms = refpy.time_steps(off, parts, cur, cells, gridmax=wl.gridmax, xlambda=wl.lambda0,
+                              steps=lat.steps, fc=[lat.fc(i, 1) for i in range(n)],
+                              slip=lat.slip, sample=wl.sample, warmup=args.warmup,
+                              ntimed=max(1, min(args.steps, 20)))
+    except Exception as e:  # the reference's classes throw on what they reject
+        return {"unavailable": str(e)[:200]}
+    return {"value": wl.nslice / (ms / 1e3), "unit": UNIT, "ms_per_step": ms,
+            "steps": max(1, min(args.steps, 20)), "warmup": args.warmup,
+            "what": "the reference's FieldSolverADICUDA, BeamSolverCUDA, ControlCUDA and "
+                    "DiagnosticCUDA (compiled unmodified) stepping the workload's state "
+                    "on this GPU, CUDA events around the timed steps, FP64"}
 
 
 # ------------------------------------------------------------- GPU arm ---

@@ -368,6 +368,88 @@ int g4ref_diag(int nslice, const int* off, const double* x, const double* y, con
   }
 }
 
+int g4ref_time_steps(int nslice, const int* off, const double* x, const double* y,
+                     const double* px, const double* py, const double* gamma,
+                     const double* theta, const double* current, int ngrid, double gridmax,
+                     double xlambda, const double* cells, int nstep, const g4b_step* steps,
+                     const double* fc, const double* slip, double sample, int first_step,
+                     int warmup, int ntimed, double* ms_per_step) {
+  try {
+    Beam beam;
+    load_beam(beam, nslice, off, x, y, px, py, gamma, theta, current);
+    beam.reflength = xlambda;
+    Field fld;
+    load_field(fld, nslice, ngrid, gridmax, xlambda, 1, 0, cells);
+    fld.slicelength = xlambda * sample;
+    std::vector<Field*> fields{&fld};
+    BeamSolverCUDA solver;
+    FieldSolverADICUDA adi(false);
+    ControlCUDA control;
+    control.init(0, 1, true, false, sample);
+    FilterDiagnostics filter;
+    DiagnosticCUDA diag;
+    diag.init(filter);
+    const int nout = warmup + ntimed;
+    g_diag = Diagnostic();
+    g_diag.zout.assign(nout, 0.0);
+    g_diag.val.resize(4);
+    static const char* kBeam[] = {
+        "energy", "energyspread", "xposition", "xsize", "yposition", "ysize",
+        "pxposition", "pyposition", "current", "emitx", "emity", "betax", "betay",
+        "alphax", "alphay", "efield", "wakefield", "LSCfield", "SSCfield", "xmin", "xmax",
+        "pxmin", "pxmax", "ymin", "ymax", "pymin", "pymax", "emin", "emax", "bunching",
+        "bunchingphase"};
+    static const char* kField[] = {"power", "xposition", "xsize", "yposition", "ysize",
+                                   "intensity-nearfield", "phase-nearfield",
+                                   "intensity-farfield", "phase-farfield"};
+    for (const char* k : kBeam) g_diag.val[2][k].assign((size_t)nout * nslice, 0.0);
+    for (const char* k : {"Global/energy", "Global/energyspread", "Global/xposition",
+                          "Global/xsize", "Global/yposition", "Global/ysize"})
+      g_diag.val[2][k].assign(nout, 0.0);
+    for (const char* k : kField) g_diag.val[3][k].assign((size_t)nout * nslice, 0.0);
+    for (const char* k : {"Global/energy", "Global/xposition", "Global/xsize",
+                          "Global/yposition", "Global/ysize", "Global/intensity-nearfield",
+                          "Global/intensity-farfield", "dgrid", "gridspacing", "ngrid"})
+      g_diag.val[3][k].assign(nout, 0.0);
+    cudaEvent_t t0, t1;
+    check(cudaEventCreate(&t0), "event");
+    check(cudaEventCreate(&t1), "event");
+    double z = 0.0;
+    for (int k = 0; k < nout; ++k) {
+      if (k == warmup) {
+        check(cudaDeviceSynchronize(), "synchronize");
+        check(cudaEventRecord(t0, 0), "event");
+      }
+      const int i = (first_step + k) % nstep;
+      const g4b_step& st = steps[i];
+      Undulator und;
+      load_step(und, &st, 1, fc[i]);
+      const double delz = st.delz;
+      // Gencore::run's step (src/Core/Gencore.cpp:172-254) with Beam::track's
+      // CUDA branch (src/Core/Beam.cpp:117-134) and Field::track
+      solver.track(delz * 0.5, &beam, &und, false);
+      solver.advance(delz, &beam, &fields, &und);
+      solver.applyR56(&beam, &und, xlambda);
+      solver.track(delz * 0.5, &beam, &und, true);
+      adi.init(delz, fld.dgrid, fld.xks, static_cast<unsigned>(ngrid));
+      adi.advance(delz, &fld, &beam, &und);
+      if (!control.applySlippage(slip[i], &fld)) throw std::runtime_error("applySlippage declined");
+      z += delz;
+      if (!diag.calc(&beam, &fields, z, g_diag)) throw std::runtime_error("calc declined");
+    }
+    check(cudaEventRecord(t1, 0), "event");
+    check(cudaEventSynchronize(t1), "synchronize");
+    float ms = 0.f;
+    check(cudaEventElapsedTime(&ms, t0, t1), "elapsed");
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    *ms_per_step = ntimed > 0 ? (double)ms / ntimed : 0.0;
+    return 0;
+  } catch (const std::exception& e) {
+    return fail(e);
+  }
+}
+
 int g4ref_diag_record(int group, const char* name, double* out, int cap) {
   const int idx = group == 0 ? 2 : 2 + group;
   if (idx >= static_cast<int>(g_diag.val.size())) return -1;

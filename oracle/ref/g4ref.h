@@ -97,6 +97,22 @@ int g4ref_diag(int nslice, const int* slice_offsets, const double* x,
  * record does not exist. */
 int g4ref_diag_record(int group, const char* name, double* out, int cap);
 
+/* Times ntimed steps (after warmup untimed ones) of the reference's own
+ * classes on one set of device-resident state, in Gencore::run's order
+ * (src/Core/Gencore.cpp:172-254): BeamSolverCUDA track / advance / applyR56 /
+ * track (Beam::track's CUDA branch, src/Core/Beam.cpp:117-134),
+ * FieldSolverADICUDA init + advance, ControlCUDA::applySlippage (time run,
+ * not periodic) and DiagnosticCUDA::calc, one field of harmonic 1.  Lattice
+ * step i of nstep gives the step parameters, fc[i] and slip[i]; steps run
+ * from first_step on (wrapping).  *ms_per_step: CUDA-event time per timed
+ * step, host work of the classes included. */
+int g4ref_time_steps(int nslice, const int* slice_offsets, const double* x, const double* y,
+                     const double* px, const double* py, const double* gamma,
+                     const double* theta, const double* current, int ngrid, double gridmax,
+                     double xlambda, const double* cells, int nstep, const g4b_step* steps,
+                     const double* fc, const double* slip, double sample, int first_step,
+                     int warmup, int ntimed, double* ms_per_step);
+
 #ifdef __cplusplus
 }
 #endif

@@ -59,6 +59,9 @@ def load():
                                         C.c_double, C.c_double, C.c_double]
     lib.g4ref_beam_advance.argtypes = [C.c_int, ip, sp, C.c_int, ip, ip, ip, dp, dp, dp, dpp,
                                        dp, dp, dp, dp, dp, dp, dp]
+    lib.g4ref_time_steps.argtypes = [C.c_int, ip, dp, dp, dp, dp, dp, dp, dp, C.c_int,
+                                     C.c_double, C.c_double, dp, C.c_int, sp, dp, dp,
+                                     C.c_double, C.c_int, C.c_int, C.c_int, dp]
     lib.g4ref_set_particle_ez.argtypes = [dp]
     lib.g4ref_set_particle_ez.restype = None
     lib.g4ref_track.argtypes = [C.c_int, sp, C.c_double, C.c_int, dp, dp, dp, dp, dp]
@@ -217,3 +220,25 @@ def diag(off, parts, *, nharm, current, fields, slicelength, eloss=None, long_es
     beam = {k: grab(0, k) for k in names}
     flds = [{k: grab(1 + i, k) for k in FIELD_RECORDS} for i in range(nf)]
     return beam, flds
+
+
+def time_steps(off, parts, current, cells, *, gridmax, xlambda, steps, fc, slip, sample,
+               first_step=0, warmup=3, ntimed=10):
+    """Milliseconds per step of the reference's own classes stepping one set of
+    device-resident state (g4ref_time_steps); parts/cells are not modified."""
+    from genesis4_cuda_port_b200._lib import Step
+    offa, offp = _i32(off)
+    n = len(steps)
+    arr = (Step * n)(*steps)
+    c = np.ascontiguousarray(cells, dtype=np.complex128)
+    fca = np.ascontiguousarray(fc, np.float64)
+    sla = np.ascontiguousarray(slip, np.float64)
+    cur = np.ascontiguousarray(current, np.float64)
+    ms = C.c_double(0.0)
+    _chk(load().g4ref_time_steps(len(offa) - 1, offp, _d(parts["x"]), _d(parts["y"]),
+                                 _d(parts["px"]), _d(parts["py"]), _d(parts["gamma"]),
+                                 _d(parts["theta"]), _d(cur), c.shape[1], gridmax, xlambda,
+                                 c.reshape(-1).view(np.float64).ctypes.data_as(dp), n, arr,
+                                 _d(fca), _d(sla), sample, first_step, warmup, ntimed,
+                                 C.byref(ms)))
+    return ms.value
