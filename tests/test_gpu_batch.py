@@ -174,7 +174,9 @@ def test_row_layout_tuner_keeps_batch_equal_to_alone(ctx):
 def test_both_row_layouts_solve_the_same_system(ctx):
     """The other row layout of a grid changes only the FP32 rounding of the
     row solve; a layout that is not one of the grid's two is refused."""
-    k, cfg = 3, CONFIGS[3]  # ngrid 101: 16 lanes x 7 by default, 32 lanes x 5 the other
+    # ngrid 101: 16 lanes x 7 by default, 32 lanes x 5 the other; steady
+    # state, so the field stays in the window
+    k, cfg = 3, dict(CONFIGS[3], time_run=False)
     a = _make(ctx, k, cfg)
     a.advance(0, cfg["nsteps"], graph=False)
     ra = _result(a, cfg["nsteps"])
@@ -185,8 +187,9 @@ def test_both_row_layouts_solve_the_same_system(ctx):
     assert b.layouts() == [other]
     b.advance(0, cfg["nsteps"], graph=False)
     rb = _result(b, cfg["nsteps"])
-    assert not np.array_equal(ra[1], rb[1])
     scale = np.max(np.abs(ra[1]))
+    assert scale > 0
+    assert not np.array_equal(ra[1], rb[1])
     assert np.max(np.abs(ra[1] - rb[1])) < 1e-4 * scale
     with pytest.raises(Exception):
         b.set_layouts([9])

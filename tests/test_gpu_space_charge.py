@@ -114,7 +114,10 @@ def test_push_with_a_per_particle_loss_three_ways(ctx):
     assert np.max(np.abs((plain["gamma"] - p["gamma"]) - dg)) > 1e-3 * np.max(np.abs(dg))
     for name, q in (("oracle", ora), ("cuda", got)):
         assert np.max(np.abs((q["gamma"] - p["gamma"]) - dg)) < 1e-12 * np.max(np.abs(dg)), name
-        np.testing.assert_allclose(q["theta"], ref["theta"], rtol=1e-13, atol=0, err_msg=name)
+        # an ulp of theta (~1e-16 at theta of a few radians): the oracle's
+        # compiler contracts some products into fused multiply-adds
+        np.testing.assert_allclose(q["theta"], ref["theta"], rtol=1e-13, atol=1e-15,
+                                   err_msg=name)
     # back to the slice loss
     beam.set_particle_ez(None)
     beam.set_eloss(None)
