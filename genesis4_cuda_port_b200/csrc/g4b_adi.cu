@@ -76,7 +76,9 @@ __device__ __forceinline__ C shfl_down_c(C v, int d) {
 
 
 // Warps per CTA and CTAs per SM (launch bounds) of the ADI kernels: FP64 9
-// warps of 32-lane rows; FP32 10 warps of 32-lane rows or 5 warps of two
+// warps of 32-lane rows, three CTAs per SM up to M = 7 (ngrid 224: pass X's
+// three tiles still fit the SM's shared memory; 416 -> 338 us per pass X of
+// 1024 x 201^2 against two); FP32 10 warps of 32-lane rows or 5 warps of two
 // 16-lane rows each (10 rows per band either way; smaller CTAs of 16-lane
 // rows keep six on an SM so that one CTA's loads and stores overlap the
 // others' solves).
@@ -85,7 +87,7 @@ template <typename T, int L> struct BandW {
 };
 template <typename T, int M, int L> struct AdiBlocks {
   static constexpr int value =
-      sizeof(T) == 8 ? (M <= 9 ? 2 : 2)
+      sizeof(T) == 8 ? (M <= 7 ? 3 : 2)
                      : (L == 16 ? (M <= 9 ? 8 : (M <= 17 ? 6 : 4)) : (M <= 9 ? 4 : 2));
 };
 

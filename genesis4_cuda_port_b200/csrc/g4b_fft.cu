@@ -302,6 +302,16 @@ __device__ __forceinline__ void line_dft(double2 (&v)[16], int lane, int n, cons
   }
 }
 
+// The circular convolution of Bluestein's algorithm: FFT, times the
+// precomputed FFT of the chirp (1/512 included), inverse FFT.
+__device__ __forceinline__ void bluestein_conv(double2 (&v)[16], int lane, const double2* tw,
+                                               const double2* H, double2* xb) {
+  fft512_fwd(v, lane, tw, xb);
+#pragma unroll
+  for (int r = 0; r < 16; ++r) v[r] = zmul(v[r], H[lane * 16 + r]);
+  fft512_inv(v, lane, tw, xb);
+}
+
 // Shared tables of a CTA: tw[512] | chirp[256] | H (one or two of 512).
 __device__ __forceinline__ void load_tables(double2* sm, const FftArgs& a, bool hf, bool hi) {
   double2* tw = sm;
@@ -399,6 +409,10 @@ __global__ void __launch_bounds__(kFftWarps * 32, FILTER ? 1 : 2) fft_cols_kerne
   if (kx >= n) return;
   double2* line = a.T + ((size_t)s * n + kx) * a.ld;
   const double2* prop = a.prop_t + (size_t)kx * n;
+  // The forward transform's closing chirp w_k and the inverse's opening
+  // conj(w_k) meet at the propagator and cancel (|w_k| = 1): between the two
+  // convolutions the line is multiplied by exp(i k2 dz) alone (and the
+  // filtered source spectrum enters without its closing chirp).
   double2 v[16];
   if (FILTER) {
     const double2* sline = a.ST + ((size_t)s * n + kx) * a.ld;
@@ -406,9 +420,9 @@ __global__ void __launch_bounds__(kFftWarps * 32, FILTER ? 1 : 2) fft_cols_kerne
 #pragma unroll
     for (int j = 0; j < 16; ++j) {
       const int i = 32 * j + lane;
-      v[j] = i < n ? sline[i] : make_double2(0.0, 0.0);
+      v[j] = i < n ? zmul(sline[i], ch[i]) : make_double2(0.0, 0.0);
     }
-    line_dft<false>(v, lane, n, tw, ch, hf, xb);
+    bluestein_conv(v, lane, tw, hf, xb);
 #pragma unroll
     for (int j = 0; j < 16; ++j) {
       const int k = 32 * j + lane;
@@ -421,22 +435,24 @@ __global__ void __launch_bounds__(kFftWarps * 32, FILTER ? 1 : 2) fft_cols_kerne
 #pragma unroll
   for (int j = 0; j < 16; ++j) {
     const int i = 32 * j + lane;
-    v[j] = i < n ? line[i] : make_double2(0.0, 0.0);
+    v[j] = i < n ? zmul(line[i], ch[i]) : make_double2(0.0, 0.0);
   }
-  line_dft<false>(v, lane, n, tw, ch, hf, xb);
+  bluestein_conv(v, lane, tw, hf, xb);
 #pragma unroll
   for (int j = 0; j < 16; ++j) {
     const int k = 32 * j + lane;
     if (k < n) {
       v[j] = zmul(v[j], prop[k]);
       if (FILTER) v[j] = zadd(v[j], stage[warp * kFftMaxN + k]);
+    } else {
+      v[j] = make_double2(0.0, 0.0);
     }
   }
-  line_dft<true>(v, lane, n, tw, ch, hi, xb);
+  bluestein_conv(v, lane, tw, hi, xb);
 #pragma unroll
   for (int j = 0; j < 16; ++j) {
     const int i = 32 * j + lane;
-    if (i < n) line[i] = v[j];
+    if (i < n) line[i] = zmulc(v[j], ch[i]);
   }
 }
 

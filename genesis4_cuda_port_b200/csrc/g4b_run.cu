@@ -974,7 +974,9 @@ __global__ void __launch_bounds__(T, 512 / T)
     deposit_diag_kernel(const __grid_constant__ DepDiagLaunch a) {
   extern __shared__ __align__(128) unsigned char smem[];
   const int bs = blockIdx.x / kDepSplit, part = blockIdx.x % kDepSplit;
-  if (part == 0) {
+  // the last part takes the diagnostics: a tile of one band leaves it no
+  // deposition, so the slice's diagnostics and deposition run side by side
+  if (part == kDepSplit - 1) {
     diag_slice<NB>(a.b, bs, 0);
     __syncthreads();
   }
@@ -1436,7 +1438,7 @@ int launch_single(g4b_run* r, const StepArgs& L) {
   // fill the GPU twice launches them as a kernel of their own: in a captured
   // graph a branch beside the deposition and the ADI passes (on SMs those
   // leave idle), joined before the finalize.  A smaller run computes them in
-  // the deposition's CTAs, before each slice's deposition.
+  // the deposition's CTAs: the slice's last deposition part, before its band.
   auto diag = [&](cudaStream_t st) {
     LaunchScope ls(c, "run_beam_diag");
     if (r->desc.nbunch == 1)
