@@ -175,20 +175,30 @@ __global__ void __launch_bounds__(kDiagThreads)
   const double shift = -0.5 * (double)(n - 1);
   double v[7] = {0, 0, 0, 0, 0, 0, 0};
   const int plane = n * n;
-  for (int ixy = tid; ixy < plane; ixy += kDiagThreads) {
-    const int iy = ixy / n;
-    const int ix = ixy - iy * n;
-    const C u = c[(size_t)iy * ld + ix];
-    const double re = u.x, im = u.y;
-    const double wei = re * re + im * im;
-    const double dx = (double)ix + shift, dy = (double)iy + shift;
-    v[0] += wei;
-    v[1] += dx * wei;
-    v[2] += dx * dx * wei;
-    v[3] += dy * wei;
-    v[4] += dy * dy * wei;
-    v[5] += re;
-    v[6] += im;
+  // a warp per row: coalesced row reads with no index division, the row's
+  // sums first, then its y moments from the row's power
+  for (int iy = w; iy < n; iy += kDiagWarps) {
+    const C* row = c + (size_t)iy * ld;
+    double p = 0, px = 0, pxx = 0, sre = 0, sim = 0;
+    for (int ix = l; ix < n; ix += 32) {
+      const C u = row[ix];
+      const double re = u.x, im = u.y;
+      const double wei = re * re + im * im;
+      const double dx = (double)ix + shift;
+      p += wei;
+      px += dx * wei;
+      pxx += dx * dx * wei;
+      sre += re;
+      sim += im;
+    }
+    const double dy = (double)iy + shift;
+    v[0] += p;
+    v[1] += px;
+    v[2] += pxx;
+    v[3] += dy * p;
+    v[4] += dy * dy * p;
+    v[5] += sre;
+    v[6] += sim;
   }
 #pragma unroll
   for (int k = 0; k < 7; ++k) {
