@@ -795,85 +795,96 @@ __device__ __forceinline__ void deposit_slice(const DepArgs& a, const int bs, co
       const int nout = hb * bw, nbase = (hb + 1) * bw;
       // with `count` the counts per base cell (ext row iy - ylo + 1) and the
       // largest charge weight (qloc), with `add` the contributions at scale
-      // Sf of charge weights capped at qc; a quad of lanes holding one
-      // quiet-start beamlet in one cell adds its count with one atomic
+      // Sf of charge weights capped at qc.  A thread takes groups of four
+      // consecutive particles: a quiet-start beamlet (nbins = 4 particles at
+      // one transverse position) when the four share a base cell, whose
+      // rounded contributions it sums in registers and adds, with its count,
+      // by one set of atomics instead of four (the same integer sums).
       float qloc = 0.f;
+      auto add8 = [&](int cid, const int* v) {
+        if (cid >= bw) {  // lower corners: output row ey = cid / bw - 1
+          const int o = cid - bw;
+          atomicAdd(&are[o], v[0]);
+          atomicAdd(&aim[o], v[1]);
+          atomicAdd(&are[o + 1], v[2]);
+          atomicAdd(&aim[o + 1], v[3]);
+        }
+        if (cid < nout) {  // upper corners: row ey + 1 inside the band
+          atomicAdd(&are[cid], v[4]);
+          atomicAdd(&aim[cid], v[5]);
+          atomicAdd(&are[cid + 1], v[6]);
+          atomicAdd(&aim[cid + 1], v[7]);
+        }
+      };
       auto pass = [&](const bool count, const bool add, const float Sf, const float qc) {
-        for (int pb = tid & ~31; pb < np; pb += U * T) {
-          float2 lxy[U];
-          float ldg[U];
-          double lth[U];
+        for (int g = tid; 4 * g < np; g += T) {
+          const int pg = 4 * g;
+          float2 lxy[4];
+          float ldg[4];
+          double lth[4];
 #pragma unroll
-          for (int u = 0; u < U; ++u) {
-            const int p = pb + u * T + l;
-            if (p < np) {
-              lxy[u] = xyp[p];
-              ldg[u] = dgp[p];
-              if (add) lth[u] = thp[p];
+          for (int u = 0; u < 4; ++u) {
+            if (pg + u < np) {
+              lxy[u] = xyp[pg + u];
+              ldg[u] = dgp[pg + u];
+              if (add) lth[u] = thp[pg + u];
             }
           }
+          int cid[4];
 #pragma unroll
-          for (int u = 0; u < U; ++u) {
-            const int p = pb + u * T + l;
-            int cidx = -1, ey = 0, ex = 0;
-            int c[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-            if (p < np) {
-              int ix, iy;
-              float wx, wy;
-              if (cell_f(mf, lxy[u].x, lxy[u].y, ix, iy, wx, wy) && iy + 1 >= ylo &&
-                  iy < ylo + hb) {
-                ex = ix - bx0;
-                ey = iy - ylo;  // output row of the lower corners
-                if (ex < 0 || ex > bw - 2) {
-                  if (count) atomicOr(a.err, kErrBadSlice);
-                } else {
-                  cidx = (ey + 1) * bw + ex;
-                  const float qraw = dep_charge(a, lxy[u], ldg[u]);
-                  if (count) qloc = fmaxf(qloc, qraw);
-                  if (add) {
-                    const float q = fminf(qraw, qc) * Sf;
-                    float sn, cs;
-                    __sincosf(reduce_angle((double)fh * lth[u]), &sn, &cs);
-                    const float vre = sn * q, vim = cs * q;
-                    const float w00 = wx * wy, w10 = (1.f - wx) * wy, w01 = wx * (1.f - wy),
-                                w11 = (1.f - wx) * (1.f - wy);
-                    c[0] = __float2int_rn(vre * w00);
-                    c[1] = __float2int_rn(vim * w00);
-                    c[2] = __float2int_rn(vre * w10);
-                    c[3] = __float2int_rn(vim * w10);
-                    c[4] = __float2int_rn(vre * w01);
-                    c[5] = __float2int_rn(vim * w01);
-                    c[6] = __float2int_rn(vre * w11);
-                    c[7] = __float2int_rn(vim * w11);
-                  }
-                }
-              }
-            }
-            const int c1 = __shfl_xor_sync(0xffffffffu, cidx, 1);
-            const int c2 = __shfl_xor_sync(0xffffffffu, cidx, 2);
-            const int c3 = __shfl_xor_sync(0xffffffffu, cidx, 3);
-            const bool quad = cidx >= 0 && c1 == cidx && c2 == cidx && c3 == cidx;
-            if (cidx >= 0 && (!quad || (l & 3) == 0))
-              if (count) atomicAdd(&hist[cidx], quad ? 4 : 1);
-            if (cidx >= 0) {
-              if (add) {
-                if (ey >= 0) {
-                  const int o = ey * bw + ex;
-                  atomicAdd(&are[o], c[0]);
-                  atomicAdd(&aim[o], c[1]);
-                  atomicAdd(&are[o + 1], c[2]);
-                  atomicAdd(&aim[o + 1], c[3]);
-                }
-                if (ey + 1 < hb) {
-                  const int o = (ey + 1) * bw + ex;
-                  atomicAdd(&are[o], c[4]);
-                  atomicAdd(&aim[o], c[5]);
-                  atomicAdd(&are[o + 1], c[6]);
-                  atomicAdd(&aim[o + 1], c[7]);
-                }
+          for (int u = 0; u < 4; ++u) {
+            cid[u] = -1;
+            int ix, iy;
+            float wx, wy;
+            if (pg + u < np && cell_f(mf, lxy[u].x, lxy[u].y, ix, iy, wx, wy) &&
+                iy + 1 >= ylo && iy < ylo + hb) {
+              const int ex = ix - bx0;
+              if (ex < 0 || ex > bw - 2) {
+                if (count) atomicOr(a.err, kErrBadSlice);
+              } else {
+                cid[u] = (iy - ylo + 1) * bw + ex;
               }
             }
           }
+          const bool same = cid[0] >= 0 && cid[1] == cid[0] && cid[2] == cid[0] &&
+                            cid[3] == cid[0];
+          if (count) {
+            if (same) {
+              atomicAdd(&hist[cid[0]], 4);
+            } else {
+#pragma unroll
+              for (int u = 0; u < 4; ++u)
+                if (cid[u] >= 0) atomicAdd(&hist[cid[u]], 1);
+            }
+          }
+          int sum[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            if (cid[u] < 0) continue;
+            const float qraw = dep_charge(a, lxy[u], ldg[u]);
+            if (count) qloc = fmaxf(qloc, qraw);
+            if (!add) continue;
+            const float q = fminf(qraw, qc) * Sf;
+            float sn, cs;
+            __sincosf(reduce_angle((double)fh * lth[u]), &sn, &cs);
+            const float vre = sn * q, vim = cs * q;
+            int ix, iy;
+            float x0, y0;
+            cell_f(mf, lxy[u].x, lxy[u].y, ix, iy, x0, y0);  // the weights again
+            const float w00 = x0 * y0, w10 = (1.f - x0) * y0, w01 = x0 * (1.f - y0),
+                        w11 = (1.f - x0) * (1.f - y0);
+            const int c[8] = {__float2int_rn(vre * w00), __float2int_rn(vim * w00),
+                              __float2int_rn(vre * w10), __float2int_rn(vim * w10),
+                              __float2int_rn(vre * w01), __float2int_rn(vim * w01),
+                              __float2int_rn(vre * w11), __float2int_rn(vim * w11)};
+            if (same) {
+#pragma unroll
+              for (int k = 0; k < 8; ++k) sum[k] += c[k];
+            } else {
+              add8(cid[u], c);
+            }
+          }
+          if (add && same) add8(cid[0], sum);
         }
       };
       auto zero_acc = [&]() {
