@@ -75,6 +75,130 @@ __device__ __forceinline__ C shfl_down_c(C v, int d) {
 }
 
 
+// ------------------------------------------------------ row arithmetic ---
+// Forced inline into the single-run and the batched pass kernels: the same
+// operations in the same order, hence the same bits, in every kernel.
+// Tables of a row layout (L lanes of M elements), lane-minor:
+//   cbet [M][L], G prefix products [M][L], H suffix products [M][L],
+//   forward scan multipliers [5][L], backward scan multipliers [5][L],
+//   S: s_k = i r cbet_k (0 at the last row) [M][L].
+template <int M, int L, typename C> struct RowTabs {
+  const C *cb, *G, *H, *F, *B, *S;
+  __device__ __forceinline__ explicit RowTabs(const C* tab)
+      : cb(tab), G(tab + M * L), H(tab + 2 * M * L), F(tab + 3 * M * L),
+        B(tab + 3 * M * L + 5 * L), S(tab + 3 * M * L + 10 * L) {}
+};
+
+// Pass X right-hand side of the band row at tile slot row + 1 (neighbours at
+// slots row and row + 2): R = u + i r d2y(u) + S
+// (src/Core/FieldSolverADICUDA.cpp:197-220); elements j >= jn are zero.
+template <typename T, int M, typename C>
+__device__ __forceinline__ void px_rhs(C (&v)[M], const C* tile, int ld, int row, int gl, int jn,
+                                       T r, unsigned long long smask, const C* srow) {
+#pragma unroll
+  for (int j = 0; j < M; ++j) {
+    const int k = gl * M + j;
+    C R = C{0, 0};
+    if (j < jn) {
+      const C u = tile[(row + 1) * ld + k];
+      const C up = tile[(row + 2) * ld + k];
+      const C dn = tile[row * ld + k];
+      const T lr = fma((T)-2, u.x, up.x + dn.x);
+      const T li = fma((T)-2, u.y, up.y + dn.y);
+      R.x = fma(-r, li, u.x);
+      R.y = fma(r, lr, u.y);
+      if ((smask >> j) & 1ull) R = cadd(R, srow[k]);
+    }
+    v[j] = R;
+  }
+}
+
+// Local part of the forward recurrence y_k = cbet_k (R_k + i r y_{k-1}) over
+// lane gl's elements, with a zero carry in.
+template <typename T, int M, int L, typename C>
+__device__ __forceinline__ void fwd_local(C (&v)[M], const RowTabs<M, L, C>& tb, int gl, T r) {
+  v[0] = cmul(__ldg(&tb.cb[gl]), v[0]);
+#pragma unroll
+  for (int j = 1; j < M; ++j) {
+    const C cb = __ldg(&tb.cb[j * L + gl]);
+    C t;
+    t.x = fma(-r, v[j - 1].y, v[j].x);
+    t.y = fma(r, v[j - 1].x, v[j].y);
+    v[j] = cmul(cb, t);
+  }
+}
+
+// Local part of the backward recurrence u_k = y_k + s_k u_{k+1}.
+template <int M, int L, typename C>
+__device__ __forceinline__ void bwd_local(C (&v)[M], const RowTabs<M, L, C>& tb, int gl) {
+#pragma unroll
+  for (int j = M - 2; j >= 0; --j) v[j] = cfma(__ldg(&tb.S[j * L + gl]), v[j + 1], v[j]);
+}
+
+// v_j += P_j carry (P: the prefix or suffix products of lane gl).
+template <int M, int L, typename C>
+__device__ __forceinline__ void add_carry(C (&v)[M], const C* P, int gl, C carry) {
+#pragma unroll
+  for (int j = 0; j < M; ++j) v[j] = cfma(__ldg(&P[j * L + gl]), carry, v[j]);
+}
+
+// The tridiagonal solve (1 - i r d2) u = R of one row held by a group of L
+// lanes, M consecutive elements each (lane gl: elements gl*M .. gl*M+M-1):
+// local recurrences, the lane carries combined by a Kogge-Stone scan of
+// affine maps, each lane's carry times the products of its coefficients.
+template <typename T, int M, int L, typename C>
+__device__ __forceinline__ void row_solve(C (&v)[M], const C* tab, int gl, T r) {
+  constexpr int kScan = L == 32 ? 5 : 4;  // log2 L
+  const RowTabs<M, L, C> tb(tab);
+  fwd_local<T, M, L>(v, tb, gl, r);
+  C b = v[M - 1];
+#pragma unroll
+  for (int t = 0; t < kScan; ++t) {
+    const int d = 1 << t;
+    const C o = shfl_up_c<L>(b, d);
+    if (gl >= d) b = cfma(__ldg(&tb.F[t * L + gl]), o, b);
+  }
+  C yin = shfl_up_c<L>(b, 1);
+  if (gl == 0) yin = C{0, 0};
+  add_carry<M, L>(v, tb.G, gl, yin);
+  bwd_local<M, L>(v, tb, gl);
+  b = v[0];
+#pragma unroll
+  for (int t = 0; t < kScan; ++t) {
+    const int d = 1 << t;
+    const C o = shfl_down_c<L>(b, d);
+    if (gl + d < L) b = cfma(__ldg(&tb.B[t * L + gl]), o, b);
+  }
+  C uin = shfl_down_c<L>(b, 1);
+  if (gl == L - 1) uin = C{0, 0};
+  add_carry<M, L>(v, tb.H, gl, uin);
+}
+
+// R' = u' + i r d2x(u') + S (src/Core/FieldSolverADICUDA.cpp:279-323) of a
+// solved row, in place with the original left neighbour carried along.
+template <typename T, int M, int L, typename C>
+__device__ __forceinline__ void px_rprime(C (&v)[M], int gl, T r, unsigned long long smask,
+                                          const C* srow) {
+  C prev = shfl_up_c<L>(v[M - 1], 1);
+  if (gl == 0) prev = C{0, 0};
+  C right = shfl_down_c<L>(v[0], 1);
+  if (gl == L - 1) right = C{0, 0};
+#pragma unroll
+  for (int j = 0; j < M; ++j) {
+    const int k = gl * M + j;
+    const C cur = v[j];
+    const C upp = j < M - 1 ? v[j + 1] : right;
+    const T lr = fma((T)-2, cur.x, upp.x + prev.x);
+    const T li = fma((T)-2, cur.y, upp.y + prev.y);
+    C R;
+    R.x = fma(-r, li, cur.x);
+    R.y = fma(r, lr, cur.y);
+    if ((smask >> j) & 1ull) R = cadd(R, srow[k]);
+    v[j] = R;
+    prev = cur;
+  }
+}
+
 // Warps per CTA and CTAs per SM (launch bounds) of the ADI kernels: FP64 9
 // warps of 32-lane rows, three CTAs per SM up to M = 7 (ngrid 224: pass X's
 // three tiles still fit the SM's shared memory; 416 -> 338 us per pass X of
@@ -105,7 +229,6 @@ __device__ __forceinline__ bool adi_band(const AdiPassArgs& a, const CUtensorMap
   using C = typename CT<T>::type;
   constexpr int R = 32 / L;                     // rows per warp
   constexpr int W = BandW<T, L>::value * R;     // rows per band
-  constexpr int kScan = L == 32 ? 5 : 4;        // log2 L
   const int n = a.n, ld = a.ld;
   const int r0 = band * W;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -123,8 +246,11 @@ __device__ __forceinline__ bool adi_band(const AdiPassArgs& a, const CUtensorMap
   const int hi = PX ? min(r0 + W, n - 1) : min(r0 + W - 1, n - 1);
   const int slot0 = PX ? lo - (r0 - 1) : 0;
   // the source is non-zero only on the slice's tile: rows [sy0, sy0+sbh),
-  // columns [sx0, sx0+sbw); stile holds the tile rows of this band
-  const int4 sd = has_src ? __ldg(&a.desc[s]) : make_int4(0, 0, 0, 0);
+  // columns [sx0, sx0+sbw); stile holds the tile rows of this band.  The
+  // descriptor is written by the deposition, which may still be draining
+  // when this kernel starts (launch_pdl): a plain load, which stays after
+  // ptx::pdl_wait, not a read-only-path load the compiler may issue earlier
+  const int4 sd = has_src ? a.desc[s] : make_int4(0, 0, 0, 0);
   const int sx0 = sd.x, sbw = sd.z;
   const int srow_lo = max(r0, sd.y);
   const int srow_hi = min(min(r0 + W, n), sd.y + sd.w);
@@ -153,15 +279,7 @@ __device__ __forceinline__ bool adi_band(const AdiPassArgs& a, const CUtensorMap
   }
   const bool arrived = ptx::mbar_wait_bounded(bar, parity, a.err);
   if (!__syncthreads_and(arrived)) return false;
-
   const T r = (T)a.r;
-  const C* tab = reinterpret_cast<const C*>(a.tab);
-  const C* tcb = tab;                // cbet        [M][L]
-  const C* tG = tab + M * L;         // prefix prod [M][L]
-  const C* tH = tab + 2 * M * L;     // suffix prod [M][L]
-  const C* tF = tab + 3 * M * L;     // fwd scan    [5][L]
-  const C* tB = tF + 5 * L;          // bwd scan    [5][L]
-  const C* tS = tB + 5 * L;          // s_k = i r cbet_k (0 at the last row) [M][L]
   const int iy = r0 + row;
   const bool active = iy < n;
   const bool row_src = band_src && iy >= srow_lo && iy < srow_hi;
@@ -179,87 +297,14 @@ __device__ __forceinline__ bool adi_band(const AdiPassArgs& a, const CUtensorMap
   // a warp with any row in the plane solves both (a row past the plane is
   // all zeros), so that every lane takes part in the group shuffles
   if (__any_sync(0xffffffffu, active)) {
-#pragma unroll
-    for (int j = 0; j < M; ++j) {
-      const int k = gl * M + j;
-      C R = C{0, 0};
-      if (j < jn) {
-        if (PX) {
-          const C u = tile[(row + 1) * ld + k];
-          const C up = tile[(row + 2) * ld + k];
-          const C dn = tile[row * ld + k];
-          const T lr = fma((T)-2, u.x, up.x + dn.x);
-          const T li = fma((T)-2, u.y, up.y + dn.y);
-          R.x = fma(-r, li, u.x);
-          R.y = fma(r, lr, u.y);
-          if ((smask >> j) & 1ull) R = cadd(R, srow[k]);
-        } else {
-          R = tile[row * ld + k];
-        }
-      }
-      v[j] = R;
-    }
-    // forward recurrence, local part: y_k = cbet_k (R_k + i r y_{k-1})
-    {
-      v[0] = cmul(__ldg(&tcb[gl]), v[0]);
-#pragma unroll
-      for (int j = 1; j < M; ++j) {
-        const C cb = __ldg(&tcb[j * L + gl]);
-        C t;
-        t.x = fma(-r, v[j - 1].y, v[j].x);
-        t.y = fma(r, v[j - 1].x, v[j].y);
-        v[j] = cmul(cb, t);
-      }
-    }
-    // forward carry scan across the row's lanes
-    C b = v[M - 1];
-#pragma unroll
-    for (int t = 0; t < kScan; ++t) {
-      const int d = 1 << t;
-      const C o = shfl_up_c<L>(b, d);
-      if (gl >= d) b = cfma(__ldg(&tF[t * L + gl]), o, b);
-    }
-    C yin = shfl_up_c<L>(b, 1);
-    if (gl == 0) yin = C{0, 0};
-#pragma unroll
-    for (int j = 0; j < M; ++j) v[j] = cfma(__ldg(&tG[j * L + gl]), yin, v[j]);
-    // backward recurrence, local part: u_k = y_k + s_k u_{k+1}
-#pragma unroll
-    for (int j = M - 2; j >= 0; --j) v[j] = cfma(__ldg(&tS[j * L + gl]), v[j + 1], v[j]);
-    b = v[0];
-#pragma unroll
-    for (int t = 0; t < kScan; ++t) {
-      const int d = 1 << t;
-      const C o = shfl_down_c<L>(b, d);
-      if (gl + d < L) b = cfma(__ldg(&tB[t * L + gl]), o, b);
-    }
-    C uin = shfl_down_c<L>(b, 1);
-    if (gl == L - 1) uin = C{0, 0};
-#pragma unroll
-    for (int j = 0; j < M; ++j) v[j] = cfma(__ldg(&tH[j * L + gl]), uin, v[j]);
-
     if (PX) {
-      // R' = u' + i r d2x(u') + S  (src/Core/FieldSolverADICUDA.cpp:279-323),
-      // in place with the original left neighbour carried along
-      C prev = shfl_up_c<L>(v[M - 1], 1);
-      if (gl == 0) prev = C{0, 0};
-      C right = shfl_down_c<L>(v[0], 1);
-      if (gl == L - 1) right = C{0, 0};
+      px_rhs<T, M>(v, tile, ld, row, gl, jn, r, smask, srow);
+    } else {
 #pragma unroll
-      for (int j = 0; j < M; ++j) {
-        const int k = gl * M + j;
-        const C cur = v[j];
-        const C upp = j < M - 1 ? v[j + 1] : right;
-        const T lr = fma((T)-2, cur.x, upp.x + prev.x);
-        const T li = fma((T)-2, cur.y, upp.y + prev.y);
-        C R;
-        R.x = fma(-r, li, cur.x);
-        R.y = fma(r, lr, cur.y);
-        if ((smask >> j) & 1ull) R = cadd(R, srow[k]);
-        v[j] = R;
-        prev = cur;
-      }
+      for (int j = 0; j < M; ++j) v[j] = j < jn ? tile[row * ld + gl * M + j] : C{0, 0};
     }
+    row_solve<T, M, L>(v, reinterpret_cast<const C*>(a.tab), gl, r);
+    if (PX) px_rprime<T, M, L>(v, gl, r, smask, srow);
   } else {
 #pragma unroll
     for (int j = 0; j < M; ++j) v[j] = C{0, 0};
@@ -374,6 +419,7 @@ __global__ void __launch_bounds__(BandW<T, L>::value * 32, AdiBlocks<T, M, L>::v
     ptx::fence_mbar_init();
   }
   __syncthreads();
+  ptx::pdl_wait();
   adi_band<T, M, PX, L>(a, &tm_out, blockIdx.x / a.nband, blockIdx.x % a.nband, smem, &bar, 0u);
 }
 
@@ -657,7 +703,7 @@ static int launch_pass_t(g4b_field* f, const AdiPassArgs& args, const CUtensorMa
   const unsigned grid = (unsigned)(f->nslice * args.nband);
   {
     LaunchScope ls(f->ctx, PX ? "adi_pass_x" : "adi_pass_y");
-    kern<<<grid, W * 32, smem, f->ctx->stream>>>(args, tm);
+    G4B_CUDA_TRY(launch_pdl(kern, grid, W * 32, smem, f->ctx->stream, args, tm));
   }
   return check_launch(f->ctx, "adi_pass_kernel");
 }

@@ -168,6 +168,30 @@ int fp64_deposit(g4b_field* f, g4b_beam* b, const g4b_step* st, double fc);
 void dev_free(g4b_ctx* ctx, void* p);
 
 int check_launch(g4b_ctx* ctx, const char* what);
+
+// Launches kern with programmatic stream serialization: it may start while
+// the preceding kernel of its stream drains (in a captured graph, a
+// programmatic edge), and waits for that kernel's completion and writes in
+// ptx::pdl_wait before its first access to global memory (a load whose
+// address needs no earlier load, read through the read-only path, could be
+// issued before the wait: such data is read with plain loads).
+#if defined(__CUDACC__)
+template <typename... P, typename... A>
+inline cudaError_t launch_pdl(void (*kern)(P...), unsigned grid, unsigned block, size_t smem,
+                              cudaStream_t st, A&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kern, static_cast<A&&>(args)...);
+}
+#endif
 int read_device_error(g4b_ctx* ctx, const char* what);
 
 struct AdiPassArgs {
@@ -357,6 +381,13 @@ __device__ __forceinline__ void tma_store_3d(const CUtensorMap* map,
 __device__ __forceinline__ void fence_tensormap_acquire(const void* map) {
   asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(map) : "memory");
 }
+
+// Programmatic dependent launch (launch_pdl): block until the preceding
+// kernel of the stream has completed and its writes are visible (returns at
+// once in a kernel launched without the attribute).  No kernel triggers its
+// dependents early: they launch as its last CTAs exit, which hides the
+// launch latency and the ramp-up, not the tail.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
 __device__ __forceinline__ void bulk_commit() {
   asm volatile("cp.async.bulk.commit_group;" ::: "memory");

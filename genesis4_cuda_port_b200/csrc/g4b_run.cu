@@ -454,6 +454,7 @@ __device__ __forceinline__ void beam_chunk(const BeamStepArgs& a, const int4 ch)
 
 template <int NF>
 __global__ void __launch_bounds__(kStepThreads, kStepBlocks) beam_step_kernel(const __grid_constant__ BeamStepArgs a) {
+  ptx::pdl_wait();
   beam_chunk<NF>(a, a.chunks[blockIdx.x]);
 }
 
@@ -966,6 +967,7 @@ __device__ __forceinline__ void deposit_slice(const DepArgs& a, const int bs, co
 
 __global__ void __launch_bounds__(kDepThreads, 2) deposit_kernel(const __grid_constant__ DepArgs a) {
   extern __shared__ __align__(128) unsigned char smem[];
+  ptx::pdl_wait();
   deposit_slice(a, blockIdx.x / kDepSplit, blockIdx.x % kDepSplit, smem);
 }
 
@@ -984,6 +986,7 @@ template <int NB, int T>
 __global__ void __launch_bounds__(T, 512 / T)
     deposit_diag_kernel(const __grid_constant__ DepDiagLaunch a) {
   extern __shared__ __align__(128) unsigned char smem[];
+  ptx::pdl_wait();
   const int bs = blockIdx.x / kDepSplit, part = blockIdx.x % kDepSplit;
   // the last part takes the diagnostics: a tile of one band leaves it no
   // deposition, so the slice's diagnostics and deposition run side by side
@@ -1090,6 +1093,7 @@ __device__ __forceinline__ void finalize_range(const FinalizeArgs& a, int i0, in
 }
 
 __global__ void diag_finalize_kernel(const __grid_constant__ FinalizeArgs a) {
+  ptx::pdl_wait();
   finalize_range(a, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
 }
 
@@ -1435,14 +1439,13 @@ int build_step(g4b_run* r, int i, const StepPlan& p, StepArgs& L) {
 // Launches one step of one run from its resolved arguments.
 int launch_single(g4b_run* r, const StepArgs& L) {
   g4b_ctx* c = r->ctx;
+  // every kernel of the step on the context's stream is a programmatic
+  // dependent launch (launch_pdl): it starts while its predecessor drains
   if (L.has_beam) {
     LaunchScope ls(c, "run_beam_step");
-    if (r->nfield == 1)
-      beam_step_kernel<1><<<r->nchunk, kStepThreads, 0, c->stream>>>(L.bs);
-    else if (r->nfield == 2)
-      beam_step_kernel<2><<<r->nchunk, kStepThreads, 0, c->stream>>>(L.bs);
-    else
-      beam_step_kernel<0><<<r->nchunk, kStepThreads, 0, c->stream>>>(L.bs);
+    auto kern = r->nfield == 1 ? beam_step_kernel<1>
+                               : (r->nfield == 2 ? beam_step_kernel<2> : beam_step_kernel<0>);
+    G4B_CUDA_TRY(launch_pdl(kern, (unsigned)r->nchunk, kStepThreads, 0, c->stream, L.bs));
   }
   if (int rc = check_launch(c, "beam_step_kernel")) return rc;
   // The beam diagnostics depend only on K1.  A run with slices enough to
@@ -1469,7 +1472,8 @@ int launch_single(g4b_run* r, const StepArgs& L) {
   if (own) {
     {
       LaunchScope ls(c, "run_deposit");
-      deposit_kernel<<<r->nslice * kDepSplit, kDepThreads, kDepSmem, c->stream>>>(L.dd);
+      G4B_CUDA_TRY(launch_pdl(deposit_kernel, (unsigned)(r->nslice * kDepSplit), kDepThreads,
+                              kDepSmem, c->stream, L.dd));
     }
     if (int rc = check_launch(c, "deposit_kernel")) return rc;
     if (!branch)
@@ -1479,18 +1483,15 @@ int launch_single(g4b_run* r, const StepArgs& L) {
     const DepDiagLaunch dl{L.dd, L.bd};
     const unsigned grid = (unsigned)(r->nslice * kDepSplit);
     const bool wide = r->nslice * kDepSplit < c->sm_count;
-    if (r->desc.nbunch == 1) {
-      if (wide)
-        deposit_diag_kernel<1, kDepWideThreads><<<grid, kDepWideThreads, kDepSmem, c->stream>>>(dl);
-      else
-        deposit_diag_kernel<1, kDepThreads><<<grid, kDepThreads, kDepSmem, c->stream>>>(dl);
-    } else {
-      if (wide)
-        deposit_diag_kernel<kMaxBunch, kDepWideThreads>
-            <<<grid, kDepWideThreads, kDepSmem, c->stream>>>(dl);
-      else
-        deposit_diag_kernel<kMaxBunch, kDepThreads><<<grid, kDepThreads, kDepSmem, c->stream>>>(dl);
-    }
+    const bool one = r->desc.nbunch == 1;
+    if (wide)
+      G4B_CUDA_TRY(launch_pdl(one ? deposit_diag_kernel<1, kDepWideThreads>
+                                  : deposit_diag_kernel<kMaxBunch, kDepWideThreads>,
+                              grid, kDepWideThreads, kDepSmem, c->stream, dl));
+    else
+      G4B_CUDA_TRY(launch_pdl(one ? deposit_diag_kernel<1, kDepThreads>
+                                  : deposit_diag_kernel<kMaxBunch, kDepThreads>,
+                              grid, kDepThreads, kDepSmem, c->stream, dl));
     if (int rc = check_launch(c, "deposit_diag_kernel")) return rc;
   }
   for (int f = 0; f < r->nfield; ++f)
@@ -1498,7 +1499,8 @@ int launch_single(g4b_run* r, const StepArgs& L) {
   if (branch) G4B_CUDA_TRY(cudaStreamWaitEvent(c->stream, r->ev_join, 0));
   {
     LaunchScope ls(c, "run_diag_finalize");
-    diag_finalize_kernel<<<(L.nfin + 255) / 256, 256, 0, c->stream>>>(L.fa);
+    G4B_CUDA_TRY(launch_pdl(diag_finalize_kernel, (unsigned)((L.nfin + 255) / 256), 256, 0,
+                            c->stream, L.fa));
   }
   return check_launch(c, "diag_finalize_kernel");
 }
