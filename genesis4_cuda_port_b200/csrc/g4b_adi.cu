@@ -518,6 +518,7 @@ __global__ void __launch_bounds__(512, 2) deposit_slice_kernel(const DepositArgs
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ double shd[16];
   __shared__ int shi[16];
+  ptx::pdl_wait();
   unsigned long long* acc = reinterpret_cast<unsigned long long*>(smem);
   const int bs = blockIdx.x;
   const int tid = threadIdx.x;
@@ -663,6 +664,7 @@ __global__ void __launch_bounds__(512, 2) deposit_slice_kernel(const DepositArgs
 __global__ void slice_scl_kernel(int nslice, const int64_t* off, const double* current,
                                  double fc, double xks, double dgrid, double delz,
                                  double vacimp, double eev, double* scl) {
+  ptx::pdl_wait();
   const int is = blockIdx.x * blockDim.x + threadIdx.x;
   if (is >= nslice) return;
   double s = 0.0;
@@ -875,9 +877,9 @@ int fp64_deposit(g4b_field* f, g4b_beam* b, const g4b_step* st, double fc) {
   const int harm = f->harm;
   {
     LaunchScope ls(c, "slice_scl");
-    slice_scl_kernel<<<(b->nslice + 127) / 128, 128, 0, c->stream>>>(
-        b->nslice, b->d_off, b->d_current, fc, f->xks, f->dgrid, st->delz, kVacimp,
-        kEev, b->d_scl);
+    G4B_CUDA_TRY(launch_pdl(slice_scl_kernel, (unsigned)((b->nslice + 127) / 128), 128, 0,
+                            c->stream, b->nslice, b->d_off, b->d_current, fc, f->xks, f->dgrid,
+                            st->delz, kVacimp, kEev, b->d_scl));
   }
   if (int rc = check_launch(c, "slice_scl_kernel")) return rc;
   DepositArgs da{};
@@ -911,7 +913,7 @@ int fp64_deposit(g4b_field* f, g4b_beam* b, const g4b_step* st, double fc) {
                                     (int)acc_bytes));  // per device, cheap
   {
     LaunchScope ls(c, "deposit");
-    deposit_slice_kernel<<<f->nslice, 512, acc_bytes, c->stream>>>(da);
+    G4B_CUDA_TRY(launch_pdl(deposit_slice_kernel, (unsigned)f->nslice, 512, acc_bytes, c->stream, da));
   }
   if (int rc = check_launch(c, "deposit_slice_kernel")) return rc;
   return G4B_OK;

@@ -68,6 +68,7 @@ struct TrackArgs {
 };
 
 __global__ void __launch_bounds__(256) track_kernel(const TrackArgs a) {
+  ptx::pdl_wait();
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += stride) {
     double x = a.x[i], y = a.y[i], px = a.px[i], py = a.py[i];
@@ -146,6 +147,7 @@ static Mat4 chicane_matrix(double angle, double lb, double ld, double lt) {
 __global__ void __launch_bounds__(256) r56_kernel(int64_t n, const double* gamma,
                                                   double* theta, double r56,
                                                   double gamma0) {
+  ptx::pdl_wait();
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
     theta[i] += r56 * (gamma[i] - gamma0);
@@ -231,6 +233,7 @@ __device__ __forceinline__ void ode(const PushArgs& a, int nf, double tgam, doub
 // (src/Core/BeamSolverCUDA.cpp:226-409); NF = 1 for one field, 0 = generic.
 template <int NF>
 __global__ void __launch_bounds__(256) push_kernel(const PushArgs a) {
+  ptx::pdl_wait();
   const int4 ch = a.chunks[blockIdx.x];
   if ((int)threadIdx.x >= ch.z) return;
   const int slice = ch.x;
@@ -347,7 +350,7 @@ int g4b_beam_track(g4b_beam* b, const g4b_step* st, double delz, int last_step) 
   }
   {
     LaunchScope ls(c, "track");
-    track_kernel<<<grid_for(c, b->npart, 256), 256, 0, c->stream>>>(a);
+    G4B_CUDA_TRY(launch_pdl(track_kernel, (unsigned)grid_for(c, b->npart, 256), 256, 0, c->stream, a));
   }
   return check_launch(c, "track_kernel");
 }
@@ -365,8 +368,8 @@ int g4b_beam_r56(g4b_beam* b, const g4b_step* st, double lambda0) {
   r56 = r56 * 4 * std::asin(1.0) / lambda0 / st->gamma_ref;
   {
     LaunchScope ls(c, "r56");
-    r56_kernel<<<grid_for(c, b->npart, 256), 256, 0, c->stream>>>(b->npart, b->gamma,
-                                                                  b->theta, r56, st->gamma_ref);
+    G4B_CUDA_TRY(launch_pdl(r56_kernel, (unsigned)grid_for(c, b->npart, 256), 256, 0, c->stream,
+                            b->npart, b->gamma, b->theta, r56, st->gamma_ref));
   }
   return check_launch(c, "r56_kernel");
 }
@@ -424,10 +427,8 @@ int g4b_beam_advance(g4b_beam* b, g4b_field* const* fields, const double* fc, in
   a.grady = st->grady;
   {
     LaunchScope ls(c, "push");
-    if (nfield == 1)
-      push_kernel<1><<<b->nchunk, 256, 0, c->stream>>>(a);
-    else
-      push_kernel<0><<<b->nchunk, 256, 0, c->stream>>>(a);
+    G4B_CUDA_TRY(launch_pdl(nfield == 1 ? push_kernel<1> : push_kernel<0>, (unsigned)b->nchunk, 256,
+                            0, c->stream, a));
   }
   return check_launch(c, "push_kernel");
 }

@@ -38,6 +38,7 @@ __global__ void __launch_bounds__(kDiagThreads, HP == 1 ? 3 : 1)
                      const double* gamma, const double* theta, double* stats, double* bre,
                      double* bim) {
   __shared__ double part[kDiagWarps][23 + 2 * HP];
+  ptx::pdl_wait();
   const int is = blockIdx.x;
   if (is >= nslice) return;
   const int tid = threadIdx.x, w = tid >> 5, l = tid & 31;
@@ -312,9 +313,9 @@ int g4b_diag_beam(g4b_beam* b, int nharm, int need_aux, double* stats, double* b
   {
     LaunchScope ls(c, "diag_beam");
     auto kern = nharm == 1 ? beam_diag_kernel<1> : beam_diag_kernel<kMaxHarmPass>;
-    kern<<<b->nslice, kDiagThreads, 0, c->stream>>>(
-        b->nslice, nharm, need_aux, b->d_off, b->x, b->y, b->px, b->py, b->gamma, b->theta,
-        d_stats, d_bre, d_bim);
+    G4B_CUDA_TRY(launch_pdl(kern, (unsigned)b->nslice, kDiagThreads, 0, c->stream, b->nslice,
+                            nharm, need_aux, b->d_off, b->x, b->y, b->px, b->py, b->gamma,
+                            b->theta, d_stats, d_bre, d_bim));
   }
   if (int rc = check_launch(c, "beam_diag_kernel")) return rc;
   G4B_CUDA_TRY(cudaMemcpyAsync(stats, d_stats, ns * 23 * sizeof(double),
