@@ -248,11 +248,13 @@ def run_reference(args, wl, rank, budget_s=240.0):
     print(json.dumps(line), flush=True)
 
 
-def reference_cuda(wl, off, parts, cur, cells, lat, args):
+def reference_cuda(wl, off, parts, cur, cells, lat, args, slip=None):
     """The reference's own CUDA classes (src/Core/*.cpp, compiled unmodified
     into oracle/_ref) stepping the same workload on this GPU from device-
     resident state, in Gencore::run's order: the reference's GPU speed beside
-    its CPU arm.  None where the library or a GPU is missing."""
+    its CPU arm (slip: per-step slippage in slices, default the lattice's;
+    zeros for a steady-state run).  None where the library or a GPU is
+    missing."""
     from oracle import refpy
     if not refpy.available():
         return None
@@ -262,7 +264,8 @@ def reference_cuda(wl, off, parts, cur, cells, lat, args):
         n = lat.nstep
         ms = refpy.time_steps(off, parts, cur, cells, gridmax=wl.gridmax, xlambda=wl.lambda0,
                               steps=lat.steps, fc=[lat.fc(i, 1) for i in range(n)],
-                              slip=lat.slip, sample=wl.sample, warmup=args.warmup,
+                              slip=lat.slip if slip is None else slip, sample=wl.sample,
+                              warmup=args.warmup,
                               ntimed=max(1, min(args.steps, 20)))
     except Exception as e:  # the reference's classes throw on what they reject
         return {"unavailable": str(e)[:200]}
@@ -595,8 +598,9 @@ def run_steady(args):
     lat = wl.make_lattice()
     run = dev.Run(ctx, off, fields=[(1, wl.ngrid, wl.gridmax)], lambda0=wl.lambda0,
                   gamma_ref=wl.gamma0, sample=1.0, time_run=False, nbunch=1)
+    cells = wl.make_field()
     run.upload_beam(parts)
-    run.upload_field(0, wl.make_field(), 0)
+    run.upload_field(0, cells, 0)
     run.set_current(np.full(1, wl.current))
     run.set_lattice(lat.steps, [[lat.fc(i, 1)] for i in range(lat.nstep)], lat.slip)
     run.advance(0, args.warmup, graph=False)
@@ -612,6 +616,14 @@ def run_steady(args):
     line = {"metric": "us per step, steady state", "value": 1e3 * ms / n, "unit": "us/step",
             "higher_is_better": False, "n_gpus": 1, "steps": n, "dtype": "f32 state, f64 theta",
             "data": "synthetic", "config": {"workload": wl.name}}
+    del run
+    # the reference's own CUDA classes on the same state (steady state: no
+    # slippage)
+    ref = reference_cuda(wl, off, parts, np.full(1, wl.current), cells, lat, args,
+                         slip=np.zeros(lat.nstep))
+    if ref and "ms_per_step" in ref:
+        ref["us_per_step"] = 1e3 * ref["ms_per_step"]
+    line["reference_cuda"] = ref
     print(json.dumps(line), flush=True)
 
 
