@@ -168,6 +168,7 @@ int fp64_deposit(g4b_field* f, g4b_beam* b, const g4b_step* st, double fc);
 void dev_free(g4b_ctx* ctx, void* p);
 
 int check_launch(g4b_ctx* ctx, const char* what);
+int read_device_error(g4b_ctx* ctx, const char* what);
 
 // Launches kern with programmatic stream serialization: it may start while
 // the preceding kernel of its stream drains (in a captured graph, a
@@ -192,7 +193,6 @@ inline cudaError_t launch_pdl(void (*kern)(P...), unsigned grid, unsigned block,
   return cudaLaunchKernelEx(&cfg, kern, static_cast<A&&>(args)...);
 }
 #endif
-int read_device_error(g4b_ctx* ctx, const char* what);
 
 struct AdiPassArgs {
   const void* in;      // pass X: field (natural); pass Y: R' (transposed)
