@@ -240,6 +240,7 @@ __device__ __forceinline__ bool adi_band(const AdiPassArgs& a, const CUtensorMap
   C* tile = reinterpret_cast<C*>(smem);
   C* stile = tile + kTileRows * ld;
   C* out = reinterpret_cast<C*>(smem + a.out_off);
+  __shared__ double dpart[PX ? 1 : W][9];  // pass Y: per-row diagnostic partials
 
   const size_t plane = (size_t)n * ld;
   const int lo = PX ? max(r0 - 1, 0) : r0;
@@ -321,7 +322,6 @@ __device__ __forceinline__ bool adi_band(const AdiPassArgs& a, const CUtensorMap
     // field diagnostics of this band (g4_field_slice_reduce_kernel,
     // src/Core/DiagnosticCUDA.cpp:305-363): this lane group holds column
     // ix = r0 + row, rows iy = gl*M + j of the solved plane
-    __shared__ double dpart[W][9];
     // each lane sums its M cells in the state precision T (exact cell
     // offsets; partials of <= 33 terms, rounding at the level of the state's
     // own); the lanes of a column add in FP64 (<= 32 terms); the power and
@@ -383,12 +383,6 @@ __device__ __forceinline__ bool adi_band(const AdiPassArgs& a, const CUtensorMap
       dpart[row][7] = cre;
       dpart[row][8] = cim;
     }
-    __syncthreads();
-    if (tid < 9) {
-      double t = dpart[0][tid], tc = 0.0;
-      for (int w = 1; w < W; ++w) ptx::csum_add(t, tc, dpart[w][tid]);
-      a.diag[((size_t)s * a.nband + band) * 9 + tid] = t + tc;
-    }
   }
   if (PX) __syncthreads();  // out overlays the input tile
 #pragma unroll
@@ -397,14 +391,21 @@ __device__ __forceinline__ bool adi_band(const AdiPassArgs& a, const CUtensorMap
     if (j < jn) out[k * W + row] = v[j];
   }
   ptx::fence_proxy_async();
-  __syncthreads();
+  __syncthreads();  // the staged rows and the diagnostic partials are complete
   if (tid == 0) {
     for (int i = 0; i < a.nbox; ++i)
       ptx::tma_store_3d(tm_out, out + (size_t)i * a.box_rows * W, 2 * r0,
                         i * a.box_rows, s);
     ptx::bulk_commit();
-    ptx::bulk_wait_read0();
   }
+  // the band's diagnostic sums, over its rows in order, while the stores run
+  if (!PX && a.diag != nullptr && tid >= 32 && tid < 32 + 9) {
+    const int q = tid - 32;
+    double t = dpart[0][q], tc = 0.0;
+    for (int w = 1; w < W; ++w) ptx::csum_add(t, tc, dpart[w][q]);
+    a.diag[((size_t)s * a.nband + band) * 9 + q] = t + tc;
+  }
+  if (tid == 0) ptx::bulk_wait_read0();
   return true;
 }
 
