@@ -436,7 +436,6 @@ __global__ void __launch_bounds__(BandW<T, L>::value * 32, AdiBlocks<T, M, L>::v
     ptx::fence_mbar_init();
   }
   __syncthreads();
-  ptx::pdl_wait();
   const int nitems = *b.nitems;
   uint32_t parity = 0;
   for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
@@ -855,7 +854,7 @@ static int batch_launch_t(g4b_ctx* c, cudaStream_t st, const AdiBatchArgs& b, si
   }
   {
     LaunchScope ls(c, PX ? "batch_adi_x" : "batch_adi_y");
-    G4B_CUDA_TRY(launch_pdl(kern, (unsigned)grid, BandW<float, L>::value * 32, smem, st, b));
+    kern<<<grid, BandW<float, L>::value * 32, smem, st>>>(b);
   }
   return check_launch(c, "adi_batch_kernel");
 }

@@ -467,7 +467,6 @@ struct BeamBatchArgs {
 
 template <int NF>
 __global__ void __launch_bounds__(kStepThreads, kStepBlocks) beam_batch_kernel(const __grid_constant__ BeamBatchArgs b) {
-  ptx::pdl_wait();
   const int nitems = *b.nitems;
   for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
     const int2 w = b.items[it];
@@ -1008,7 +1007,6 @@ struct DepBatchArgs {
 __global__ void __launch_bounds__(kDepThreads, 2)
     deposit_batch_kernel(const __grid_constant__ DepBatchArgs b) {
   extern __shared__ __align__(128) unsigned char smem[];
-  ptx::pdl_wait();
   const int nitems = *b.nitems * kDepSplit;
   for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
     const int2 w = b.items[it / kDepSplit];
@@ -1026,7 +1024,6 @@ struct DiagBatchArgs {
 template <int NB>
 __global__ void __launch_bounds__(kDiagThreads, 2)
     beam_diag_batch_kernel(const __grid_constant__ DiagBatchArgs b) {
-  ptx::pdl_wait();
   const int nitems = *b.nitems * kDepParts;  // (run, slice) items, kDepParts parts each
   for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
     const int2 w = b.items[it / kDepParts];
@@ -1102,7 +1099,6 @@ __global__ void diag_finalize_kernel(const __grid_constant__ FinalizeArgs a) {
 
 // Batched form: one CTA per run at a time.
 __global__ void finalize_batch_kernel(const FinalizeArgs* args, const int* nruns) {
-  ptx::pdl_wait();
   const int n = *nruns;
   for (int r = blockIdx.x; r < n; r += gridDim.x) finalize_range(args[r], threadIdx.x, blockDim.x);
 }
@@ -2250,9 +2246,12 @@ int batch_launch(g4b_batch* b, bool timed) {
     BeamBatchArgs a{reinterpret_cast<const BeamStepArgs*>(b->d_args + b->off_bs),
                     reinterpret_cast<const int2*>(b->d_items + b->off_beam), counts + 0};
     LaunchScope ls(c, "batch_beam_step");
-    auto kern = b->nf_kind == 1 ? beam_batch_kernel<1>
-                                : (b->nf_kind == 2 ? beam_batch_kernel<2> : beam_batch_kernel<0>);
-    G4B_CUDA_TRY(launch_pdl(kern, (unsigned)b->grid[0], kStepThreads, 0, c->stream, a));
+    if (b->nf_kind == 1)
+      beam_batch_kernel<1><<<b->grid[0], kStepThreads, 0, c->stream>>>(a);
+    else if (b->nf_kind == 2)
+      beam_batch_kernel<2><<<b->grid[0], kStepThreads, 0, c->stream>>>(a);
+    else
+      beam_batch_kernel<0><<<b->grid[0], kStepThreads, 0, c->stream>>>(a);
   }
   if (int rc = check_launch(c, "beam_batch_kernel")) return rc;
   ev(1);
@@ -2260,8 +2259,7 @@ int batch_launch(g4b_batch* b, bool timed) {
     DepBatchArgs a{reinterpret_cast<const DepArgs*>(b->d_args + b->off_dd),
                    reinterpret_cast<const int2*>(b->d_items + b->off_dep), counts + 1};
     LaunchScope ls(c, "batch_deposit");
-    G4B_CUDA_TRY(launch_pdl(deposit_batch_kernel, (unsigned)b->grid[1], kDepThreads, kDepSmem,
-                            c->stream, a));
+    deposit_batch_kernel<<<b->grid[1], kDepThreads, kDepSmem, c->stream>>>(a);
   }
   if (int rc = check_launch(c, "deposit_batch_kernel")) return rc;
   // branches (not while the tuner or the profiler times single kernels)
@@ -2270,9 +2268,10 @@ int batch_launch(g4b_batch* b, bool timed) {
     DiagBatchArgs a{reinterpret_cast<const BeamDiagArgs*>(b->d_args + b->off_bd),
                     reinterpret_cast<const int2*>(b->d_items + b->off_dep), counts + 1};
     LaunchScope ls(c, "batch_beam_diag");
-    G4B_CUDA_TRY(launch_pdl(b->nb_kind == 1 ? beam_diag_batch_kernel<1>
-                                            : beam_diag_batch_kernel<kMaxBunch>,
-                            (unsigned)(2 * c->sm_count), kDiagThreads, 0, st, a));
+    if (b->nb_kind == 1)
+      beam_diag_batch_kernel<1><<<2 * c->sm_count, kDiagThreads, 0, st>>>(a);
+    else
+      beam_diag_batch_kernel<kMaxBunch><<<2 * c->sm_count, kDiagThreads, 0, st>>>(a);
     return check_launch(c, "beam_diag_batch_kernel");
   };
   if (fork) {
@@ -2319,9 +2318,8 @@ int batch_launch(g4b_batch* b, bool timed) {
   if (fork) G4B_CUDA_TRY(cudaStreamWaitEvent(c->stream, b->ev_diag, 0));
   {
     LaunchScope ls(c, "batch_diag_finalize");
-    G4B_CUDA_TRY(launch_pdl(finalize_batch_kernel, (unsigned)b->grid[3], 256, 0, c->stream,
-                            reinterpret_cast<const FinalizeArgs*>(b->d_args + b->off_fa),
-                            counts + 2));
+    finalize_batch_kernel<<<b->grid[3], 256, 0, c->stream>>>(
+        reinterpret_cast<const FinalizeArgs*>(b->d_args + b->off_fa), counts + 2);
   }
   return check_launch(c, "finalize_batch_kernel");
 }
