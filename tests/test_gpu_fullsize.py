@@ -1,0 +1,141 @@
+"""Size-independent properties at the headline size: time-dependent SASE,
+1024 slices x 8192 particles, ngrid 201 (the oracle is too slow to step
+this size; the smaller parity tests pin the arithmetic, these pin what must
+hold at any size).
+
+* The mixed run gives the same bits by direct launches, by graph replay and
+  in the batch engine (whose kernels are launched without the programmatic
+  dependencies of the single run's): field, beam and every step's
+  diagnostics, over undulator steps with sources and slippage.
+* Source-free propagation conserves every slice's field power: the
+  Peaceman-Rachford step (1 - i r Ay)^-1 (1 + i r Ax) (1 - i r Ax)^-1
+  (1 + i r Ay) is unitary for the commuting Dirichlet second differences of
+  a square grid, so the power changes only by rounding: FP64 drop-in and
+  mixed (FP32 field) form, every slice.
+"""
+import numpy as np
+import pytest
+
+from genesis4_cuda_port_b200 import device as dev, workloads
+
+pytestmark = pytest.mark.gpu
+
+NSTEP = 6
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = dev.Context(0)
+    yield c
+    c.synchronize()
+
+
+@pytest.fixture(scope="module")
+def sase():
+    wl = workloads.sase()
+    assert (wl.nslice, wl.npart, wl.ngrid) == (1024, 8192, 201)
+    lat = wl.make_lattice()
+    off, parts = wl.make_beam()
+    cells = wl.make_field()
+    return wl, lat, off, parts, cells
+
+
+def _run(ctx, wl, lat, off, parts, cells, *, time_run=True, current=None, fc=None):
+    run = dev.Run(ctx, off, fields=[(1, wl.ngrid, wl.gridmax)], lambda0=wl.lambda0,
+                  gamma_ref=wl.gamma0, sample=wl.sample, time_run=time_run, nbunch=1)
+    run.set_current(np.full(wl.nslice, wl.current if current is None else current))
+    fcs = [[lat.fc(i, 1) if fc is None else fc] for i in range(lat.nstep)]
+    run.set_lattice(lat.steps, fcs, lat.slip)
+    run.upload_beam(parts)
+    run.upload_field(0, cells, 0)
+    return run
+
+
+def _result(run, nstep):
+    return run.download_beam(), run.download_field(0), run.history_range(0, nstep)
+
+
+def _same(a, b):
+    for k in a[0]:
+        assert np.array_equal(a[0][k], b[0][k]), k
+    assert a[1][1] == b[1][1]
+    assert np.array_equal(a[1][0], b[1][0])
+    assert np.array_equal(a[2][0], b[2][0]) and np.array_equal(a[2][1], b[2][1])
+
+
+def test_direct_graph_and_batch_give_the_same_bits(ctx, sase):
+    wl, lat, off, parts, cells = sase
+    assert all(lat.steps[i].in_undulator for i in range(NSTEP))
+    direct = _run(ctx, wl, lat, off, parts, cells)
+    direct.advance(0, NSTEP, graph=False)
+    ref = _result(direct, NSTEP)
+    direct.close()
+    # the beam moved and the deposited sources grew a field from zero
+    assert not np.array_equal(ref[0]["theta"], parts["theta"])
+    assert np.max(np.abs(ref[1][0])) > 0
+    assert ref[1][1] != 0  # slippage rotated the planes
+    graphed = _run(ctx, wl, lat, off, parts, cells)
+    graphed.advance(0, NSTEP, graph=True)
+    _same(_result(graphed, NSTEP), ref)
+    graphed.close()
+    batch = dev.Batch(ctx, 1)
+    run = _run(ctx, wl, lat, off, parts, cells)
+    batch.attach(run, 0, NSTEP)
+    batch.step(NSTEP, graph=False)
+    ctx.synchronize()
+    _same(_result(run, NSTEP), ref)
+    batch.close()
+    run.close()
+
+
+def _random_field(wl, seed):
+    """A Gaussian mode per slice with random amplitude and phase noise."""
+    rng = np.random.default_rng(seed)
+    x = np.linspace(-wl.gridmax, wl.gridmax, wl.ngrid)
+    env = np.exp(-(x[:, None] ** 2 + x[None, :] ** 2) / (2 * (0.3 * wl.gridmax) ** 2))
+    amp = 1e9 * (1.0 + 0.2 * rng.random((wl.nslice, 1, 1)))
+    noise = 1.0 + 0.05 * rng.standard_normal((wl.nslice, wl.ngrid, wl.ngrid))
+    phase = np.exp(2j * np.pi * rng.random((wl.nslice, wl.ngrid, wl.ngrid)) * 0.1)
+    return amp * env[None] * noise * phase
+
+
+def test_source_free_propagation_conserves_power_fp64(ctx, sase):
+    wl, lat, off, parts, _ = sase
+    cells = _random_field(wl, 7)
+    beam = dev.BeamState(ctx, off, wl.gamma0)
+    beam.upload(parts)
+    beam.set_current(np.zeros(wl.nslice))
+    fld = dev.FieldState(ctx, wl.nslice, wl.ngrid, wl.gridmax, wl.lambda0)
+    fld.upload(cells)
+    adi = dev.FieldSolverADICUDA(ctx)
+    st = lat.steps[0]
+    p0 = np.sum(np.abs(cells) ** 2, axis=(1, 2))
+    adi.init(st.delz, fld.dgrid, fld.xks, fld.ngrid)
+    for _ in range(5):
+        adi.advance(fld, beam, st, 0.0)
+    out = fld.download()
+    p1 = np.sum(np.abs(out) ** 2, axis=(1, 2))
+    assert not np.allclose(out, cells, rtol=1e-3)  # the field did propagate
+    assert np.max(np.abs(p1 / p0 - 1)) < 1e-12, np.max(np.abs(p1 / p0 - 1))
+    stats, _ = fld.diagnostics()  # the device's power sum agrees
+    np.testing.assert_allclose(stats[:, 0], p1, rtol=1e-12)
+    for o in (adi, fld, beam):
+        o.close()
+
+
+def test_source_free_propagation_conserves_power_mixed(ctx, sase):
+    wl, lat, off, parts, _ = sase
+    cells = _random_field(wl, 8)
+    nstep = 20
+    run = _run(ctx, wl, lat, off, parts, cells, time_run=False, current=0.0, fc=0.0)
+    run.advance(0, nstep, graph=True)
+    _, hf = run.history_range(0, nstep)
+    power = hf[:, 0, :, 0]  # [step, slice]
+    out, _ = run.download_field(0)
+    run.close()
+    assert not np.allclose(out, cells, rtol=1e-3)
+    # FP32 cells: each step rounds every cell once (relative 2^-24)
+    drift = np.max(np.abs(power[-1] / power[0] - 1))
+    assert drift < 2e-5, drift
+    p_final = np.sum(np.abs(out) ** 2, axis=(1, 2))
+    np.testing.assert_allclose(power[-1], p_final, rtol=1e-5)
