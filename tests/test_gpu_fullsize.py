@@ -7,6 +7,9 @@ hold at any size).
   in the batch engine (whose kernels are launched without the programmatic
   dependencies of the single run's): field, beam and every step's
   diagnostics, over undulator steps with sources and slippage.
+* Slippage is bit-exact: without sources, a time-dependent run holds plane
+  for plane the planes of the same run without slippage, except the zeroed
+  ones.
 * Source-free propagation conserves every slice's field power: the
   Peaceman-Rachford step (1 - i r Ay)^-1 (1 + i r Ax) (1 - i r Ax)^-1
   (1 + i r Ay) is unitary for the commuting Dirichlet second differences of
@@ -139,3 +142,28 @@ def test_source_free_propagation_conserves_power_mixed(ctx, sase):
     assert drift < 2e-5, drift
     p_final = np.sum(np.abs(out) ** 2, axis=(1, 2))
     np.testing.assert_allclose(power[-1], p_final, rtol=1e-5)
+
+
+def test_slippage_rotates_and_zeroes_planes_bit_exactly(ctx, sase):
+    """Without sources every plane evolves on its own, so a time-dependent
+    run (one slice of slippage per undulator step: the window's pointer moves
+    and the plane that slips in is zeroed, src/Core/ControlCUDA.cpp:148-252)
+    holds, plane for plane in memory order, exactly the planes of the same
+    run without slippage, except the zeroed ones."""
+    wl, lat, off, parts, _ = sase
+    cells = _random_field(wl, 9)
+    out = {}
+    for time_run in (True, False):
+        run = _run(ctx, wl, lat, off, parts, cells, time_run=time_run, current=0.0, fc=0.0)
+        run.advance(0, NSTEP, graph=True)
+        out[time_run] = run.download_field(0)
+        run.close()
+    (tc, tfirst), (sc, sfirst) = out[True], out[False]
+    assert sfirst == 0
+    shifts = (wl.nslice - tfirst) % wl.nslice
+    assert shifts == NSTEP  # one slice per undulator step
+    zeroed = [(wl.nslice - k) % wl.nslice for k in range(1, shifts + 1)]
+    keep = np.setdiff1d(np.arange(wl.nslice), zeroed)
+    assert np.all(tc[zeroed] == 0)
+    assert np.array_equal(tc[keep], sc[keep])
+    assert np.max(np.abs(sc[zeroed])) > 0  # those planes held a field without slippage
