@@ -10,6 +10,8 @@ hold at any size).
 * Slippage is bit-exact: without sources, a time-dependent run holds plane
   for plane the planes of the same run without slippage, except the zeroed
   ones.
+* The mixed run stays within its gates of the FP64 drop-in (per-slice power
+  and bunching, 10 steps of the headline beam).
 * Source-free propagation conserves every slice's field power: the
   Peaceman-Rachford step (1 - i r Ay)^-1 (1 + i r Ax) (1 - i r Ax)^-1
   (1 + i r Ay) is unitary for the commuting Dirichlet second differences of
@@ -167,3 +169,47 @@ def test_slippage_rotates_and_zeroes_planes_bit_exactly(ctx, sase):
     assert np.all(tc[zeroed] == 0)
     assert np.array_equal(tc[keep], sc[keep])
     assert np.max(np.abs(sc[zeroed])) > 0  # those planes held a field without slippage
+
+
+def test_mixed_run_tracks_the_fp64_drop_in(ctx, sase):
+    """The mixed run against the FP64 drop-in (per-phase calls in the
+    reference's order) on the headline beam over 10 steps: every slice's
+    field power and bunching within the mixed form's gates (1e-3)."""
+    wl, lat, off, parts, cells = sase
+    nstep = 10
+    run = _run(ctx, wl, lat, off, parts, cells)
+    run.advance(0, nstep, graph=True)
+    hb, hf = run.history_range(0, nstep)
+    run.close()
+    beam = dev.BeamState(ctx, off, wl.gamma0)
+    beam.upload(parts)
+    beam.set_current(np.full(wl.nslice, wl.current))
+    fld = dev.FieldState(ctx, wl.nslice, wl.ngrid, wl.gridmax, wl.lambda0)
+    fld.upload(cells)
+    adi = dev.FieldSolverADICUDA(ctx)
+    p64, b64 = [], []
+    for i in range(nstep):
+        st = lat.steps[i]
+        fc = lat.fc(i, 1)
+        beam.track(st, st.delz * 0.5, False)
+        beam.advance([fld], [fc], st)
+        beam.apply_r56(st, wl.lambda0)
+        beam.track(st, st.delz * 0.5, True)
+        adi.init(st.delz, fld.dgrid, fld.xks, fld.ngrid)
+        adi.advance(fld, beam, st, fc)
+        fld.apply_slippage(lat.slip[i], wl.sample)
+        stats, bre, bim = beam.diagnostics(1, False)
+        fstats, _ = fld.diagnostics()
+        p64.append(fstats[:, 0])
+        b64.append(np.hypot(bre[:, 0], bim[:, 0]) / np.maximum(stats[:, 12], 1))
+    for o in (adi, fld, beam):
+        o.close()
+    pm = hf[:, 0, :, 0]
+    bm = np.hypot(hb[:, :, 23], hb[:, :, 24]) / np.maximum(hb[:, :, 12], 1)
+    p64, b64 = np.array(p64), np.array(b64)
+    # shot noise has radiated into every slice but the head, whose plane is
+    # the one that has just slipped in (zeroed)
+    assert p64[-1][0] == 0 and np.min(p64[-1][1:]) > 0
+    rel = np.max(np.abs(pm - p64) / np.max(p64, axis=1, keepdims=True))
+    assert rel < 1e-3, rel
+    assert np.max(np.abs(bm - b64)) < 1e-3, np.max(np.abs(bm - b64))
