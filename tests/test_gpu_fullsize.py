@@ -16,7 +16,8 @@ hold at any size).
   Peaceman-Rachford step (1 - i r Ay)^-1 (1 + i r Ax) (1 - i r Ax)^-1
   (1 + i r Ay) is unitary for the commuting Dirichlet second differences of
   a square grid, so the power changes only by rounding: FP64 drop-in and
-  mixed (FP32 field) form, every slice.
+  mixed (FP32 field) form, every slice; likewise the FFT solver's spectral
+  step.
 """
 import numpy as np
 import pytest
@@ -213,3 +214,28 @@ def test_mixed_run_tracks_the_fp64_drop_in(ctx, sase):
     rel = np.max(np.abs(pm - p64) / np.max(p64, axis=1, keepdims=True))
     assert rel < 1e-3, rel
     assert np.max(np.abs(bm - b64)) < 1e-3, np.max(np.abs(bm - b64))
+
+
+def test_source_free_fft_propagation_conserves_power(ctx, sase):
+    """The FFT field solver's step, a spectral propagator exp(i k^2 dz)
+    between a forward and an inverse DFT of the plane, is unitary: every
+    slice's power is kept to FP64 rounding at the headline size."""
+    wl, lat, off, parts, _ = sase
+    cells = _random_field(wl, 10)
+    beam = dev.BeamState(ctx, off, wl.gamma0)
+    beam.upload(parts)
+    beam.set_current(np.zeros(wl.nslice))
+    fld = dev.FieldState(ctx, wl.nslice, wl.ngrid, wl.gridmax, wl.lambda0)
+    fld.upload(cells)
+    fft = dev.FieldSolverFFTCUDA(ctx)
+    st = lat.steps[0]
+    fft.init(st.delz, fld.dgrid, fld.xks, fld.ngrid)
+    for _ in range(3):
+        fft.advance(fld, beam, st, 0.0)
+    out = fld.download()
+    p0 = np.sum(np.abs(cells) ** 2, axis=(1, 2))
+    p1 = np.sum(np.abs(out) ** 2, axis=(1, 2))
+    assert not np.allclose(out, cells, rtol=1e-3)
+    assert np.max(np.abs(p1 / p0 - 1)) < 1e-12, np.max(np.abs(p1 / p0 - 1))
+    for o in (fft, fld, beam):
+        o.close()
